@@ -1,0 +1,226 @@
+// Fluid–body coupling of the IBPM step: the regularisation weights of E
+// (src/interface-coupling/interface-coupling.jl:6-137), E itself, the
+// projection source C'E'F̃b as a deterministic segmented reduction over
+// contributions sorted by target, the dense Schur-complement solve and the
+// drag/lift reduction (src/timestepping/timestepping.jl:154-163, 204-223,
+// 330-354).
+#include "ibpm_internal.cuh"
+
+namespace ibpm {
+
+// Yang et al. (2009) smoothed delta function with support ±3 dr, in the
+// rounded-coefficient form of interface-coupling.jl:24-61 (result is δ·h).
+__device__ double delta_h(double rf, double rb, double dr) {
+    const double r = fabs(rf - rb);
+    const double r1 = r / dr, r2 = r1 * r1, r3 = r2 * r1, r4 = r3 * r1;
+    if (r1 <= 1.0) {
+        const double a5 = asin((1.0 / 2.0) * sqrt(3.0) * (2.0 * r1 - 1.0));
+        const double a8 = sqrt(1.0 - 12.0 * r2 + 12.0 * r1);
+        return 4.166666667e-2 * r4 + (-0.1388888889 + 3.472222222e-2 * a8) * r3 +
+               (-7.121664902e-2 - 5.208333333e-2 * a8 + 0.2405626122 * a5) * r2 +
+               (-.2405626122 * a5 - 0.3792313933 + 0.1012731481 * a8) * r1 + 8.0187537413e-2 * a5 -
+               4.195601852e-2 * a8 + 0.6485698427;
+    } else if (r1 <= 2.0) {
+        const double a6 = asin((1.0 / 2.0) * sqrt(3.0) * (-3.0 + 2.0 * r1));
+        const double a9 = sqrt(-23.0 + 36.0 * r1 - 12.0 * r2);
+        return -6.250000000e-2 * r4 + (0.4861111111 - 1.736111111e-2 * a9) * r3 +
+               (-1.143175026 + 7.812500000e-2 * a9 - 0.1202813061 * a6) * r2 +
+               (0.8751991178 + 0.3608439183 * a6 - 0.1548032407 * a9) * r1 - 0.2806563809 * a6 +
+               8.22848104e-3 + 0.1150173611 * a9;
+    } else if (r1 <= 3.0) {
+        const double a1 = asin((1.0 / 2.0 * (2.0 * r1 - 5.0)) * sqrt(3.0));
+        const double a7 = sqrt(-71.0 - 12.0 * r2 + 60.0 * r1);
+        return 2.083333333e-2 * r4 + (3.472222222e-3 * a7 - 0.2638888889) * r3 +
+               (1.214391675 - 2.604166667e-2 * a7 + 2.405626122e-2 * a1) * r2 +
+               (-0.1202813061 * a1 - 2.449273192 + 7.262731481e-2 * a7) * r1 + 0.1523563211 * a1 +
+               1.843201677 - 7.306134259e-2 * a7;
+    }
+    return 0.0;
+}
+
+// w[kk][l][m], kk = comp·nb + k: weight of flux point (bidx + l − 6, bidx + m − 6)
+// for body point k (interface-coupling.jl:89-96).
+__global__ void weights_kernel(BodyDev b, double h, double offx, double offy) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b.nf * 169) return;
+    const int kk = t / 169, lm = t % 169, l = lm / 13, m = lm % 13;
+    const int comp = kk / b.nb, k = kk % b.nb;
+    const double xk = b.xb[k], yk = b.xb[b.nb + k];
+    const double x = h * (double)((b.bidx[k] - 1) + (l - 6)) - offx;
+    const double y = h * (double)((b.bidx[b.nb + k] - 1) + (m - 6)) - offy;
+    double w;
+    if (comp == 0) w = delta_h(x, xk, h) * delta_h(y + h / 2, yk, h);
+    else w = delta_h(x + h / 2, xk, h) * delta_h(y, yk, h);
+    b.w[t] = w;
+}
+
+cudaError_t launch_weights(const Geom& g, double h, double offx, double offy, const BodyDev& b,
+                           cudaStream_t st) {
+    const int n = b.nf * 169;
+    weights_kernel<<<(n + 255) / 256, 256, 0, st>>>(b, h, offx, offy);
+    return cudaGetLastError();
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// E (regT!, interface-coupling.jl:122-133) on (q + q0): one warp per force
+// component and batch member.  F[bt*F_bstride + kk*F_kstride].
+__global__ void E_kernel(BodyDev b, Geom g, const double* __restrict__ q, long long q_stride, int nbatch,
+                         double q0x, double q0y, double* F, long long F_bstride, long long F_kstride) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= b.nf * nbatch) return;
+    const int bt = warp / b.nf, kk = warp % b.nf;
+    const int comp = kk / b.nb, k = kk % b.nb;
+    const double* qq = q + (long long)bt * q_stride;
+    const int bx = b.bidx[k], by = b.bidx[b.nb + k];
+    const double* w = b.w + (long long)kk * 169;
+    double acc = 0.0;
+    for (int t = lane; t < 169; t += 32) {
+        const int l = t / 13, m = t % 13;
+        const int I = bx + l - 6, J = by + m - 6;
+        double qv;
+        if (comp == 0) qv = qq[(I - 1) + (long long)(J - 1) * (g.nx + 1)] + q0x;
+        else qv = qq[g.nu + (I - 1) + (long long)(J - 1) * g.nx] + q0y;
+        acc += w[t] * qv;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) F[(long long)bt * F_bstride + (long long)kk * F_kstride] = acc;
+}
+
+cudaError_t launch_E(const Geom& g, const BodyDev& b, const double* q, long long q_stride, int nbatch,
+                     double q0x, double q0y, double* F, long long F_stride, cudaStream_t st) {
+    // F_stride > 0: batch stride with unit component stride; F_stride < 0:
+    // component stride |F_stride| with unit batch stride (columns of B).
+    const long long bs = F_stride > 0 ? F_stride : 1;
+    const long long ks = F_stride > 0 ? 1 : -F_stride;
+    const long long warps = (long long)b.nf * nbatch;
+    const int blocks = (int)((warps * 32 + 255) / 256);
+    E_kernel<<<blocks, 256, 0, st>>>(b, g, q, q_stride, nbatch, q0x, q0y, F, bs, ks);
+    return cudaGetLastError();
+}
+
+// y = A x, A row-major n×n: one warp per row (F̃b .= Binv*F̃b, timestepping.jl:160).
+__global__ void gemv_kernel(const double* __restrict__ A, const double* __restrict__ x, double* y, int n) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const double* a = A + (long long)row * n;
+    double acc = 0.0;
+    for (int c = lane; c < n; c += 32) acc += a[c] * x[c];
+    acc = warp_sum(acc);
+    if (lane == 0) y[row] = acc;
+}
+
+cudaError_t launch_gemv(const double* A, const double* x, double* y, int n, cudaStream_t st) {
+    gemv_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(A, x, y, n);
+    return cudaGetLastError();
+}
+
+// update_stress! (timestepping.jl:330-354): fb = F̃b (h/dt) ./ ds,
+// CD_j = 2 Σ ds fb_x, CL_j = 2 Σ ds fb_y, written to hist[step][2][nbodies].
+// One block; a non-finite CD/CL sets bit 0 of *status.
+__global__ void stress_kernel(BodyDev b, const double* __restrict__ Fb, double h, double dt, double* hist,
+                              int* counter, int* status) {
+    __shared__ double red[2][256];
+    const int step = *counter;
+    const double hdt = h / dt;
+    for (int j = 0; j < b.nbodies; ++j) {
+        const int p0 = b.body_start[j], p1 = b.body_start[j + 1];
+        double sx = 0.0, sy = 0.0;
+        for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+            const double ds = b.ds[p];
+            sx += ds * ((Fb[p] * hdt) / ds);
+            sy += ds * ((Fb[b.nb + p] * hdt) / ds);
+        }
+        red[0][threadIdx.x] = sx;
+        red[1][threadIdx.x] = sy;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) {
+                red[0][threadIdx.x] += red[0][threadIdx.x + s];
+                red[1][threadIdx.x] += red[1][threadIdx.x + s];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            const double cd = 2.0 * red[0][0], cl = 2.0 * red[1][0];
+            hist[((long long)step * 2 + 0) * b.nbodies + j] = cd;
+            hist[((long long)step * 2 + 1) * b.nbodies + j] = cl;
+            if (!isfinite(cd) || !isfinite(cl)) atomicOr(status, 1);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *counter = step + 1;
+}
+
+cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double dt, double* hist, int* counter,
+                          int* status, cudaStream_t st) {
+    stress_kernel<<<1, 256, 0, st>>>(b, Fb, h, dt, hist, counter, status);
+    return cudaGetLastError();
+}
+
+// Γsrc = C'(E' F̃b) at the Γ points whose rot! stencil touches a regularised
+// flux point (timestepping.jl:217, curl.jl:300-312).  Each flux value is the
+// sum over its sorted contributor list (ascending force component, the order
+// reg! accumulates in, interface-coupling.jl:103-107).
+__global__ void proj_src_kernel(BodyDev b, const double* __restrict__ Fb, double* Gsrc) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= b.n_src) return;
+    double v[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int row = b.src_rows[4 * p + r];
+        double acc = 0.0;
+        if (row >= 0) {
+            for (int e = b.et_ptr[row]; e < b.et_ptr[row + 1]; ++e) acc += b.w[b.et_w[e]] * Fb[b.et_k[e]];
+        }
+        v[r] = acc;
+    }
+    Gsrc[b.src_pts[p]] = (v[0] - v[1]) + (v[2] - v[3]);
+}
+
+cudaError_t launch_proj_src(const Geom& g, const BodyDev& b, const double* Fb, double* Gsrc, cudaStream_t st) {
+    if (b.n_src == 0) return cudaSuccess;
+    proj_src_kernel<<<(b.n_src + 127) / 128, 128, 0, st>>>(b, Fb, Gsrc);
+    return cudaGetLastError();
+}
+
+// C'E' e_kk for unit forces kk = col0 + r (B_times!, laplacian.jl:318), written
+// into the level-1 slab of batch member r (slab zeroed beforehand).  One thread
+// per point of the 14×14 box of Γ points the 13×13 flux window can reach.
+__global__ void unit_src_kernel(BodyDev b, Geom g, int col0, int ncol, double* G, long long bstride) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ncol * 196) return;
+    const int r = t / 196, ab = t % 196, da = ab / 14, db = ab % 14;
+    const int kk = col0 + r;
+    const int comp = kk / b.nb, k = kk % b.nb;
+    const int bx = b.bidx[k], by = b.bidx[b.nb + k];
+    const double* w = b.w + (long long)kk * 169;
+    const int gi = bx - 7 + da, gj = by - 7 + db;  // Julia Γ index
+    if (gi < 1 || gi > g.n1 || gj < 1 || gj > g.n2) return;
+    auto qx = [&](int I, int J) -> double {
+        const int l = I - bx + 6, m = J - by + 6;
+        return (comp == 0 && l >= 0 && l < 13 && m >= 0 && m < 13) ? w[l * 13 + m] : 0.0;
+    };
+    auto qy = [&](int I, int J) -> double {
+        const int l = I - bx + 6, m = J - by + 6;
+        return (comp == 1 && l >= 0 && l < 13 && m >= 0 && m < 13) ? w[l * 13 + m] : 0.0;
+    };
+    // Γ[i-1, j-1] = (qx[i, j-1] − qx[i, j]) + (qy[i, j] − qy[i-1, j]), (i, j) = (gi+1, gj+1)
+    const double v = (qx(gi + 1, gj) - qx(gi + 1, gj + 1)) + (qy(gi + 1, gj + 1) - qy(gi, gj + 1));
+    G[(long long)r * bstride + (long long)(gj - 1) * g.P + (gi - 1)] = v;
+}
+
+cudaError_t launch_unit_src(const Geom& g, const BodyDev& b, int col0, int ncol, double* G, long long bstride,
+                            cudaStream_t st) {
+    const int n = ncol * 196;
+    unit_src_kernel<<<(n + 255) / 256, 256, 0, st>>>(b, g, col0, ncol, G, bstride);
+    return cudaGetLastError();
+}
+
+}  // namespace ibpm

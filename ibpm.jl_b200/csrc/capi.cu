@@ -1,0 +1,594 @@
+// C ABI of libibpm_gpu.so: problem setup, state transfer and the time step
+// advance!(state, prob, t) of src/timestepping/timestepping.jl:35-67 for
+// static bodies, run as CUDA-graph replays of hand-written sm_100a kernels.
+#include "../../include/ibpm_gpu.h"
+#include "ibpm_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+using namespace ibpm;
+
+#define IBPM_VERSION_STR "ibpm_gpu 0.1.0 (sm_100a, FP64)"
+
+struct ibpm_handle {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    Geom g;
+    double h = 0, offx = 0, offy = 0, Re = 0, dt = 0, Ux = 0, Uy = 0, incl = 0;
+    double beta[2] = {1.5, -0.5};
+    int nb = 0, nf = 0, nbodies = 0;
+    std::vector<int> body_start;
+    DstPlan px{}, py{};
+    bool have_px = false, have_py = false;
+    // state
+    double* G[2] = {nullptr, nullptr};     // Γ (ping-pong: state / trial)
+    double* Nl[2] = {nullptr, nullptr};    // nonlinear term (ping-pong)
+    int cur = 0;                           // parity: G[cur], Nl[cur] hold the state
+    double* psi = nullptr;                 // ψ, mg slabs
+    double* q = nullptr;                   // q, (nq, mg) reference layout
+    double* qs = nullptr;                  // trial flux, level 1 only
+    double* rhs = nullptr;                 // mg slabs of scratch
+    double* Gsrc = nullptr;                // projection source, one slab, zero off-support
+    double* F = nullptr;                   // E (qs + q0)
+    double* Fb = nullptr;                  // F̃b
+    double* Binv = nullptr;                // nf×nf row-major
+    double* nonlin1_shadow = nullptr;      // nonlin[1] as set, until the next step
+    bool nonlin1_valid = false;
+    double q0x[8] = {0}, q0y[8] = {0};
+    // body
+    double* d_xb = nullptr; double* d_ds = nullptr; int* d_bidx = nullptr; double* d_w = nullptr;
+    int* d_body_start = nullptr;
+    int* d_src_pts = nullptr; int* d_src_rows = nullptr; int* d_et_ptr = nullptr; int* d_et_k = nullptr;
+    int* d_et_w = nullptr;
+    BodyDev body{};
+    // per-step outputs
+    double* hist = nullptr; int hist_cap = 0;
+    int* counter = nullptr; int* status = nullptr;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    bool graphs_ready = false;
+    std::string err;
+};
+
+static std::string g_create_err;
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                      \
+            return IBPM_ERR_CUDA;                                                             \
+        }                                                                                     \
+    } while (0)
+
+static int fail(ibpm_handle* h, int code, const std::string& msg) {
+    h->err = msg;
+    return code;
+}
+
+template <class T>
+static int dalloc(ibpm_handle* h, T** p, size_t n) {
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        h->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return IBPM_ERR_NOMEM;
+    }
+    return IBPM_OK;
+}
+
+static SlabMap levmap(const Geom& g, int lev0, int nlev, long long bstride = 0) {
+    SlabMap m;
+    m.nlev = nlev; m.lev0 = lev0; m.lstride = g.S; m.bstride = bstride ? bstride : g.S * g.mg;
+    return m;
+}
+
+static SpecParams spec(const ibpm_handle* h, int mode) {
+    SpecParams sp;
+    sp.mode = mode;
+    sp.scale = 1.0 / (4.0 * h->g.nx * h->g.ny);  // laplacian.jl:194
+    sp.dt = h->dt;
+    for (int l = 0; l < 8; ++l) {
+        const double hc = h->h * std::ldexp(1.0, l);
+        sp.den[l] = 2.0 * h->Re * (hc * hc);       // laplacian.jl:225
+    }
+    return sp;
+}
+
+// One Poisson-type solve x = S((S b) ./ M .* scale) on the slabs of `map`:
+// x-pass (b → tmp), y-pass with the spectral divide (tmp in place), x-pass
+// (tmp → out, stored or subtracted).  b may equal tmp; tmp may equal out.
+static int poisson(ibpm_handle* h, const double* b, SlabMap bmap, double* tmp, SlabMap tmap, double* out,
+                   SlabMap omap, int nslabs, int mode, int emit, const double* coarse = nullptr,
+                   SlabMap cmap = SlabMap{}) {
+    const Geom& g = h->g;
+    XPassArgs a{};
+    a.in = b; a.out = tmp; a.in_map = bmap; a.out_map = tmap;
+    a.coarse = coarse; a.coarse_map = cmap;
+    a.nslabs = nslabs; a.line0 = 0; a.line1 = g.n2;
+    a.load = coarse ? XLOAD_BC : XLOAD_PLAIN; a.emit = XEMIT_STORE;
+    CK(launch_dst_x(g, h->px, a, h->st));
+    CK(launch_dst_y_solve(g, h->py, h->px, tmp, tmap, nslabs, spec(h, mode), h->st));
+    XPassArgs c{};
+    c.in = tmp; c.out = out; c.in_map = tmap; c.out_map = omap;
+    c.nslabs = nslabs; c.line0 = 0; c.line1 = g.n2;
+    c.load = XLOAD_PLAIN; c.emit = emit;
+    CK(launch_dst_x(g, h->px, c, h->st));
+    return IBPM_OK;
+}
+
+// vort2flux! (curl.jl:411-443) on `nbatch` independent fields G (slab-major,
+// batch stride bstride): coarsify chain, telescoping Δ⁻¹ solves from the
+// coarsest level, then q = curl ψ on levels [qlev0, qlev0 + qnlev) into q
+// (nq per level, batch stride q_bstride).
+static int vort2flux(ibpm_handle* h, double* G, double* psi, long long bstride, int nbatch, double* q,
+                     long long q_bstride, int qlev0, int qnlev) {
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    for (int lev = 1; lev < mg; ++lev)
+        CK(launch_coarsify(g, G, levmap(g, lev - 1, 1, bstride), levmap(g, lev, 1, bstride), nbatch, h->st));
+    for (int lev = mg - 1; lev >= 0; --lev) {
+        SlabMap m = levmap(g, lev, 1, bstride);
+        const double* coarse = (lev < mg - 1) ? psi : nullptr;
+        int rc = poisson(h, G, m, psi, m, psi, m, nbatch, SPEC_DELTA, XEMIT_STORE, coarse,
+                         levmap(g, lev + 1, 1, bstride));
+        if (rc) return rc;
+    }
+    CurlArgs ca{};
+    ca.psi = psi; ca.psi_map = levmap(g, qlev0, qnlev, bstride);
+    ca.coarse = psi; ca.coarse_map = levmap(g, qlev0 + 1, qnlev, bstride);
+    ca.q = q; ca.q_bstride = q_bstride; ca.q_lstride = g.nq; ca.q_lev0 = qlev0;
+    ca.nlev = qnlev; ca.nbatch = nbatch; ca.mg = mg;
+    CK(launch_curl(g, ca, h->st));
+    return IBPM_OK;
+}
+
+// One step, reading the state from parity p and leaving it in parity p^1.
+static int enqueue_step(ibpm_handle* h, int p) {
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    double* Gold = h->G[p];
+    double* Gnew = h->G[p ^ 1];
+    // --- get_trial_state! (timestepping.jl:86-129)
+    RhsArgs ra{};
+    ra.G = Gold; ra.Gmap = levmap(g, 0, mg); ra.q = h->q;
+    ra.Nprev = h->Nl[p]; ra.Nnew = h->Nl[p ^ 1]; ra.rhs = h->rhs;
+    for (int l = 0; l < mg; ++l) {
+        const double hc = h->h * std::ldexp(1.0, l);
+        ra.q0x[l] = h->q0x[l]; ra.q0y[l] = h->q0y[l];
+        ra.fac_bc[l] = 0.25 * h->dt / (h->Re * (hc * hc));
+        ra.c_lap[l] = h->dt / (2.0 * h->Re * (hc * hc));
+        ra.nl_scale[l] = 1.0 / (4.0 * (hc * hc));
+    }
+    ra.b1dt = h->beta[0] * h->dt; ra.b2dt = h->beta[1] * h->dt; ra.mg = mg;
+    CK(launch_trial_rhs(g, ra, h->st));
+    SlabMap all = levmap(g, 0, mg);
+    int rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg, SPEC_AINV, XEMIT_STORE);
+    if (rc) return rc;
+    rc = vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->qs, 0, 0, 1);  // only the level-1 trial flux is read
+    if (rc) return rc;
+    // --- boundary_forces! (timestepping.jl:154-163) and update_stress! (:330-354)
+    CK(launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st));
+    CK(launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
+    CK(launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
+    // --- project_circ! (timestepping.jl:204-223): Γ = Γs − A⁻¹ C'E' F̃b on level 1
+    CK(launch_proj_src(g, h->body, h->Fb, h->Gsrc, h->st));
+    SlabMap one = levmap(g, 0, 1);
+    rc = poisson(h, h->Gsrc, one, h->rhs, one, Gnew, one, 1, SPEC_AINV, XEMIT_SUB);
+    if (rc) return rc;
+    // --- vort2flux!(state.ψ, state.q, state.Γ) (timestepping.jl:64)
+    return vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->q, 0, 0, mg);
+}
+
+// ---------------------------------------------------------------------------
+// Setup helpers
+// ---------------------------------------------------------------------------
+static int build_coupling(ibpm_handle* h, const ibpm_problem_desc* d) {
+    const Geom& g = h->g;
+    const int nb = h->nb;
+    std::vector<int> bidx(2 * nb);
+    for (int k = 0; k < nb; ++k) {
+        // body_idx = floor((xb + off)/h) (interface-coupling.jl:86-87)
+        bidx[k] = (int)std::floor((d->xb[k] + d->offx) / d->h);
+        bidx[nb + k] = (int)std::floor((d->xb[nb + k] + d->offy) / d->h);
+        const int bx = bidx[k], by = bidx[nb + k];
+        if (bx - 6 < 1 || bx + 6 > g.nx || by - 6 < 1 || by + 6 > g.ny)
+            return fail(h, IBPM_ERR_INVALID, "body point " + std::to_string(k) +
+                                                 ": the 13x13 regularisation stencil leaves the finest grid");
+    }
+    // E' as CSR over touched flux points, contributors in ascending component order.
+    std::map<int, std::vector<std::pair<int, int>>> rows;  // flux index -> (kk, widx)
+    for (int kk = 0; kk < h->nf; ++kk) {
+        const int comp = kk / nb, k = kk % nb;
+        const int bx = bidx[k], by = bidx[nb + k];
+        for (int l = 0; l < 13; ++l)
+            for (int m = 0; m < 13; ++m) {
+                const int I = bx + l - 6, J = by + m - 6;
+                const int f = comp == 0 ? (I - 1) + (J - 1) * (g.nx + 1) : g.nu + (I - 1) + (J - 1) * g.nx;
+                rows[f].push_back({kk, (kk * 13 + l) * 13 + m});
+            }
+    }
+    std::vector<int> et_ptr, et_k, et_w;
+    std::map<int, int> row_of;
+    et_ptr.push_back(0);
+    for (auto& kv : rows) {
+        row_of[kv.first] = (int)et_ptr.size() - 1;
+        for (auto& e : kv.second) { et_k.push_back(e.first); et_w.push_back(e.second); }
+        et_ptr.push_back((int)et_k.size());
+    }
+    // Γ points whose rot! stencil touches a regularised flux: Γ(i0, j0) uses
+    // qx[i0+2, j0+1], qx[i0+2, j0+2], qy[i0+2, j0+2], qy[i0+1, j0+2] (1-based).
+    auto fx = [&](int I, int J) { return (I - 1) + (J - 1) * (g.nx + 1); };
+    auto fy = [&](int I, int J) { return g.nu + (I - 1) + (J - 1) * g.nx; };
+    std::vector<int> src_pts, src_rows;
+    for (int j0 = 0; j0 < g.n2; ++j0)
+        for (int i0 = 0; i0 < g.n1; ++i0) {
+            const int f4[4] = {fx(i0 + 2, j0 + 1), fx(i0 + 2, j0 + 2), fy(i0 + 2, j0 + 2), fy(i0 + 1, j0 + 2)};
+            int r4[4];
+            bool any = false;
+            for (int r = 0; r < 4; ++r) {
+                auto it = row_of.find(f4[r]);
+                r4[r] = it == row_of.end() ? -1 : it->second;
+                any |= r4[r] >= 0;
+            }
+            if (!any) continue;
+            src_pts.push_back(j0 * g.P + i0);
+            for (int r = 0; r < 4; ++r) src_rows.push_back(r4[r]);
+        }
+    int rc;
+    if ((rc = dalloc(h, &h->d_xb, 2 * nb)) || (rc = dalloc(h, &h->d_ds, nb)) || (rc = dalloc(h, &h->d_bidx, 2 * nb)) ||
+        (rc = dalloc(h, &h->d_w, (size_t)h->nf * 169)) || (rc = dalloc(h, &h->d_body_start, h->nbodies + 1)) ||
+        (rc = dalloc(h, &h->d_src_pts, src_pts.size())) || (rc = dalloc(h, &h->d_src_rows, src_rows.size())) ||
+        (rc = dalloc(h, &h->d_et_ptr, et_ptr.size())) || (rc = dalloc(h, &h->d_et_k, et_k.size())) ||
+        (rc = dalloc(h, &h->d_et_w, et_w.size())))
+        return rc;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->st);
+    };
+    CK(up(h->d_xb, d->xb, sizeof(double) * 2 * nb));
+    CK(up(h->d_ds, d->ds, sizeof(double) * nb));
+    CK(up(h->d_bidx, bidx.data(), sizeof(int) * 2 * nb));
+    CK(up(h->d_body_start, h->body_start.data(), sizeof(int) * (h->nbodies + 1)));
+    if (!src_pts.empty()) {
+        CK(up(h->d_src_pts, src_pts.data(), sizeof(int) * src_pts.size()));
+        CK(up(h->d_src_rows, src_rows.data(), sizeof(int) * src_rows.size()));
+    }
+    CK(up(h->d_et_ptr, et_ptr.data(), sizeof(int) * et_ptr.size()));
+    CK(up(h->d_et_k, et_k.data(), sizeof(int) * et_k.size()));
+    CK(up(h->d_et_w, et_w.data(), sizeof(int) * et_w.size()));
+    CK(cudaStreamSynchronize(h->st));  // host vectors go out of scope
+    BodyDev& b = h->body;
+    b.nb = nb; b.nf = h->nf; b.nbodies = h->nbodies;
+    b.xb = h->d_xb; b.ds = h->d_ds; b.bidx = h->d_bidx; b.w = h->d_w; b.body_start = h->d_body_start;
+    b.n_src = (int)src_pts.size(); b.src_pts = h->d_src_pts; b.src_rows = h->d_src_rows;
+    b.et_ptr = h->d_et_ptr; b.et_k = h->d_et_k; b.et_w = h->d_et_w;
+    CK(launch_weights(g, d->h, d->offx, d->offy, b, h->st));
+    return IBPM_OK;
+}
+
+// B[:, j] = E · vort2flux(A⁻¹₁ C'E' e_j)[level-1 flux] (B_times!,
+// laplacian.jl:299-325), `chunk` columns per batch, then Binv = B⁻¹.
+static int build_binv(ibpm_handle* h) {
+    const Geom& g = h->g;
+    const int nf = h->nf, mg = g.mg;
+    const int chunk = std::min(nf, 128);
+    double *GB = nullptr, *PB = nullptr, *QB = nullptr, *work = nullptr;
+    int* info = nullptr;
+    int rc;
+    const long long bstride = g.S * mg;
+    if ((rc = dalloc(h, &GB, (size_t)bstride * chunk)) || (rc = dalloc(h, &PB, (size_t)bstride * chunk)) ||
+        (rc = dalloc(h, &QB, (size_t)g.nq * chunk)) || (rc = dalloc(h, &work, (size_t)2 * nf * nf + 2 * nf)) ||
+        (rc = dalloc(h, &info, 1))) {
+        cudaFree(GB); cudaFree(PB); cudaFree(QB); cudaFree(work); cudaFree(info);
+        return rc;
+    }
+    auto cleanup = [&]() { cudaFree(GB); cudaFree(PB); cudaFree(QB); cudaFree(work); cudaFree(info); };
+    for (int c0 = 0; c0 < nf && rc == IBPM_OK; c0 += chunk) {
+        const int R = std::min(chunk, nf - c0);
+        if (cudaMemsetAsync(GB, 0, sizeof(double) * bstride * R, h->st) != cudaSuccess) { rc = IBPM_ERR_CUDA; break; }
+        if (launch_unit_src(g, h->body, c0, R, GB, bstride, h->st) != cudaSuccess) { rc = IBPM_ERR_CUDA; break; }
+        SlabMap l0 = levmap(g, 0, 1, bstride);
+        rc = poisson(h, GB, l0, GB, l0, GB, l0, R, SPEC_AINV, XEMIT_STORE);
+        if (rc) break;
+        rc = vort2flux(h, GB, PB, bstride, R, QB, g.nq, 0, 1);  // level-1 flux of each column
+        if (rc) break;
+        if (launch_E(g, h->body, QB, g.nq, R, 0.0, 0.0, h->Binv + c0, -(long long)nf, h->st) != cudaSuccess) {
+            rc = IBPM_ERR_CUDA;
+            break;
+        }
+    }
+    if (rc == IBPM_OK) {
+        if (launch_gj_inverse(h->Binv, nf, work, info, h->st) != cudaSuccess) rc = fail(h, IBPM_ERR_CUDA, "gj inverse launch");
+    }
+    int hinfo = 0;
+    if (rc == IBPM_OK) {
+        cudaError_t e = cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, h->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+        if (e != cudaSuccess) rc = fail(h, IBPM_ERR_CUDA, std::string("B setup: ") + cudaGetErrorString(e));
+        else if (hinfo) rc = fail(h, IBPM_ERR_INVALID, "Schur complement B is singular (zero pivot at column " +
+                                                              std::to_string(hinfo) + ")");
+    }
+    cleanup();
+    return rc;
+}
+
+static void free_handle(ibpm_handle* h) {
+    if (!h) return;
+    for (int p = 0; p < 2; ++p) if (h->gexec[p]) cudaGraphExecDestroy(h->gexec[p]);
+    void* ptrs[] = {h->G[0], h->G[1], h->Nl[0], h->Nl[1], h->psi, h->q, h->qs, h->rhs, h->Gsrc, h->F, h->Fb,
+                    h->Binv, h->nonlin1_shadow, h->d_xb, h->d_ds, h->d_bidx, h->d_w, h->d_body_start,
+                    h->d_src_pts, h->d_src_rows, h->d_et_ptr, h->d_et_k, h->d_et_w, h->hist, h->counter, h->status};
+    for (void* p : ptrs) if (p) cudaFree(p);
+    if (h->have_px) dst_plan_destroy(&h->px);
+    if (h->have_py) dst_plan_destroy(&h->py);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+// ---------------------------------------------------------------------------
+// Public API
+// ---------------------------------------------------------------------------
+extern "C" const char* ibpm_version(void) { return IBPM_VERSION_STR; }
+
+extern "C" const char* ibpm_last_error(const ibpm_handle* h) {
+    return h ? h->err.c_str() : g_create_err.c_str();
+}
+
+static int create_impl(ibpm_handle* h, const ibpm_problem_desc* d) {
+    if (d->nx < 8 || d->ny < 8 || d->nx % 4 || d->ny % 4)
+        return fail(h, IBPM_ERR_INVALID, "nx and ny must be multiples of 4 and at least 8");
+    if (d->mg < 1 || d->mg > 8) return fail(h, IBPM_ERR_INVALID, "mg must be in 1..8");
+    if (!(d->h > 0) || !(d->dt > 0) || !(d->Re > 0)) return fail(h, IBPM_ERR_INVALID, "h, dt and Re must be positive");
+    if (d->nb < 1 || d->nbodies < 1 || !d->xb || !d->ds || !d->body_npts)
+        return fail(h, IBPM_ERR_INVALID, "at least one body with one point is required");
+    if (d->precision != IBPM_PREC_FP64) return fail(h, IBPM_ERR_UNSUPPORTED, "only IBPM_PREC_FP64 is built");
+    int tot = 0;
+    for (int j = 0; j < d->nbodies; ++j) {
+        if (d->body_npts[j] < 1) return fail(h, IBPM_ERR_INVALID, "every body needs at least one point");
+        tot += d->body_npts[j];
+    }
+    if (tot != d->nb) return fail(h, IBPM_ERR_INVALID, "sum(body_npts) != nb");
+    h->device = d->device;
+    CK(cudaSetDevice(d->device));
+    CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    h->g = make_geom(d->nx, d->ny, d->mg);
+    h->h = d->h; h->offx = d->offx; h->offy = d->offy; h->Re = d->Re; h->dt = d->dt;
+    h->Ux = d->Ux; h->Uy = d->Uy; h->incl = d->inclination;
+    h->beta[0] = d->beta[0]; h->beta[1] = d->beta[1];
+    h->nb = d->nb; h->nf = 2 * d->nb; h->nbodies = d->nbodies;
+    h->body_start.assign(d->nbodies + 1, 0);
+    for (int j = 0; j < d->nbodies; ++j) h->body_start[j + 1] = h->body_start[j] + d->body_npts[j];
+    const Geom& g = h->g;
+    const char* sup = "32, 64, 128, 192, 200, 256, 384, 400, 512, 768, 1024, 2048";
+    if (!dst_supported(g.nx)) return fail(h, IBPM_ERR_UNSUPPORTED, std::string("nx must be one of ") + sup);
+    if (!dst_supported(g.ny)) return fail(h, IBPM_ERR_UNSUPPORTED, std::string("ny must be one of ") + sup);
+    if (dst_plan_create(&h->px, g.nx, h->st)) return fail(h, IBPM_ERR_CUDA, "DST plan (x) setup failed");
+    h->have_px = true;
+    if (dst_plan_create(&h->py, g.ny, h->st)) return fail(h, IBPM_ERR_CUDA, "DST plan (y) setup failed");
+    h->have_py = true;
+    // base_flux! for inertial motion (timestepping.jl:252-270)
+    for (int l = 0; l < g.mg; ++l) {
+        const double hc = d->h * std::ldexp(1.0, l);
+        const double a = d->inclination;
+        h->q0x[l] = (d->Ux * std::cos(a) - d->Uy * std::sin(a)) * hc;
+        h->q0y[l] = (d->Ux * std::sin(a) + d->Uy * std::cos(a)) * hc;
+    }
+    const size_t slabs = (size_t)g.S * g.mg;
+    int rc;
+    if ((rc = dalloc(h, &h->G[0], slabs)) || (rc = dalloc(h, &h->G[1], slabs)) || (rc = dalloc(h, &h->Nl[0], slabs)) ||
+        (rc = dalloc(h, &h->Nl[1], slabs)) || (rc = dalloc(h, &h->psi, slabs)) ||
+        (rc = dalloc(h, &h->q, (size_t)g.nq * g.mg)) || (rc = dalloc(h, &h->qs, (size_t)g.nq * g.mg)) ||
+        (rc = dalloc(h, &h->rhs, slabs)) || (rc = dalloc(h, &h->Gsrc, g.S)) || (rc = dalloc(h, &h->F, h->nf)) ||
+        (rc = dalloc(h, &h->Fb, h->nf)) || (rc = dalloc(h, &h->Binv, (size_t)h->nf * h->nf)) ||
+        (rc = dalloc(h, &h->nonlin1_shadow, slabs)) || (rc = dalloc(h, &h->counter, 1)) ||
+        (rc = dalloc(h, &h->status, 1)))
+        return rc;
+    for (double* p : {h->G[0], h->G[1], h->Nl[0], h->Nl[1], h->psi, h->rhs, h->nonlin1_shadow})
+        CK(cudaMemsetAsync(p, 0, sizeof(double) * slabs, h->st));
+    CK(cudaMemsetAsync(h->q, 0, sizeof(double) * g.nq * g.mg, h->st));
+    CK(cudaMemsetAsync(h->qs, 0, sizeof(double) * g.nq * g.mg, h->st));
+    CK(cudaMemsetAsync(h->Gsrc, 0, sizeof(double) * g.S, h->st));
+    CK(cudaMemsetAsync(h->Fb, 0, sizeof(double) * h->nf, h->st));
+    CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
+    if ((rc = build_coupling(h, d))) return rc;
+    if ((rc = build_binv(h))) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_create(const ibpm_problem_desc* desc, ibpm_handle** out) {
+    if (!desc || !out) {
+        g_create_err = "null argument";
+        return IBPM_ERR_INVALID;
+    }
+    *out = nullptr;
+    ibpm_handle* h = new ibpm_handle();
+    int rc = create_impl(h, desc);
+    if (rc != IBPM_OK) {
+        g_create_err = h->err;
+        free_handle(h);
+        return rc;
+    }
+    g_create_err.clear();
+    *out = h;
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_destroy(ibpm_handle* h) {
+    if (!h) return IBPM_ERR_INVALID;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->st);
+    free_handle(h);
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_sizes(const ibpm_handle* h, int64_t* nGamma, int64_t* nq, int32_t* mg, int32_t* nf,
+                          int32_t* nbodies) {
+    if (!h) return IBPM_ERR_INVALID;
+    if (nGamma) *nGamma = (int64_t)h->g.n1 * h->g.n2;
+    if (nq) *nq = h->g.nq;
+    if (mg) *mg = h->g.mg;
+    if (nf) *nf = h->nf;
+    if (nbodies) *nbodies = h->nbodies;
+    return IBPM_OK;
+}
+
+// Γ-like (nΓ, mg) column-major host matrix <-> padded device slabs: the rows
+// of all levels are consecutive on both sides, so one 2-D copy moves them.
+static cudaError_t slab_copy(ibpm_handle* h, double* dst, const double* src, bool to_device) {
+    const Geom& g = h->g;
+    const size_t w = sizeof(double) * g.n1, rows = (size_t)g.n2 * g.mg;
+    if (to_device) return cudaMemcpy2DAsync(dst, sizeof(double) * g.P, src, w, w, rows, cudaMemcpyHostToDevice, h->st);
+    return cudaMemcpy2DAsync(dst, w, src, sizeof(double) * g.P, w, rows, cudaMemcpyDeviceToHost, h->st);
+}
+
+extern "C" int ibpm_set_state(ibpm_handle* h, const double* Gamma, const double* q, const double* q0,
+                              const double* psi, const double* nonlin1, const double* nonlin2, const double* Fb) {
+    if (!h) return IBPM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    const Geom& g = h->g;
+    if (q0) {
+        double nx0[8], ny0[8];
+        for (int l = 0; l < g.mg; ++l) {
+            const double* ql = q0 + (size_t)l * g.nq;
+            nx0[l] = ql[0];
+            ny0[l] = ql[g.nu];
+            for (int e = 0; e < g.nu; ++e)
+                if (ql[e] != nx0[l]) return fail(h, IBPM_ERR_UNSUPPORTED, "q0 must be uniform per level (x part)");
+            for (int e = g.nu; e < g.nq; ++e)
+                if (ql[e] != ny0[l]) return fail(h, IBPM_ERR_UNSUPPORTED, "q0 must be uniform per level (y part)");
+        }
+        for (int l = 0; l < g.mg; ++l) { h->q0x[l] = nx0[l]; h->q0y[l] = ny0[l]; }
+        h->graphs_ready = false;  // q0 is baked into the captured step
+    }
+    if (Gamma) CK(slab_copy(h, h->G[h->cur], Gamma, true));
+    if (psi) CK(slab_copy(h, h->psi, psi, true));
+    if (q) CK(cudaMemcpyAsync(h->q, q, sizeof(double) * g.nq * g.mg, cudaMemcpyHostToDevice, h->st));
+    if (nonlin2) CK(slab_copy(h, h->Nl[h->cur], nonlin2, true));
+    if (nonlin1) {
+        CK(slab_copy(h, h->nonlin1_shadow, nonlin1, true));
+        h->nonlin1_valid = true;
+    }
+    if (Fb) CK(cudaMemcpyAsync(h->Fb, Fb, sizeof(double) * h->nf, cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_get_state(ibpm_handle* h, double* Gamma, double* q, double* q0, double* psi, double* nonlin1,
+                              double* nonlin2, double* Fb) {
+    if (!h) return IBPM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    const Geom& g = h->g;
+    if (Gamma) CK(slab_copy(h, Gamma, h->G[h->cur], false));
+    if (psi) CK(slab_copy(h, psi, h->psi, false));
+    if (q) CK(cudaMemcpyAsync(q, h->q, sizeof(double) * g.nq * g.mg, cudaMemcpyDeviceToHost, h->st));
+    if (nonlin2) CK(slab_copy(h, nonlin2, h->Nl[h->cur], false));
+    if (nonlin1) CK(slab_copy(h, nonlin1, h->nonlin1_valid ? h->nonlin1_shadow : h->Nl[h->cur], false));
+    if (Fb) CK(cudaMemcpyAsync(Fb, h->Fb, sizeof(double) * h->nf, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (q0) {
+        for (int l = 0; l < g.mg; ++l) {
+            double* ql = q0 + (size_t)l * g.nq;
+            for (int e = 0; e < g.nu; ++e) ql[e] = h->q0x[l];
+            for (int e = g.nu; e < g.nq; ++e) ql[e] = h->q0y[l];
+        }
+    }
+    return IBPM_OK;
+}
+
+static int ensure_graphs(ibpm_handle* h, int cap) {
+    if (h->graphs_ready && h->hist_cap >= cap) return IBPM_OK;
+    if (h->hist_cap < cap) {
+        if (h->hist) cudaFree(h->hist);
+        h->hist = nullptr;
+        int rc = dalloc(h, &h->hist, (size_t)cap * 2 * h->nbodies);
+        if (rc) return rc;
+        h->hist_cap = cap;
+    }
+    for (int p = 0; p < 2; ++p) {
+        if (h->gexec[p]) { cudaGraphExecDestroy(h->gexec[p]); h->gexec[p] = nullptr; }
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(h, p);
+        cudaError_t e = cudaStreamEndCapture(h->st, &graph);
+        if (rc) return rc;
+        if (e != cudaSuccess) return fail(h, IBPM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&h->gexec[p], graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(h, IBPM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    h->graphs_ready = true;
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_advance(ibpm_handle* h, double t, int32_t nsteps, double* CD_out, double* CL_out) {
+    (void)t;
+    if (!h || nsteps < 0) return IBPM_ERR_INVALID;
+    if (nsteps == 0) return IBPM_OK;
+    CK(cudaSetDevice(h->device));
+    const int cap = std::max(1024, std::min(nsteps, 4096));
+    int rc = ensure_graphs(h, std::max(cap, h->hist_cap));
+    if (rc) return rc;
+    CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
+    std::vector<double> hb;
+    int done = 0;
+    while (done < nsteps) {
+        const int n = std::min(h->hist_cap, nsteps - done);
+        CK(cudaMemsetAsync(h->counter, 0, sizeof(int), h->st));
+        for (int s = 0; s < n; ++s) {
+            CK(cudaGraphLaunch(h->gexec[h->cur], h->st));
+            h->cur ^= 1;
+        }
+        h->nonlin1_valid = false;
+        if (CD_out || CL_out) {
+            hb.resize((size_t)n * 2 * h->nbodies);
+            CK(cudaMemcpyAsync(hb.data(), h->hist, sizeof(double) * hb.size(), cudaMemcpyDeviceToHost, h->st));
+            CK(cudaStreamSynchronize(h->st));
+            for (int s = 0; s < n; ++s)
+                for (int j = 0; j < h->nbodies; ++j) {
+                    if (CD_out) CD_out[(size_t)(done + s) * h->nbodies + j] = hb[((size_t)s * 2 + 0) * h->nbodies + j];
+                    if (CL_out) CL_out[(size_t)(done + s) * h->nbodies + j] = hb[((size_t)s * 2 + 1) * h->nbodies + j];
+                }
+        }
+        done += n;
+    }
+    int hstatus = 0;
+    CK(cudaMemcpyAsync(&hstatus, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (hstatus) return fail(h, IBPM_ERR_NONFINITE, "CD/CL became non-finite");
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_vort2flux(ibpm_handle* h) {
+    if (!h) return IBPM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    int rc = vort2flux(h, h->G[h->cur], h->psi, h->g.S * h->g.mg, 1, h->q, 0, 0, h->g.mg);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_get_binv(ibpm_handle* h, double* Binv) {
+    if (!h || !Binv) return IBPM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    const int nf = h->nf;
+    std::vector<double> rm((size_t)nf * nf);
+    CK(cudaMemcpyAsync(rm.data(), h->Binv, sizeof(double) * rm.size(), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int i = 0; i < nf; ++i)
+        for (int j = 0; j < nf; ++j) Binv[(size_t)i + (size_t)j * nf] = rm[(size_t)i * nf + j];
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_sync(ibpm_handle* h) {
+    if (!h) return IBPM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->st));
+    return IBPM_OK;
+}

@@ -1,0 +1,206 @@
+// Internal definitions shared by the kernels and the C ABI of libibpm_gpu.so.
+//
+// Device layout (all FP64):
+//   * A Γ-like field (Γ, ψ, nonlinear term, right-hand sides) of one level is a
+//     "slab" of (ny-1) rows of pitch P = nx doubles; element (i, j) (0-based,
+//     i < nx-1 fastest, j < ny-1) sits at row j, column i.  The reference keeps
+//     the same field as a column-major (nx-1)×(ny-1) matrix
+//     (src/fluid-domain/fluid-domain.jl:192); the pitch pads each row to 32 B.
+//   * A field with levels (and optionally a batch of right-hand sides) is
+//     slab-major: slab index = batch * mg + level.
+//   * A flux field of one level is the reference's flat vector of nq doubles:
+//     qx (nx+1)×ny column-major, then qy nx×(ny+1) (fluid-domain.jl:201-202).
+//   * Boundary vectors (Γbc / ψbc) use the reference's segment offsets
+//     LEFT = 0, RIGHT = ny+1, BOT = 2(ny+1), TOP = 2(ny+1)+nx+1
+//     (fluid-domain.jl:205-206); element v of a segment belongs to the edge
+//     vertex v (0 … nx or 0 … ny).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ibpm {
+
+struct Geom {
+    int nx, ny, mg;
+    int n1, n2;          // nx-1, ny-1
+    int P;               // slab pitch (doubles) = nx
+    long long S;         // slab size (doubles) = P * n2
+    int nu, nv, nq;      // flux sizes
+    int L, R, B, T, nbc; // boundary vector offsets and length
+};
+
+inline Geom make_geom(int nx, int ny, int mg) {
+    Geom g;
+    g.nx = nx; g.ny = ny; g.mg = mg;
+    g.n1 = nx - 1; g.n2 = ny - 1;
+    g.P = nx;
+    g.S = (long long)g.P * g.n2;
+    g.nu = ny * (nx + 1);
+    g.nv = nx * (ny + 1);
+    g.nq = g.nu + g.nv;
+    g.L = 0; g.R = ny + 1; g.B = 2 * (ny + 1); g.T = 2 * (ny + 1) + nx + 1;
+    g.nbc = 2 * (nx + 1) + 2 * (ny + 1);
+    return g;
+}
+
+// Maps blockIdx.y (or any flat slab counter) to (batch, level) and offsets.
+struct SlabMap {
+    int nlev;            // levels per batch member handled by the launch
+    int lev0;            // first level
+    long long bstride;   // doubles between batch members
+    long long lstride;   // doubles between levels
+    __host__ __device__ int level(int y) const { return lev0 + y % nlev; }
+    __host__ __device__ int batch(int y) const { return y / nlev; }
+    __host__ __device__ long long off(int y) const {
+        return (long long)(y / nlev) * bstride + (long long)(lev0 + y % nlev) * lstride;
+    }
+};
+
+// Edge value of get_bc! (src/fluid-operators/mg-utils.jl:7-32) for vertex v of
+// one segment, read from the coarser level's slab `rc`.  Along the segment the
+// coarse samples start at coarse index c0 (x for BOT/TOP, y for LEFT/RIGHT)
+// and sit at fixed cross index cfix: even v copies coarse point c0 + v/2, odd v
+// averages the two coarse points around it.
+//   BOT: c0 = nx/4-1 along x, cfix = ny/4-1      TOP: same, cfix = 3ny/4-1
+//   LEFT: c0 = ny/4-1 along y, cfix = nx/4-1     RIGHT: same, cfix = 3nx/4-1
+__device__ __forceinline__ double getbc_x(const double* __restrict__ rc, int P, int v,
+                                          int c0, int jfix) {
+    if ((v & 1) == 0) return rc[(long long)jfix * P + c0 + (v >> 1)];
+    int ia = c0 + ((v + 1) >> 1);
+    return 0.5 * (rc[(long long)jfix * P + ia] + rc[(long long)jfix * P + ia - 1]);
+}
+__device__ __forceinline__ double getbc_y(const double* __restrict__ rc, int P, int v,
+                                          int c0, int ifix) {
+    if ((v & 1) == 0) return rc[(long long)(c0 + (v >> 1)) * P + ifix];
+    int ja = c0 + ((v + 1) >> 1);
+    return 0.5 * (rc[(long long)ja * P + ifix] + rc[(long long)(ja - 1) * P + ifix]);
+}
+
+// The four edges of a fine level's boundary, sampled from the coarser slab.
+struct CoarseBC {
+    const double* rc;    // coarser-level slab, or nullptr for zero BCs
+    int P, nx, ny;
+    __device__ __forceinline__ double bot(int v) const {
+        return rc ? getbc_x(rc, P, v, nx / 4 - 1, ny / 4 - 1) : 0.0;
+    }
+    __device__ __forceinline__ double top(int v) const {
+        return rc ? getbc_x(rc, P, v, nx / 4 - 1, 3 * ny / 4 - 1) : 0.0;
+    }
+    __device__ __forceinline__ double left(int v) const {
+        return rc ? getbc_y(rc, P, v, ny / 4 - 1, nx / 4 - 1) : 0.0;
+    }
+    __device__ __forceinline__ double right(int v) const {
+        return rc ? getbc_y(rc, P, v, ny / 4 - 1, 3 * nx / 4 - 1) : 0.0;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Host-side launchers (defined in the .cu files).
+// ---------------------------------------------------------------------------
+struct DstPlan {
+    int N;               // transform length nx (x-pass) or ny (y-pass) = n + 1
+    double2* W;          // device: exp(+2πi t/N), t < N
+    double* s;           // device: sin(π m/N), m < N
+    double* c;           // device: cos(π (k+1)/N), k < N-1 (Laplacian eigenvalues)
+};
+
+bool dst_supported(int N);
+int dst_plan_create(DstPlan* p, int N, cudaStream_t st);  // 0 on success
+cudaError_t dst_init_attributes(int N);
+void dst_plan_destroy(DstPlan* p);
+
+// Spectral divisor applied between the two y-transforms of a Poisson solve:
+//   DELTA: w ← (w / Λ) · scale                       (Δ⁻¹, laplacian.jl:180-197)
+//   AINV:  w ← (w / (1 + Λ·dt / den[lev])) · scale    (A⁻¹, laplacian.jl:217-227)
+enum SpecMode { SPEC_DELTA = 0, SPEC_AINV = 1 };
+struct SpecParams {
+    int mode;
+    double scale;        // 1 / (4 nx ny)
+    double dt;
+    double den[8];       // 2 Re hc² per level
+};
+
+// x-direction DST-I of every line of the slabs selected by `map` over lines
+// [line0, line1).  Load/emit variants:
+enum XLoad { XLOAD_PLAIN = 0, XLOAD_BC = 1 };   // BC: add apply_bc!(·, get_bc!(coarser), 1)
+enum XEmit { XEMIT_STORE = 0, XEMIT_SUB = 1 };  // SUB: out ← out − value
+struct XPassArgs {
+    const double* in; double* out;
+    SlabMap in_map, out_map;
+    const double* coarse;  SlabMap coarse_map;   // XLOAD_BC: coarser-level field
+    int nslabs, line0, line1;
+    int load, emit;
+};
+cudaError_t launch_dst_x(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st);
+
+// y-direction: DST-I, spectral divide, DST-I (the middle of a Poisson solve),
+// in place on every slab selected by `map`.
+cudaError_t launch_dst_y_solve(const Geom& g, const DstPlan& py, const DstPlan& px_cos,
+                               double* data, SlabMap map, int nslabs,
+                               const SpecParams& sp, cudaStream_t st);
+
+// Stencil kernels (stencil.cu)
+struct RhsArgs {
+    const double* G; SlabMap Gmap;        // state Γ (all levels)
+    const double* q;                      // state q, nq per level
+    const double* Nprev;                  // nonlin from the previous step
+    double* Nnew;                         // nonlin of this step
+    double* rhs;                          // right-hand side of the trial solve
+    double q0x[8], q0y[8];                // uniform base flux per level
+    double fac_bc[8];                     // 0.25 dt / (Re hc²)
+    double c_lap[8];                      // dt / (2 Re hc²)
+    double nl_scale[8];                   // 1 / (4 hc²)
+    double b1dt, b2dt;                    // β1 dt, β2 dt
+    int mg;
+};
+cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st);
+
+cudaError_t launch_coarsify(const Geom& g, double* G, SlabMap fine_map, SlabMap coarse_map,
+                            int nslabs, cudaStream_t st);
+
+struct CurlArgs {
+    const double* psi; SlabMap psi_map;
+    const double* coarse; SlabMap coarse_map;  // coarser level ψ, or nullptr
+    double* q; long long q_bstride, q_lstride; int q_lev0;
+    int nlev;                                  // levels in this launch
+    int nbatch;
+    int mg;                                    // for "is coarsest" test
+};
+cudaError_t launch_curl(const Geom& g, const CurlArgs& a, cudaStream_t st);
+
+// Body / coupling kernels (body.cu)
+struct BodyDev {
+    int nb, nf, nbodies;
+    const double* xb;       // (nb, 2) column-major
+    const double* ds;       // nb
+    const int* bidx;        // (nb, 2) column-major, Julia 1-based floor((x+off)/h)
+    double* w;              // [nf][13][13] weights (k-major, x components then y)
+    const int* body_start;  // nbodies + 1 prefix of points
+    // E' then C' as a sorted segmented reduction
+    int n_src;              // Γ points in the support of C'E'
+    const int* src_pts;     // [n_src] flat (j * P + i) offsets into a slab
+    const int* src_rows;    // [n_src * 4] flux rows (index into et_ptr) or -1
+    const int* et_ptr;      // CSR row pointer over touched flux points
+    const int* et_k;        // CSR: force component index (0..nf-1), sorted ascending
+    const int* et_w;        // CSR: index into w[]
+};
+cudaError_t launch_weights(const Geom& g, double h, double offx, double offy,
+                           const BodyDev& b, cudaStream_t st);
+cudaError_t launch_E(const Geom& g, const BodyDev& b, const double* q, long long q_stride,
+                     int nbatch, double q0x, double q0y, double* F, long long F_stride,
+                     cudaStream_t st);
+cudaError_t launch_gemv(const double* A, const double* x, double* y, int n, cudaStream_t st);
+cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double dt,
+                          double* hist, int* counter, int* status, cudaStream_t st);
+cudaError_t launch_proj_src(const Geom& g, const BodyDev& b, const double* Fb, double* Gsrc,
+                            cudaStream_t st);
+cudaError_t launch_unit_src(const Geom& g, const BodyDev& b, int col0, int ncol, double* G,
+                            long long bstride, cudaStream_t st);
+
+// Dense linear algebra (linalg.cu): in-place inverse by Gauss–Jordan with
+// partial pivoting of the row-major n×n matrix A; `work` holds 2 n² + 2 n
+// doubles and `info` one int (set to the failing column + 1 on a zero pivot).
+cudaError_t launch_gj_inverse(double* A, int n, double* work, int* info, cudaStream_t st);
+
+}  // namespace ibpm

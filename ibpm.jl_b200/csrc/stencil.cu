@@ -1,0 +1,162 @@
+// Grid stencils of the IBPM step: the right-hand side of the trial solve
+// (nonlinear term + AB2 + explicit viscous term + cross-level BCs), coarsify!
+// and the multigrid curl.  Index comments use the reference's 1-based
+// (Julia) indices; device arrays are 0-based (see ibpm_internal.cuh).
+#include "ibpm_internal.cuh"
+
+namespace ibpm {
+
+// ---------------------------------------------------------------------------
+// Trial right-hand side, one thread per Γ point of one level:
+//   bc   = get_bc!(Γ[lev+1])                   (timestepping.jl:101-106)
+//   rhsbc= apply_bc!(0, bc, 0.25 dt/(Re hc²))
+//   N    = nonlinear!(Γ, q, q0, 0.25 bc)       (nonlinear.jl:168-201)
+//   rhs  = A Γ + β1 dt N + β2 dt Nprev + rhsbc  (timestepping.jl:111-118)
+// A Γ is evaluated as the 5-point stencil Γ + c (Σ neighbours − 4Γ), c =
+// dt/(2 Re hc²), with zero Dirichlet edges: the operator the reference applies
+// through two DSTs with the eigenvalues 1 − Λ c (laplacian.jl:229-232), whose
+// eigenvectors are exactly the DST-I basis.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j0 = blockIdx.y * blockDim.y + threadIdx.y;
+    const int lev = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, n1 = g.n1, n2 = g.n2, P = g.P;
+    if (i0 >= n1 || j0 >= n2) return;
+    const double* G = a.G + a.Gmap.off(lev);
+    const double* q = a.q + (long long)lev * g.nq;
+    const double* qy = q + g.nu;
+    const double q0x = a.q0x[lev], q0y = a.q0y[lev];
+
+    CoarseBC cb;
+    cb.rc = (lev < a.mg - 1) ? a.G + a.Gmap.off(lev + 1) : nullptr;
+    cb.P = P; cb.nx = nx; cb.ny = ny;
+
+    // Γ extended by the (0.25-scaled) edge values, vertex indices 0 … nx, 0 … ny.
+    auto Ge = [&](int vi, int vj) -> double {
+        if (vj == 0) return 0.25 * cb.bot(vi);
+        if (vj == ny) return 0.25 * cb.top(vi);
+        if (vi == 0) return 0.25 * cb.left(vj);
+        if (vi == nx) return 0.25 * cb.right(vj);
+        return G[(long long)(vj - 1) * P + (vi - 1)];
+    };
+    auto qxJ = [&](int I, int J) -> double { return q[(I - 1) + (long long)(J - 1) * (nx + 1)]; };
+    auto qyJ = [&](int I, int J) -> double { return qy[(I - 1) + (long long)(J - 1) * nx]; };
+    // avg_flux (nonlinear.jl:17-38)
+    auto QxJ = [&](int I, int J) -> double { return ((qxJ(I, J) + q0x) + qxJ(I, J - 1)) + q0x; };
+    auto QyJ = [&](int I, int J) -> double { return ((qyJ(I, J) + q0y) + qyJ(I - 1, J)) + q0y; };
+    // direct_product_loops! (nonlinear.jl:73-114)
+    auto fqxJ = [&](int I, int J) -> double { return QyJ(I, J + 1) * Ge(I - 1, J) + QyJ(I, J) * Ge(I - 1, J - 1); };
+    auto fqyJ = [&](int I, int J) -> double {
+        return -1.0 * (QxJ(I + 1, J) * Ge(I, J - 1) + QxJ(I, J) * Ge(I - 1, J - 1));
+    };
+    const int i = i0 + 1, j = j0 + 1;  // Julia Γ index
+    // C' fq (rot!, curl.jl:300-312) scaled by 1/(4 hc²)
+    const double N = ((fqxJ(i + 1, j) - fqxJ(i + 1, j + 1)) + (fqyJ(i + 1, j + 1) - fqyJ(i, j + 1))) * a.nl_scale[lev];
+
+    // explicit viscous operator
+    const double gc = G[(long long)j0 * P + i0];
+    const double ge = (i0 + 1 < n1) ? G[(long long)j0 * P + i0 + 1] : 0.0;
+    const double gw = (i0 > 0) ? G[(long long)j0 * P + i0 - 1] : 0.0;
+    const double gn = (j0 + 1 < n2) ? G[(long long)(j0 + 1) * P + i0] : 0.0;
+    const double gs = (j0 > 0) ? G[(long long)(j0 - 1) * P + i0] : 0.0;
+    const double AG = gc + a.c_lap[lev] * ((((ge + gw) + gn) + gs) - 4.0 * gc);
+
+    // apply_bc!(rhsbc = 0, bc, fac) (mg-utils.jl:43-60)
+    double rbc = 0.0;
+    if (cb.rc) {
+        const double fac = a.fac_bc[lev];
+        if (j0 == 0) rbc += fac * cb.bot(i0 + 1);
+        if (j0 == n2 - 1) rbc += fac * cb.top(i0 + 1);
+        if (i0 == 0) rbc += fac * cb.left(j0 + 1);
+        if (i0 == n1 - 1) rbc += fac * cb.right(j0 + 1);
+    }
+    const long long o = a.Gmap.off(lev) + (long long)j0 * P + i0;
+    const double Np = a.Nprev[o];
+    a.Nnew[o] = N;
+    a.rhs[o] = ((AG + a.b1dt * N) + a.b2dt * Np) + rbc;
+}
+
+cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st) {
+    dim3 blk(32, 8);
+    dim3 grid((g.n1 + 31) / 32, (g.n2 + 7) / 8, a.mg);
+    trial_rhs_kernel<<<grid, blk, 0, st>>>(a, g);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// coarsify! (mg-utils.jl:71-106): the centre half of the coarse level gets the
+// full-weighting restriction of the fine level, Γc[ic, jc] =
+//   Γ[i,j] + ½ (Γ[i+1,j] + Γ[i,j+1] + Γ[i-1,j] + Γ[i,j-1])
+//          + ¼ (Γ[i+1,j+1] + Γ[i+1,j-1] + Γ[i-1,j-1] + Γ[i-1,j+1]),
+// i = 2:2:nx-2 ↔ ic = nx/4 + i/2.
+// ---------------------------------------------------------------------------
+__global__ void coarsify_kernel(double* G, SlabMap fmap, SlabMap cmap, Geom g) {
+    const int nxc = g.nx / 2 - 1, nyc = g.ny / 2 - 1;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y * blockDim.y + threadIdx.y;
+    if (a >= nxc || b >= nyc) return;
+    const int P = g.P;
+    const double* F = G + fmap.off(blockIdx.z);
+    double* C = G + cmap.off(blockIdx.z);
+    const int i = 2 * a + 1, j = 2 * b + 1;  // 0-based fine point
+    auto f = [&](int ii, int jj) -> double { return F[(long long)jj * P + ii]; };
+    const double e = ((f(i + 1, j) + f(i, j + 1)) + f(i - 1, j)) + f(i, j - 1);
+    const double d = ((f(i + 1, j + 1) + f(i + 1, j - 1)) + f(i - 1, j - 1)) + f(i - 1, j + 1);
+    C[(long long)(g.ny / 4 + b) * P + (g.nx / 4 + a)] = (f(i, j) + 0.5 * e) + 0.25 * d;
+}
+
+cudaError_t launch_coarsify(const Geom& g, double* G, SlabMap fine_map, SlabMap coarse_map, int nslabs,
+                            cudaStream_t st) {
+    dim3 blk(32, 8);
+    dim3 grid((g.nx / 2 - 1 + 31) / 32, (g.ny / 2 - 1 + 7) / 8, nslabs);
+    coarsify_kernel<<<grid, blk, 0, st>>>(G, fine_map, coarse_map, g);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Multigrid curl (curl.jl:359-394): q = C ψ with edge streamfunction from
+// ψbc = get_bc!(ψ[lev+1]) (zero on the coarsest level).  Reproduces the
+// reference exactly, including the bottom row of x-fluxes reading ψbc[(B-1)+i]
+// (curl.jl:370), i.e. edge vertex i-2, where the top row reads vertex i-1.
+// One thread per flux element; blockIdx.y = batch × levels.
+// ---------------------------------------------------------------------------
+__global__ void curl_kernel(CurlArgs a, Geom g) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= g.nq) return;
+    const int y = blockIdx.y;
+    const int lev = a.psi_map.level(y);
+    const int bt = a.psi_map.batch(y);
+    const int nx = g.nx, ny = g.ny, P = g.P;
+    const double* psi = a.psi + a.psi_map.off(y);
+    CoarseBC cb;
+    cb.rc = (lev < a.mg - 1 && a.coarse) ? a.coarse + a.coarse_map.off(y) : nullptr;
+    cb.P = P; cb.nx = nx; cb.ny = ny;
+    auto ps = [&](int I, int J) -> double { return psi[(long long)(J - 1) * P + (I - 1)]; };
+    double v;
+    if (e < g.nu) {
+        const int I = e % (nx + 1) + 1, J = e / (nx + 1) + 1;
+        if (I == 1) v = cb.left(J) - cb.left(J - 1);
+        else if (I == nx + 1) v = cb.right(J) - cb.right(J - 1);
+        else if (J == 1) v = ps(I - 1, 1) - cb.bot(I - 2);
+        else if (J == ny) v = cb.top(I - 1) - ps(I - 1, ny - 1);
+        else v = ps(I - 1, J) - ps(I - 1, J - 1);
+    } else {
+        const int f = e - g.nu;
+        const int I = f % nx + 1, J = f / nx + 1;
+        if (J == 1) v = cb.bot(I - 1) - cb.bot(I);
+        else if (J == ny + 1) v = cb.top(I - 1) - cb.top(I);
+        else if (I == 1) v = cb.left(J - 1) - ps(1, J - 1);
+        else if (I == nx) v = ps(nx - 1, J - 1) - cb.right(J - 1);
+        else v = ps(I - 1, J - 1) - ps(I, J - 1);
+    }
+    a.q[(long long)bt * a.q_bstride + (long long)(lev - a.q_lev0) * a.q_lstride + e] = v;
+}
+
+cudaError_t launch_curl(const Geom& g, const CurlArgs& a, cudaStream_t st) {
+    dim3 grid((g.nq + 255) / 256, a.nlev * a.nbatch);
+    curl_kernel<<<grid, 256, 0, st>>>(a, g);
+    return cudaGetLastError();
+}
+
+}  // namespace ibpm

@@ -1,0 +1,355 @@
+"""Python host mirror of IBPM.jl's interface over libibpm_gpu.so (ctypes).
+
+The reference's user-facing pieces for the static-body time step are kept,
+with the same names and argument meanings:
+
+* ``make_grid(h, boundary, mg)``       src/fluid-domain/fluid-domain.jl:181-210
+* ``make_cylinder``, ``make_plate``, ``make_naca``
+                                       src/structure-domain/sample-bodies.jl:17-134
+* ``IBProblem(grid, bodies, dt, Re, freestream=...)``
+                                       src/pre-processing/problem-types.jl:188-199
+* ``IBState(prob)``                    src/pre-processing/state-types.jl:271-293
+* ``advance(state, prob, t)``          advance!(state, prob, t), src/timestepping/timestepping.jl:35-67
+* ``vort2flux(state, prob)``           vort2flux!(ψ, q, Γ, model, mg), src/fluid-operators/curl.jl:411-443
+
+All arrays use the reference's shapes and column-major layouts (``order='F'``
+views are not needed: ``state.Gamma`` is the (nΓ, mg) matrix flattened by
+column, exactly ``vec`` of the Julia matrix).  Every compute call runs in the
+CUDA library; there is no CPU fallback: if the library or a GPU is missing,
+the calls raise ``IBPMError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.normpath(os.path.join(_HERE, "..", "..", "lib", "libibpm_gpu.so"))
+HEADER_PATH = os.path.normpath(os.path.join(_HERE, "..", "..", "..", "include", "ibpm_gpu.h"))
+
+IBPM_OK = 0
+IBPM_ERR_INVALID = -1
+IBPM_ERR_CUDA = -2
+IBPM_ERR_NONFINITE = -3
+IBPM_ERR_UNSUPPORTED = -4
+IBPM_ERR_NOMEM = -5
+IBPM_PREC_FP64 = 0
+
+_ERRNAMES = {IBPM_ERR_INVALID: "INVALID", IBPM_ERR_CUDA: "CUDA", IBPM_ERR_NONFINITE: "NONFINITE",
+             IBPM_ERR_UNSUPPORTED: "UNSUPPORTED", IBPM_ERR_NOMEM: "NOMEM"}
+
+
+class IBPMError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("ibpm error %d (%s): %s" % (code, _ERRNAMES.get(code, "?"), msg))
+        self.code = code
+
+
+class ProblemDesc(C.Structure):
+    """Mirror of ``ibpm_problem_desc`` in include/ibpm_gpu.h."""
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("mg", C.c_int32),
+                ("h", C.c_double), ("offx", C.c_double), ("offy", C.c_double),
+                ("Re", C.c_double), ("dt", C.c_double),
+                ("Ux", C.c_double), ("Uy", C.c_double), ("inclination", C.c_double),
+                ("beta", C.c_double * 2),
+                ("nbodies", C.c_int32), ("nb", C.c_int32),
+                ("body_npts", C.POINTER(C.c_int32)), ("xb", C.POINTER(C.c_double)),
+                ("ds", C.POINTER(C.c_double)),
+                ("precision", C.c_int32), ("device", C.c_int32)]
+
+
+_DP = C.POINTER(C.c_double)
+_lib = None
+
+
+def load_library(path=None):
+    """Load libibpm_gpu.so (built in-tree by ``make -C ibpm.jl_b200/csrc``)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise IBPMError(IBPM_ERR_INVALID, "CUDA library not built: %s (run make -C ibpm.jl_b200/csrc)" % p)
+    lib = C.CDLL(p)
+    H = C.c_void_p
+    lib.ibpm_version.restype = C.c_char_p
+    lib.ibpm_version.argtypes = []
+    lib.ibpm_create.restype = C.c_int
+    lib.ibpm_create.argtypes = [C.POINTER(ProblemDesc), C.POINTER(H)]
+    lib.ibpm_destroy.restype = C.c_int
+    lib.ibpm_destroy.argtypes = [H]
+    lib.ibpm_last_error.restype = C.c_char_p
+    lib.ibpm_last_error.argtypes = [H]
+    lib.ibpm_sizes.restype = C.c_int
+    lib.ibpm_sizes.argtypes = [H, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                               C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    lib.ibpm_set_state.restype = C.c_int
+    lib.ibpm_set_state.argtypes = [H] + [_DP] * 7
+    lib.ibpm_get_state.restype = C.c_int
+    lib.ibpm_get_state.argtypes = [H] + [_DP] * 7
+    lib.ibpm_advance.restype = C.c_int
+    lib.ibpm_advance.argtypes = [H, C.c_double, C.c_int32, _DP, _DP]
+    lib.ibpm_vort2flux.restype = C.c_int
+    lib.ibpm_vort2flux.argtypes = [H]
+    lib.ibpm_get_binv.restype = C.c_int
+    lib.ibpm_get_binv.argtypes = [H, _DP]
+    lib.ibpm_sync.restype = C.c_int
+    lib.ibpm_sync.argtypes = [H]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def version():
+    return load_library().ibpm_version().decode()
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if a.dtype != np.float64 or not (a.flags["C_CONTIGUOUS"] or a.flags["F_CONTIGUOUS"]):
+        raise IBPMError(IBPM_ERR_INVALID, "arrays must be contiguous float64")
+    return a.ctypes.data_as(_DP)
+
+
+# --------------------------------------------------------------------------
+# Grid and bodies (host-side setup, as in the reference)
+# --------------------------------------------------------------------------
+@dataclass
+class MultiGrid:
+    """fluid-domain.jl:147-162."""
+    nx: int
+    ny: int
+    mg: int
+    offx: float
+    offy: float
+    len: float
+    h: float
+
+    @property
+    def nGamma(self):
+        return (self.nx - 1) * (self.ny - 1)
+
+    @property
+    def nq(self):
+        return self.ny * (self.nx + 1) + self.nx * (self.ny + 1)
+
+    @property
+    def nu(self):
+        return self.ny * (self.nx + 1)
+
+
+def make_grid(h, boundary, mg=1):
+    """fluid-domain.jl:181-210: nx = round(len/h), ny = round(ylen nx/len), h = len/nx."""
+    offx = -boundary[0]
+    offy = -boundary[2]
+    ln = boundary[1] - boundary[0]
+    ylen = boundary[3] - boundary[2]
+    nx = int(round(ln / h))
+    ny = int(round(ylen * nx / ln))
+    return MultiGrid(nx=nx, ny=ny, mg=mg, offx=offx, offy=offy, len=ln, h=ln / nx)
+
+
+@dataclass
+class RigidBody:
+    """RigidBody{Static} (body-types.jl:10-16): points xb (nb, 2) and ds (nb,)."""
+    xb: np.ndarray
+    ds: np.ndarray
+
+
+def make_cylinder(r, h, x0, y0, n=0):
+    """sample-bodies.jl:42-65 (n = 0 chooses ds ≈ 2h)."""
+    if n == 0:
+        n = int(math.floor(2 * math.pi * r / h / 2))
+    spt = np.arange(n) * (2 * math.pi / n)
+    xhat = r * np.cos(spt)
+    yhat = r * np.sin(spt)
+    ds = math.sqrt((xhat[1] - xhat[0]) ** 2 + (yhat[1] - yhat[0]) ** 2)
+    return RigidBody(xb=np.stack([xhat + x0, yhat + y0], axis=1), ds=np.full(n, ds))
+
+
+def make_plate(L, alpha, h, x0, y0, n=0):
+    """sample-bodies.jl:17-33 (n = 0 chooses ds ≈ 2h)."""
+    if n == 0:
+        n = int(math.floor(L / h / 2)) + 1
+    spt = L * np.arange(n) / (n - 1)
+    xhat = spt * math.cos(-alpha)
+    yhat = spt * math.sin(-alpha)
+    ds = math.sqrt((xhat[1] - xhat[0]) ** 2 + (yhat[1] - yhat[0]) ** 2)
+    return RigidBody(xb=np.stack([xhat + x0, yhat + y0], axis=1), ds=np.full(n, ds))
+
+
+def make_naca(x0, N, t, m=0.0, p=0.0, chord=1.0, aoa=0.0, pivot=(0.0, 0.0)):
+    """sample-bodies.jl:72-134 with a real thickness ``t``, chord scale and a
+    rotation by ``aoa`` (rad, nose up) about ``pivot``; panel midpoints and
+    lengths as the reference."""
+    dth = math.pi / (N - 1)
+    x = 0.5 * (1 + np.cos(dth * np.arange(N)))
+    yc = np.zeros_like(x)
+    th = np.zeros_like(x)
+    if m > 0 and p > 0:
+        mi = np.nonzero(x < p)[0][-1]
+        yc[:mi + 1] = (m / p ** 2) * (2 * p * x[:mi + 1] - x[:mi + 1] ** 2)
+        yc[mi + 1:] = (m / (1 - p) ** 2) * (1 - 2 * p + 2 * p * x[mi + 1:] - x[mi + 1:] ** 2)
+        dyc = np.zeros_like(x)
+        dyc[:mi + 1] = (2 * m / p ** 2) * (p - x[:mi + 1])
+        dyc[mi + 1:] = (2 * m / (1 - p ** 2)) * (p - x[mi + 1:])
+        th = np.arctan(dyc)
+    yt = 5 * t * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1036 * x ** 4)
+    yU = yc + yt * np.cos(th)
+    yL = yc - yt * np.cos(th)
+    xe = np.zeros((2 * N - 1, 2))
+    for i in range(N):
+        xe[i] = [x[i] - x0, yU[i]]
+    for i in range(N - 1):
+        xe[i + N] = [x[N - 2 - i] - x0, yL[N - 2 - i]]
+    xe *= chord
+    if aoa != 0.0:
+        c, s = math.cos(-aoa), math.sin(-aoa)
+        X = xe[:, 0] - pivot[0]
+        Y = xe[:, 1] - pivot[1]
+        xe = np.stack([c * X - s * Y + pivot[0], s * X + c * Y + pivot[1]], axis=1)
+    return RigidBody(xb=(xe[1:] + xe[:-1]) / 2.0, ds=np.sqrt(np.sum((xe[1:] - xe[:-1]) ** 2, axis=1)))
+
+
+# --------------------------------------------------------------------------
+# Problem and state
+# --------------------------------------------------------------------------
+class IBProblem:
+    """IBProblem(grid, bodies, dt, Re; freestream) on the GPU.
+
+    ``freestream`` = (Ux, Uy, inclination): constants or callables of t,
+    evaluated at t = 0 as the reference's IBState does for static bodies
+    (state-types.jl:291, timestepping.jl:252-270).  The handle owns the device
+    state; ``IBState`` objects are host mirrors of it.
+    """
+
+    def __init__(self, grid, bodies, dt, Re, freestream=(1.0, 0.0, 0.0), beta=(1.5, -0.5),
+                 device=0, sync_fields=True):
+        self.lib = load_library()
+        self.grid = grid
+        self.bodies = list(bodies)
+        self.dt = float(dt)
+        self.Re = float(Re)
+        ev = [f(0.0) if callable(f) else float(f) for f in freestream]
+        self.freestream = tuple(ev)
+        self.sync_fields = sync_fields
+        xb = np.concatenate([b.xb for b in self.bodies], axis=0)
+        self.nb = xb.shape[0]
+        self.nf = 2 * self.nb
+        self._xb = np.ascontiguousarray(xb.T.reshape(-1))      # column-major (nb, 2)
+        self._ds = np.ascontiguousarray(np.concatenate([b.ds for b in self.bodies]).astype(np.float64))
+        self._npts = (C.c_int32 * len(self.bodies))(*[b.xb.shape[0] for b in self.bodies])
+        d = ProblemDesc()
+        d.nx, d.ny, d.mg = grid.nx, grid.ny, grid.mg
+        d.h, d.offx, d.offy = grid.h, grid.offx, grid.offy
+        d.Re, d.dt = self.Re, self.dt
+        d.Ux, d.Uy, d.inclination = ev
+        d.beta[0], d.beta[1] = beta
+        d.nbodies, d.nb = len(self.bodies), self.nb
+        d.body_npts = C.cast(self._npts, C.POINTER(C.c_int32))
+        d.xb = self._xb.ctypes.data_as(_DP)
+        d.ds = self._ds.ctypes.data_as(_DP)
+        d.precision = IBPM_PREC_FP64
+        d.device = device
+        self._desc = d
+        h = C.c_void_p()
+        rc = self.lib.ibpm_create(C.byref(d), C.byref(h))
+        if rc != IBPM_OK:
+            raise IBPMError(rc, self.lib.ibpm_last_error(None).decode())
+        self.handle = h
+
+    def _check(self, rc):
+        if rc != IBPM_OK:
+            raise IBPMError(rc, self.lib.ibpm_last_error(self.handle).decode())
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.ibpm_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def binv(self):
+        """prob.Binv (laplacian.jl:274) as an (nf, nf) array."""
+        out = np.empty((self.nf, self.nf), order="F")
+        self._check(self.lib.ibpm_get_binv(self.handle, out.ctypes.data_as(_DP)))
+        return out
+
+    def sync(self):
+        self._check(self.lib.ibpm_sync(self.handle))
+
+
+class IBState:
+    """Host mirror of IBState (state-types.jl:253-268): q, q0 (nq, mg); Γ, ψ,
+    nonlin[k] (nΓ, mg); F̃b (nf, 1); CD, CL per body — all column-major."""
+
+    def __init__(self, prob):
+        g = prob.grid
+        self.q = np.zeros((g.nq, g.mg), order="F")
+        self.q0 = np.zeros((g.nq, g.mg), order="F")
+        self.Gamma = np.zeros((g.nGamma, g.mg), order="F")
+        self.psi = np.zeros((g.nGamma, g.mg), order="F")
+        self.nonlin = [np.zeros((g.nGamma, g.mg), order="F"), np.zeros((g.nGamma, g.mg), order="F")]
+        self.Fb = np.zeros((prob.nf, 1), order="F")
+        self.CD = np.zeros(len(prob.bodies))
+        self.CL = np.zeros(len(prob.bodies))
+        pull_state(self, prob)
+
+
+def pull_state(state, prob):
+    """Copy the device state into ``state``."""
+    prob._check(prob.lib.ibpm_get_state(prob.handle, _ptr(state.Gamma), _ptr(state.q), _ptr(state.q0),
+                                        _ptr(state.psi), _ptr(state.nonlin[0]), _ptr(state.nonlin[1]),
+                                        _ptr(state.Fb)))
+
+
+def push_state(state, prob, fields=("Gamma", "q", "q0", "psi", "nonlin", "Fb")):
+    """Copy ``state`` (the listed fields) to the device."""
+    f = set(fields)
+
+    def arr(name, a):
+        return np.asfortranarray(a, dtype=np.float64) if name in f else None
+
+    keep = [arr("Gamma", state.Gamma), arr("q", state.q), arr("q0", state.q0), arr("psi", state.psi),
+            arr("nonlin", state.nonlin[0]), arr("nonlin", state.nonlin[1]), arr("Fb", state.Fb)]
+    prob._check(prob.lib.ibpm_set_state(prob.handle, *[_ptr(a) for a in keep]))
+
+
+def advance(state, prob, t=0.0, nsteps=1):
+    """advance!(state, prob, t) — ``nsteps`` steps on the device.  Returns the
+    (nsteps, nbodies) CD and CL histories; state.CD/CL hold the last row.
+    Fields are copied back when ``prob.sync_fields`` is set."""
+    nbod = len(prob.bodies)
+    cd = np.zeros((nsteps, nbod))
+    cl = np.zeros((nsteps, nbod))
+    rc = prob.lib.ibpm_advance(prob.handle, float(t), int(nsteps), cd.ctypes.data_as(_DP),
+                               cl.ctypes.data_as(_DP))
+    if nsteps:
+        state.CD[:] = cd[-1]
+        state.CL[:] = cl[-1]
+    if prob.sync_fields:
+        pull_state(state, prob)
+    prob._check(rc)
+    return cd, cl
+
+
+def vort2flux(state, prob):
+    """vort2flux!(state.ψ, state.q, state.Γ, model, mg) on the device state."""
+    prob._check(prob.lib.ibpm_vort2flux(prob.handle))
+    pull_state(state, prob)
+
+
+def run_sim(t, state, prob):
+    """run_sim! of src/ibpm.jl:90-106 without logging: one step per entry of
+    ``t``; stops (like the reference) on a non-finite lift coefficient."""
+    cd, cl = advance(state, prob, t[0] if len(t) else 0.0, nsteps=len(t))
+    return cd, cl

@@ -1,0 +1,133 @@
+/*
+ * ibpm_gpu.h — C ABI of libibpm_gpu.so, a B200 (sm_100a) implementation of the
+ * static-body time step of the immersed boundary projection method
+ * (NUFgroup/IBPM.jl), meant to be bound from Julia with `ccall`, from Python
+ * with ctypes, or from C/C++ directly.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and
+ * returns an int status (IBPM_OK = 0, negative = error).  The text of the last
+ * error of a handle is returned by ibpm_last_error().  A handle owns all of its
+ * device memory and one CUDA stream; it is not thread-safe (one thread at a
+ * time per handle), like the reference's IBProblem whose working memory is
+ * shared across calls (src/pre-processing/models.jl:79-106).
+ *
+ * Array layouts are exactly the reference's (Julia column-major):
+ *   Γ, ψ, nonlin[k] : (nΓ, mg),  nΓ = (nx-1)(ny-1), index (i,j) -> i + (j-1)(nx-1)
+ *   q, q0           : (nq, mg),  nq = ny(nx+1) + nx(ny+1), [qx (nx+1)×ny ; qy nx×(ny+1)]
+ *   F̃b              : (nf, 1),   nf = 2 nb, [x-components of all points ; y-components]
+ *   xb              : (nb, 2),   [x of all points ; y of all points]
+ */
+#ifndef IBPM_GPU_H
+#define IBPM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define IBPM_OK               0
+#define IBPM_ERR_INVALID     -1   /* bad argument, size or handle               */
+#define IBPM_ERR_CUDA        -2   /* a CUDA runtime call failed                  */
+#define IBPM_ERR_NONFINITE   -3   /* CD/CL became NaN/Inf during ibpm_advance    */
+#define IBPM_ERR_UNSUPPORTED -4   /* valid in the reference, not in this build   */
+#define IBPM_ERR_NOMEM       -5   /* device allocation failed                    */
+
+/* Arithmetic of the step. */
+#define IBPM_PREC_FP64        0   /* plain FP64 everywhere                        */
+
+typedef struct ibpm_handle ibpm_handle;
+
+/*
+ * Problem description: the data of IBProblem(grid, bodies, dt, Re; freestream)
+ * (src/pre-processing/problem-types.jl:188-199) for RigidBody{Static} bodies.
+ * Grid fields are those of make_grid (src/fluid-domain/fluid-domain.jl:181-210)
+ * after its rounding: h = len/nx.  nx and ny must be multiples of 4
+ * (get_bc!/coarsify! of src/fluid-operators/mg-utils.jl need nx/4, ny/4).
+ */
+typedef struct ibpm_problem_desc {
+    int32_t nx, ny, mg;        /* cells per level and number of nested levels   */
+    double  h;                 /* finest grid spacing                           */
+    double  offx, offy;        /* -xmin, -ymin of the finest domain             */
+    double  Re, dt;            /* Reynolds number, time step                    */
+    double  Ux, Uy, inclination; /* freestream at t = 0 (timestepping.jl:252-270) */
+    double  beta[2];           /* explicit scheme coefficients, AB2 = {1.5,-0.5} */
+    int32_t nbodies;           /* number of bodies                              */
+    int32_t nb;                /* total number of boundary points               */
+    const int32_t* body_npts;  /* [nbodies] points per body (in xb order)       */
+    const double*  xb;         /* [nb*2] column-major (nb, 2)                   */
+    const double*  ds;         /* [nb] segment lengths                          */
+    int32_t precision;         /* IBPM_PREC_*                                   */
+    int32_t device;            /* CUDA device ordinal                           */
+} ibpm_problem_desc;
+
+/* Library version string. */
+const char* ibpm_version(void);
+
+/*
+ * Build a problem on the device: grid tables, the regularisation weights of E
+ * (interface-coupling.jl:72-137), the Schur complement B column by column with
+ * B_times! (laplacian.jl:254-275, 299-325) and its inverse.  Replaces
+ * IBProblem(...) (problem-types.jl:188-199).  The state starts as IBState(prob)
+ * (state-types.jl:271-293): zeros, with the uniform base flux q0.
+ */
+int ibpm_create(const ibpm_problem_desc* desc, ibpm_handle** out);
+
+/* Release every device resource of the handle. */
+int ibpm_destroy(ibpm_handle* h);
+
+/* Text of the last error recorded on `h` (or of the last failed create). */
+const char* ibpm_last_error(const ibpm_handle* h);
+
+/* Sizes of the arrays used by get/set_state: nΓ, nq, mg, nf, nbodies. */
+int ibpm_sizes(const ibpm_handle* h, int64_t* nGamma, int64_t* nq, int32_t* mg,
+               int32_t* nf, int32_t* nbodies);
+
+/*
+ * Copy a state in.  Any pointer may be NULL (field left unchanged).  The
+ * layouts are IBState's (state-types.jl:253-268).  q0 must be uniform per
+ * level and component, as base_flux! makes it for static bodies
+ * (timestepping.jl:252-270); anything else returns IBPM_ERR_UNSUPPORTED.
+ * q is stored as given: the next step's nonlinear term reads it, as the
+ * reference does, even if it is not the curl of ψ.
+ */
+int ibpm_set_state(ibpm_handle* h, const double* Gamma, const double* q,
+                   const double* q0, const double* psi, const double* nonlin1,
+                   const double* nonlin2, const double* Fb);
+
+/* Copy the state out (NULL pointers are skipped). */
+int ibpm_get_state(ibpm_handle* h, double* Gamma, double* q, double* q0,
+                   double* psi, double* nonlin1, double* nonlin2, double* Fb);
+
+/*
+ * Advance the state by `nsteps` steps of advance!(state, prob, t)
+ * (timestepping.jl:35-67).  t is accepted for interface parity; static bodies
+ * with a fixed base flux do not depend on it.  CD_out and CL_out (may be NULL)
+ * receive the per-step drag and lift coefficients of update_stress!
+ * (timestepping.jl:330-354) as [nsteps][nbodies].  Returns IBPM_ERR_NONFINITE
+ * if any CD/CL became non-finite (the reference's run_sim! stops on a
+ * non-finite CL, src/ibpm.jl:95-97); the state is then whatever the steps
+ * produced.
+ */
+int ibpm_advance(ibpm_handle* h, double t, int32_t nsteps, double* CD_out,
+                 double* CL_out);
+
+/*
+ * vort2flux!(state.ψ, state.q, state.Γ, model, mg) (curl.jl:411-443): make ψ
+ * and q consistent with Γ (coarsifies Γ into the coarse-level centres first).
+ */
+int ibpm_vort2flux(ibpm_handle* h);
+
+/* Copy out the precomputed inverse Schur complement (nf×nf, column-major),
+ * the reference's prob.Binv (laplacian.jl:274). */
+int ibpm_get_binv(ibpm_handle* h, double* Binv);
+
+/* Block until all work queued on the handle's stream is done. */
+int ibpm_sync(ibpm_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IBPM_GPU_H */
