@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of the IBPM time step (advance!) on B200.
+
+Workload: a circular cylinder, D = 1 at the origin, with
+314 boundary points (≈ 1 point per h), at Re = 100 in a uniform freestream
+U = 1 along x; 512×512 cells per level, h = 0.01 (finest domain
+x ∈ [-1, 4.12], y ∈ [-2.56, 2.56]), 5 nested levels, dt = 0.002.  The start
+state is a Gaussian vortex perturbation ω = 1e-3 exp(-r²/0.2²) centred at
+(1.5, 0.1) on the finest level (Γ = h² ω, then vort2flux!).  All inputs are
+synthetic; nothing is read from a dataset.
+
+Our arm (default): one process per GPU (torchrun for N > 1, replicas of the
+same simulation — the step does not shard), K steps replayed
+from a CUDA graph, each timed by CUDA events on the library's stream with a
+512 MiB L2 flush between steps (outside the timed pairs).  value =
+Σ_ranks nx·ny·mg·K / max_ranks(Σ step times).
+
+--impl reference: the FP64 CPU restatement of the reference's step
+(oracle/ibpm_ref.py, numpy + scipy.fft with all host threads) on the same
+workload, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "ibpm.jl_b200", "python"))
+
+# Config 2 of the benchmark definition.
+H = 0.01
+BOUNDARY = (-1.0, 4.12, -2.56, 2.56)
+MG = 5
+RE = 100.0
+DT = 0.002
+NB = 314
+VORTEX = dict(amp=1e-3, width=0.2, x0=1.5, y0=0.1)
+WORKLOAD = ("config 2: cylinder D=1 (314 pts) Re=100, 512x512 cells x 5 levels, h=0.01, dt=0.002, "
+            "Gaussian-vortex start (1e-3, 0.2, (1.5, 0.1))")
+METRIC = "cell-steps/s"
+FALLBACK_HBM_GBS = 6650.0
+REF_MAX_STEPS = 100
+
+# Algorithmic bytes of one FP64 step: s·nΓ·(34.5·mg + 3.5) + 8·nf² with s = 8
+# (every operator reads its inputs once and writes its outputs once; each 2-D
+# DST-I one read + one write of nΓ; 8·mg+2 DSTs per step).
+def step_bytes_model(nx, ny, mg, nf, s=8):
+    nG = (nx - 1) * (ny - 1)
+    return s * nG * (34.5 * mg + 3.5) + 8 * nf * nf
+
+
+def vortex_gamma(nx, ny, mg, h, offx, offy):
+    """Γ (nΓ, mg) column-major: h²·ω at the finest-level vertices, 0 elsewhere."""
+    i = np.arange(1, nx)
+    j = np.arange(1, ny)
+    X = i[:, None] * h - offx
+    Y = j[None, :] * h - offy
+    r2 = (X - VORTEX["x0"]) ** 2 + (Y - VORTEX["y0"]) ** 2
+    w = VORTEX["amp"] * np.exp(-r2 / VORTEX["width"] ** 2)
+    G = np.zeros(((nx - 1) * (ny - 1), mg), order="F")
+    G[:, 0] = (h * h * w).flatten(order="F")
+    return G
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def read_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from a committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        d = json.load(open(p))
+        return d.get(kernel)
+    except Exception:
+        return None
+
+
+# --------------------------------------------------------------------------
+# Clock sampling (nvidia-smi, during the timed region)
+# --------------------------------------------------------------------------
+SMI_Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + SMI_Q,
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.15)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# Distributed plumbing (replicas; barrier and max only)
+# --------------------------------------------------------------------------
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Dist:
+    def __init__(self):
+        self.world, self.rank, self.local = dist_env()
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+            self.dist = dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------
+# CPU arms (oracle)
+# --------------------------------------------------------------------------
+def cpu_problem(threads):
+    from oracle import ibpm_ref as R
+    R.WORKERS = threads
+    g = R.make_grid(H, BOUNDARY, MG)
+    p = R.IBProblem(grid=g, bodies=[R.make_cylinder(0.5, g.h, 0.0, 0.0, n=NB)], dt=DT, Re=RE,
+                    build_binv=False)
+    # The dense Schur solve costs one nf×nf GEMV per step whatever the matrix;
+    # a seeded dense matrix of the right size stands in for B⁻¹ in timing runs.
+    p.Binv = np.random.default_rng(0).standard_normal((p.nf, p.nf)) * 1e-3
+    st = R.make_state(p)
+    st.Gamma = np.stack([R.gamma_from_ref(vortex_gamma(g.nx, g.ny, g.mg, g.h, g.offx, g.offy), g)[l]
+                         for l in range(g.mg)])
+    R.refresh_flux(st, p)
+    return R, g, p, st
+
+
+def cpu_step_rate(steps, threads):
+    R, g, p, st = cpu_problem(threads)
+    R.advance(st, p)  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        R.advance(st, p)
+    dt = time.perf_counter() - t0
+    return g.nx * g.ny * g.mg * steps / dt, dt
+
+
+def run_reference(args, d):
+    if d.rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    R, g, p, st = cpu_problem(threads)
+    # bounded sample: at most REF_MAX_STEPS timed steps (≈ 0.2 s each on 8 cores)
+    nsteps = min(args.steps, REF_MAX_STEPS)
+    nwarm = min(args.warmup, 3)
+    for _ in range(nwarm):
+        R.advance(st, p)
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        R.advance(st, p)
+    wall = time.perf_counter() - t0
+    value = g.nx * g.ny * g.mg * nsteps / wall
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": nsteps, "warmup": nwarm, "ms_per_step": 1e3 * wall / nsteps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": "fp64", "implementation":
+                   "oracle/ibpm_ref.py: FP64 numpy/scipy restatement of the reference's advance! "
+                   "(the Julia reference itself cannot run here: no Julia toolchain)"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": "%d steps of the workload after %d warm-up steps (requested %d, capped "
+                                   "at %d); B^-1 replaced by a seeded dense matrix of the same size"
+                                   % (nsteps, nwarm, args.steps, REF_MAX_STEPS)},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------------------
+# Our arm
+# --------------------------------------------------------------------------
+def run_ours(args, d):
+    import ibpm_gpu as G
+    dev = d.local
+    g = G.make_grid(H, BOUNDARY, MG)
+    body = G.make_cylinder(0.5, g.h, 0.0, 0.0, n=NB)
+    prob = G.IBProblem(g, [body], DT, RE, freestream=(1.0, 0.0, 0.0), device=dev, sync_fields=False)
+    cells = g.nx * g.ny * g.mg
+
+    # seeded start state through the public API (pinned host mirror)
+    st = G.pinned_state(prob)
+    st.Gamma[...] = vortex_gamma(g.nx, g.ny, g.mg, g.h, g.offx, g.offy)
+    G.push_state(st, prob, fields=("Gamma",))
+    G.vort2flux(st, prob)
+    init = {k: np.array(getattr(st, k)) for k in ("Gamma", "q", "q0", "psi")}
+    init_nl = [np.array(a) for a in st.nonlin]
+
+    # warm-up (graph capture + first replays)
+    G.bench_steps(prob, max(args.warmup, 3), flush_l2=True)
+
+    # ---- device-timed region
+    d.barrier()
+    sampler = ClockSampler(dev)
+    sampler.start()
+    step_ms = G.bench_steps(prob, args.steps, flush_l2=True)
+    clocks = sampler.stop()
+    total_ms = float(np.sum(step_ms))
+    max_ms = d.max(total_ms)
+    value = d.world * cells * args.steps / (max_ms / 1e3)
+
+    # ---- end to end through the public API with host buffers: upload the
+    # state from pinned memory, K calls of advance! (each reads CD/CL back),
+    # download the state.
+    for k, v in init.items():
+        getattr(st, k)[...] = v
+    st.nonlin[0][...] = init_nl[0]
+    st.nonlin[1][...] = init_nl[1]
+    prob.sync()
+    d.barrier()
+    t0 = time.perf_counter()
+    G.push_state(st, prob)
+    for k in range(args.steps):
+        G.advance(st, prob, k * DT, nsteps=1)
+    G.pull_state(st, prob)
+    e2e_s = d.max(time.perf_counter() - t0)
+    state_bytes = 8 * (st.Gamma.size * 4 + st.q.size * 2 + st.Fb.size)
+    e2e = {"value": d.world * cells * args.steps / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": state_bytes / args.steps,
+           "d2h_bytes_per_step": (state_bytes + 16 * len(prob.bodies) * args.steps) / args.steps,
+           "note": "state uploaded once and downloaded once (amortised over the K steps); each "
+                   "advance! call returns CD/CL to the host"}
+
+    # ---- per-kernel profile (eager launches between CUDA events, L2 flushed per step)
+    prof = G.profile_steps(prob, 4, flush_l2=True)
+    lps = G.launches_per_step(prob)
+    dom = max(prof, key=lambda k: prof[k][0])
+    dms, dbytes, dcalls = prof[dom]
+    peak, peak_kind = read_peaks()
+    achieved = dbytes / (dms / 1e3) / 1e9
+    traffic = read_traffic(dom)
+    bstep = step_bytes_model(g.nx, g.ny, g.mg, prob.nf)
+    step_s = (total_ms / 1e3) / args.steps
+    out = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": d.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": "fp64 plain", "l2": "flushed between steps "
+                   "(512 MiB write outside the timed event pairs)", "parallelism": "replicas x%d" % d.world,
+                   "graph": "one CUDA graph replay per step"},
+        "e2e": e2e,
+        "gpu_launches": lps * args.steps,
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+                     if peak_kind == "measured" else "fallback 6.65 TB/s",
+                     "traffic": traffic, "launches_per_step": dcalls / 4.0,
+                     "bytes_per_launch": dbytes / dcalls, "avg_launch_us": 1e3 * dms / dcalls},
+        "step_roofline": {"model_bytes_per_step": bstep, "achieved_GBs": bstep / step_s / 1e9,
+                          "frac": bstep / step_s / 1e9 / peak},
+        "kernels": {k: {"ms_per_step": v[0] / 4.0, "GBs": (v[1] / (v[0] / 1e3) / 1e9) if v[0] > 0 else 0,
+                        "launches_per_step": v[2] / 4.0} for k, v in prof.items()},
+        "clocks": clocks,
+    }
+    if d.world == 1 and not args.no_cpu:
+        try:
+            rate, secs = cpu_step_rate(args.cpu_steps, os.cpu_count() or 1)
+            out["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": os.cpu_count() or 1, "kind": "port",
+                                   "sample": "%d steps of the same workload in oracle/ibpm_ref.py (%.1f s), "
+                                             "scipy.fft on all host threads; B^-1 replaced by a seeded dense "
+                                             "matrix of the same size" % (args.cpu_steps, secs)}
+        except Exception as e:  # the CPU leg is a reported baseline only
+            out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    prob.close()
+    if d.rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=20)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    d = Dist()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, d)
+        return run_ours(args, d)
+    finally:
+        d.close()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

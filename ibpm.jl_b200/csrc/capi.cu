@@ -52,6 +52,15 @@ struct ibpm_handle {
     int* counter = nullptr; int* status = nullptr;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     bool graphs_ready = false;
+    // measurement
+    int launches = 0;                      // kernel launches enqueued (counted always)
+    bool prof_on = false;                  // eager profiling: events around every launch
+    std::vector<cudaEvent_t> prof_ev;      // start/stop pairs
+    std::vector<int> prof_lab;
+    std::vector<double> prof_bytes;
+    int prof_n = 0;
+    void* flush_buf = nullptr;             // > L2, written between timed steps
+    size_t flush_bytes = 0;
     std::string err;
 };
 
@@ -64,6 +73,39 @@ static std::string g_create_err;
             h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                      \
             return IBPM_ERR_CUDA;                                                             \
         }                                                                                     \
+    } while (0)
+
+// Kernel classes reported by ibpm_profile (order of IBPM_KERNEL_* in the header).
+static const char* kKernelNames[] = {"trial_rhs", "dst_x", "dst_y_solve", "coarsify", "curl",
+                                     "E_gather", "binv_gemv", "stress", "proj_src"};
+enum { K_RHS = 0, K_DSTX, K_DSTY, K_COARSIFY, K_CURL, K_E, K_GEMV, K_STRESS, K_SRC, K_COUNT };
+
+static int prof_pre(ibpm_handle* h, int label, double bytes) {
+    ++h->launches;
+    if (!h->prof_on) return -1;
+    const int i = h->prof_n++;
+    if ((int)h->prof_ev.size() < 2 * (i + 1)) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        h->prof_ev.push_back(a);
+        h->prof_ev.push_back(b);
+    }
+    h->prof_lab.push_back(label);
+    h->prof_bytes.push_back(bytes);
+    cudaEventRecord(h->prof_ev[2 * i], h->st);
+    return i;
+}
+static void prof_post(ibpm_handle* h, int i) {
+    if (i >= 0) cudaEventRecord(h->prof_ev[2 * i + 1], h->st);
+}
+// Launch `call` (a cudaError_t expression) as kernel class `label` moving
+// `bytes` algorithmic bytes.
+#define LAUNCH(label, bytes, call)                 \
+    do {                                           \
+        const int pi_ = prof_pre(h, label, bytes); \
+        CK(call);                                  \
+        prof_post(h, pi_);                         \
     } while (0)
 
 static int fail(ibpm_handle* h, int code, const std::string& msg) {
@@ -113,13 +155,14 @@ static int poisson(ibpm_handle* h, const double* b, SlabMap bmap, double* tmp, S
     a.coarse = coarse; a.coarse_map = cmap;
     a.nslabs = nslabs; a.line0 = 0; a.line1 = g.n2;
     a.load = coarse ? XLOAD_BC : XLOAD_PLAIN; a.emit = XEMIT_STORE;
-    CK(launch_dst_x(g, h->px, a, h->st));
-    CK(launch_dst_y_solve(g, h->py, h->px, tmp, tmap, nslabs, spec(h, mode), h->st));
+    const double slab_bytes = 16.0 * g.n1 * g.n2 * nslabs;  // read + write every element once
+    LAUNCH(K_DSTX, slab_bytes, launch_dst_x(g, h->px, a, h->st));
+    LAUNCH(K_DSTY, slab_bytes, launch_dst_y_solve(g, h->py, h->px, tmp, tmap, nslabs, spec(h, mode), h->st));
     XPassArgs c{};
     c.in = tmp; c.out = out; c.in_map = tmap; c.out_map = omap;
     c.nslabs = nslabs; c.line0 = 0; c.line1 = g.n2;
     c.load = XLOAD_PLAIN; c.emit = emit;
-    CK(launch_dst_x(g, h->px, c, h->st));
+    LAUNCH(K_DSTX, slab_bytes * (emit == XEMIT_SUB ? 1.5 : 1.0), launch_dst_x(g, h->px, c, h->st));
     return IBPM_OK;
 }
 
@@ -132,7 +175,8 @@ static int vort2flux(ibpm_handle* h, double* G, double* psi, long long bstride, 
     const Geom& g = h->g;
     const int mg = g.mg;
     for (int lev = 1; lev < mg; ++lev)
-        CK(launch_coarsify(g, G, levmap(g, lev - 1, 1, bstride), levmap(g, lev, 1, bstride), nbatch, h->st));
+        LAUNCH(K_COARSIFY, 8.0 * 1.25 * g.n1 * g.n2 * nbatch,
+               launch_coarsify(g, G, levmap(g, lev - 1, 1, bstride), levmap(g, lev, 1, bstride), nbatch, h->st));
     for (int lev = mg - 1; lev >= 0; --lev) {
         SlabMap m = levmap(g, lev, 1, bstride);
         const double* coarse = (lev < mg - 1) ? psi : nullptr;
@@ -145,7 +189,7 @@ static int vort2flux(ibpm_handle* h, double* G, double* psi, long long bstride, 
     ca.coarse = psi; ca.coarse_map = levmap(g, qlev0 + 1, qnlev, bstride);
     ca.q = q; ca.q_bstride = q_bstride; ca.q_lstride = g.nq; ca.q_lev0 = qlev0;
     ca.nlev = qnlev; ca.nbatch = nbatch; ca.mg = mg;
-    CK(launch_curl(g, ca, h->st));
+    LAUNCH(K_CURL, 8.0 * ((double)g.n1 * g.n2 + g.nq) * qnlev * nbatch, launch_curl(g, ca, h->st));
     return IBPM_OK;
 }
 
@@ -167,18 +211,19 @@ static int enqueue_step(ibpm_handle* h, int p) {
         ra.nl_scale[l] = 1.0 / (4.0 * (hc * hc));
     }
     ra.b1dt = h->beta[0] * h->dt; ra.b2dt = h->beta[1] * h->dt; ra.mg = mg;
-    CK(launch_trial_rhs(g, ra, h->st));
+    LAUNCH(K_RHS, 8.0 * (4.0 * g.n1 * g.n2 + g.nq) * mg, launch_trial_rhs(g, ra, h->st));
     SlabMap all = levmap(g, 0, mg);
     int rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg, SPEC_AINV, XEMIT_STORE);
     if (rc) return rc;
     rc = vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->qs, 0, 0, 1);  // only the level-1 trial flux is read
     if (rc) return rc;
     // --- boundary_forces! (timestepping.jl:154-163) and update_stress! (:330-354)
-    CK(launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st));
-    CK(launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
-    CK(launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
+    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st));
+    LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
+    LAUNCH(K_STRESS, 8.0 * 3 * h->nb,
+           launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
     // --- project_circ! (timestepping.jl:204-223): Γ = Γs − A⁻¹ C'E' F̃b on level 1
-    CK(launch_proj_src(g, h->body, h->Fb, h->Gsrc, h->st));
+    LAUNCH(K_SRC, 8.0 * 4 * 169 * h->nf, launch_proj_src(g, h->body, h->Fb, h->Gsrc, h->st));
     SlabMap one = levmap(g, 0, 1);
     rc = poisson(h, h->Gsrc, one, h->rhs, one, Gnew, one, 1, SPEC_AINV, XEMIT_SUB);
     if (rc) return rc;
@@ -325,6 +370,8 @@ static void free_handle(ibpm_handle* h) {
                     h->Binv, h->nonlin1_shadow, h->d_xb, h->d_ds, h->d_bidx, h->d_w, h->d_body_start,
                     h->d_src_pts, h->d_src_rows, h->d_et_ptr, h->d_et_k, h->d_et_w, h->hist, h->counter, h->status};
     for (void* p : ptrs) if (p) cudaFree(p);
+    if (h->flush_buf) cudaFree(h->flush_buf);
+    for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
     if (h->have_px) dst_plan_destroy(&h->px);
     if (h->have_py) dst_plan_destroy(&h->py);
     if (h->st) cudaStreamDestroy(h->st);
@@ -591,4 +638,111 @@ extern "C" int ibpm_sync(ibpm_handle* h) {
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->st));
     return IBPM_OK;
+}
+
+extern "C" int ibpm_launches_per_step(ibpm_handle* h) {
+    if (!h) return IBPM_ERR_INVALID;
+    int rc = ensure_graphs(h, std::max(1024, h->hist_cap));
+    if (rc) return rc;
+    const int before = h->launches;
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue_step(h, h->cur);
+    cudaError_t e = cudaStreamEndCapture(h->st, &graph);
+    if (e == cudaSuccess) cudaGraphDestroy(graph);
+    if (rc) return rc;
+    return h->launches - before;
+}
+
+extern "C" int ibpm_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, double* step_ms) {
+    if (!h || nsteps < 1 || !step_ms) return IBPM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    int rc = ensure_graphs(h, std::max(1024, h->hist_cap));
+    if (rc) return rc;
+    if (flush_l2 && !h->flush_buf) {
+        h->flush_bytes = (size_t)512 << 20;  // 4x the 126 MB L2
+        if ((rc = dalloc(h, (char**)&h->flush_buf, h->flush_bytes))) return rc;
+    }
+    std::vector<cudaEvent_t> ev(2 * nsteps);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    int done = 0;
+    while (done < nsteps) {
+        const int n = std::min(h->hist_cap, nsteps - done);
+        CK(cudaMemsetAsync(h->counter, 0, sizeof(int), h->st));
+        for (int s = 0; s < n; ++s) {
+            if (flush_l2) CK(cudaMemsetAsync(h->flush_buf, (done + s) & 0xff, h->flush_bytes, h->st));
+            CK(cudaEventRecord(ev[2 * (done + s)], h->st));
+            CK(cudaGraphLaunch(h->gexec[h->cur], h->st));
+            CK(cudaEventRecord(ev[2 * (done + s) + 1], h->st));
+            h->cur ^= 1;
+        }
+        done += n;
+    }
+    h->nonlin1_valid = false;
+    CK(cudaStreamSynchronize(h->st));
+    for (int s = 0; s < nsteps; ++s) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev[2 * s], ev[2 * s + 1]));
+        step_ms[s] = ms;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_profile(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, double* ms_out,
+                            double* bytes_out, int32_t* calls_out) {
+    if (!h || nsteps < 1 || !ms_out || !bytes_out || !calls_out) return IBPM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    if (flush_l2 && !h->flush_buf) {
+        h->flush_bytes = (size_t)512 << 20;
+        int rc = dalloc(h, (char**)&h->flush_buf, h->flush_bytes);
+        if (rc) return rc;
+    }
+    if (h->hist_cap < nsteps) {
+        int rc = ensure_graphs(h, std::max(nsteps, 1024));
+        if (rc) return rc;
+    }
+    for (int k = 0; k < K_COUNT; ++k) { ms_out[k] = 0; bytes_out[k] = 0; calls_out[k] = 0; }
+    CK(cudaMemsetAsync(h->counter, 0, sizeof(int), h->st));
+    h->prof_on = true;
+    h->prof_n = 0;
+    h->prof_lab.clear();
+    h->prof_bytes.clear();
+    int rc = IBPM_OK;
+    for (int s = 0; s < nsteps && rc == IBPM_OK; ++s) {
+        if (flush_l2) {
+            cudaError_t e = cudaMemsetAsync(h->flush_buf, s & 0xff, h->flush_bytes, h->st);
+            if (e != cudaSuccess) { rc = fail(h, IBPM_ERR_CUDA, cudaGetErrorString(e)); break; }
+        }
+        rc = enqueue_step(h, h->cur);
+        h->cur ^= 1;
+    }
+    h->prof_on = false;
+    h->nonlin1_valid = false;
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    for (int i = 0; i < h->prof_n; ++i) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, h->prof_ev[2 * i], h->prof_ev[2 * i + 1]));
+        const int k = h->prof_lab[i];
+        ms_out[k] += ms;
+        bytes_out[k] += h->prof_bytes[i];
+        calls_out[k] += 1;
+    }
+    return IBPM_OK;
+}
+
+extern "C" const char* ibpm_kernel_name(int32_t k) {
+    return (k >= 0 && k < K_COUNT) ? kKernelNames[k] : "";
+}
+
+extern "C" void* ibpm_host_alloc(int64_t bytes) {
+    void* p = nullptr;
+    if (bytes <= 0 || cudaHostAlloc(&p, (size_t)bytes, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+    return p;
+}
+
+extern "C" int ibpm_host_free(void* p) {
+    if (!p) return IBPM_ERR_INVALID;
+    return cudaFreeHost(p) == cudaSuccess ? IBPM_OK : IBPM_ERR_CUDA;
 }

@@ -38,6 +38,7 @@ IBPM_ERR_NONFINITE = -3
 IBPM_ERR_UNSUPPORTED = -4
 IBPM_ERR_NOMEM = -5
 IBPM_PREC_FP64 = 0
+KERNEL_COUNT = 9
 
 _ERRNAMES = {IBPM_ERR_INVALID: "INVALID", IBPM_ERR_CUDA: "CUDA", IBPM_ERR_NONFINITE: "NONFINITE",
              IBPM_ERR_UNSUPPORTED: "UNSUPPORTED", IBPM_ERR_NOMEM: "NOMEM"}
@@ -99,6 +100,18 @@ def load_library(path=None):
     lib.ibpm_get_binv.argtypes = [H, _DP]
     lib.ibpm_sync.restype = C.c_int
     lib.ibpm_sync.argtypes = [H]
+    lib.ibpm_host_alloc.restype = C.c_void_p
+    lib.ibpm_host_alloc.argtypes = [C.c_int64]
+    lib.ibpm_host_free.restype = C.c_int
+    lib.ibpm_host_free.argtypes = [C.c_void_p]
+    lib.ibpm_kernel_name.restype = C.c_char_p
+    lib.ibpm_kernel_name.argtypes = [C.c_int32]
+    lib.ibpm_launches_per_step.restype = C.c_int
+    lib.ibpm_launches_per_step.argtypes = [H]
+    lib.ibpm_bench.restype = C.c_int
+    lib.ibpm_bench.argtypes = [H, C.c_int32, C.c_int32, _DP]
+    lib.ibpm_profile.restype = C.c_int
+    lib.ibpm_profile.argtypes = [H, C.c_int32, C.c_int32, _DP, _DP, C.POINTER(C.c_int32)]
     if path is None:
         _lib = lib
     return lib
@@ -303,6 +316,78 @@ class IBState:
         self.CD = np.zeros(len(prob.bodies))
         self.CL = np.zeros(len(prob.bodies))
         pull_state(self, prob)
+
+
+class PinnedArray:
+    """A float64 numpy array over page-locked host memory from ibpm_host_alloc."""
+
+    def __init__(self, shape, order="F"):
+        lib = load_library()
+        n = int(np.prod(shape))
+        self._lib = lib
+        self._p = lib.ibpm_host_alloc(8 * max(n, 1))
+        if not self._p:
+            raise IBPMError(IBPM_ERR_NOMEM, "ibpm_host_alloc failed")
+        buf = (C.c_double * max(n, 1)).from_address(self._p)
+        self.array = np.ndarray(shape, dtype=np.float64, buffer=buf, order=order)
+        self.array[...] = 0.0
+
+    def free(self):
+        if self._p:
+            self.array = None
+            self._lib.ibpm_host_free(self._p)
+            self._p = None
+
+
+def pinned_state(prob):
+    """An IBState whose arrays live in page-locked host memory."""
+    g = prob.grid
+    keep = []
+
+    def mk(shape):
+        pa = PinnedArray(shape)
+        keep.append(pa)
+        return pa.array
+
+    st = IBState.__new__(IBState)
+    st.q, st.q0 = mk((g.nq, g.mg)), mk((g.nq, g.mg))
+    st.Gamma, st.psi = mk((g.nGamma, g.mg)), mk((g.nGamma, g.mg))
+    st.nonlin = [mk((g.nGamma, g.mg)), mk((g.nGamma, g.mg))]
+    st.Fb = mk((prob.nf, 1))
+    st.CD = np.zeros(len(prob.bodies))
+    st.CL = np.zeros(len(prob.bodies))
+    st._pinned = keep
+    pull_state(st, prob)
+    return st
+
+
+def kernel_names():
+    lib = load_library()
+    return [lib.ibpm_kernel_name(k).decode() for k in range(KERNEL_COUNT)]
+
+
+def bench_steps(prob, nsteps, flush_l2=True):
+    """Per-step device times (ms) of nsteps graph replays (ibpm_bench)."""
+    out = np.zeros(nsteps)
+    prob._check(prob.lib.ibpm_bench(prob.handle, int(nsteps), int(bool(flush_l2)), out.ctypes.data_as(_DP)))
+    return out
+
+
+def profile_steps(prob, nsteps, flush_l2=True):
+    """Per-kernel-class (ms, algorithmic bytes, launches) over nsteps eager steps."""
+    ms = np.zeros(KERNEL_COUNT)
+    by = np.zeros(KERNEL_COUNT)
+    calls = np.zeros(KERNEL_COUNT, dtype=np.int32)
+    prob._check(prob.lib.ibpm_profile(prob.handle, int(nsteps), int(bool(flush_l2)), ms.ctypes.data_as(_DP),
+                                      by.ctypes.data_as(_DP), calls.ctypes.data_as(C.POINTER(C.c_int32))))
+    return {n: (ms[k], by[k], int(calls[k])) for k, n in enumerate(kernel_names())}
+
+
+def launches_per_step(prob):
+    n = prob.lib.ibpm_launches_per_step(prob.handle)
+    if n < 0:
+        prob._check(n)
+    return n
 
 
 def pull_state(state, prob):

@@ -126,6 +126,37 @@ int ibpm_get_binv(ibpm_handle* h, double* Binv);
 /* Block until all work queued on the handle's stream is done. */
 int ibpm_sync(ibpm_handle* h);
 
+/* Page-locked host memory for state mirrors (faster get/set_state); NULL on
+ * failure.  No counterpart in the reference (Julia arrays are pageable). */
+void* ibpm_host_alloc(int64_t bytes);
+int ibpm_host_free(void* p);
+
+/* ---- Measurement (no counterpart in the reference, which times runs with
+ * @elapsed around run_sim!, src/ibpm.jl:71) ---------------------------- */
+
+/* Kernel classes reported by ibpm_profile. */
+#define IBPM_KERNEL_COUNT 9   /* trial_rhs, dst_x, dst_y_solve, coarsify, curl,
+                                 E_gather, binv_gemv, stress, proj_src */
+
+/* Name of kernel class k (0 <= k < IBPM_KERNEL_COUNT). */
+const char* ibpm_kernel_name(int32_t k);
+
+/* Number of kernel launches in one step (one replay of the step graph). */
+int ibpm_launches_per_step(ibpm_handle* h);
+
+/* Advance nsteps steps as graph replays and return each step's device time
+ * (CUDA events on the handle's stream) in step_ms[nsteps].  With flush_l2, a
+ * 512 MiB buffer is written between steps, outside the timed event pairs, so
+ * each step starts with a cold L2. */
+int ibpm_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, double* step_ms);
+
+/* Advance nsteps steps with every kernel launched eagerly between CUDA events
+ * and accumulate, per kernel class, device milliseconds, algorithmic bytes
+ * (each operand read once, each result written once) and launch counts into
+ * ms_out / bytes_out / calls_out [IBPM_KERNEL_COUNT]. */
+int ibpm_profile(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, double* ms_out,
+                 double* bytes_out, int32_t* calls_out);
+
 #ifdef __cplusplus
 }
 #endif
