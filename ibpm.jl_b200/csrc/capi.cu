@@ -66,6 +66,8 @@ struct ibpm_handle {
 
 static std::string g_create_err;
 
+void ibpm::set_global_error(const char* msg) { g_create_err = msg ? msg : ""; }
+
 #define CK(call)                                                                              \
     do {                                                                                      \
         cudaError_t e_ = (call);                                                              \

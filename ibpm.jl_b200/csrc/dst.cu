@@ -89,6 +89,11 @@ int dst_plan_create(DstPlan* p, int N, cudaStream_t st) {
     return 0;
 }
 
+cudaError_t dst_tables_build(int N, double2* W, double* s, double* c, cudaStream_t st) {
+    dst_tables_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, W, s, c);
+    return cudaGetLastError();
+}
+
 void dst_plan_destroy(DstPlan* p) {
     if (p->W) cudaFree(p->W);
     if (p->s) cudaFree(p->s);

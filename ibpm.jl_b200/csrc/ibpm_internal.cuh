@@ -108,6 +108,10 @@ struct DstPlan {
 bool dst_supported(int N);
 int dst_plan_create(DstPlan* p, int N, cudaStream_t st);  // 0 on success
 cudaError_t dst_init_attributes(int N);
+// Fill transform tables of length N into caller-provided device memory.
+cudaError_t dst_tables_build(int N, double2* W, double* s, double* c, cudaStream_t st);
+// Error text returned by ibpm_last_error(NULL).
+void set_global_error(const char* msg);
 void dst_plan_destroy(DstPlan* p);
 
 // Spectral divisor applied between the two y-transforms of a Poisson solve:

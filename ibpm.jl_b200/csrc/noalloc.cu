@@ -1,0 +1,122 @@
+// Inverse-Laplacian solve that allocates no device memory.
+//
+// Some callers cannot call cudaMalloc: hosts whose device memory is owned by a
+// pool or arena they do not share (a Julia or Python runtime with its own
+// caching allocator, a solver embedded in a larger application with a fixed
+// memory budget), or code that must run with no allocation at all once it is
+// set up.  ibpm_lap_inv_noalloc serves them: the caller passes the right-hand
+// side and the result buffer; the one intermediate slab of the solve and the
+// transform tables live in file-scope __device__ arrays of fixed size, which
+// every GPU that loads the library holds until the process exits
+// (2.1 MB + 32 KB).
+#include "../../include/ibpm_gpu.h"
+#include "ibpm_internal.cuh"
+
+#include <mutex>
+#include <string>
+
+using namespace ibpm;
+
+namespace {
+
+constexpr int kMaxN = 512;                                         // nx, ny <= 512
+constexpr size_t kSlabDoubles = (size_t)(kMaxN - 1) * kMaxN;       // (ny-1) rows of pitch nx
+constexpr size_t kTableDoubles = 4 * (size_t)kMaxN;                // exp (2N) + sin (N) + cos (N)
+
+__device__ __align__(256) double g_noalloc_slab[kSlabDoubles];
+__device__ __align__(256) double g_noalloc_tables[2 * kTableDoubles];  // x tables, then y tables
+
+struct DeviceScratch {
+    bool ready = false;
+    double* slab = nullptr;    // device address of g_noalloc_slab on this device
+    double* tables = nullptr;  // device address of g_noalloc_tables on this device
+    int nx = 0, ny = 0;        // lengths the tables currently hold
+};
+constexpr int kMaxDevices = 64;
+std::mutex g_mutex;
+DeviceScratch g_scratch[kMaxDevices];
+
+int noalloc_fail(int code, const std::string& msg) {
+    set_global_error(msg.c_str());
+    return code;
+}
+
+DstPlan plan_at(double* tables, int N) {
+    DstPlan p;
+    p.N = N;
+    p.W = reinterpret_cast<double2*>(tables);
+    p.s = tables + 2 * N;
+    p.c = tables + 3 * N;
+    return p;
+}
+
+}  // namespace
+
+extern "C" int ibpm_lap_inv_noalloc(int32_t nx, int32_t ny, const double* rhs, double* x, void* stream) {
+    if (!rhs || !x) return noalloc_fail(IBPM_ERR_INVALID, "ibpm_lap_inv_noalloc: null buffer");
+    if (nx > kMaxN || ny > kMaxN)
+        return noalloc_fail(IBPM_ERR_INVALID, "ibpm_lap_inv_noalloc: nx and ny must be at most 512 (got " +
+                                                  std::to_string(nx) + " x " + std::to_string(ny) + ")");
+    if (!dst_supported(nx) || !dst_supported(ny))
+        return noalloc_fail(IBPM_ERR_UNSUPPORTED,
+                            "ibpm_lap_inv_noalloc: nx and ny must be one of 32, 64, 128, 192, 200, 256, 384, "
+                            "400, 512");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_fail(IBPM_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(IBPM_ERR_INVALID, "device ordinal out of range");
+
+    std::lock_guard<std::mutex> lock(g_mutex);
+    DeviceScratch& ds = g_scratch[dev];
+    if (!ds.ready) {
+        // Once per device, with that device current: the host-side names of
+        // the __device__ arrays are not device addresses, so ask the runtime.
+        e = cudaGetSymbolAddress(reinterpret_cast<void**>(&ds.slab), g_noalloc_slab);
+        if (e != cudaSuccess)
+            return noalloc_fail(IBPM_ERR_CUDA, std::string("cudaGetSymbolAddress(slab): ") + cudaGetErrorString(e));
+        e = cudaGetSymbolAddress(reinterpret_cast<void**>(&ds.tables), g_noalloc_tables);
+        if (e != cudaSuccess)
+            return noalloc_fail(IBPM_ERR_CUDA, std::string("cudaGetSymbolAddress(tables): ") + cudaGetErrorString(e));
+        for (int N : {32, 64, 128, 192, 200, 256, 384, 400, 512}) {
+            e = dst_init_attributes(N);
+            if (e != cudaSuccess)
+                return noalloc_fail(IBPM_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(e));
+        }
+        ds.ready = true;
+    }
+    double* tx = ds.tables;
+    double* ty = ds.tables + kTableDoubles;
+    if (ds.nx != nx) {
+        e = dst_tables_build(nx, reinterpret_cast<double2*>(tx), tx + 2 * nx, tx + 3 * nx, st);
+        if (e != cudaSuccess) return noalloc_fail(IBPM_ERR_CUDA, std::string("tables: ") + cudaGetErrorString(e));
+        ds.nx = nx;
+    }
+    if (ds.ny != ny) {
+        e = dst_tables_build(ny, reinterpret_cast<double2*>(ty), ty + 2 * ny, ty + 3 * ny, st);
+        if (e != cudaSuccess) return noalloc_fail(IBPM_ERR_CUDA, std::string("tables: ") + cudaGetErrorString(e));
+        ds.ny = ny;
+    }
+    const Geom g = make_geom(nx, ny, 1);
+    const DstPlan px = plan_at(tx, nx), py = plan_at(ty, ny);
+    // Every slab element that the transforms read (columns < nx-1) is written
+    // by this copy, so nothing left by an earlier call is read.
+    const size_t row = sizeof(double) * g.n1;
+    e = cudaMemcpy2DAsync(ds.slab, sizeof(double) * g.P, rhs, row, row, g.n2, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return noalloc_fail(IBPM_ERR_CUDA, std::string("copy in: ") + cudaGetErrorString(e));
+    SlabMap m;
+    m.nlev = 1; m.lev0 = 0; m.lstride = g.S; m.bstride = g.S;
+    XPassArgs a{};
+    a.in = ds.slab; a.out = ds.slab; a.in_map = m; a.out_map = m;
+    a.nslabs = 1; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_PLAIN; a.emit = XEMIT_STORE;
+    SpecParams sp{};
+    sp.mode = SPEC_DELTA;
+    sp.scale = 1.0 / (4.0 * nx * ny);  // laplacian.jl:194
+    if ((e = launch_dst_x(g, px, a, st)) != cudaSuccess ||
+        (e = launch_dst_y_solve(g, py, px, ds.slab, m, 1, sp, st)) != cudaSuccess ||
+        (e = launch_dst_x(g, px, a, st)) != cudaSuccess)
+        return noalloc_fail(IBPM_ERR_CUDA, std::string("solve: ") + cudaGetErrorString(e));
+    e = cudaMemcpy2DAsync(x, row, ds.slab, sizeof(double) * g.P, row, g.n2, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return noalloc_fail(IBPM_ERR_CUDA, std::string("copy out: ") + cudaGetErrorString(e));
+    return IBPM_OK;
+}

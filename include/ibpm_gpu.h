@@ -126,6 +126,26 @@ int ibpm_get_binv(ibpm_handle* h, double* Binv);
 /* Block until all work queued on the handle's stream is done. */
 int ibpm_sync(ibpm_handle* h);
 
+/*
+ * x = Δ⁻¹ rhs on one (nx-1)×(ny-1) field with zero Dirichlet edges — the
+ * operator the reference applies on every level of vort2flux!
+ * (src/fluid-operators/laplacian.jl:180-197) — without allocating any device
+ * memory.  No counterpart in the reference: it is for callers that cannot call
+ * cudaMalloc (a host runtime that owns the device memory through its own pool,
+ * an application with a fixed memory budget).  rhs and x are device pointers
+ * in the reference layout (column-major, no padding); the work is queued on
+ * `stream` (a cudaStream_t, or NULL for the legacy default stream) and the call
+ * returns without waiting for it.  Limit: nx, ny <= 512 and in the supported
+ * transform lengths; larger sizes return IBPM_ERR_INVALID.  The intermediate
+ * slab and transform tables are file-scope device arrays (2.1 MB + 32 KB on
+ * every GPU that loads the library, held until exit), shared by all calls:
+ * calls that overlap on the GPU (other streams, other threads) race on them.
+ * The first call on a device looks up their device addresses and sets kernel
+ * attributes; make that first call before any stream capture.  Errors are
+ * reported by ibpm_last_error(NULL).
+ */
+int ibpm_lap_inv_noalloc(int32_t nx, int32_t ny, const double* rhs, double* x, void* stream);
+
 /* Page-locked host memory for state mirrors (faster get/set_state); NULL on
  * failure.  No counterpart in the reference (Julia arrays are pageable). */
 void* ibpm_host_alloc(int64_t bytes);
