@@ -41,6 +41,8 @@ __device__ double delta_h(double rf, double rb, double dr) {
 // w[kk][l][m], kk = comp·nb + k: weight of flux point (bidx + l − 6, bidx + m − 6)
 // for body point k (interface-coupling.jl:89-96).
 __global__ void weights_kernel(BodyDev b, double h, double offx, double offy) {
+    pdl_wait();
+    pdl_trigger();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= b.nf * 169) return;
     const int kk = t / 169, lm = t % 169, l = lm / 13, m = lm % 13;
@@ -71,6 +73,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 // component and batch member.  F[bt*F_bstride + kk*F_kstride].
 __global__ void E_kernel(BodyDev b, Geom g, const double* __restrict__ q, long long q_stride, int nbatch,
                          double q0x, double q0y, double* F, long long F_bstride, long long F_kstride) {
+    pdl_wait();
+    pdl_trigger();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= b.nf * nbatch) return;
@@ -100,12 +104,13 @@ cudaError_t launch_E(const Geom& g, const BodyDev& b, const double* q, long long
     const long long ks = F_stride > 0 ? 1 : -F_stride;
     const long long warps = (long long)b.nf * nbatch;
     const int blocks = (int)((warps * 32 + 255) / 256);
-    E_kernel<<<blocks, 256, 0, st>>>(b, g, q, q_stride, nbatch, q0x, q0y, F, bs, ks);
-    return cudaGetLastError();
+    return launch_k(E_kernel, dim3(blocks), dim3(256), 0, st, b, g, q, q_stride, nbatch, q0x, q0y, F, bs, ks);
 }
 
 // y = A x, A row-major n×n: one warp per row (F̃b .= Binv*F̃b, timestepping.jl:160).
 __global__ void gemv_kernel(const double* __restrict__ A, const double* __restrict__ x, double* y, int n) {
+    pdl_wait();
+    pdl_trigger();
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
@@ -117,8 +122,7 @@ __global__ void gemv_kernel(const double* __restrict__ A, const double* __restri
 }
 
 cudaError_t launch_gemv(const double* A, const double* x, double* y, int n, cudaStream_t st) {
-    gemv_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(A, x, y, n);
-    return cudaGetLastError();
+    return launch_k(gemv_kernel, dim3((n * 32 + 255) / 256), dim3(256), 0, st, A, x, y, n);
 }
 
 // update_stress! (timestepping.jl:330-354): fb = F̃b (h/dt) ./ ds,
@@ -126,6 +130,8 @@ cudaError_t launch_gemv(const double* A, const double* x, double* y, int n, cuda
 // One block; a non-finite CD/CL sets bit 0 of *status.
 __global__ void stress_kernel(BodyDev b, const double* __restrict__ Fb, double h, double dt, double* hist,
                               int* counter, int* status) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double red[2][256];
     const int step = *counter;
     const double hdt = h / dt;
@@ -160,8 +166,7 @@ __global__ void stress_kernel(BodyDev b, const double* __restrict__ Fb, double h
 
 cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double dt, double* hist, int* counter,
                           int* status, cudaStream_t st) {
-    stress_kernel<<<1, 256, 0, st>>>(b, Fb, h, dt, hist, counter, status);
-    return cudaGetLastError();
+    return launch_k(stress_kernel, dim3(1), dim3(256), 0, st, b, Fb, h, dt, hist, counter, status);
 }
 
 // Γsrc = C'(E' F̃b) at the Γ points whose rot! stencil touches a regularised
@@ -169,6 +174,8 @@ cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double d
 // sum over its sorted contributor list (ascending force component, the order
 // reg! accumulates in, interface-coupling.jl:103-107).
 __global__ void proj_src_kernel(BodyDev b, const double* __restrict__ Fb, double* Gsrc) {
+    pdl_wait();
+    pdl_trigger();
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= b.n_src) return;
     double v[4];
@@ -186,14 +193,15 @@ __global__ void proj_src_kernel(BodyDev b, const double* __restrict__ Fb, double
 
 cudaError_t launch_proj_src(const Geom& g, const BodyDev& b, const double* Fb, double* Gsrc, cudaStream_t st) {
     if (b.n_src == 0) return cudaSuccess;
-    proj_src_kernel<<<(b.n_src + 127) / 128, 128, 0, st>>>(b, Fb, Gsrc);
-    return cudaGetLastError();
+    return launch_k(proj_src_kernel, dim3((b.n_src + 127) / 128), dim3(128), 0, st, b, Fb, Gsrc);
 }
 
 // C'E' e_kk for unit forces kk = col0 + r (B_times!, laplacian.jl:318), written
 // into the level-1 slab of batch member r (slab zeroed beforehand).  One thread
 // per point of the 14×14 box of Γ points the 13×13 flux window can reach.
 __global__ void unit_src_kernel(BodyDev b, Geom g, int col0, int ncol, double* G, long long bstride) {
+    pdl_wait();
+    pdl_trigger();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ncol * 196) return;
     const int r = t / 196, ab = t % 196, da = ab / 14, db = ab % 14;

@@ -1,46 +1,58 @@
 // Transform tables and length dispatch of the batched DST-I kernels
 // (kernels: dst_kernels.cuh, one instantiation unit per length: dst_n<N>.cu).
-#include "ibpm_internal.cuh"
+#include "dst_kernels.cuh"
 
 #include <math.h>
 
 namespace ibpm {
 
 cudaError_t dst_x_32(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_32(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_32(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_32();
 cudaError_t dst_x_64(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_64(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_64(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_64();
 cudaError_t dst_x_128(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_128(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_128(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_128();
 cudaError_t dst_x_192(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_192(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_192(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_192();
 cudaError_t dst_x_200(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_200(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_200(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_200();
 cudaError_t dst_x_256(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_256(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_256(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_256();
 cudaError_t dst_x_384(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_384(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_384(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_384();
 cudaError_t dst_x_400(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_400(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_400(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_400();
 cudaError_t dst_x_512(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_512(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_512(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_512();
 cudaError_t dst_x_768(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_768(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_768(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_768();
 cudaError_t dst_x_1024(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_1024(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_1024(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_1024();
 cudaError_t dst_x_2048(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_2048(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_2048(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
+                     const RankFour&, cudaStream_t);
 cudaError_t dst_attr_2048();
 
 // Supported transform lengths N = nx or ny: 32, 64, 128, 192, 200, 256, 384, 400, 512, 768, 1024, 2048.
@@ -64,40 +76,77 @@ bool dst_supported(int N) {
     }
 }
 
-__global__ void dst_tables_kernel(int N, double2* W, double* s, double* c) {
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
-        double sn, cs;
-        sincospi(2.0 * (double)t / (double)N, &sn, &cs);
-        W[t] = make_double2(cs, sn);            // exp(+2πi t/N)
-        s[t] = sinpi((double)t / (double)N);    // sin(π t/N)
-        // cos(π (t+1)/N), evaluated as the reference forms the Laplacian
-        // eigenvalues: cos.(π*(1:(n-1))/n) (laplacian.jl:173)
-        if (t < N - 1) c[t] = cos(M_PI * (double)(t + 1) / (double)N);
+// Stage layout of the length-N FFT, for the twiddle table kernel.
+struct StageDesc {
+    int n;
+    int ns[8], r[8], off[8];
+};
+
+static StageDesc stage_desc(int N) {
+    StageDesc d{};
+    const int S = dstk::ct_nstages(N);
+    for (int s = 0; s < S; ++s) {
+        d.ns[d.n] = dstk::ct_stage_ns(N, s);
+        d.r[d.n] = dstk::ct_radix(N, s);
+        d.off[d.n] = dstk::ct_tw_off(N, s);
+        if (d.ns[d.n] > 1) ++d.n;
     }
+    return d;
+}
+
+// Table block of 4N doubles: cos(π(t+1)/N) at [0, N), sin(πt/N) at [N, 2N),
+// stage twiddles exp(+2πi k r/(Ns R)) (complex) from 2N on.
+__global__ void dst_tables_kernel(int N, double* base, StageDesc d, int ntw) {
+    double* c = base;
+    double* s = base + N;
+    double2* W = reinterpret_cast<double2*>(base + 2 * N);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
+        s[t] = sinpi((double)t / (double)N);
+        // evaluated as the reference forms the Laplacian eigenvalues:
+        // cos.(π*(1:(n-1))/n) (laplacian.jl:173)
+        c[t] = (t < N - 1) ? cos(M_PI * (double)(t + 1) / (double)N) : 0.0;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntw; i += gridDim.x * blockDim.x) {
+        int st = 0;
+        while (st + 1 < d.n && i >= d.off[st + 1]) ++st;
+        const int j = i - d.off[st];
+        const int r = j / d.ns[st] + 1, k = j % d.ns[st];
+        double sn, cs;
+        sincospi(2.0 * (double)(k * r) / (double)(d.ns[st] * d.r[st]), &sn, &cs);
+        W[i] = make_double2(cs, sn);
+    }
+}
+
+cudaError_t dst_tables_build(int N, double* base, cudaStream_t st) {
+    const StageDesc d = stage_desc(N);
+    const int ntw = dstk::ct_tw_count(N);
+    dst_tables_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, base, d, ntw);
+    return cudaGetLastError();
+}
+
+DstPlan dst_plan_at(double* base, int N) {
+    DstPlan p;
+    p.N = N;
+    p.c = base;
+    p.s = base + N;
+    p.W = reinterpret_cast<double2*>(base + 2 * N);
+    return p;
 }
 
 int dst_plan_create(DstPlan* p, int N, cudaStream_t st) {
     p->N = N;
     p->W = nullptr; p->s = nullptr; p->c = nullptr;
     if (!dst_supported(N)) return -1;
-    if (cudaMalloc(&p->W, sizeof(double2) * N) != cudaSuccess) return -2;
-    if (cudaMalloc(&p->s, sizeof(double) * N) != cudaSuccess) return -2;
-    if (cudaMalloc(&p->c, sizeof(double) * N) != cudaSuccess) return -2;
-    dst_tables_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, p->W, p->s, p->c);
-    if (cudaGetLastError() != cudaSuccess) return -2;
+    double* base = nullptr;
+    if (cudaMalloc(&base, sizeof(double) * 4 * N) != cudaSuccess) return -2;
+    *p = dst_plan_at(base, N);
+    if (dst_tables_build(N, base, st) != cudaSuccess) return -2;
     if (dst_init_attributes(N) != cudaSuccess) return -2;
     return 0;
 }
 
-cudaError_t dst_tables_build(int N, double2* W, double* s, double* c, cudaStream_t st) {
-    dst_tables_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, W, s, c);
-    return cudaGetLastError();
-}
-
 void dst_plan_destroy(DstPlan* p) {
-    if (p->W) cudaFree(p->W);
-    if (p->s) cudaFree(p->s);
-    if (p->c) cudaFree(p->c);
+    if (p->c) cudaFree(p->c);  // the block starts at c
     p->W = nullptr; p->s = nullptr; p->c = nullptr;
 }
 
@@ -139,22 +188,22 @@ cudaError_t launch_dst_x(const Geom& g, const DstPlan& px, const XPassArgs& a, c
     }
 }
 
-cudaError_t launch_dst_y_solve(const Geom& g, const DstPlan& py, const DstPlan& px, double* data, SlabMap map,
-                               int nslabs, const SpecParams& sp, cudaStream_t st) {
+cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px, double* data, SlabMap map, int nslabs,
+                         const SpecParams& sp, int mode, const RankFour& r4, cudaStream_t st) {
     if (nslabs <= 0) return cudaSuccess;
     switch (py.N) {
-        case 32: return dst_y_32(g, py, px, data, map, nslabs, sp, st);
-        case 64: return dst_y_64(g, py, px, data, map, nslabs, sp, st);
-        case 128: return dst_y_128(g, py, px, data, map, nslabs, sp, st);
-        case 192: return dst_y_192(g, py, px, data, map, nslabs, sp, st);
-        case 200: return dst_y_200(g, py, px, data, map, nslabs, sp, st);
-        case 256: return dst_y_256(g, py, px, data, map, nslabs, sp, st);
-        case 384: return dst_y_384(g, py, px, data, map, nslabs, sp, st);
-        case 400: return dst_y_400(g, py, px, data, map, nslabs, sp, st);
-        case 512: return dst_y_512(g, py, px, data, map, nslabs, sp, st);
-        case 768: return dst_y_768(g, py, px, data, map, nslabs, sp, st);
-        case 1024: return dst_y_1024(g, py, px, data, map, nslabs, sp, st);
-        case 2048: return dst_y_2048(g, py, px, data, map, nslabs, sp, st);
+        case 32: return dst_y_32(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 64: return dst_y_64(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 128: return dst_y_128(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 192: return dst_y_192(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 200: return dst_y_200(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 256: return dst_y_256(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 384: return dst_y_384(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 400: return dst_y_400(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 512: return dst_y_512(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 768: return dst_y_768(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 1024: return dst_y_1024(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 2048: return dst_y_2048(g, py, px, data, map, nslabs, sp, mode, r4, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -53,6 +53,26 @@ __host__ __device__ constexpr int ct_tp(int N) {
 __host__ __device__ constexpr int ct_pad(int i) { return i + (i >> 3); }
 __host__ __device__ constexpr int ct_buf(int N) { return ct_pad(N) + 8; }  // + scan scratch
 
+// Twiddles of stage S (sub-transform length Ns before it, radix R) are stored
+// contiguously as T[(r-1)·Ns + k] = exp(+2πi k r/(Ns R)), r = 1…R-1, k < Ns, so
+// the threads of a stage (consecutive k) read consecutive entries.
+__host__ __device__ constexpr int ct_stage_ns(int N, int S) {
+    int ns = 1;
+    for (int s = 0; s < S; ++s) ns *= ct_radix(N, s);
+    return ns;
+}
+__host__ __device__ constexpr int ct_tw_off(int N, int S) {
+    int off = 0;
+    for (int s = 0; s < S; ++s) {
+        const int ns = ct_stage_ns(N, s);
+        if (ns > 1) off += (ct_radix(N, s) - 1) * ns;
+    }
+    return off;
+}
+__host__ __device__ constexpr int ct_tw_count(int N) { return ct_tw_off(N, ct_nstages(N)); }
+// Groups (line pairs) per CTA: 128-thread CTAs for N <= 1024.
+__host__ __device__ constexpr int ct_groups(int N) { return ct_tp(N) >= 128 ? 1 : 128 / ct_tp(N); }
+
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -135,12 +155,11 @@ template <int TP> __device__ __forceinline__ void gsync(int gid) {
     }
 }
 
-template <int N, int TP, int R, int Ns>
-__device__ __forceinline__ void fft_stage(double2* buf, const double2* __restrict__ W, int tid, int gid) {
+template <int N, int TP, int R, int Ns, int TWOFF>
+__device__ __forceinline__ void fft_stage(double2* buf, const double2* W, int tid, int gid) {
     constexpr int nb = N / R;
     constexpr int QM = (nb + TP - 1) / TP;
     constexpr bool exact = (QM * TP == nb);
-    constexpr int ts = N / (Ns * R);
     double2 v[QM][R];
 #pragma unroll
     for (int q = 0; q < QM; ++q) {
@@ -158,7 +177,7 @@ __device__ __forceinline__ void fft_stage(double2* buf, const double2* __restric
             const int k = b % Ns;
             if constexpr (Ns > 1) {
 #pragma unroll
-                for (int r = 1; r < R; ++r) v[q][r] = cmul(v[q][r], __ldg(&W[k * r * ts]));
+                for (int r = 1; r < R; ++r) v[q][r] = cmul(v[q][r], W[TWOFF + (r - 1) * Ns + k]);
             }
             dft<R>(v[q]);
             const int base = (b - k) * R + k;
@@ -170,34 +189,42 @@ __device__ __forceinline__ void fft_stage(double2* buf, const double2* __restric
 }
 
 template <int N, int TP, int S, int Ns>
-__device__ __forceinline__ void fft_stages(double2* buf, const double2* __restrict__ W, int tid, int gid) {
+__device__ __forceinline__ void fft_stages(double2* buf, const double2* W, int tid, int gid) {
     if constexpr (S < ct_nstages(N)) {
         constexpr int R = ct_radix(N, S);
-        fft_stage<N, TP, R, Ns>(buf, W, tid, gid);
+        fft_stage<N, TP, R, Ns, ct_tw_off(N, S)>(buf, W, tid, gid);
         fft_stages<N, TP, S + 1, Ns * R>(buf, W, tid, gid);
     }
 }
 
 // Pre-processing: buf[m] = y_m from load(m-1) = (a_{m-1}, b_{m-1}).
 template <int N, int TP, class Load>
-__device__ __forceinline__ void dst_pre(double2* buf, const double* __restrict__ s, int tid, Load load) {
+__device__ __forceinline__ void dst_pre(double2* buf, const double* s, int tid, Load load) {
     constexpr int half = N >> 1;
-    for (int m = tid; m <= half; m += TP) {
+    constexpr int IT = (half + TP) / TP;  // m = tid + it·TP covers 0 … half
+    double2 fm[IT], fn[IT];
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {  // issue every load before using any
+        const int m = tid + it * TP;
+        if (m >= 1 && m <= half) {
+            fm[it] = load(m - 1);
+            if (m < half) fn[it] = load(N - m - 1);
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int m = tid + it * TP;
         if (m == 0) {
             buf[0] = make_double2(0.0, 0.0);
-            continue;
+        } else if (m == half) {  // sin(π/2) = 1
+            buf[ct_pad(m)] = make_double2(2.0 * fm[it].x, 2.0 * fm[it].y);
+        } else if (m < half) {
+            const double sm = s[m];
+            const double2 sum = cadd(fm[it], fn[it]), dif = csub(fm[it], fn[it]);
+            const double2 ys = make_double2(sm * sum.x, sm * sum.y);
+            buf[ct_pad(m)] = make_double2(ys.x + 0.5 * dif.x, ys.y + 0.5 * dif.y);
+            buf[ct_pad(N - m)] = make_double2(ys.x - 0.5 * dif.x, ys.y - 0.5 * dif.y);
         }
-        const double2 fm = load(m - 1);
-        if (m == half) {  // sin(π/2) = 1
-            buf[ct_pad(m)] = make_double2(2.0 * fm.x, 2.0 * fm.y);
-            continue;
-        }
-        const double2 fn = load(N - m - 1);
-        const double sm = __ldg(&s[m]);
-        const double2 sum = cadd(fm, fn), dif = csub(fm, fn);
-        const double2 ys = make_double2(sm * sum.x, sm * sum.y);
-        buf[ct_pad(m)] = make_double2(ys.x + 0.5 * dif.x, ys.y + 0.5 * dif.y);
-        buf[ct_pad(N - m)] = make_double2(ys.x - 0.5 * dif.x, ys.y - 0.5 * dif.y);
     }
 }
 
@@ -270,25 +297,44 @@ __device__ __forceinline__ void dst_post(double2* buf, int tid, int gid, double2
 
 // One DST-I of a line pair: load → pre → FFT → post → emit.
 template <int N, int TP, class Load, class Emit>
-__device__ __forceinline__ void dst_pair(double2* buf, const double2* __restrict__ W, const double* __restrict__ s,
-                                         int tid, int gid, Load load, Emit emit) {
+__device__ __forceinline__ void dst_pair(double2* buf, const double2* W, const double* s, int tid, int gid, Load load,
+                                         Emit emit) {
     dst_pre<N, TP>(buf, s, tid, load);
     gsync<TP>(gid);
     fft_stages<N, TP, 0, 1>(buf, W, tid, gid);
     dst_post<N, TP>(buf, tid, gid, buf + ct_pad(N), emit);
 }
 
+// Copy the transform tables into shared memory: stage twiddles (complex),
+// then sin(πm/N) for m ≤ N/2.
+template <int N>
+__device__ __forceinline__ void stage_tables(double2* tw, double* sn, const DstPlan& p) {
+    for (int i = threadIdx.x; i < ct_tw_count(N); i += blockDim.x) cp_async16(tw + i, p.W + i);
+    for (int i = threadIdx.x; i <= N / 2; i += blockDim.x) cp_async8(sn + i, p.s + i);
+}
+template <int N>
+__host__ __device__ constexpr size_t tables_bytes() {
+    return (size_t)ct_tw_count(N) * sizeof(double2) + (size_t)((N / 2 + 2) & ~1) * sizeof(double);
+}
+
 // ---------------------------------------------------------------------------
 // x-pass: lines are rows of a slab (contiguous).  One group per line pair.
 // ---------------------------------------------------------------------------
 template <int N, int LOAD, int EMIT>
-__global__ void __launch_bounds__(256) dst_x_kernel(XPassArgs a, Geom g, const double2* __restrict__ W,
-                                                    const double* __restrict__ s) {
+__global__ void __launch_bounds__(256) dst_x_kernel(XPassArgs a, Geom g, DstPlan p) {
     constexpr int TP = ct_tp(N);
-    constexpr int G = 256 / TP;
+    constexpr int G = ct_groups(N);
     extern __shared__ double2 smem2[];
+    double2* tw = smem2;
+    double* sn = reinterpret_cast<double*>(smem2 + ct_tw_count(N));
+    double2* bufs = reinterpret_cast<double2*>(reinterpret_cast<char*>(smem2) + tables_bytes<N>());
+    stage_tables<N>(tw, sn, p);  // constant tables: before the dependency wait
+    cp_async_wait();
+    __syncthreads();
+    pdl_wait();
+    pdl_trigger();
     const int gid = threadIdx.x / TP, tid = threadIdx.x % TP;
-    double2* buf = smem2 + gid * ct_buf(N);
+    double2* buf = bufs + gid * ct_buf(N);
     const int la = a.line0 + 2 * (blockIdx.x * G + gid);
     if (la >= a.line1) return;  // the whole group leaves together
     const bool hasb = (la + 1) < a.line1;
@@ -319,7 +365,7 @@ __global__ void __launch_bounds__(256) dst_x_kernel(XPassArgs a, Geom g, const d
         }
         return make_double2(va, vb);
     };
-    dst_pair<N, TP>(buf, W, s, tid, gid, load, [&](int o, double2 v) { buf[ct_pad(o)] = v; });
+    dst_pair<N, TP>(buf, tw, sn, tid, gid, load, [&](int o, double2 v) { buf[ct_pad(o)] = v; });
     gsync<TP>(gid);
     double* oa = a.out + a.out_map.off(y) + (long long)la * P;
     double* ob = oa + P;
@@ -336,74 +382,116 @@ __global__ void __launch_bounds__(256) dst_x_kernel(XPassArgs a, Geom g, const d
 }
 
 // ---------------------------------------------------------------------------
-// y-pass of a Poisson solve: DST-I along y, spectral divide, DST-I along y,
-// in place on a tile of TW = 2G columns (all rows) staged in shared memory.
+// y-pass on a tile of TW = 2G columns (all rows) staged in shared memory, in
+// place.  YMODE_SOLVE: DST-I, spectral divide, DST-I (the middle of a
+// Poisson-type solve).  YMODE_FWD: one DST-I.  YMODE_INV: add the rank-4
+// spectral image of the edge terms, divide by Λ, scale, one DST-I.
 // ---------------------------------------------------------------------------
 template <int N>
-__host__ __device__ constexpr int y_tile_w() { return 2 * (256 / ct_tp(N)); }
+__host__ __device__ constexpr int y_groups() { return ct_groups(N); }
+template <int N>
+__host__ __device__ constexpr int y_tile_w() { return 2 * y_groups<N>(); }
 template <int N>
 __host__ __device__ constexpr size_t y_smem_bytes(int n2) {
-    return (size_t)(((n2 * (y_tile_w<N>() + 1) + 1) / 2) * 2) * sizeof(double) +
-           (size_t)(256 / ct_tp(N)) * ct_buf(N) * sizeof(double2);
+    return tables_bytes<N>() + (size_t)(((n2 + 1) / 2) * 2) * sizeof(double) +  // cos(π(j+1)/ny)
+           (size_t)(((n2 * (y_tile_w<N>() + 1) + 1) / 2) * 2) * sizeof(double) +
+           (size_t)y_groups<N>() * ct_buf(N) * sizeof(double2);
 }
 
-template <int N>
-__global__ void __launch_bounds__(256) dst_y_solve_kernel(double* data, SlabMap map, Geom g,
-                                                          const double2* __restrict__ W, const double* __restrict__ s,
-                                                          const double* __restrict__ cy,
-                                                          const double* __restrict__ cx, SpecParams sp) {
+template <int N, int MODE>
+__global__ void __launch_bounds__(256) dst_y_kernel(double* data, SlabMap map, Geom g, DstPlan p,
+                                                    const double* __restrict__ cx, SpecParams sp, RankFour r4) {
     constexpr int TP = ct_tp(N);
     constexpr int TW = y_tile_w<N>();
     constexpr int TWp = TW + 1;
-    extern __shared__ double smemd[];
-    const int gid = threadIdx.x / TP, tid = threadIdx.x % TP;
+    extern __shared__ double2 smem2[];
     const int P = g.P, n1 = g.n1, n2 = g.n2;
-    double* tile = smemd;
+    double2* tw = smem2;
+    double* sn = reinterpret_cast<double*>(smem2 + ct_tw_count(N));
+    double* cyv = reinterpret_cast<double*>(reinterpret_cast<char*>(smem2) + tables_bytes<N>());
+    double* tile = cyv + ((n2 + 1) / 2) * 2;
     const int tile_d = ((n2 * TWp + 1) / 2) * 2;
-    double2* buf = reinterpret_cast<double2*>(smemd + tile_d) + gid * ct_buf(N);
+    const int gid = threadIdx.x / TP, tid = threadIdx.x % TP;
+    double2* buf = reinterpret_cast<double2*>(tile + tile_d) + gid * ct_buf(N);
     const int i0 = blockIdx.x * TW;
     double* base = data + map.off(blockIdx.y);
     const int lev = map.level(blockIdx.y);
+    const int bt = map.batch(blockIdx.y);
 
+    stage_tables<N>(tw, sn, p);  // constant tables: before the dependency wait
+    for (int j = threadIdx.x; j < n2; j += blockDim.x) cp_async8(cyv + j, p.c + j);
+    pdl_wait();
+    pdl_trigger();
     for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
         const int j = idx / TW, c = idx - j * TW;
         const int i = i0 + c;
-        tile[j * TWp + c] = (i < n1) ? base[(long long)j * P + i] : 0.0;
+        if (i < n1) cp_async8(tile + j * TWp + c, base + (long long)j * P + i);
+        else tile[j * TWp + c] = 0.0;
     }
+    cp_async_wait();
     __syncthreads();
 
     const int ca = 2 * gid;
     const int ia = i0 + ca;
     if (ia < n1) {
+        const bool hasb = ia + 1 < n1;
         auto load = [&](int m) -> double2 { return make_double2(tile[m * TWp + ca], tile[m * TWp + ca + 1]); };
         auto emit = [&](int o, double2 v) {
             tile[o * TWp + ca] = v.x;
             tile[o * TWp + ca + 1] = v.y;
         };
-        dst_pair<N, TP>(buf, W, s, tid, gid, load, emit);
-        gsync<TP>(gid);
         // w ./= M ; w .*= scale  with Λ = -2 (cos(π i/nx) + cos(π j/ny) - 2)
-        const bool hasb = ia + 1 < n1;
-        const double cxa = __ldg(&cx[ia]);
-        const double cxb = hasb ? __ldg(&cx[ia + 1]) : 0.0;
-        const double den = sp.den[lev];
-        for (int o = tid; o < n2; o += TP) {
-            const double c2 = __ldg(&cy[o]);
-            const double la = -2.0 * ((cxa + c2) - 2.0);
-            const double lb = -2.0 * ((cxb + c2) - 2.0);
-            double Ma, Mb;
-            if (sp.mode == SPEC_DELTA) {
-                Ma = la;
-                Mb = lb;
-            } else {
-                Ma = 1.0 + la * sp.dt / den;
-                Mb = 1.0 + lb * sp.dt / den;
+        auto divide = [&](bool add_r4) {
+            const double cxa = __ldg(&cx[ia]);
+            const double cxb = hasb ? __ldg(&cx[ia + 1]) : 0.0;
+            const double den = sp.den[lev];
+            const double* rv = add_r4 ? r4.v + (long long)(bt * r4.mg + lev) * 4 * r4.len : nullptr;
+            double bxa = 0, txa = 0, bxb = 0, txb = 0, s0a = 0, sNa = 0, s0b = 0, sNb = 0;
+            if (rv) {
+                bxa = rv[ia]; txa = rv[r4.len + ia];
+                s0a = __ldg(&r4.sx0[ia]); sNa = __ldg(&r4.sxN[ia]);
+                if (hasb) {
+                    bxb = rv[ia + 1]; txb = rv[r4.len + ia + 1];
+                    s0b = __ldg(&r4.sx0[ia + 1]); sNb = __ldg(&r4.sxN[ia + 1]);
+                }
             }
-            tile[o * TWp + ca] = (tile[o * TWp + ca] / Ma) * sp.scale;
-            tile[o * TWp + ca + 1] = hasb ? (tile[o * TWp + ca + 1] / Mb) * sp.scale : 0.0;
+            for (int o = tid; o < n2; o += TP) {
+                const double c2 = cyv[o];
+                const double la = -2.0 * ((cxa + c2) - 2.0);
+                const double lb = -2.0 * ((cxb + c2) - 2.0);
+                double Ma, Mb;
+                if (sp.mode == SPEC_DELTA) {
+                    Ma = la;
+                    Mb = lb;
+                } else {
+                    Ma = 1.0 + la * sp.dt / den;
+                    Mb = 1.0 + lb * sp.dt / den;
+                }
+                double va = tile[o * TWp + ca], vb = tile[o * TWp + ca + 1];
+                if (rv) {
+                    const double y0 = __ldg(&r4.sy0[o]), yN = __ldg(&r4.syN[o]);
+                    const double lf = rv[2 * r4.len + o], rt = rv[3 * r4.len + o];
+                    va = (((va + bxa * y0) + txa * yN) + s0a * lf) + sNa * rt;
+                    vb = (((vb + bxb * y0) + txb * yN) + s0b * lf) + sNb * rt;
+                }
+                tile[o * TWp + ca] = (va * nr_rcp(Ma)) * sp.scale;
+                tile[o * TWp + ca + 1] = hasb ? (vb * nr_rcp(Mb)) * sp.scale : 0.0;
+            }
+        };
+        if (MODE == YMODE_INV) {
+            divide(true);
+            gsync<TP>(gid);
         }
-        gsync<TP>(gid);
-        dst_pair<N, TP>(buf, W, s, tid, gid, load, emit);
+        constexpr int NPASS = (MODE == YMODE_SOLVE) ? 2 : 1;
+#pragma unroll 1
+        for (int pass = 0; pass < NPASS; ++pass) {
+            dst_pair<N, TP>(buf, tw, sn, tid, gid, load, emit);
+            gsync<TP>(gid);
+            if (MODE == YMODE_SOLVE && pass == 0) {
+                divide(false);
+                gsync<TP>(gid);
+            }
+        }
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
@@ -419,14 +507,13 @@ __global__ void __launch_bounds__(256) dst_y_solve_kernel(double* data, SlabMap 
 template <int N, int LOAD, int EMIT>
 cudaError_t launch_x_n(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {
     constexpr int TP = ct_tp(N);
-    constexpr int G = 256 / TP;
+    constexpr int G = ct_groups(N);
     const int lines = a.line1 - a.line0;
     if (lines <= 0 || a.nslabs <= 0) return cudaSuccess;
     const int pairs = (lines + 1) / 2;
     dim3 grid((pairs + G - 1) / G, a.nslabs);
-    const size_t smem = (size_t)G * ct_buf(N) * sizeof(double2);
-    dst_x_kernel<N, LOAD, EMIT><<<grid, G * TP, smem, st>>>(a, g, px.W, px.s);
-    return cudaGetLastError();
+    const size_t smem = tables_bytes<N>() + (size_t)G * ct_buf(N) * sizeof(double2);
+    return launch_k(dst_x_kernel<N, LOAD, EMIT>, grid, dim3(G * TP), smem, st, a, g, px);
 }
 
 template <int N>
@@ -440,24 +527,38 @@ cudaError_t launch_x_t(const Geom& g, const DstPlan& px, const XPassArgs& a, cud
 
 template <int N>
 cudaError_t launch_y_t(const Geom& g, const DstPlan& py, const DstPlan& px, double* data, SlabMap map, int nslabs,
-                       const SpecParams& sp, cudaStream_t st) {
+                       const SpecParams& sp, int mode, const RankFour& r4, cudaStream_t st) {
     constexpr int TW = y_tile_w<N>();
     const size_t smem = y_smem_bytes<N>(g.n2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     dim3 grid((g.n1 + TW - 1) / TW, nslabs);
-    dst_y_solve_kernel<N><<<grid, 256, smem, st>>>(data, map, g, py.W, py.s, py.c, px.c, sp);
-    return cudaGetLastError();
+    const int threads = y_groups<N>() * ct_tp(N);
+    const double* cx = px.c;
+    if (mode == YMODE_FWD)
+        return launch_k(dst_y_kernel<N, YMODE_FWD>, grid, dim3(threads), smem, st, data, map, g, py, cx, sp, r4);
+    if (mode == YMODE_INV)
+        return launch_k(dst_y_kernel<N, YMODE_INV>, grid, dim3(threads), smem, st, data, map, g, py, cx, sp, r4);
+    return launch_k(dst_y_kernel<N, YMODE_SOLVE>, grid, dim3(threads), smem, st, data, map, g, py, cx, sp, r4);
+}
+
+template <class K>
+cudaError_t smem_attrs(K kernel) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
+    // the largest shared-memory carveout, so that occupancy is not capped by L1
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
 template <int N>
 cudaError_t attr_t() {
-    const int big = 227 * 1024;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(dst_x_kernel<N, XLOAD_PLAIN, XEMIT_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
-    if ((e = cudaFuncSetAttribute(dst_x_kernel<N, XLOAD_PLAIN, XEMIT_SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
-    if ((e = cudaFuncSetAttribute(dst_x_kernel<N, XLOAD_BC, XEMIT_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
-    if ((e = cudaFuncSetAttribute(dst_x_kernel<N, XLOAD_BC, XEMIT_SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
-    return cudaFuncSetAttribute(dst_y_solve_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if ((e = smem_attrs(dst_x_kernel<N, XLOAD_PLAIN, XEMIT_STORE>))) return e;
+    if ((e = smem_attrs(dst_x_kernel<N, XLOAD_PLAIN, XEMIT_SUB>))) return e;
+    if ((e = smem_attrs(dst_x_kernel<N, XLOAD_BC, XEMIT_STORE>))) return e;
+    if ((e = smem_attrs(dst_x_kernel<N, XLOAD_BC, XEMIT_SUB>))) return e;
+    if ((e = smem_attrs(dst_y_kernel<N, YMODE_SOLVE>))) return e;
+    if ((e = smem_attrs(dst_y_kernel<N, YMODE_FWD>))) return e;
+    return smem_attrs(dst_y_kernel<N, YMODE_INV>);
 }
 
 }  // namespace dstk
@@ -469,8 +570,8 @@ cudaError_t attr_t() {
         return dstk::launch_x_t<N>(g, px, a, st);                                                          \
     }                                                                                                      \
     cudaError_t dst_y_##N(const Geom& g, const DstPlan& py, const DstPlan& px, double* d, SlabMap m, int n, \
-                          const SpecParams& sp, cudaStream_t st) {                                         \
-        return dstk::launch_y_t<N>(g, py, px, d, m, n, sp, st);                                            \
+                          const SpecParams& sp, int mode, const RankFour& r4, cudaStream_t st) {           \
+        return dstk::launch_y_t<N>(g, py, px, d, m, n, sp, mode, r4, st);                                  \
     }                                                                                                      \
     cudaError_t dst_attr_##N() { return dstk::attr_t<N>(); }
 

@@ -96,11 +96,63 @@ struct CoarseBC {
 };
 
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch: every kernel of the step is launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization, so it can be scheduled
+// while its predecessor drains.  A kernel may stage constant tables first, but
+// must call pdl_wait() before touching anything an earlier kernel wrote;
+// pdl_trigger() lets the next kernel launch.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Asynchronous global → shared copies (cp.async): all of a thread's copies
+// are in flight together; cp_async_wait() + a barrier makes them visible.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+bool pdl_enabled();
+
+// 1/d by Newton–Raphson: a single-precision seed (relative error ≤ 2^-23),
+// refined twice with r ← r + r(1 − d r), which squares the error each time
+// (2^-46, then below the double rounding).  Within 1-2 ulp of 1/d, with no
+// branches; used where a full IEEE division per element would dominate.
+__device__ __forceinline__ double nr_rcp(double d) {
+    double r = (double)__frcp_rn((float)d);
+    double e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-d, r, 1.0);
+    return fma(r, e, r);
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                     Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
+// ---------------------------------------------------------------------------
 // Host-side launchers (defined in the .cu files).
 // ---------------------------------------------------------------------------
 struct DstPlan {
     int N;               // transform length nx (x-pass) or ny (y-pass) = n + 1
-    double2* W;          // device: exp(+2πi t/N), t < N
+    double2* W;          // device: per-stage FFT twiddles (stage-contiguous, ≤ N entries)
     double* s;           // device: sin(π m/N), m < N
     double* c;           // device: cos(π (k+1)/N), k < N-1 (Laplacian eigenvalues)
 };
@@ -108,8 +160,10 @@ struct DstPlan {
 bool dst_supported(int N);
 int dst_plan_create(DstPlan* p, int N, cudaStream_t st);  // 0 on success
 cudaError_t dst_init_attributes(int N);
-// Fill transform tables of length N into caller-provided device memory.
-cudaError_t dst_tables_build(int N, double2* W, double* s, double* c, cudaStream_t st);
+// Fill the 4N-double table block of length N in caller-provided device memory
+// and view it as a plan.
+cudaError_t dst_tables_build(int N, double* base, cudaStream_t st);
+DstPlan dst_plan_at(double* base, int N);
 // Error text returned by ibpm_last_error(NULL).
 void set_global_error(const char* msg);
 void dst_plan_destroy(DstPlan* p);
@@ -138,11 +192,56 @@ struct XPassArgs {
 };
 cudaError_t launch_dst_x(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st);
 
-// y-direction: DST-I, spectral divide, DST-I (the middle of a Poisson solve),
-// in place on every slab selected by `map`.
-cudaError_t launch_dst_y_solve(const Geom& g, const DstPlan& py, const DstPlan& px_cos,
-                               double* data, SlabMap map, int nslabs,
-                               const SpecParams& sp, cudaStream_t st);
+// y-direction pass, in place on every slab selected by `map`:
+//   YMODE_SOLVE  DST-I, spectral divide, DST-I (the middle of a Poisson solve)
+//   YMODE_FWD    DST-I only
+//   YMODE_INV    add the rank-4 spectral image of edge terms (RankFour), divide,
+//                DST-I
+enum YMode { YMODE_SOLVE = 0, YMODE_FWD = 1, YMODE_INV = 2 };
+// Spectral image S b of an edge-only field b (apply_bc! of edge vectors): for
+// slab (batch, level), v + (batch·mg + level)·4·len holds [Sx bot | Sx top |
+// Sy left | Sy right], each of length len; S b(k, m) = Sx bot(k)·sy0(m) +
+// Sx top(k)·syN(m) + sx0(k)·Sy left(m) + sxN(k)·Sy right(m), with sx0(k) =
+// 2 sin(π(k+1)/nx), sxN(k) = 2 sin(π(nx-1)(k+1)/nx) and likewise in y.
+struct RankFour {
+    const double* v;
+    int mg, len;
+    const double *sx0, *sxN, *sy0, *syN;
+};
+cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px_cos, double* data, SlabMap map,
+                         int nslabs, const SpecParams& sp, int mode, const RankFour& r4, cudaStream_t st);
+inline cudaError_t launch_dst_y_solve(const Geom& g, const DstPlan& py, const DstPlan& px_cos, double* data,
+                                      SlabMap map, int nslabs, const SpecParams& sp, cudaStream_t st) {
+    return launch_dst_y(g, py, px_cos, data, map, nslabs, sp, YMODE_SOLVE, RankFour{}, st);
+}
+
+// Spectral level chain of vort2flux! (ring_kernels.cuh).  Tables, 0-based:
+//   cx[k] = cos(π(k+1)/nx), cy[m] = cos(π(m+1)/ny)
+//   sxl[k] = 2 sin(π (nx/4)(k+1)/nx), sxr[k] = 2 sin(π (3nx/4)(k+1)/nx)
+//   syb[m] = 2 sin(π (ny/4)(m+1)/ny), syt[m] = 2 sin(π (3ny/4)(m+1)/ny)
+//   sx0, sxN, sy0, syN as in RankFour.
+struct RingTabs {
+    const double *cx, *cy, *sxl, *sxr, *syb, *syt, *sx0, *sxN, *sy0, *syN;
+};
+struct RingArgs {
+    const double* T; SlabMap tmap;   // spectra Ĝ of every level (batch-major, nlev = mg)
+    RankFour r4;                     // rank-4 images (read: level lev+1)
+    double* r4w;                     // same buffer (written: level lev)
+    double* part; long long part_bstride;  // per-block partial row sums [band][2][len]
+    double* ucol;                    // [batch][2][len] column sums
+    double* bcw;                     // [batch][mg][nbc] real-space ψbc of each level (written: level lev)
+    int* counter;                    // [batch] blocks finished (reset by the last block)
+    RingTabs tabs;
+    int lev;                         // level whose edge image is produced (reads lev+1)
+    double scale;                    // 1/(4 nx ny)
+};
+bool ring_supported(int nx, int ny);
+cudaError_t ring_init_attributes(int nx, int ny);
+cudaError_t launch_ring(const Geom& g, const DstPlan& px, const DstPlan& py, const RingArgs& a, int nbatch,
+                        cudaStream_t st);
+int ring_nbands(const Geom& g);
+// Fill the sine tables of RingTabs (8 arrays of `len` doubles from base).
+cudaError_t ring_tables_build(const Geom& g, int len, double* base, cudaStream_t st);
 
 // Stencil kernels (stencil.cu)
 struct RhsArgs {
@@ -166,6 +265,7 @@ cudaError_t launch_coarsify(const Geom& g, double* G, SlabMap fine_map, SlabMap 
 struct CurlArgs {
     const double* psi; SlabMap psi_map;
     const double* coarse; SlabMap coarse_map;  // coarser level ψ, or nullptr
+    const double* bcv;                         // or: ψbc vectors [batch][mg][nbc] (used when non-null)
     double* q; long long q_bstride, q_lstride; int q_lev0;
     int nlev;                                  // levels in this launch
     int nbatch;

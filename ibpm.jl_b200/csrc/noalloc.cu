@@ -21,7 +21,7 @@ namespace {
 
 constexpr int kMaxN = 512;                                         // nx, ny <= 512
 constexpr size_t kSlabDoubles = (size_t)(kMaxN - 1) * kMaxN;       // (ny-1) rows of pitch nx
-constexpr size_t kTableDoubles = 4 * (size_t)kMaxN;                // exp (2N) + sin (N) + cos (N)
+constexpr size_t kTableDoubles = 4 * (size_t)kMaxN;                // cos (N) + sin (N) + twiddles (<= 2N)
 
 __device__ __align__(256) double g_noalloc_slab[kSlabDoubles];
 __device__ __align__(256) double g_noalloc_tables[2 * kTableDoubles];  // x tables, then y tables
@@ -39,15 +39,6 @@ DeviceScratch g_scratch[kMaxDevices];
 int noalloc_fail(int code, const std::string& msg) {
     set_global_error(msg.c_str());
     return code;
-}
-
-DstPlan plan_at(double* tables, int N) {
-    DstPlan p;
-    p.N = N;
-    p.W = reinterpret_cast<double2*>(tables);
-    p.s = tables + 2 * N;
-    p.c = tables + 3 * N;
-    return p;
 }
 
 }  // namespace
@@ -88,17 +79,17 @@ extern "C" int ibpm_lap_inv_noalloc(int32_t nx, int32_t ny, const double* rhs, d
     double* tx = ds.tables;
     double* ty = ds.tables + kTableDoubles;
     if (ds.nx != nx) {
-        e = dst_tables_build(nx, reinterpret_cast<double2*>(tx), tx + 2 * nx, tx + 3 * nx, st);
+        e = dst_tables_build(nx, tx, st);
         if (e != cudaSuccess) return noalloc_fail(IBPM_ERR_CUDA, std::string("tables: ") + cudaGetErrorString(e));
         ds.nx = nx;
     }
     if (ds.ny != ny) {
-        e = dst_tables_build(ny, reinterpret_cast<double2*>(ty), ty + 2 * ny, ty + 3 * ny, st);
+        e = dst_tables_build(ny, ty, st);
         if (e != cudaSuccess) return noalloc_fail(IBPM_ERR_CUDA, std::string("tables: ") + cudaGetErrorString(e));
         ds.ny = ny;
     }
     const Geom g = make_geom(nx, ny, 1);
-    const DstPlan px = plan_at(tx, nx), py = plan_at(ty, ny);
+    const DstPlan px = dst_plan_at(tx, nx), py = dst_plan_at(ty, ny);
     // Every slab element that the transforms read (columns < nx-1) is written
     // by this copy, so nothing left by an earlier call is read.
     const size_t row = sizeof(double) * g.n1;

@@ -1,0 +1,6 @@
+// Spectral level chain for 64 x 32 grids (see ring_kernels.cuh).
+#include "ring_kernels.cuh"
+
+namespace ibpm {
+IBPM_RING_DEFINE(64, 32)
+}  // namespace ibpm

@@ -1,0 +1,6 @@
+// Spectral level chain for 64 x 64 grids (see ring_kernels.cuh).
+#include "ring_kernels.cuh"
+
+namespace ibpm {
+IBPM_RING_DEFINE(64, 64)
+}  // namespace ibpm

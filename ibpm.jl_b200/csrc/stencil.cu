@@ -18,6 +18,8 @@ namespace ibpm {
 // eigenvectors are exactly the DST-I basis.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
+    pdl_wait();
+    pdl_trigger();
     const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
     const int j0 = blockIdx.y * blockDim.y + threadIdx.y;
     const int lev = blockIdx.z;
@@ -80,8 +82,7 @@ __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
 cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st) {
     dim3 blk(32, 8);
     dim3 grid((g.n1 + 31) / 32, (g.n2 + 7) / 8, a.mg);
-    trial_rhs_kernel<<<grid, blk, 0, st>>>(a, g);
-    return cudaGetLastError();
+    return launch_k(trial_rhs_kernel, grid, blk, 0, st, a, g);
 }
 
 // ---------------------------------------------------------------------------
@@ -92,6 +93,8 @@ cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st) {
 // i = 2:2:nx-2 ↔ ic = nx/4 + i/2.
 // ---------------------------------------------------------------------------
 __global__ void coarsify_kernel(double* G, SlabMap fmap, SlabMap cmap, Geom g) {
+    pdl_wait();
+    pdl_trigger();
     const int nxc = g.nx / 2 - 1, nyc = g.ny / 2 - 1;
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     const int b = blockIdx.y * blockDim.y + threadIdx.y;
@@ -110,8 +113,7 @@ cudaError_t launch_coarsify(const Geom& g, double* G, SlabMap fine_map, SlabMap 
                             cudaStream_t st) {
     dim3 blk(32, 8);
     dim3 grid((g.nx / 2 - 1 + 31) / 32, (g.ny / 2 - 1 + 7) / 8, nslabs);
-    coarsify_kernel<<<grid, blk, 0, st>>>(G, fine_map, coarse_map, g);
-    return cudaGetLastError();
+    return launch_k(coarsify_kernel, grid, blk, 0, st, G, fine_map, coarse_map, g);
 }
 
 // ---------------------------------------------------------------------------
@@ -122,6 +124,8 @@ cudaError_t launch_coarsify(const Geom& g, double* G, SlabMap fine_map, SlabMap 
 // One thread per flux element; blockIdx.y = batch × levels.
 // ---------------------------------------------------------------------------
 __global__ void curl_kernel(CurlArgs a, Geom g) {
+    pdl_wait();
+    pdl_trigger();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= g.nq) return;
     const int y = blockIdx.y;
@@ -130,24 +134,32 @@ __global__ void curl_kernel(CurlArgs a, Geom g) {
     const int nx = g.nx, ny = g.ny, P = g.P;
     const double* psi = a.psi + a.psi_map.off(y);
     CoarseBC cb;
-    cb.rc = (lev < a.mg - 1 && a.coarse) ? a.coarse + a.coarse_map.off(y) : nullptr;
+    cb.rc = (lev < a.mg - 1 && a.coarse && !a.bcv) ? a.coarse + a.coarse_map.off(y) : nullptr;
     cb.P = P; cb.nx = nx; cb.ny = ny;
+    const double* bv = (lev < a.mg - 1 && a.bcv) ? a.bcv + (long long)(bt * a.mg + lev) * g.nbc : nullptr;
+    struct {
+        const CoarseBC& c; const double* v; const Geom& g;
+        __device__ double bot(int i) const { return v ? v[g.B + i] : c.bot(i); }
+        __device__ double top(int i) const { return v ? v[g.T + i] : c.top(i); }
+        __device__ double left(int i) const { return v ? v[g.L + i] : c.left(i); }
+        __device__ double right(int i) const { return v ? v[g.R + i] : c.right(i); }
+    } eb{cb, bv, g};
     auto ps = [&](int I, int J) -> double { return psi[(long long)(J - 1) * P + (I - 1)]; };
     double v;
     if (e < g.nu) {
         const int I = e % (nx + 1) + 1, J = e / (nx + 1) + 1;
-        if (I == 1) v = cb.left(J) - cb.left(J - 1);
-        else if (I == nx + 1) v = cb.right(J) - cb.right(J - 1);
-        else if (J == 1) v = ps(I - 1, 1) - cb.bot(I - 2);
-        else if (J == ny) v = cb.top(I - 1) - ps(I - 1, ny - 1);
+        if (I == 1) v = eb.left(J) - eb.left(J - 1);
+        else if (I == nx + 1) v = eb.right(J) - eb.right(J - 1);
+        else if (J == 1) v = ps(I - 1, 1) - eb.bot(I - 2);
+        else if (J == ny) v = eb.top(I - 1) - ps(I - 1, ny - 1);
         else v = ps(I - 1, J) - ps(I - 1, J - 1);
     } else {
         const int f = e - g.nu;
         const int I = f % nx + 1, J = f / nx + 1;
-        if (J == 1) v = cb.bot(I - 1) - cb.bot(I);
-        else if (J == ny + 1) v = cb.top(I - 1) - cb.top(I);
-        else if (I == 1) v = cb.left(J - 1) - ps(1, J - 1);
-        else if (I == nx) v = ps(nx - 1, J - 1) - cb.right(J - 1);
+        if (J == 1) v = eb.bot(I - 1) - eb.bot(I);
+        else if (J == ny + 1) v = eb.top(I - 1) - eb.top(I);
+        else if (I == 1) v = eb.left(J - 1) - ps(1, J - 1);
+        else if (I == nx) v = ps(nx - 1, J - 1) - eb.right(J - 1);
         else v = ps(I - 1, J - 1) - ps(I, J - 1);
     }
     a.q[(long long)bt * a.q_bstride + (long long)(lev - a.q_lev0) * a.q_lstride + e] = v;
@@ -155,8 +167,7 @@ __global__ void curl_kernel(CurlArgs a, Geom g) {
 
 cudaError_t launch_curl(const Geom& g, const CurlArgs& a, cudaStream_t st) {
     dim3 grid((g.nq + 255) / 256, a.nlev * a.nbatch);
-    curl_kernel<<<grid, 256, 0, st>>>(a, g);
-    return cudaGetLastError();
+    return launch_k(curl_kernel, grid, dim3(256), 0, st, a, g);
 }
 
 }  // namespace ibpm

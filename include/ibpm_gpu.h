@@ -155,8 +155,8 @@ int ibpm_host_free(void* p);
  * @elapsed around run_sim!, src/ibpm.jl:71) ---------------------------- */
 
 /* Kernel classes reported by ibpm_profile. */
-#define IBPM_KERNEL_COUNT 9   /* trial_rhs, dst_x, dst_y_solve, coarsify, curl,
-                                 E_gather, binv_gemv, stress, proj_src */
+#define IBPM_KERNEL_COUNT 10  /* trial_rhs, dst_x, dst_y, coarsify, curl, E_gather,
+                                 binv_gemv, stress, proj_src, level_chain */
 
 /* Name of kernel class k (0 <= k < IBPM_KERNEL_COUNT). */
 const char* ibpm_kernel_name(int32_t k);
@@ -170,10 +170,12 @@ int ibpm_launches_per_step(ibpm_handle* h);
  * each step starts with a cold L2. */
 int ibpm_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, double* step_ms);
 
-/* Advance nsteps steps with every kernel launched eagerly between CUDA events
- * and accumulate, per kernel class, device milliseconds, algorithmic bytes
- * (each operand read once, each result written once) and launch counts into
- * ms_out / bytes_out / calls_out [IBPM_KERNEL_COUNT]. */
+/* Advance nsteps steps, each a replay of a step graph captured with a CUDA
+ * event pair around every kernel, and accumulate per kernel class the device
+ * milliseconds, algorithmic bytes (each operand read once, each result written
+ * once) and launch counts into ms_out / bytes_out / calls_out
+ * [IBPM_KERNEL_COUNT].  The event nodes serialise the kernels, so the sum is a
+ * little above the plain graph's step time. */
 int ibpm_profile(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, double* ms_out,
                  double* bytes_out, int32_t* calls_out);
 
