@@ -53,15 +53,6 @@ struct ibpm_handle {
     int* counter = nullptr; int* status = nullptr;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     bool graphs_ready = false;
-    // spectral level chain of vort2flux (ring_kernels.cuh)
-    bool chain = false;                    // grid shape supported by the chain kernels
-    int chain_cap = 0, r4len = 0, nbands = 0;
-    double* r4 = nullptr;                  // [cap][mg][4][r4len] rank-4 edge images
-    double* part = nullptr;                // [cap][nbands][2][r4len]
-    double* ucol = nullptr;                // [cap][2][r4len]
-    double* bcv = nullptr;                 // [cap][mg][nbc] ψbc vectors
-    int* ring_counter = nullptr;           // [cap]
-    double* ring_tabs = nullptr;           // [8][r4len]
     // measurement
     int launches = 0;                      // kernel launches enqueued (counted always)
     bool prof_on = false;                  // eager profiling: events around every launch
@@ -99,8 +90,8 @@ void ibpm::set_global_error(const char* msg) { g_create_err = msg ? msg : ""; }
 
 // Kernel classes reported by ibpm_profile (order of IBPM_KERNEL_* in the header).
 static const char* kKernelNames[] = {"trial_rhs", "dst_x", "dst_y", "coarsify", "curl",
-                                     "E_gather", "binv_gemv", "stress", "proj_src", "level_chain"};
-enum { K_RHS = 0, K_DSTX, K_DSTY, K_COARSIFY, K_CURL, K_E, K_GEMV, K_STRESS, K_SRC, K_RING, K_COUNT };
+                                     "E_gather", "binv_gemv", "stress", "proj_src"};
+enum { K_RHS = 0, K_DSTX, K_DSTY, K_COARSIFY, K_CURL, K_E, K_GEMV, K_STRESS, K_SRC, K_COUNT };
 
 static int prof_pre(ibpm_handle* h, int label, double bytes) {
     ++h->launches;
@@ -174,7 +165,7 @@ static int poisson(ibpm_handle* h, const double* b, SlabMap bmap, double* tmp, S
     a.load = coarse ? XLOAD_BC : XLOAD_PLAIN; a.emit = XEMIT_STORE;
     const double slab_bytes = 16.0 * g.n1 * g.n2 * nslabs;  // read + write every element once
     LAUNCH(K_DSTX, slab_bytes, launch_dst_x(g, h->px, a, h->st));
-    LAUNCH(K_DSTY, slab_bytes, launch_dst_y_solve(g, h->py, h->px, tmp, tmap, nslabs, spec(h, mode), h->st));
+    LAUNCH(K_DSTY, slab_bytes, launch_dst_y(g, h->py, h->px, tmp, tmap, nslabs, spec(h, mode), h->st));
     XPassArgs c{};
     c.in = tmp; c.out = out; c.in_map = tmap; c.out_map = omap;
     c.nslabs = nslabs; c.line0 = 0; c.line1 = g.n2;
@@ -188,8 +179,8 @@ static int poisson(ibpm_handle* h, const double* b, SlabMap bmap, double* tmp, S
 // Δ⁻¹ solves from the coarsest level inwards with the edge values of the next
 // coarser ψ, then q = curl ψ on levels [qlev0, qlev0 + qnlev) into q (nq per
 // level, batch stride q_bstride).
-static int vort2flux_seq(ibpm_handle* h, double* G, double* psi, long long bstride, int nbatch, double* q,
-                         long long q_bstride, int qlev0, int qnlev) {
+static int vort2flux(ibpm_handle* h, double* G, double* psi, long long bstride, int nbatch, double* q,
+                     long long q_bstride, int qlev0, int qnlev) {
     const Geom& g = h->g;
     const int mg = g.mg;
     for (int lev = 1; lev < mg; ++lev)
@@ -209,74 +200,6 @@ static int vort2flux_seq(ibpm_handle* h, double* G, double* psi, long long bstri
     ca.nlev = qnlev; ca.nbatch = nbatch; ca.mg = mg;
     LAUNCH(K_CURL, 8.0 * ((double)g.n1 * g.n2 + g.nq) * qnlev * nbatch, launch_curl(g, ca, h->st));
     return IBPM_OK;
-}
-
-static RankFour rank_four(const ibpm_handle* h) {
-    RankFour r;
-    r.v = h->r4; r.mg = h->g.mg; r.len = h->r4len;
-    r.sx0 = h->ring_tabs + 4 * h->r4len; r.sxN = h->ring_tabs + 5 * h->r4len;
-    r.sy0 = h->ring_tabs + 6 * h->r4len; r.syN = h->ring_tabs + 7 * h->r4len;
-    return r;
-}
-
-// The same operator with every level transformed at once (ring_kernels.cuh):
-// coarsify chain; Ĝ = S Γ for all levels (into T); the spectral level chain
-// (one launch per level, coarsest first) producing each level's edge image and
-// ψbc; ψ = S Ŵ for levels [0, ninv) (into psi); curl.  Only levels whose ψ or
-// q is used need the inverse transform: the trial state and B's columns use
-// level 1 alone.
-static int vort2flux_chain(ibpm_handle* h, double* G, double* T, double* psi, long long bstride, int nbatch,
-                           double* q, long long q_bstride, int qlev0, int qnlev, int ninv) {
-    const Geom& g = h->g;
-    const int mg = g.mg;
-    if (nbatch > h->chain_cap) return fail(h, IBPM_ERR_INVALID, "level chain batch above capacity");
-    for (int lev = 1; lev < mg; ++lev)
-        LAUNCH(K_COARSIFY, 8.0 * 1.25 * g.n1 * g.n2 * nbatch,
-               launch_coarsify(g, G, levmap(g, lev - 1, 1, bstride), levmap(g, lev, 1, bstride), nbatch, h->st));
-    const double slab = 16.0 * g.n1 * g.n2;
-    const RankFour r4 = rank_four(h);
-    SlabMap all = levmap(g, 0, mg, bstride);
-    XPassArgs a{};
-    a.in = G; a.out = T; a.in_map = all; a.out_map = all;
-    a.nslabs = mg * nbatch; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_PLAIN; a.emit = XEMIT_STORE;
-    LAUNCH(K_DSTX, slab * mg * nbatch, launch_dst_x(g, h->px, a, h->st));
-    LAUNCH(K_DSTY, slab * mg * nbatch,
-           launch_dst_y(g, h->py, h->px, T, all, mg * nbatch, spec(h, SPEC_DELTA), YMODE_FWD, r4, h->st));
-    RingArgs ra{};
-    ra.T = T; ra.tmap = all; ra.r4 = r4; ra.r4w = h->r4;
-    ra.part = h->part; ra.part_bstride = (long long)h->nbands * 2 * h->r4len; ra.ucol = h->ucol;
-    ra.bcw = h->bcv; ra.counter = h->ring_counter;
-    ra.tabs.cx = h->px.c; ra.tabs.cy = h->py.c;
-    ra.tabs.sxl = h->ring_tabs; ra.tabs.sxr = h->ring_tabs + h->r4len;
-    ra.tabs.syb = h->ring_tabs + 2 * h->r4len; ra.tabs.syt = h->ring_tabs + 3 * h->r4len;
-    ra.tabs.sx0 = r4.sx0; ra.tabs.sxN = r4.sxN; ra.tabs.sy0 = r4.sy0; ra.tabs.syN = r4.syN;
-    ra.scale = spec(h, SPEC_DELTA).scale;
-    for (int lev = mg - 2; lev >= 0; --lev) {
-        ra.lev = lev;
-        LAUNCH(K_RING, 8.0 * g.n1 * g.n2 * nbatch, launch_ring(g, h->px, h->py, ra, nbatch, h->st));
-    }
-    SlabMap inv = levmap(g, 0, ninv, bstride);
-    LAUNCH(K_DSTY, slab * ninv * nbatch,
-           launch_dst_y(g, h->py, h->px, T, inv, ninv * nbatch, spec(h, SPEC_DELTA), YMODE_INV, r4, h->st));
-    XPassArgs c2{};
-    c2.in = T; c2.out = psi; c2.in_map = inv; c2.out_map = inv;
-    c2.nslabs = ninv * nbatch; c2.line0 = 0; c2.line1 = g.n2; c2.load = XLOAD_PLAIN; c2.emit = XEMIT_STORE;
-    LAUNCH(K_DSTX, slab * ninv * nbatch, launch_dst_x(g, h->px, c2, h->st));
-    CurlArgs ca{};
-    ca.psi = psi; ca.psi_map = levmap(g, qlev0, qnlev, bstride);
-    ca.bcv = h->bcv;
-    ca.q = q; ca.q_bstride = q_bstride; ca.q_lstride = g.nq; ca.q_lev0 = qlev0;
-    ca.nlev = qnlev; ca.nbatch = nbatch; ca.mg = mg;
-    LAUNCH(K_CURL, 8.0 * ((double)g.n1 * g.n2 + g.nq) * qnlev * nbatch, launch_curl(g, ca, h->st));
-    return IBPM_OK;
-}
-
-// vort2flux! with q on levels [qlev0, qlev0 + qnlev) and ψ at least on levels
-// [0, ninv); T is spectral scratch of the same shape as G.
-static int vort2flux(ibpm_handle* h, double* G, double* T, double* psi, long long bstride, int nbatch, double* q,
-                     long long q_bstride, int qlev0, int qnlev, int ninv) {
-    if (h->chain) return vort2flux_chain(h, G, T, psi, bstride, nbatch, q, q_bstride, qlev0, qnlev, ninv);
-    return vort2flux_seq(h, G, psi, bstride, nbatch, q, q_bstride, qlev0, qnlev);
 }
 
 // One step, reading the state from parity p and leaving it in parity p^1.
@@ -301,7 +224,7 @@ static int enqueue_step(ibpm_handle* h, int p) {
     SlabMap all = levmap(g, 0, mg);
     int rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg, SPEC_AINV, XEMIT_STORE);
     if (rc) return rc;
-    rc = vort2flux(h, Gnew, h->rhs, h->psi, g.S * mg, 1, h->qs, 0, 0, 1, 1);  // only the level-1 trial flux is read
+    rc = vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->qs, 0, 0, 1);  // only the level-1 trial flux is read
     if (rc) return rc;
     // --- boundary_forces! (timestepping.jl:154-163) and update_stress! (:330-354)
     LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st));
@@ -314,7 +237,7 @@ static int enqueue_step(ibpm_handle* h, int p) {
     rc = poisson(h, h->Gsrc, one, h->rhs, one, Gnew, one, 1, SPEC_AINV, XEMIT_SUB);
     if (rc) return rc;
     // --- vort2flux!(state.ψ, state.q, state.Γ) (timestepping.jl:64)
-    return vort2flux(h, Gnew, h->rhs, h->psi, g.S * mg, 1, h->q, 0, 0, mg, mg);
+    return vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->q, 0, 0, mg);
 }
 
 // ---------------------------------------------------------------------------
@@ -409,18 +332,17 @@ static int build_binv(ibpm_handle* h) {
     const Geom& g = h->g;
     const int nf = h->nf, mg = g.mg;
     const int chunk = std::min(nf, kBChunk);
-    double *GB = nullptr, *PB = nullptr, *QB = nullptr, *TB = nullptr, *work = nullptr;
+    double *GB = nullptr, *PB = nullptr, *QB = nullptr, *work = nullptr;
     int* info = nullptr;
     int rc;
     const long long bstride = g.S * mg;
     if ((rc = dalloc(h, &GB, (size_t)bstride * chunk)) || (rc = dalloc(h, &PB, (size_t)bstride * chunk)) ||
-        (rc = dalloc(h, &TB, (size_t)bstride * chunk)) ||
         (rc = dalloc(h, &QB, (size_t)g.nq * chunk)) || (rc = dalloc(h, &work, (size_t)2 * nf * nf + 2 * nf)) ||
         (rc = dalloc(h, &info, 1))) {
-        cudaFree(GB); cudaFree(PB); cudaFree(TB); cudaFree(QB); cudaFree(work); cudaFree(info);
+        cudaFree(GB); cudaFree(PB); cudaFree(QB); cudaFree(work); cudaFree(info);
         return rc;
     }
-    auto cleanup = [&]() { cudaFree(GB); cudaFree(PB); cudaFree(TB); cudaFree(QB); cudaFree(work); cudaFree(info); };
+    auto cleanup = [&]() { cudaFree(GB); cudaFree(PB); cudaFree(QB); cudaFree(work); cudaFree(info); };
     for (int c0 = 0; c0 < nf && rc == IBPM_OK; c0 += chunk) {
         const int R = std::min(chunk, nf - c0);
         if (cudaMemsetAsync(GB, 0, sizeof(double) * bstride * R, h->st) != cudaSuccess) { rc = IBPM_ERR_CUDA; break; }
@@ -428,7 +350,7 @@ static int build_binv(ibpm_handle* h) {
         SlabMap l0 = levmap(g, 0, 1, bstride);
         rc = poisson(h, GB, l0, GB, l0, GB, l0, R, SPEC_AINV, XEMIT_STORE);
         if (rc) break;
-        rc = vort2flux(h, GB, TB, PB, bstride, R, QB, g.nq, 0, 1, 1);  // level-1 flux of each column
+        rc = vort2flux(h, GB, PB, bstride, R, QB, g.nq, 0, 1);  // level-1 flux of each column
         if (rc) break;
         if (launch_E(g, h->body, QB, g.nq, R, 0.0, 0.0, h->Binv + c0, -(long long)nf, h->st) != cudaSuccess) {
             rc = IBPM_ERR_CUDA;
@@ -455,8 +377,7 @@ static void free_handle(ibpm_handle* h) {
     for (int p = 0; p < 2; ++p) if (h->gexec[p]) cudaGraphExecDestroy(h->gexec[p]);
     void* ptrs[] = {h->G[0], h->G[1], h->Nl[0], h->Nl[1], h->psi, h->q, h->qs, h->rhs, h->Gsrc, h->F, h->Fb,
                     h->Binv, h->nonlin1_shadow, h->d_xb, h->d_ds, h->d_bidx, h->d_w, h->d_body_start,
-                    h->d_src_pts, h->d_src_rows, h->d_et_ptr, h->d_et_k, h->d_et_w, h->hist, h->counter, h->status,
-                    h->r4, h->part, h->ucol, h->bcv, h->ring_counter, h->ring_tabs};
+                    h->d_src_pts, h->d_src_rows, h->d_et_ptr, h->d_et_k, h->d_et_w, h->hist, h->counter, h->status};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (h->flush_buf) cudaFree(h->flush_buf);
     for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
@@ -531,28 +452,6 @@ static int create_impl(ibpm_handle* h, const ibpm_problem_desc* d) {
     CK(cudaMemsetAsync(h->Gsrc, 0, sizeof(double) * g.S, h->st));
     CK(cudaMemsetAsync(h->Fb, 0, sizeof(double) * h->nf, h->st));
     CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
-    // vort2flux path: level by level (default), or the spectral level chain
-    // (IBPM_VORT2FLUX=chain), which transforms every level at once
-    const char* v2f = getenv("IBPM_VORT2FLUX");
-    const bool want_chain = v2f && std::string(v2f) == "chain";
-    if (g.mg >= 2 && want_chain && ring_supported(g.nx, g.ny)) {
-        h->chain = true;
-        h->chain_cap = std::max(1, std::min(h->nf, kBChunk));
-        h->r4len = ((std::max(g.n1, g.n2) + 3) / 4) * 4;
-        h->nbands = ring_nbands(g);
-        const size_t cap = h->chain_cap;
-        if ((rc = dalloc(h, &h->r4, cap * g.mg * 4 * h->r4len)) ||
-            (rc = dalloc(h, &h->part, cap * h->nbands * 2 * h->r4len)) ||
-            (rc = dalloc(h, &h->ucol, cap * 2 * h->r4len)) || (rc = dalloc(h, &h->bcv, cap * g.mg * g.nbc)) ||
-            (rc = dalloc(h, &h->ring_counter, cap)) || (rc = dalloc(h, &h->ring_tabs, (size_t)8 * h->r4len)))
-            return rc;
-        CK(cudaMemsetAsync(h->r4, 0, sizeof(double) * cap * g.mg * 4 * h->r4len, h->st));
-        CK(cudaMemsetAsync(h->bcv, 0, sizeof(double) * cap * g.mg * g.nbc, h->st));
-        CK(cudaMemsetAsync(h->ring_counter, 0, sizeof(int) * cap, h->st));
-        CK(cudaMemsetAsync(h->ring_tabs, 0, sizeof(double) * 8 * h->r4len, h->st));
-        CK(ring_tables_build(g, h->r4len, h->ring_tabs, h->st));
-        CK(ring_init_attributes(g.nx, g.ny));
-    }
     if ((rc = build_coupling(h, d))) return rc;
     if ((rc = build_binv(h))) return rc;
     CK(cudaStreamSynchronize(h->st));
@@ -725,7 +624,7 @@ extern "C" int ibpm_advance(ibpm_handle* h, double t, int32_t nsteps, double* CD
 extern "C" int ibpm_vort2flux(ibpm_handle* h) {
     if (!h) return IBPM_ERR_INVALID;
     CK(cudaSetDevice(h->device));
-    int rc = vort2flux(h, h->G[h->cur], h->rhs, h->psi, h->g.S * h->g.mg, 1, h->q, 0, 0, h->g.mg, h->g.mg);
+    int rc = vort2flux(h, h->G[h->cur], h->psi, h->g.S * h->g.mg, 1, h->q, 0, 0, h->g.mg);
     if (rc) return rc;
     CK(cudaStreamSynchronize(h->st));
     return IBPM_OK;

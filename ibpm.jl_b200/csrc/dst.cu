@@ -7,52 +7,40 @@
 namespace ibpm {
 
 cudaError_t dst_x_32(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_32(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_32(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_32();
 cudaError_t dst_x_64(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_64(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_64(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_64();
 cudaError_t dst_x_128(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_128(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_128(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_128();
 cudaError_t dst_x_192(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_192(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_192(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_192();
 cudaError_t dst_x_200(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_200(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_200(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_200();
 cudaError_t dst_x_256(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_256(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_256(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_256();
 cudaError_t dst_x_384(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_384(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_384(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_384();
 cudaError_t dst_x_400(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_400(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_400(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_400();
 cudaError_t dst_x_512(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_512(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_512(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_512();
 cudaError_t dst_x_768(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_768(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_768(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_768();
 cudaError_t dst_x_1024(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_1024(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_1024(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_1024();
 cudaError_t dst_x_2048(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_2048(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, int,
-                     const RankFour&, cudaStream_t);
+cudaError_t dst_y_2048(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_2048();
 
 // Supported transform lengths N = nx or ny: 32, 64, 128, 192, 200, 256, 384, 400, 512, 768, 1024, 2048.
@@ -189,21 +177,21 @@ cudaError_t launch_dst_x(const Geom& g, const DstPlan& px, const XPassArgs& a, c
 }
 
 cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px, double* data, SlabMap map, int nslabs,
-                         const SpecParams& sp, int mode, const RankFour& r4, cudaStream_t st) {
+                         const SpecParams& sp, cudaStream_t st) {
     if (nslabs <= 0) return cudaSuccess;
     switch (py.N) {
-        case 32: return dst_y_32(g, py, px, data, map, nslabs, sp, mode, r4, st);
-        case 64: return dst_y_64(g, py, px, data, map, nslabs, sp, mode, r4, st);
-        case 128: return dst_y_128(g, py, px, data, map, nslabs, sp, mode, r4, st);
-        case 192: return dst_y_192(g, py, px, data, map, nslabs, sp, mode, r4, st);
-        case 200: return dst_y_200(g, py, px, data, map, nslabs, sp, mode, r4, st);
-        case 256: return dst_y_256(g, py, px, data, map, nslabs, sp, mode, r4, st);
-        case 384: return dst_y_384(g, py, px, data, map, nslabs, sp, mode, r4, st);
-        case 400: return dst_y_400(g, py, px, data, map, nslabs, sp, mode, r4, st);
-        case 512: return dst_y_512(g, py, px, data, map, nslabs, sp, mode, r4, st);
-        case 768: return dst_y_768(g, py, px, data, map, nslabs, sp, mode, r4, st);
-        case 1024: return dst_y_1024(g, py, px, data, map, nslabs, sp, mode, r4, st);
-        case 2048: return dst_y_2048(g, py, px, data, map, nslabs, sp, mode, r4, st);
+        case 32: return dst_y_32(g, py, px, data, map, nslabs, sp, st);
+        case 64: return dst_y_64(g, py, px, data, map, nslabs, sp, st);
+        case 128: return dst_y_128(g, py, px, data, map, nslabs, sp, st);
+        case 192: return dst_y_192(g, py, px, data, map, nslabs, sp, st);
+        case 200: return dst_y_200(g, py, px, data, map, nslabs, sp, st);
+        case 256: return dst_y_256(g, py, px, data, map, nslabs, sp, st);
+        case 384: return dst_y_384(g, py, px, data, map, nslabs, sp, st);
+        case 400: return dst_y_400(g, py, px, data, map, nslabs, sp, st);
+        case 512: return dst_y_512(g, py, px, data, map, nslabs, sp, st);
+        case 768: return dst_y_768(g, py, px, data, map, nslabs, sp, st);
+        case 1024: return dst_y_1024(g, py, px, data, map, nslabs, sp, st);
+        case 2048: return dst_y_2048(g, py, px, data, map, nslabs, sp, st);
         default: return cudaErrorInvalidValue;
     }
 }

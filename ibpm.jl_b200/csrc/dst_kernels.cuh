@@ -147,11 +147,21 @@ template <> __device__ __forceinline__ void dft<8>(double2* v) {
 
 // Synchronise the TP threads of group `gid` (named barrier 1 + gid when the
 // group spans several warps).
+// The barrier id is an immediate in each branch, so ptxas reserves only the
+// barriers a kernel can use (a run-time id reserves all sixteen, which caps
+// the resident blocks per SM).
 template <int TP> __device__ __forceinline__ void gsync(int gid) {
     if constexpr (TP == 32) {
         __syncwarp();
+    } else if constexpr (TP >= 128) {
+        asm volatile("bar.sync 1, %0;" ::"n"(TP) : "memory");
     } else {
-        asm volatile("bar.sync %0, %1;" ::"r"(gid + 1), "n"(TP) : "memory");
+        switch (gid) {
+            case 0: asm volatile("bar.sync 1, %0;" ::"n"(TP) : "memory"); break;
+            case 1: asm volatile("bar.sync 2, %0;" ::"n"(TP) : "memory"); break;
+            case 2: asm volatile("bar.sync 3, %0;" ::"n"(TP) : "memory"); break;
+            default: asm volatile("bar.sync 4, %0;" ::"n"(TP) : "memory"); break;
+        }
     }
 }
 
@@ -321,7 +331,7 @@ __host__ __device__ constexpr size_t tables_bytes() {
 // x-pass: lines are rows of a slab (contiguous).  One group per line pair.
 // ---------------------------------------------------------------------------
 template <int N, int LOAD, int EMIT>
-__global__ void __launch_bounds__(256) dst_x_kernel(XPassArgs a, Geom g, DstPlan p) {
+__global__ void __launch_bounds__((N <= 1024 ? 128 : 256)) dst_x_kernel(XPassArgs a, Geom g, DstPlan p) {
     constexpr int TP = ct_tp(N);
     constexpr int G = ct_groups(N);
     extern __shared__ double2 smem2[];
@@ -382,10 +392,8 @@ __global__ void __launch_bounds__(256) dst_x_kernel(XPassArgs a, Geom g, DstPlan
 }
 
 // ---------------------------------------------------------------------------
-// y-pass on a tile of TW = 2G columns (all rows) staged in shared memory, in
-// place.  YMODE_SOLVE: DST-I, spectral divide, DST-I (the middle of a
-// Poisson-type solve).  YMODE_FWD: one DST-I.  YMODE_INV: add the rank-4
-// spectral image of the edge terms, divide by Λ, scale, one DST-I.
+// y-pass of a Poisson-type solve on a tile of TW = 2G columns (all rows)
+// staged in shared memory, in place: DST-I, spectral divide, DST-I.
 // ---------------------------------------------------------------------------
 template <int N>
 __host__ __device__ constexpr int y_groups() { return ct_groups(N); }
@@ -398,9 +406,9 @@ __host__ __device__ constexpr size_t y_smem_bytes(int n2) {
            (size_t)y_groups<N>() * ct_buf(N) * sizeof(double2);
 }
 
-template <int N, int MODE>
-__global__ void __launch_bounds__(256) dst_y_kernel(double* data, SlabMap map, Geom g, DstPlan p,
-                                                    const double* __restrict__ cx, SpecParams sp, RankFour r4) {
+template <int N>
+__global__ void __launch_bounds__((N <= 1024 ? 128 : 256), (N <= 512 ? 5 : 1))
+    dst_y_kernel(double* data, SlabMap map, Geom g, DstPlan p, const double* __restrict__ cx, SpecParams sp) {
     constexpr int TP = ct_tp(N);
     constexpr int TW = y_tile_w<N>();
     constexpr int TWp = TW + 1;
@@ -416,7 +424,6 @@ __global__ void __launch_bounds__(256) dst_y_kernel(double* data, SlabMap map, G
     const int i0 = blockIdx.x * TW;
     double* base = data + map.off(blockIdx.y);
     const int lev = map.level(blockIdx.y);
-    const int bt = map.batch(blockIdx.y);
 
     stage_tables<N>(tw, sn, p);  // constant tables: before the dependency wait
     for (int j = threadIdx.x; j < n2; j += blockDim.x) cp_async8(cyv + j, p.c + j);
@@ -441,20 +448,10 @@ __global__ void __launch_bounds__(256) dst_y_kernel(double* data, SlabMap map, G
             tile[o * TWp + ca + 1] = v.y;
         };
         // w ./= M ; w .*= scale  with Λ = -2 (cos(π i/nx) + cos(π j/ny) - 2)
-        auto divide = [&](bool add_r4) {
+        auto divide = [&]() {
             const double cxa = __ldg(&cx[ia]);
             const double cxb = hasb ? __ldg(&cx[ia + 1]) : 0.0;
             const double den = sp.den[lev];
-            const double* rv = add_r4 ? r4.v + (long long)(bt * r4.mg + lev) * 4 * r4.len : nullptr;
-            double bxa = 0, txa = 0, bxb = 0, txb = 0, s0a = 0, sNa = 0, s0b = 0, sNb = 0;
-            if (rv) {
-                bxa = rv[ia]; txa = rv[r4.len + ia];
-                s0a = __ldg(&r4.sx0[ia]); sNa = __ldg(&r4.sxN[ia]);
-                if (hasb) {
-                    bxb = rv[ia + 1]; txb = rv[r4.len + ia + 1];
-                    s0b = __ldg(&r4.sx0[ia + 1]); sNb = __ldg(&r4.sxN[ia + 1]);
-                }
-            }
             for (int o = tid; o < n2; o += TP) {
                 const double c2 = cyv[o];
                 const double la = -2.0 * ((cxa + c2) - 2.0);
@@ -467,31 +464,15 @@ __global__ void __launch_bounds__(256) dst_y_kernel(double* data, SlabMap map, G
                     Ma = 1.0 + la * sp.dt / den;
                     Mb = 1.0 + lb * sp.dt / den;
                 }
-                double va = tile[o * TWp + ca], vb = tile[o * TWp + ca + 1];
-                if (rv) {
-                    const double y0 = __ldg(&r4.sy0[o]), yN = __ldg(&r4.syN[o]);
-                    const double lf = rv[2 * r4.len + o], rt = rv[3 * r4.len + o];
-                    va = (((va + bxa * y0) + txa * yN) + s0a * lf) + sNa * rt;
-                    vb = (((vb + bxb * y0) + txb * yN) + s0b * lf) + sNb * rt;
-                }
-                tile[o * TWp + ca] = (va * nr_rcp(Ma)) * sp.scale;
-                tile[o * TWp + ca + 1] = hasb ? (vb * nr_rcp(Mb)) * sp.scale : 0.0;
+                tile[o * TWp + ca] = (tile[o * TWp + ca] * nr_rcp(Ma)) * sp.scale;
+                tile[o * TWp + ca + 1] = hasb ? (tile[o * TWp + ca + 1] * nr_rcp(Mb)) * sp.scale : 0.0;
             }
         };
-        if (MODE == YMODE_INV) {
-            divide(true);
-            gsync<TP>(gid);
-        }
-        constexpr int NPASS = (MODE == YMODE_SOLVE) ? 2 : 1;
-#pragma unroll 1
-        for (int pass = 0; pass < NPASS; ++pass) {
-            dst_pair<N, TP>(buf, tw, sn, tid, gid, load, emit);
-            gsync<TP>(gid);
-            if (MODE == YMODE_SOLVE && pass == 0) {
-                divide(false);
-                gsync<TP>(gid);
-            }
-        }
+        dst_pair<N, TP>(buf, tw, sn, tid, gid, load, emit);
+        gsync<TP>(gid);
+        divide();
+        gsync<TP>(gid);
+        dst_pair<N, TP>(buf, tw, sn, tid, gid, load, emit);
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
@@ -527,18 +508,13 @@ cudaError_t launch_x_t(const Geom& g, const DstPlan& px, const XPassArgs& a, cud
 
 template <int N>
 cudaError_t launch_y_t(const Geom& g, const DstPlan& py, const DstPlan& px, double* data, SlabMap map, int nslabs,
-                       const SpecParams& sp, int mode, const RankFour& r4, cudaStream_t st) {
+                       const SpecParams& sp, cudaStream_t st) {
     constexpr int TW = y_tile_w<N>();
     const size_t smem = y_smem_bytes<N>(g.n2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     dim3 grid((g.n1 + TW - 1) / TW, nslabs);
     const int threads = y_groups<N>() * ct_tp(N);
-    const double* cx = px.c;
-    if (mode == YMODE_FWD)
-        return launch_k(dst_y_kernel<N, YMODE_FWD>, grid, dim3(threads), smem, st, data, map, g, py, cx, sp, r4);
-    if (mode == YMODE_INV)
-        return launch_k(dst_y_kernel<N, YMODE_INV>, grid, dim3(threads), smem, st, data, map, g, py, cx, sp, r4);
-    return launch_k(dst_y_kernel<N, YMODE_SOLVE>, grid, dim3(threads), smem, st, data, map, g, py, cx, sp, r4);
+    return launch_k(dst_y_kernel<N>, grid, dim3(threads), smem, st, data, map, g, py, px.c, sp);
 }
 
 template <class K>
@@ -556,9 +532,7 @@ cudaError_t attr_t() {
     if ((e = smem_attrs(dst_x_kernel<N, XLOAD_PLAIN, XEMIT_SUB>))) return e;
     if ((e = smem_attrs(dst_x_kernel<N, XLOAD_BC, XEMIT_STORE>))) return e;
     if ((e = smem_attrs(dst_x_kernel<N, XLOAD_BC, XEMIT_SUB>))) return e;
-    if ((e = smem_attrs(dst_y_kernel<N, YMODE_SOLVE>))) return e;
-    if ((e = smem_attrs(dst_y_kernel<N, YMODE_FWD>))) return e;
-    return smem_attrs(dst_y_kernel<N, YMODE_INV>);
+    return smem_attrs(dst_y_kernel<N>);
 }
 
 }  // namespace dstk
@@ -570,8 +544,8 @@ cudaError_t attr_t() {
         return dstk::launch_x_t<N>(g, px, a, st);                                                          \
     }                                                                                                      \
     cudaError_t dst_y_##N(const Geom& g, const DstPlan& py, const DstPlan& px, double* d, SlabMap m, int n, \
-                          const SpecParams& sp, int mode, const RankFour& r4, cudaStream_t st) {           \
-        return dstk::launch_y_t<N>(g, py, px, d, m, n, sp, mode, r4, st);                                  \
+                          const SpecParams& sp, cudaStream_t st) {                                         \
+        return dstk::launch_y_t<N>(g, py, px, d, m, n, sp, st);                                            \
     }                                                                                                      \
     cudaError_t dst_attr_##N() { return dstk::attr_t<N>(); }
 

@@ -192,56 +192,10 @@ struct XPassArgs {
 };
 cudaError_t launch_dst_x(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st);
 
-// y-direction pass, in place on every slab selected by `map`:
-//   YMODE_SOLVE  DST-I, spectral divide, DST-I (the middle of a Poisson solve)
-//   YMODE_FWD    DST-I only
-//   YMODE_INV    add the rank-4 spectral image of edge terms (RankFour), divide,
-//                DST-I
-enum YMode { YMODE_SOLVE = 0, YMODE_FWD = 1, YMODE_INV = 2 };
-// Spectral image S b of an edge-only field b (apply_bc! of edge vectors): for
-// slab (batch, level), v + (batch·mg + level)·4·len holds [Sx bot | Sx top |
-// Sy left | Sy right], each of length len; S b(k, m) = Sx bot(k)·sy0(m) +
-// Sx top(k)·syN(m) + sx0(k)·Sy left(m) + sxN(k)·Sy right(m), with sx0(k) =
-// 2 sin(π(k+1)/nx), sxN(k) = 2 sin(π(nx-1)(k+1)/nx) and likewise in y.
-struct RankFour {
-    const double* v;
-    int mg, len;
-    const double *sx0, *sxN, *sy0, *syN;
-};
+// y-direction pass of a Poisson-type solve, in place on every slab selected by
+// `map`: DST-I, spectral divide (SpecParams), DST-I.
 cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px_cos, double* data, SlabMap map,
-                         int nslabs, const SpecParams& sp, int mode, const RankFour& r4, cudaStream_t st);
-inline cudaError_t launch_dst_y_solve(const Geom& g, const DstPlan& py, const DstPlan& px_cos, double* data,
-                                      SlabMap map, int nslabs, const SpecParams& sp, cudaStream_t st) {
-    return launch_dst_y(g, py, px_cos, data, map, nslabs, sp, YMODE_SOLVE, RankFour{}, st);
-}
-
-// Spectral level chain of vort2flux! (ring_kernels.cuh).  Tables, 0-based:
-//   cx[k] = cos(π(k+1)/nx), cy[m] = cos(π(m+1)/ny)
-//   sxl[k] = 2 sin(π (nx/4)(k+1)/nx), sxr[k] = 2 sin(π (3nx/4)(k+1)/nx)
-//   syb[m] = 2 sin(π (ny/4)(m+1)/ny), syt[m] = 2 sin(π (3ny/4)(m+1)/ny)
-//   sx0, sxN, sy0, syN as in RankFour.
-struct RingTabs {
-    const double *cx, *cy, *sxl, *sxr, *syb, *syt, *sx0, *sxN, *sy0, *syN;
-};
-struct RingArgs {
-    const double* T; SlabMap tmap;   // spectra Ĝ of every level (batch-major, nlev = mg)
-    RankFour r4;                     // rank-4 images (read: level lev+1)
-    double* r4w;                     // same buffer (written: level lev)
-    double* part; long long part_bstride;  // per-block partial row sums [band][2][len]
-    double* ucol;                    // [batch][2][len] column sums
-    double* bcw;                     // [batch][mg][nbc] real-space ψbc of each level (written: level lev)
-    int* counter;                    // [batch] blocks finished (reset by the last block)
-    RingTabs tabs;
-    int lev;                         // level whose edge image is produced (reads lev+1)
-    double scale;                    // 1/(4 nx ny)
-};
-bool ring_supported(int nx, int ny);
-cudaError_t ring_init_attributes(int nx, int ny);
-cudaError_t launch_ring(const Geom& g, const DstPlan& px, const DstPlan& py, const RingArgs& a, int nbatch,
-                        cudaStream_t st);
-int ring_nbands(const Geom& g);
-// Fill the sine tables of RingTabs (8 arrays of `len` doubles from base).
-cudaError_t ring_tables_build(const Geom& g, int len, double* base, cudaStream_t st);
+                         int nslabs, const SpecParams& sp, cudaStream_t st);
 
 // Stencil kernels (stencil.cu)
 struct RhsArgs {
@@ -265,7 +219,6 @@ cudaError_t launch_coarsify(const Geom& g, double* G, SlabMap fine_map, SlabMap 
 struct CurlArgs {
     const double* psi; SlabMap psi_map;
     const double* coarse; SlabMap coarse_map;  // coarser level ψ, or nullptr
-    const double* bcv;                         // or: ψbc vectors [batch][mg][nbc] (used when non-null)
     double* q; long long q_bstride, q_lstride; int q_lev0;
     int nlev;                                  // levels in this launch
     int nbatch;

@@ -104,7 +104,7 @@ extern "C" int ibpm_lap_inv_noalloc(int32_t nx, int32_t ny, const double* rhs, d
     sp.mode = SPEC_DELTA;
     sp.scale = 1.0 / (4.0 * nx * ny);  // laplacian.jl:194
     if ((e = launch_dst_x(g, px, a, st)) != cudaSuccess ||
-        (e = launch_dst_y_solve(g, py, px, ds.slab, m, 1, sp, st)) != cudaSuccess ||
+        (e = launch_dst_y(g, py, px, ds.slab, m, 1, sp, st)) != cudaSuccess ||
         (e = launch_dst_x(g, px, a, st)) != cudaSuccess)
         return noalloc_fail(IBPM_ERR_CUDA, std::string("solve: ") + cudaGetErrorString(e));
     e = cudaMemcpy2DAsync(x, row, ds.slab, sizeof(double) * g.P, row, g.n2, cudaMemcpyDeviceToDevice, st);

@@ -133,17 +133,9 @@ __global__ void curl_kernel(CurlArgs a, Geom g) {
     const int bt = a.psi_map.batch(y);
     const int nx = g.nx, ny = g.ny, P = g.P;
     const double* psi = a.psi + a.psi_map.off(y);
-    CoarseBC cb;
-    cb.rc = (lev < a.mg - 1 && a.coarse && !a.bcv) ? a.coarse + a.coarse_map.off(y) : nullptr;
-    cb.P = P; cb.nx = nx; cb.ny = ny;
-    const double* bv = (lev < a.mg - 1 && a.bcv) ? a.bcv + (long long)(bt * a.mg + lev) * g.nbc : nullptr;
-    struct {
-        const CoarseBC& c; const double* v; const Geom& g;
-        __device__ double bot(int i) const { return v ? v[g.B + i] : c.bot(i); }
-        __device__ double top(int i) const { return v ? v[g.T + i] : c.top(i); }
-        __device__ double left(int i) const { return v ? v[g.L + i] : c.left(i); }
-        __device__ double right(int i) const { return v ? v[g.R + i] : c.right(i); }
-    } eb{cb, bv, g};
+    CoarseBC eb;
+    eb.rc = (lev < a.mg - 1) ? a.coarse + a.coarse_map.off(y) : nullptr;
+    eb.P = P; eb.nx = nx; eb.ny = ny;
     auto ps = [&](int I, int J) -> double { return psi[(long long)(J - 1) * P + (I - 1)]; };
     double v;
     if (e < g.nu) {

@@ -38,7 +38,7 @@ IBPM_ERR_NONFINITE = -3
 IBPM_ERR_UNSUPPORTED = -4
 IBPM_ERR_NOMEM = -5
 IBPM_PREC_FP64 = 0
-KERNEL_COUNT = 10
+KERNEL_COUNT = 9
 
 _ERRNAMES = {IBPM_ERR_INVALID: "INVALID", IBPM_ERR_CUDA: "CUDA", IBPM_ERR_NONFINITE: "NONFINITE",
              IBPM_ERR_UNSUPPORTED: "UNSUPPORTED", IBPM_ERR_NOMEM: "NOMEM"}

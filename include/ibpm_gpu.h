@@ -155,8 +155,8 @@ int ibpm_host_free(void* p);
  * @elapsed around run_sim!, src/ibpm.jl:71) ---------------------------- */
 
 /* Kernel classes reported by ibpm_profile. */
-#define IBPM_KERNEL_COUNT 10  /* trial_rhs, dst_x, dst_y, coarsify, curl, E_gather,
-                                 binv_gemv, stress, proj_src, level_chain */
+#define IBPM_KERNEL_COUNT 9  /* trial_rhs, dst_x, dst_y, coarsify, curl, E_gather,
+                                binv_gemv, stress, proj_src */
 
 /* Name of kernel class k (0 <= k < IBPM_KERNEL_COUNT). */
 const char* ibpm_kernel_name(int32_t k);
