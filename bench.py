@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the IBPM time step (advance!) on B200.
 
-Workload (BASELINE config 2): a circular cylinder, D = 1 at the origin, with
+Workload: a circular cylinder, D = 1 at the origin, with
 314 boundary points (≈ 1 point per h), at Re = 100 in a uniform freestream
 U = 1 along x; 512×512 cells per level, h = 0.01 (finest domain
 x ∈ [-1, 4.12], y ∈ [-2.56, 2.56]), 5 nested levels, dt = 0.002.  The start
@@ -10,10 +10,12 @@ state is a Gaussian vortex perturbation ω = 1e-3 exp(-r²/0.2²) centred at
 synthetic; nothing is read from a dataset.
 
 Our arm (default): one process per GPU (torchrun for N > 1, replicas of the
-same simulation — the step does not shard), K steps replayed
-from a CUDA graph, each timed by CUDA events on the library's stream with a
-512 MiB L2 flush between steps (outside the timed pairs).  value =
-Σ_ranks nx·ny·mg·K / max_ranks(Σ step times).
+same simulation: one simulation does not shard, every 2-D sine transform
+couples a whole level), K steps replayed from a CUDA graph, each timed by CUDA
+events on the library's stream with a 512 MiB L2 flush between steps (outside
+the timed pairs).  value = Σ_ranks nx·ny·mg·K / max_ranks(Σ step times) of the
+FP32-refined path; the plain FP64 path is timed the same way beside it, with
+the CD/CL differences between the two over the same K steps.
 
 --impl reference: the FP64 CPU restatement of the reference's step
 (oracle/ibpm_ref.py, numpy + scipy.fft with all host threads) on the same
@@ -36,7 +38,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "ibpm.jl_b200", "python"))
 
-# Config 2 of the benchmark definition.
+# The workload: 512x512 cells x 5 levels, h = 0.01, Re = 100, dt = 0.002.
 H = 0.01
 BOUNDARY = (-1.0, 4.12, -2.56, 2.56)
 MG = 5
@@ -44,7 +46,7 @@ RE = 100.0
 DT = 0.002
 NB = 314
 VORTEX = dict(amp=1e-3, width=0.2, x0=1.5, y0=0.1)
-WORKLOAD = ("config 2: cylinder D=1 (314 pts) Re=100, 512x512 cells x 5 levels, h=0.01, dt=0.002, "
+WORKLOAD = ("cylinder D=1 (314 pts) Re=100, 512x512 cells x 5 levels, h=0.01, dt=0.002, "
             "Gaussian-vortex start (1e-3, 0.2, (1.5, 0.1))")
 METRIC = "cell-steps/s"
 FALLBACK_HBM_GBS = 6650.0
@@ -248,12 +250,16 @@ def run_reference(args, d):
 # --------------------------------------------------------------------------
 # Our arm
 # --------------------------------------------------------------------------
-def run_ours(args, d):
+def measure(args, d, precision, sampler=None):
+    """Time one precision mode on the workload: K graph replays (device-timed,
+    L2 flushed between steps), then K advance! calls through the public API
+    with host buffers (e2e, CD/CL history kept), then a per-kernel profile."""
     import ibpm_gpu as G
     dev = d.local
     g = G.make_grid(H, BOUNDARY, MG)
     body = G.make_cylinder(0.5, g.h, 0.0, 0.0, n=NB)
-    prob = G.IBProblem(g, [body], DT, RE, freestream=(1.0, 0.0, 0.0), device=dev, sync_fields=False)
+    prob = G.IBProblem(g, [body], DT, RE, freestream=(1.0, 0.0, 0.0), device=dev, sync_fields=False,
+                       precision=precision, refine_sweeps=1)
     cells = g.nx * g.ny * g.mg
 
     # seeded start state through the public API (pinned host mirror)
@@ -264,70 +270,109 @@ def run_ours(args, d):
     init = {k: np.array(getattr(st, k)) for k in ("Gamma", "q", "q0", "psi")}
     init_nl = [np.array(a) for a in st.nonlin]
 
-    # warm-up (graph capture + first replays)
-    G.bench_steps(prob, max(args.warmup, 3), flush_l2=True)
+    G.bench_steps(prob, max(args.warmup, 3), flush_l2=True)   # graph capture + first replays
 
-    # ---- device-timed region
     d.barrier()
-    sampler = ClockSampler(dev)
-    sampler.start()
+    if sampler:
+        sampler.start()
     step_ms = G.bench_steps(prob, args.steps, flush_l2=True)
-    clocks = sampler.stop()
-    total_ms = float(np.sum(step_ms))
-    max_ms = d.max(total_ms)
-    value = d.world * cells * args.steps / (max_ms / 1e3)
+    clocks = sampler.stop() if sampler else None
+    total_ms = d.max(float(np.sum(step_ms)))
 
-    # ---- end to end through the public API with host buffers: upload the
-    # state from pinned memory, K calls of advance! (each reads CD/CL back),
-    # download the state.
+    # end to end: upload the state from pinned memory, K advance! calls (each
+    # returns CD/CL to the host), download the state
     for k, v in init.items():
         getattr(st, k)[...] = v
     st.nonlin[0][...] = init_nl[0]
     st.nonlin[1][...] = init_nl[1]
     prob.sync()
+    cd = np.zeros(args.steps)
+    cl = np.zeros(args.steps)
     d.barrier()
     t0 = time.perf_counter()
     G.push_state(st, prob)
     for k in range(args.steps):
-        G.advance(st, prob, k * DT, nsteps=1)
+        c, l = G.advance(st, prob, k * DT, nsteps=1)
+        cd[k], cl[k] = c[0, 0], l[0, 0]
     G.pull_state(st, prob)
     e2e_s = d.max(time.perf_counter() - t0)
     state_bytes = 8 * (st.Gamma.size * 4 + st.q.size * 2 + st.Fb.size)
-    e2e = {"value": d.world * cells * args.steps / e2e_s, "unit": METRIC,
-           "h2d_bytes_per_step": state_bytes / args.steps,
-           "d2h_bytes_per_step": (state_bytes + 16 * len(prob.bodies) * args.steps) / args.steps,
-           "note": "state uploaded once and downloaded once (amortised over the K steps); each "
-                   "advance! call returns CD/CL to the host"}
 
-    # ---- per-kernel profile (eager launches between CUDA events, L2 flushed per step)
     prof = G.profile_steps(prob, 4, flush_l2=True)
     lps = G.launches_per_step(prob)
+    nf = prob.nf
+    prob.close()
+    return dict(cells=cells, nf=nf, g=g, total_ms=total_ms, e2e_s=e2e_s, cd=cd, cl=cl, prof=prof, lps=lps,
+                clocks=clocks, state_bytes=state_bytes, bodies=1)
+
+
+def run_ours(args, d):
+    K = args.steps
+    sampler = ClockSampler(d.local)
+    r32 = measure(args, d, "fp32_refined", sampler)
+    r64 = measure(args, d, "fp64")
+    g, cells = r32["g"], r32["cells"]
+    value = d.world * cells * K / (r32["total_ms"] / 1e3)
+    value64 = d.world * cells * K / (r64["total_ms"] / 1e3)
+
+    def e2e_of(r):
+        return {"value": d.world * cells * K / r["e2e_s"], "unit": METRIC,
+                "h2d_bytes_per_step": r["state_bytes"] / K,
+                "d2h_bytes_per_step": (r["state_bytes"] + 16 * r["bodies"] * K) / K,
+                "note": "state uploaded once and downloaded once (amortised over the K steps); each "
+                        "advance! call returns CD/CL to the host"}
+
+    prof = r32["prof"]
     dom = max(prof, key=lambda k: prof[k][0])
     dms, dbytes, dcalls = prof[dom]
     peak, peak_kind = read_peaks()
     achieved = dbytes / (dms / 1e3) / 1e9
-    traffic = read_traffic(dom)
-    bstep = step_bytes_model(g.nx, g.ny, g.mg, prob.nf)
-    step_s = (total_ms / 1e3) / args.steps
+    step_s = (r32["total_ms"] / 1e3) / K
+    step_s64 = (r64["total_ms"] / 1e3) / K
+    launch_bytes = sum(v[1] for v in prof.values()) / 4.0
+    launch_bytes64 = sum(v[1] for v in r64["prof"].values()) / 4.0
+    bstep64 = step_bytes_model(g.nx, g.ny, g.mg, r64["nf"])
+    cd32, cd64, cl32, cl64 = r32["cd"], r64["cd"], r32["cl"], r64["cl"]
+    accuracy = {
+        "reference": "the FP64 GPU path on the same start state (it matches the FP64 oracle to 1e-10)",
+        "steps": K,
+        "cd_max_rel_err": float(np.max(np.abs(cd32 - cd64) / np.abs(cd64))),
+        "cd_max_rel_err_after_10_steps": float(np.max(np.abs(cd32[10:] - cd64[10:]) / np.abs(cd64[10:])))
+        if K > 10 else None,
+        "cl_max_abs_err": float(np.max(np.abs(cl32 - cl64))),
+        "cl_err_rel_to_max_cl": float(np.max(np.abs(cl32 - cl64)) / np.max(np.abs(cl64))),
+        "cl_err_rel_to_max_cd": float(np.max(np.abs(cl32 - cl64)) / np.max(np.abs(cd64))),
+    }
     out = {
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": d.world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "precision": "fp64 plain", "l2": "flushed between steps "
-                   "(512 MiB write outside the timed event pairs)", "parallelism": "replicas x%d" % d.world,
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": d.world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": r32["total_ms"] / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 transforms / f64 state, residuals, forces",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": "fp32_refined (1 FP64-residual sweep per Poisson solve, "
+                   "warm start; FP64 trial solve)", "l2": "flushed between steps (512 MiB write outside the "
+                   "timed event pairs)", "parallelism": "replicas x%d" % d.world,
                    "graph": "one CUDA graph replay per step"},
-        "e2e": e2e,
-        "gpu_launches": lps * args.steps,
+        "e2e": e2e_of(r32),
+        "gpu_launches": r32["lps"] * K,
+        "fp64_plain": {"value": value64, "ms_per_step": r64["total_ms"] / K, "e2e": e2e_of(r64),
+                       "gpu_launches": r64["lps"] * K,
+                       "step_roofline": {"model_bytes_per_step": bstep64, "achieved_GBs": bstep64 / step_s64 / 1e9,
+                                         "frac": bstep64 / step_s64 / 1e9 / peak,
+                                         "launch_bytes_per_step": launch_bytes64},
+                       "kernels": {k: {"ms_per_step": v[0] / 4.0, "launches_per_step": v[2] / 4.0}
+                                   for k, v in r64["prof"].items()}},
+        "refined_vs_fp64": value / value64,
+        "accuracy": accuracy,
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
                      if peak_kind == "measured" else "fallback 6.65 TB/s",
-                     "traffic": traffic, "launches_per_step": dcalls / 4.0,
+                     "traffic": read_traffic(dom), "launches_per_step": dcalls / 4.0,
                      "bytes_per_launch": dbytes / dcalls, "avg_launch_us": 1e3 * dms / dcalls},
-        "step_roofline": {"model_bytes_per_step": bstep, "achieved_GBs": bstep / step_s / 1e9,
-                          "frac": bstep / step_s / 1e9 / peak},
+        "step_roofline": {"launch_bytes_per_step": launch_bytes, "achieved_GBs": launch_bytes / step_s / 1e9,
+                          "frac": launch_bytes / step_s / 1e9 / peak},
         "kernels": {k: {"ms_per_step": v[0] / 4.0, "GBs": (v[1] / (v[0] / 1e3) / 1e9) if v[0] > 0 else 0,
                         "launches_per_step": v[2] / 4.0} for k, v in prof.items()},
-        "clocks": clocks,
+        "clocks": r32["clocks"],
     }
     if d.world == 1 and not args.no_cpu:
         try:
@@ -338,7 +383,6 @@ def run_ours(args, d):
                                              "matrix of the same size" % (args.cpu_steps, secs)}
         except Exception as e:  # the CPU leg is a reported baseline only
             out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
-    prob.close()
     if d.rank == 0:
         print(json.dumps(out))
     return 0

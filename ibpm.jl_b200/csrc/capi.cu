@@ -52,7 +52,14 @@ struct ibpm_handle {
     double* hist = nullptr; int hist_cap = 0;
     int* counter = nullptr; int* status = nullptr;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    cudaGraphExec_t gcold[2] = {nullptr, nullptr};  // FP32_REFINED: first step after a state change
     bool graphs_ready = false;
+    // FP32_REFINED
+    int prec = IBPM_PREC_FP64;
+    int sweeps = 1;                        // correction sweeps per solve
+    int cold = 2;                          // steps left that lack good initial guesses
+    float* T32 = nullptr;                  // mg slabs of FP32 transform scratch
+    double* Pp = nullptr;                  // A⁻¹C'E'F̃b of the previous step (level 1)
     // measurement
     int launches = 0;                      // kernel launches enqueued (counted always)
     bool prof_on = false;                  // eager profiling: events around every launch
@@ -139,9 +146,10 @@ static SlabMap levmap(const Geom& g, int lev0, int nlev, long long bstride = 0) 
     return m;
 }
 
-static SpecParams spec(const ibpm_handle* h, int mode) {
+static SpecParams spec(const ibpm_handle* h, int mode, int f32 = 0) {
     SpecParams sp;
     sp.mode = mode;
+    sp.f32 = f32;
     sp.scale = 1.0 / (4.0 * h->g.nx * h->g.ny);  // laplacian.jl:194
     sp.dt = h->dt;
     for (int l = 0; l < 8; ++l) {
@@ -174,6 +182,27 @@ static int poisson(ibpm_handle* h, const double* b, SlabMap bmap, double* tmp, S
     return IBPM_OK;
 }
 
+static double c_lap(const ibpm_handle* h, int lev) {
+    const double hc = h->h * std::ldexp(1.0, lev);
+    return h->dt / (2.0 * h->Re * (hc * hc));  // laplacian.jl:225
+}
+
+static RhsArgs rhs_args(const ibpm_handle* h, int p) {
+    const Geom& g = h->g;
+    RhsArgs ra{};
+    ra.G = h->G[p]; ra.Gmap = levmap(g, 0, g.mg); ra.q = h->q;
+    ra.Nprev = h->Nl[p]; ra.Nnew = h->Nl[p ^ 1];
+    for (int l = 0; l < g.mg; ++l) {
+        const double hc = h->h * std::ldexp(1.0, l);
+        ra.q0x[l] = h->q0x[l]; ra.q0y[l] = h->q0y[l];
+        ra.fac_bc[l] = 0.25 * h->dt / (h->Re * (hc * hc));
+        ra.c_lap[l] = c_lap(h, l);
+        ra.nl_scale[l] = 1.0 / (4.0 * (hc * hc));
+    }
+    ra.b1dt = h->beta[0] * h->dt; ra.b2dt = h->beta[1] * h->dt; ra.mg = g.mg;
+    return ra;
+}
+
 // vort2flux! (curl.jl:411-443) on `nbatch` independent fields G (slab-major,
 // batch stride bstride), level by level as the reference: coarsify chain,
 // Δ⁻¹ solves from the coarsest level inwards with the edge values of the next
@@ -203,23 +232,13 @@ static int vort2flux(ibpm_handle* h, double* G, double* psi, long long bstride, 
 }
 
 // One step, reading the state from parity p and leaving it in parity p^1.
-static int enqueue_step(ibpm_handle* h, int p) {
+static int enqueue_step_fp64(ibpm_handle* h, int p) {
     const Geom& g = h->g;
     const int mg = g.mg;
-    double* Gold = h->G[p];
     double* Gnew = h->G[p ^ 1];
     // --- get_trial_state! (timestepping.jl:86-129)
-    RhsArgs ra{};
-    ra.G = Gold; ra.Gmap = levmap(g, 0, mg); ra.q = h->q;
-    ra.Nprev = h->Nl[p]; ra.Nnew = h->Nl[p ^ 1]; ra.rhs = h->rhs;
-    for (int l = 0; l < mg; ++l) {
-        const double hc = h->h * std::ldexp(1.0, l);
-        ra.q0x[l] = h->q0x[l]; ra.q0y[l] = h->q0y[l];
-        ra.fac_bc[l] = 0.25 * h->dt / (h->Re * (hc * hc));
-        ra.c_lap[l] = h->dt / (2.0 * h->Re * (hc * hc));
-        ra.nl_scale[l] = 1.0 / (4.0 * (hc * hc));
-    }
-    ra.b1dt = h->beta[0] * h->dt; ra.b2dt = h->beta[1] * h->dt; ra.mg = mg;
+    RhsArgs ra = rhs_args(h, p);
+    ra.rhs = h->rhs;
     LAUNCH(K_RHS, 8.0 * (4.0 * g.n1 * g.n2 + g.nq) * mg, launch_trial_rhs(g, ra, h->st));
     SlabMap all = levmap(g, 0, mg);
     int rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg, SPEC_AINV, XEMIT_STORE);
@@ -238,6 +257,103 @@ static int enqueue_step(ibpm_handle* h, int p) {
     if (rc) return rc;
     // --- vort2flux!(state.ψ, state.q, state.Γ) (timestepping.jl:64)
     return vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->q, 0, 0, mg);
+}
+
+// ---------------------------------------------------------------------------
+// FP32-refined step.  Each Poisson-type solve x = M⁻¹ b (M = L for Δ⁻¹,
+// I + cL for A⁻¹, L x = 4x − Σ neighbours) is one or more sweeps of
+//     x ← x + S32(b − M x)
+// with the residual formed in FP64 inside the first x-pass and the correction
+// S32 = the DST-I solve in FP32 (x-pass, y-pass, x-pass), starting from the
+// previous solution of the same system (ψ of the previous vort2flux, the
+// previous projection).  The error left is the FP32 error of the correction
+// alone, i.e. relative to the change of x since its previous solution.
+// The trial solve Γs = A⁻¹ rhs stays FP64: near the wall its change per step
+// is O(Γ), and the force F = E(qs + q0) is a difference that cancels to
+// O(dt)·|q0| there, so an FP32 error in Γs − Γ reaches CD amplified by
+// |q0|/|F| (≈ 500 at dt = 0.002).  A second FP32 sweep would fix it at three
+// more launches, which cost more than the FP64 solve of all levels at once.
+// ---------------------------------------------------------------------------
+static int correction32(ibpm_handle* h, int load, const double* b, const double* coarse, double* xg, double cA,
+                        int lev, int emit, double* out) {
+    const Geom& g = h->g;
+    const long long bs = g.S * g.mg;
+    SlabMap m = levmap(g, lev, 1, bs);
+    const double slab = (double)g.n1 * g.n2;
+    XPassArgs a{};
+    a.in = b; a.out = h->T32; a.in_map = m; a.out_map = m;
+    a.coarse = coarse; a.coarse_map = levmap(g, lev + 1, 1, bs);
+    a.aux = xg; a.aux_map = m; a.cA = cA;
+    a.nslabs = 1; a.line0 = 0; a.line1 = g.n2; a.load = load; a.emit = XEMIT_F32;
+    LAUNCH(K_DSTX, slab * (8.0 + 8.0 + 4.0), launch_dst_x(g, h->px, a, h->st));
+    LAUNCH(K_DSTY, slab * 8.0,
+           launch_dst_y(g, h->py, h->px, h->T32, m, 1, spec(h, load == XLOAD_RES_A ? SPEC_AINV : SPEC_DELTA, 1),
+                        h->st));
+    XPassArgs c{};
+    c.in = h->T32; c.out = out; c.in_map = m; c.out_map = m;
+    c.aux = xg; c.aux_map = m;
+    c.nslabs = 1; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_F32; c.emit = emit;
+    LAUNCH(K_DSTX, slab * (4.0 + 16.0 + (emit == XEMIT_ACC_SUB ? 16.0 : 0.0)), launch_dst_x(g, h->px, c, h->st));
+    return IBPM_OK;
+}
+
+// vort2flux! with every level's Δ⁻¹ solve refined from the ψ in h->psi.
+static int vort2flux_refined(ibpm_handle* h, double* G, int nsw, double* q, int qnlev) {
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    const long long bs = g.S * mg;
+    for (int lev = 1; lev < mg; ++lev)
+        LAUNCH(K_COARSIFY, 8.0 * 1.25 * g.n1 * g.n2,
+               launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), 1, h->st));
+    for (int lev = mg - 1; lev >= 0; --lev) {
+        const double* coarse = (lev < mg - 1) ? h->psi : nullptr;
+        for (int s = 0; s < nsw; ++s) {
+            int rc = correction32(h, XLOAD_RES_LAP, G, coarse, h->psi, 0.0, lev, XEMIT_ADD, h->psi);
+            if (rc) return rc;
+        }
+    }
+    CurlArgs ca{};
+    ca.psi = h->psi; ca.psi_map = levmap(g, 0, qnlev, bs);
+    ca.coarse = h->psi; ca.coarse_map = levmap(g, 1, qnlev, bs);
+    ca.q = q; ca.q_bstride = 0; ca.q_lstride = g.nq; ca.q_lev0 = 0;
+    ca.nlev = qnlev; ca.nbatch = 1; ca.mg = mg;
+    LAUNCH(K_CURL, 8.0 * ((double)g.n1 * g.n2 + g.nq) * qnlev, launch_curl(g, ca, h->st));
+    return IBPM_OK;
+}
+
+static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    double* Gnew = h->G[p ^ 1];
+    const long long bs = g.S * mg;
+    // --- get_trial_state! (FP64 trial solve: see the note above)
+    RhsArgs ra = rhs_args(h, p);
+    ra.rhs = h->rhs;
+    LAUNCH(K_RHS, 8.0 * (4.0 * g.n1 * g.n2 + g.nq) * mg, launch_trial_rhs(g, ra, h->st));
+    SlabMap all = levmap(g, 0, mg, bs);
+    int rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg, SPEC_AINV, XEMIT_STORE);
+    if (rc) return rc;
+    rc = vort2flux_refined(h, Gnew, nsw, h->qs, 1);  // only the level-1 trial flux is read
+    if (rc) return rc;
+    // --- boundary_forces! and update_stress! (FP64)
+    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st));
+    LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
+    LAUNCH(K_STRESS, 8.0 * 3 * h->nb,
+           launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
+    // --- project_circ!: P = A⁻¹ C'E' F̃b refined from the previous P; Γ[1] −= P
+    LAUNCH(K_SRC, 8.0 * 4 * 169 * h->nf, launch_proj_src(g, h->body, h->Fb, h->Gsrc, h->st));
+    for (int s = 0; s < nsw; ++s) {
+        rc = correction32(h, XLOAD_RES_A, h->Gsrc, nullptr, h->Pp, c_lap(h, 0), 0,
+                          s + 1 < nsw ? XEMIT_ADD : XEMIT_ACC_SUB, s + 1 < nsw ? h->Pp : Gnew);
+        if (rc) return rc;
+    }
+    // --- vort2flux!(state.ψ, state.q, state.Γ)
+    return vort2flux_refined(h, Gnew, nsw, h->q, mg);
+}
+
+static int enqueue_step(ibpm_handle* h, int p, bool cold = false) {
+    if (h->prec == IBPM_PREC_FP32_REFINED) return enqueue_step_refined(h, p, cold ? h->sweeps + 1 : h->sweeps);
+    return enqueue_step_fp64(h, p);
 }
 
 // ---------------------------------------------------------------------------
@@ -374,7 +490,12 @@ static int build_binv(ibpm_handle* h) {
 
 static void free_handle(ibpm_handle* h) {
     if (!h) return;
-    for (int p = 0; p < 2; ++p) if (h->gexec[p]) cudaGraphExecDestroy(h->gexec[p]);
+    for (int p = 0; p < 2; ++p) {
+        if (h->gexec[p]) cudaGraphExecDestroy(h->gexec[p]);
+        if (h->gcold[p]) cudaGraphExecDestroy(h->gcold[p]);
+    }
+    if (h->T32) cudaFree(h->T32);
+    if (h->Pp) cudaFree(h->Pp);
     void* ptrs[] = {h->G[0], h->G[1], h->Nl[0], h->Nl[1], h->psi, h->q, h->qs, h->rhs, h->Gsrc, h->F, h->Fb,
                     h->Binv, h->nonlin1_shadow, h->d_xb, h->d_ds, h->d_bidx, h->d_w, h->d_body_start,
                     h->d_src_pts, h->d_src_rows, h->d_et_ptr, h->d_et_k, h->d_et_w, h->hist, h->counter, h->status};
@@ -403,7 +524,11 @@ static int create_impl(ibpm_handle* h, const ibpm_problem_desc* d) {
     if (!(d->h > 0) || !(d->dt > 0) || !(d->Re > 0)) return fail(h, IBPM_ERR_INVALID, "h, dt and Re must be positive");
     if (d->nb < 1 || d->nbodies < 1 || !d->xb || !d->ds || !d->body_npts)
         return fail(h, IBPM_ERR_INVALID, "at least one body with one point is required");
-    if (d->precision != IBPM_PREC_FP64) return fail(h, IBPM_ERR_UNSUPPORTED, "only IBPM_PREC_FP64 is built");
+    if (d->precision != IBPM_PREC_FP64 && d->precision != IBPM_PREC_FP32_REFINED)
+        return fail(h, IBPM_ERR_INVALID, "precision must be IBPM_PREC_FP64 or IBPM_PREC_FP32_REFINED");
+    if (d->refine_sweeps < 0 || d->refine_sweeps > 8) return fail(h, IBPM_ERR_INVALID, "refine_sweeps must be in 0..8");
+    h->prec = d->precision;
+    h->sweeps = std::max(1, (int)d->refine_sweeps);
     int tot = 0;
     for (int j = 0; j < d->nbodies; ++j) {
         if (d->body_npts[j] < 1) return fail(h, IBPM_ERR_INVALID, "every body needs at least one point");
@@ -452,6 +577,11 @@ static int create_impl(ibpm_handle* h, const ibpm_problem_desc* d) {
     CK(cudaMemsetAsync(h->Gsrc, 0, sizeof(double) * g.S, h->st));
     CK(cudaMemsetAsync(h->Fb, 0, sizeof(double) * h->nf, h->st));
     CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
+    if (h->prec == IBPM_PREC_FP32_REFINED) {
+        if ((rc = dalloc(h, &h->T32, slabs)) || (rc = dalloc(h, &h->Pp, g.S))) return rc;
+        CK(cudaMemsetAsync(h->T32, 0, sizeof(float) * slabs, h->st));
+        CK(cudaMemsetAsync(h->Pp, 0, sizeof(double) * g.S, h->st));
+    }
     if ((rc = build_coupling(h, d))) return rc;
     if ((rc = build_binv(h))) return rc;
     CK(cudaStreamSynchronize(h->st));
@@ -533,6 +663,14 @@ extern "C" int ibpm_set_state(ibpm_handle* h, const double* Gamma, const double*
     }
     if (Fb) CK(cudaMemcpyAsync(h->Fb, Fb, sizeof(double) * h->nf, cudaMemcpyHostToDevice, h->st));
     CK(cudaStreamSynchronize(h->st));
+    if (Gamma || psi) {
+        // the refined mode's hidden initial guess of the projection solve is
+        // cleared, so results depend only on the state given (ψ is the other
+        // guess; it is part of the state)
+        h->cold = 2;
+        if (h->Pp) CK(cudaMemsetAsync(h->Pp, 0, sizeof(double) * g.S, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    }
     return IBPM_OK;
 }
 
@@ -567,20 +705,37 @@ static int ensure_graphs(ibpm_handle* h, int cap) {
         if (rc) return rc;
         h->hist_cap = cap;
     }
-    for (int p = 0; p < 2; ++p) {
-        if (h->gexec[p]) { cudaGraphExecDestroy(h->gexec[p]); h->gexec[p] = nullptr; }
-        cudaGraph_t graph;
-        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-        int rc = enqueue_step(h, p);
-        cudaError_t e = cudaStreamEndCapture(h->st, &graph);
-        if (rc) return rc;
-        if (e != cudaSuccess) return fail(h, IBPM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&h->gexec[p], graph, 0);
-        cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return fail(h, IBPM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-    }
+    const int nkind = h->prec == IBPM_PREC_FP32_REFINED ? 2 : 1;
+    for (int kind = 0; kind < nkind; ++kind)
+        for (int p = 0; p < 2; ++p) {
+            cudaGraphExec_t& ge = kind ? h->gcold[p] : h->gexec[p];
+            if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+            cudaGraph_t graph;
+            CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+            int rc = enqueue_step(h, p, kind == 1);
+            cudaError_t e = cudaStreamEndCapture(h->st, &graph);
+            if (rc) return rc;
+            if (e != cudaSuccess) return fail(h, IBPM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&ge, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess)
+                return fail(h, IBPM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
     h->graphs_ready = true;
     return IBPM_OK;
+}
+
+// Queue one step from the current parity.  In FP32_REFINED mode the first two
+// steps after create or set_state run one more correction sweep per solve:
+// the initial guesses of the first (ψ, the previous projection) may not belong
+// to the state, and those of the second come from a step whose changes can be
+// orders of magnitude larger (an impulsive start).
+static cudaError_t launch_step(ibpm_handle* h) {
+    cudaGraphExec_t ge = (h->cold > 0 && h->gcold[h->cur]) ? h->gcold[h->cur] : h->gexec[h->cur];
+    if (h->cold > 0) --h->cold;
+    const cudaError_t e = cudaGraphLaunch(ge, h->st);
+    h->cur ^= 1;
+    return e;
 }
 
 extern "C" int ibpm_advance(ibpm_handle* h, double t, int32_t nsteps, double* CD_out, double* CL_out) {
@@ -597,10 +752,7 @@ extern "C" int ibpm_advance(ibpm_handle* h, double t, int32_t nsteps, double* CD
     while (done < nsteps) {
         const int n = std::min(h->hist_cap, nsteps - done);
         CK(cudaMemsetAsync(h->counter, 0, sizeof(int), h->st));
-        for (int s = 0; s < n; ++s) {
-            CK(cudaGraphLaunch(h->gexec[h->cur], h->st));
-            h->cur ^= 1;
-        }
+        for (int s = 0; s < n; ++s) CK(launch_step(h));
         h->nonlin1_valid = false;
         if (CD_out || CL_out) {
             hb.resize((size_t)n * 2 * h->nbodies);
@@ -681,9 +833,8 @@ extern "C" int ibpm_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, doub
         for (int s = 0; s < n; ++s) {
             if (flush_l2) CK(cudaMemsetAsync(h->flush_buf, (done + s) & 0xff, h->flush_bytes, h->st));
             CK(cudaEventRecord(ev[2 * (done + s)], h->st));
-            CK(cudaGraphLaunch(h->gexec[h->cur], h->st));
+            CK(launch_step(h));
             CK(cudaEventRecord(ev[2 * (done + s) + 1], h->st));
-            h->cur ^= 1;
         }
         done += n;
     }

@@ -7,40 +7,40 @@
 namespace ibpm {
 
 cudaError_t dst_x_32(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_32(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_32(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_32();
 cudaError_t dst_x_64(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_64(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_64(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_64();
 cudaError_t dst_x_128(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_128(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_128(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_128();
 cudaError_t dst_x_192(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_192(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_192(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_192();
 cudaError_t dst_x_200(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_200(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_200(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_200();
 cudaError_t dst_x_256(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_256(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_256(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_256();
 cudaError_t dst_x_384(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_384(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_384(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_384();
 cudaError_t dst_x_400(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_400(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_400(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_400();
 cudaError_t dst_x_512(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_512(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_512(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_512();
 cudaError_t dst_x_768(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_768(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_768(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_768();
 cudaError_t dst_x_1024(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_1024(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_1024(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_1024();
 cudaError_t dst_x_2048(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_2048(const Geom&, const DstPlan&, const DstPlan&, double*, SlabMap, int, const SpecParams&, cudaStream_t);
+cudaError_t dst_y_2048(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
 cudaError_t dst_attr_2048();
 
 // Supported transform lengths N = nx or ny: 32, 64, 128, 192, 200, 256, 384, 400, 512, 768, 1024, 2048.
@@ -82,17 +82,27 @@ static StageDesc stage_desc(int N) {
     return d;
 }
 
-// Table block of 4N doubles: cos(π(t+1)/N) at [0, N), sin(πt/N) at [N, 2N),
-// stage twiddles exp(+2πi k r/(Ns R)) (complex) from 2N on.
+// Table block of dst_table_doubles(N) = 6N doubles:
+//   FP64: cos(π(t+1)/N) at [0, N), sin(πt/N) at [N, 2N), stage twiddles
+//         exp(+2πi k r/(Ns R)) (complex) from 2N on (≤ N of them);
+//   FP32 (from double 4N on, as floats): 4 sin²(π(t+1)/(2N)) at [0, N),
+//         sin(πt/N) at [N, 2N), the twiddles (complex) from 2N on;
+// each FP32 entry is the FP64 value rounded once.
 __global__ void dst_tables_kernel(int N, double* base, StageDesc d, int ntw) {
     double* c = base;
     double* s = base + N;
     double2* W = reinterpret_cast<double2*>(base + 2 * N);
+    float* a32 = reinterpret_cast<float*>(base + 4 * N);
+    float* s32 = a32 + N;
+    float2* W32 = reinterpret_cast<float2*>(a32 + 2 * N);
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
         s[t] = sinpi((double)t / (double)N);
+        s32[t] = (float)s[t];
         // evaluated as the reference forms the Laplacian eigenvalues:
         // cos.(π*(1:(n-1))/n) (laplacian.jl:173)
         c[t] = (t < N - 1) ? cos(M_PI * (double)(t + 1) / (double)N) : 0.0;
+        const double h = sinpi((double)(t + 1) / (2.0 * (double)N));
+        a32[t] = (t < N - 1) ? (float)(4.0 * h * h) : 0.0f;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntw; i += gridDim.x * blockDim.x) {
         int st = 0;
@@ -102,6 +112,7 @@ __global__ void dst_tables_kernel(int N, double* base, StageDesc d, int ntw) {
         double sn, cs;
         sincospi(2.0 * (double)(k * r) / (double)(d.ns[st] * d.r[st]), &sn, &cs);
         W[i] = make_double2(cs, sn);
+        W32[i] = make_float2((float)cs, (float)sn);
     }
 }
 
@@ -118,6 +129,9 @@ DstPlan dst_plan_at(double* base, int N) {
     p.c = base;
     p.s = base + N;
     p.W = reinterpret_cast<double2*>(base + 2 * N);
+    p.a32 = reinterpret_cast<float*>(base + 4 * N);
+    p.s32 = p.a32 + N;
+    p.W32 = reinterpret_cast<float2*>(p.a32 + 2 * N);
     return p;
 }
 
@@ -126,7 +140,7 @@ int dst_plan_create(DstPlan* p, int N, cudaStream_t st) {
     p->W = nullptr; p->s = nullptr; p->c = nullptr;
     if (!dst_supported(N)) return -1;
     double* base = nullptr;
-    if (cudaMalloc(&base, sizeof(double) * 4 * N) != cudaSuccess) return -2;
+    if (cudaMalloc(&base, sizeof(double) * dst_table_doubles(N)) != cudaSuccess) return -2;
     *p = dst_plan_at(base, N);
     if (dst_tables_build(N, base, st) != cudaSuccess) return -2;
     if (dst_init_attributes(N) != cudaSuccess) return -2;
@@ -136,6 +150,7 @@ int dst_plan_create(DstPlan* p, int N, cudaStream_t st) {
 void dst_plan_destroy(DstPlan* p) {
     if (p->c) cudaFree(p->c);  // the block starts at c
     p->W = nullptr; p->s = nullptr; p->c = nullptr;
+    p->W32 = nullptr; p->s32 = nullptr; p->a32 = nullptr;
 }
 
 // Opt the kernels of length N into large dynamic shared memory (before any
@@ -176,7 +191,7 @@ cudaError_t launch_dst_x(const Geom& g, const DstPlan& px, const XPassArgs& a, c
     }
 }
 
-cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px, double* data, SlabMap map, int nslabs,
+cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px, void* data, SlabMap map, int nslabs,
                          const SpecParams& sp, cudaStream_t st) {
     if (nslabs <= 0) return cudaSuccess;
     switch (py.N) {

@@ -22,6 +22,8 @@
 // free of bank conflicts.
 #pragma once
 
+#include <type_traits>
+
 #include "ibpm_internal.cuh"
 
 namespace ibpm {
@@ -73,77 +75,105 @@ __host__ __device__ constexpr int ct_tw_count(int N) { return ct_tw_off(N, ct_ns
 // Groups (line pairs) per CTA: 128-thread CTAs for N <= 1024.
 __host__ __device__ constexpr int ct_groups(int N) { return ct_tp(N) >= 128 ? 1 : 128 / ct_tp(N); }
 
+// Complex arithmetic for both precisions (V = double2 or float2).
+template <class T> struct cplx_of;
+template <> struct cplx_of<double> { using type = double2; };
+template <> struct cplx_of<float> { using type = float2; };
+template <class T> using cplx_t = typename cplx_of<T>::type;
+
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 __device__ __forceinline__ double2 cmuli(double2 a) { return make_double2(-a.y, a.x); }  // i·a
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmuli(float2 a) { return make_float2(-a.y, a.x); }
+template <class V, class T> __device__ __forceinline__ V cmk(T a, T b) { return V{a, b}; }
 
 // Small DFTs with the +2πi sign: V_b = Σ_a v_a e^{+2πi ab/R}.
-template <int R> __device__ __forceinline__ void dft(double2* v);
+template <int R, class T> struct dft_t;
 
-template <> __device__ __forceinline__ void dft<2>(double2* v) {
-    const double2 t = v[0];
-    v[0] = cadd(t, v[1]);
-    v[1] = csub(t, v[1]);
-}
-
-template <> __device__ __forceinline__ void dft<3>(double2* v) {
-    const double h3 = 0.86602540378443864676;  // √3 / 2
-    const double2 s = cadd(v[1], v[2]);
-    const double2 d = csub(v[1], v[2]);
-    const double2 a = make_double2(v[0].x - 0.5 * s.x, v[0].y - 0.5 * s.y);
-    const double2 b = make_double2(-h3 * d.y, h3 * d.x);  // i (√3/2) d
-    v[0] = cadd(v[0], s);
-    v[1] = cadd(a, b);
-    v[2] = csub(a, b);
-}
-
-template <> __device__ __forceinline__ void dft<4>(double2* v) {
-    const double2 t0 = cadd(v[0], v[2]);
-    const double2 t1 = csub(v[0], v[2]);
-    const double2 t2 = cadd(v[1], v[3]);
-    const double2 t3 = cmuli(csub(v[1], v[3]));
-    v[0] = cadd(t0, t2);
-    v[2] = csub(t0, t2);
-    v[1] = cadd(t1, t3);
-    v[3] = csub(t1, t3);
-}
-
-template <> __device__ __forceinline__ void dft<5>(double2* v) {
-    const double c1 = 0.30901699437494742410;   // cos(2π/5)
-    const double c2 = -0.80901699437494742410;  // cos(4π/5)
-    const double s1 = 0.95105651629515357212;   // sin(2π/5)
-    const double s2 = 0.58778525229247312917;   // sin(4π/5)
-    const double2 s14 = cadd(v[1], v[4]), d14 = csub(v[1], v[4]);
-    const double2 s23 = cadd(v[2], v[3]), d23 = csub(v[2], v[3]);
-    const double2 a1 = make_double2(v[0].x + c1 * s14.x + c2 * s23.x, v[0].y + c1 * s14.y + c2 * s23.y);
-    const double2 a2 = make_double2(v[0].x + c2 * s14.x + c1 * s23.x, v[0].y + c2 * s14.y + c1 * s23.y);
-    const double2 b1 = cmuli(make_double2(s1 * d14.x + s2 * d23.x, s1 * d14.y + s2 * d23.y));
-    const double2 b2 = cmuli(make_double2(s2 * d14.x - s1 * d23.x, s2 * d14.y - s1 * d23.y));
-    v[0] = cadd(v[0], cadd(s14, s23));
-    v[1] = cadd(a1, b1);
-    v[4] = csub(a1, b1);
-    v[2] = cadd(a2, b2);
-    v[3] = csub(a2, b2);
-}
-
-template <> __device__ __forceinline__ void dft<8>(double2* v) {
-    const double r2 = 0.70710678118654752440;  // √2 / 2
-    double2 e[4] = {v[0], v[2], v[4], v[6]};
-    double2 o[4] = {v[1], v[3], v[5], v[7]};
-    dft<4>(e);
-    dft<4>(o);
-    o[1] = make_double2(r2 * (o[1].x - o[1].y), r2 * (o[1].x + o[1].y));    // × e^{iπ/4}
-    o[2] = cmuli(o[2]);                                                    // × i
-    o[3] = make_double2(-r2 * (o[3].x + o[3].y), r2 * (o[3].x - o[3].y));  // × e^{3iπ/4}
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        v[b] = cadd(e[b], o[b]);
-        v[b + 4] = csub(e[b], o[b]);
+template <class T> struct dft_t<2, T> {
+    using V = cplx_t<T>;
+    __device__ __forceinline__ static void run(V* v) {
+        const V t = v[0];
+        v[0] = cadd(t, v[1]);
+        v[1] = csub(t, v[1]);
     }
-}
+};
+
+template <class T> struct dft_t<3, T> {
+    using V = cplx_t<T>;
+    __device__ __forceinline__ static void run(V* v) {
+        const T h3 = T(0.86602540378443864676);  // √3 / 2
+        const V s = cadd(v[1], v[2]);
+        const V d = csub(v[1], v[2]);
+        const V a = V{v[0].x - T(0.5) * s.x, v[0].y - T(0.5) * s.y};
+        const V b = V{-h3 * d.y, h3 * d.x};  // i (√3/2) d
+        v[0] = cadd(v[0], s);
+        v[1] = cadd(a, b);
+        v[2] = csub(a, b);
+    }
+};
+
+template <class T> struct dft_t<4, T> {
+    using V = cplx_t<T>;
+    __device__ __forceinline__ static void run(V* v) {
+        const V t0 = cadd(v[0], v[2]);
+        const V t1 = csub(v[0], v[2]);
+        const V t2 = cadd(v[1], v[3]);
+        const V t3 = cmuli(csub(v[1], v[3]));
+        v[0] = cadd(t0, t2);
+        v[2] = csub(t0, t2);
+        v[1] = cadd(t1, t3);
+        v[3] = csub(t1, t3);
+    }
+};
+
+template <class T> struct dft_t<5, T> {
+    using V = cplx_t<T>;
+    __device__ __forceinline__ static void run(V* v) {
+        const T c1 = T(0.30901699437494742410);   // cos(2π/5)
+        const T c2 = T(-0.80901699437494742410);  // cos(4π/5)
+        const T s1 = T(0.95105651629515357212);   // sin(2π/5)
+        const T s2 = T(0.58778525229247312917);   // sin(4π/5)
+        const V s14 = cadd(v[1], v[4]), d14 = csub(v[1], v[4]);
+        const V s23 = cadd(v[2], v[3]), d23 = csub(v[2], v[3]);
+        const V a1 = V{v[0].x + c1 * s14.x + c2 * s23.x, v[0].y + c1 * s14.y + c2 * s23.y};
+        const V a2 = V{v[0].x + c2 * s14.x + c1 * s23.x, v[0].y + c2 * s14.y + c1 * s23.y};
+        const V b1 = cmuli(V{s1 * d14.x + s2 * d23.x, s1 * d14.y + s2 * d23.y});
+        const V b2 = cmuli(V{s2 * d14.x - s1 * d23.x, s2 * d14.y - s1 * d23.y});
+        v[0] = cadd(v[0], cadd(s14, s23));
+        v[1] = cadd(a1, b1);
+        v[4] = csub(a1, b1);
+        v[2] = cadd(a2, b2);
+        v[3] = csub(a2, b2);
+    }
+};
+
+template <class T> struct dft_t<8, T> {
+    using V = cplx_t<T>;
+    __device__ __forceinline__ static void run(V* v) {
+        const T r2 = T(0.70710678118654752440);  // √2 / 2
+        V e[4] = {v[0], v[2], v[4], v[6]};
+        V o[4] = {v[1], v[3], v[5], v[7]};
+        dft_t<4, T>::run(e);
+        dft_t<4, T>::run(o);
+        o[1] = V{r2 * (o[1].x - o[1].y), r2 * (o[1].x + o[1].y)};    // × e^{iπ/4}
+        o[2] = cmuli(o[2]);                                          // × i
+        o[3] = V{-r2 * (o[3].x + o[3].y), r2 * (o[3].x - o[3].y)};   // × e^{3iπ/4}
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            v[b] = cadd(e[b], o[b]);
+            v[b + 4] = csub(e[b], o[b]);
+        }
+    }
+};
 
 // Synchronise the TP threads of group `gid` (named barrier 1 + gid when the
 // group spans several warps).
@@ -165,12 +195,13 @@ template <int TP> __device__ __forceinline__ void gsync(int gid) {
     }
 }
 
-template <int N, int TP, int R, int Ns, int TWOFF>
-__device__ __forceinline__ void fft_stage(double2* buf, const double2* W, int tid, int gid) {
+template <int N, int TP, int R, int Ns, int TWOFF, class T>
+__device__ __forceinline__ void fft_stage(cplx_t<T>* buf, const cplx_t<T>* W, int tid, int gid) {
+    using V = cplx_t<T>;
     constexpr int nb = N / R;
     constexpr int QM = (nb + TP - 1) / TP;
     constexpr bool exact = (QM * TP == nb);
-    double2 v[QM][R];
+    V v[QM][R];
 #pragma unroll
     for (int q = 0; q < QM; ++q) {
         const int b = tid + q * TP;
@@ -189,7 +220,7 @@ __device__ __forceinline__ void fft_stage(double2* buf, const double2* W, int ti
 #pragma unroll
                 for (int r = 1; r < R; ++r) v[q][r] = cmul(v[q][r], W[TWOFF + (r - 1) * Ns + k]);
             }
-            dft<R>(v[q]);
+            dft_t<R, T>::run(v[q]);
             const int base = (b - k) * R + k;
 #pragma unroll
             for (int r = 0; r < R; ++r) buf[ct_pad(base + r * Ns)] = v[q][r];
@@ -198,21 +229,22 @@ __device__ __forceinline__ void fft_stage(double2* buf, const double2* W, int ti
     gsync<TP>(gid);
 }
 
-template <int N, int TP, int S, int Ns>
-__device__ __forceinline__ void fft_stages(double2* buf, const double2* W, int tid, int gid) {
+template <int N, int TP, int S, int Ns, class T>
+__device__ __forceinline__ void fft_stages(cplx_t<T>* buf, const cplx_t<T>* W, int tid, int gid) {
     if constexpr (S < ct_nstages(N)) {
         constexpr int R = ct_radix(N, S);
-        fft_stage<N, TP, R, Ns, ct_tw_off(N, S)>(buf, W, tid, gid);
-        fft_stages<N, TP, S + 1, Ns * R>(buf, W, tid, gid);
+        fft_stage<N, TP, R, Ns, ct_tw_off(N, S), T>(buf, W, tid, gid);
+        fft_stages<N, TP, S + 1, Ns * R, T>(buf, W, tid, gid);
     }
 }
 
 // Pre-processing: buf[m] = y_m from load(m-1) = (a_{m-1}, b_{m-1}).
-template <int N, int TP, class Load>
-__device__ __forceinline__ void dst_pre(double2* buf, const double* s, int tid, Load load) {
+template <int N, int TP, class T, class Load>
+__device__ __forceinline__ void dst_pre(cplx_t<T>* buf, const T* s, int tid, Load load) {
+    using V = cplx_t<T>;
     constexpr int half = N >> 1;
     constexpr int IT = (half + TP) / TP;  // m = tid + it·TP covers 0 … half
-    double2 fm[IT], fn[IT];
+    V fm[IT], fn[IT];
 #pragma unroll
     for (int it = 0; it < IT; ++it) {  // issue every load before using any
         const int m = tid + it * TP;
@@ -225,15 +257,15 @@ __device__ __forceinline__ void dst_pre(double2* buf, const double* s, int tid, 
     for (int it = 0; it < IT; ++it) {
         const int m = tid + it * TP;
         if (m == 0) {
-            buf[0] = make_double2(0.0, 0.0);
+            buf[0] = V{T(0), T(0)};
         } else if (m == half) {  // sin(π/2) = 1
-            buf[ct_pad(m)] = make_double2(2.0 * fm[it].x, 2.0 * fm[it].y);
+            buf[ct_pad(m)] = V{T(2) * fm[it].x, T(2) * fm[it].y};
         } else if (m < half) {
-            const double sm = s[m];
-            const double2 sum = cadd(fm[it], fn[it]), dif = csub(fm[it], fn[it]);
-            const double2 ys = make_double2(sm * sum.x, sm * sum.y);
-            buf[ct_pad(m)] = make_double2(ys.x + 0.5 * dif.x, ys.y + 0.5 * dif.y);
-            buf[ct_pad(N - m)] = make_double2(ys.x - 0.5 * dif.x, ys.y - 0.5 * dif.y);
+            const T sm = s[m];
+            const V sum = cadd(fm[it], fn[it]), dif = csub(fm[it], fn[it]);
+            const V ys = V{sm * sum.x, sm * sum.y};
+            buf[ct_pad(m)] = V{ys.x + T(0.5) * dif.x, ys.y + T(0.5) * dif.y};
+            buf[ct_pad(N - m)] = V{ys.x - T(0.5) * dif.x, ys.y - T(0.5) * dif.y};
         }
     }
 }
@@ -241,23 +273,27 @@ __device__ __forceinline__ void dst_pre(double2* buf, const double* s, int tid, 
 __device__ __forceinline__ double2 shfl_up2(double2 v, int off) {
     return make_double2(__shfl_up_sync(0xffffffffu, v.x, off), __shfl_up_sync(0xffffffffu, v.y, off));
 }
+__device__ __forceinline__ float2 shfl_up2(float2 v, int off) {
+    return make_float2(__shfl_up_sync(0xffffffffu, v.x, off), __shfl_up_sync(0xffffffffu, v.y, off));
+}
 
-// Exclusive prefix sum of one double2 per thread over the TP threads of a group.
-template <int TP>
-__device__ __forceinline__ double2 group_excl_scan(double2 v, int tid, int gid, double2* scratch) {
+// Exclusive prefix sum of one complex value per thread over the TP threads of
+// a group.
+template <int TP, class V>
+__device__ __forceinline__ V group_excl_scan(V v, int tid, int gid, V* scratch) {
     const int lane = tid & 31, w = tid >> 5;
-    double2 inc = v;
+    V inc = v;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-        const double2 n = shfl_up2(inc, off);
+        const V n = shfl_up2(inc, off);
         if (lane >= off) inc = cadd(inc, n);
     }
-    double2 ex = shfl_up2(inc, 1);
-    if (lane == 0) ex = make_double2(0.0, 0.0);
+    V ex = shfl_up2(inc, 1);
+    if (lane == 0) ex = V{0, 0};
     if constexpr (TP > 32) {
         if (lane == 31) scratch[w] = inc;
         gsync<TP>(gid);
-        double2 base = make_double2(0.0, 0.0);
+        V base = V{0, 0};
         for (int u = 0; u < w; ++u) base = cadd(base, scratch[u]);
         ex = cadd(base, ex);
     }
@@ -267,33 +303,34 @@ __device__ __forceinline__ double2 group_excl_scan(double2 v, int tid, int gid, 
 // Post-processing: from Z (in buf) produce the N-1 outputs of both lines and
 // hand them to emit(o, (a_o, b_o)).  All reads of buf precede every emit, so
 // emit may write into buf.
-template <int N, int TP, class Emit>
-__device__ __forceinline__ void dst_post(double2* buf, int tid, int gid, double2* scratch, Emit emit) {
+template <int N, int TP, class T, class Emit>
+__device__ __forceinline__ void dst_post(cplx_t<T>* buf, int tid, int gid, cplx_t<T>* scratch, Emit emit) {
+    using V = cplx_t<T>;
     constexpr int half = N >> 1;
     constexpr int C = (half + TP - 1) / TP;
     const int k0 = tid * C;
-    double2 D[C], O[C];
-    double2 tot = make_double2(0.0, 0.0);
+    V D[C], O[C];
+    V tot = V{T(0), T(0)};
 #pragma unroll
     for (int t = 0; t < C; ++t) {
         const int k = k0 + t;
         if (k < half) {
-            const double2 zk = buf[ct_pad(k)];
-            double2 d;
+            const V zk = buf[ct_pad(k)];
+            V d;
             if (k == 0) {
                 d = zk;
-                O[t] = make_double2(0.0, 0.0);
+                O[t] = V{T(0), T(0)};
             } else {
-                const double2 zn = buf[ct_pad(N - k)];
+                const V zn = buf[ct_pad(N - k)];
                 d = cadd(zk, zn);
-                const double2 dl = csub(zk, zn);
-                O[t] = make_double2(dl.y, -dl.x);  // −i (Z_k − Z_{N−k})
+                const V dl = csub(zk, zn);
+                O[t] = V{dl.y, -dl.x};  // −i (Z_k − Z_{N−k})
             }
             tot = cadd(tot, d);
             D[t] = tot;
         }
     }
-    const double2 ex = group_excl_scan<TP>(tot, tid, gid, scratch);
+    const V ex = group_excl_scan<TP>(tot, tid, gid, scratch);
     gsync<TP>(gid);
 #pragma unroll
     for (int t = 0; t < C; ++t) {
@@ -306,56 +343,86 @@ __device__ __forceinline__ void dst_post(double2* buf, int tid, int gid, double2
 }
 
 // One DST-I of a line pair: load → pre → FFT → post → emit.
-template <int N, int TP, class Load, class Emit>
-__device__ __forceinline__ void dst_pair(double2* buf, const double2* W, const double* s, int tid, int gid, Load load,
-                                         Emit emit) {
-    dst_pre<N, TP>(buf, s, tid, load);
+template <int N, int TP, class T, class Load, class Emit>
+__device__ __forceinline__ void dst_pair(cplx_t<T>* buf, const cplx_t<T>* W, const T* s, int tid, int gid,
+                                         Load load, Emit emit) {
+    dst_pre<N, TP, T>(buf, s, tid, load);
     gsync<TP>(gid);
-    fft_stages<N, TP, 0, 1>(buf, W, tid, gid);
-    dst_post<N, TP>(buf, tid, gid, buf + ct_pad(N), emit);
+    fft_stages<N, TP, 0, 1, T>(buf, W, tid, gid);
+    dst_post<N, TP, T>(buf, tid, gid, buf + ct_pad(N), emit);
 }
+
+// Tables of one precision: stage twiddles, sin(π m/N) and the spectral table
+// used by the divide (FP64: cos(π(k+1)/N); FP32: 4 sin²(π(k+1)/(2N))).
+template <class T> struct Tabs {
+    const cplx_t<T>* W;
+    const T* s;
+    const T* c;
+};
+template <class T> __host__ __device__ Tabs<T> tabs_of(const DstPlan& p);
+template <> __host__ __device__ inline Tabs<double> tabs_of<double>(const DstPlan& p) { return {p.W, p.s, p.c}; }
+template <> __host__ __device__ inline Tabs<float> tabs_of<float>(const DstPlan& p) { return {p.W32, p.s32, p.a32}; }
 
 // Copy the transform tables into shared memory: stage twiddles (complex),
 // then sin(πm/N) for m ≤ N/2.
-template <int N>
-__device__ __forceinline__ void stage_tables(double2* tw, double* sn, const DstPlan& p) {
-    for (int i = threadIdx.x; i < ct_tw_count(N); i += blockDim.x) cp_async16(tw + i, p.W + i);
-    for (int i = threadIdx.x; i <= N / 2; i += blockDim.x) cp_async8(sn + i, p.s + i);
+template <int N, class T>
+__device__ __forceinline__ void stage_tables(cplx_t<T>* tw, T* sn, const Tabs<T>& p) {
+    for (int i = threadIdx.x; i < ct_tw_count(N); i += blockDim.x) cp_async<sizeof(cplx_t<T>)>(tw + i, p.W + i);
+    for (int i = threadIdx.x; i <= N / 2; i += blockDim.x) cp_async<sizeof(T)>(sn + i, p.s + i);
 }
-template <int N>
+template <int N, class T>
 __host__ __device__ constexpr size_t tables_bytes() {
-    return (size_t)ct_tw_count(N) * sizeof(double2) + (size_t)((N / 2 + 2) & ~1) * sizeof(double);
+    return (size_t)ct_tw_count(N) * sizeof(cplx_t<T>) + (size_t)((N / 2 + 4) & ~3) * sizeof(T);
 }
 
 // ---------------------------------------------------------------------------
 // x-pass: lines are rows of a slab (contiguous).  One group per line pair.
 // ---------------------------------------------------------------------------
+template <int LOAD>
+using x_real_t = std::conditional_t<(LOAD == XLOAD_PLAIN || LOAD == XLOAD_BC), double, float>;
+template <int LOAD>
+__host__ __device__ constexpr bool x_res() { return LOAD == XLOAD_RES_LAP || LOAD == XLOAD_RES_A; }
+// Shared memory of the x-pass: tables, one FFT buffer per group, and for the
+// residual loads six staged rows of N doubles per group (16-byte aligned).
+template <int N, int LOAD>
+__host__ __device__ constexpr size_t x_res_off() {
+    return ((tables_bytes<N, x_real_t<LOAD>>() + (size_t)ct_groups(N) * ct_buf(N) * sizeof(cplx_t<x_real_t<LOAD>>) +
+             15) / 16) * 16;
+}
+template <int N, int LOAD>
+__host__ __device__ constexpr size_t x_smem_bytes() {
+    return x_res_off<N, LOAD>() + (x_res<LOAD>() ? (size_t)ct_groups(N) * 6 * N * sizeof(double) : 0);
+}
+
 template <int N, int LOAD, int EMIT>
 __global__ void __launch_bounds__((N <= 1024 ? 128 : 256)) dst_x_kernel(XPassArgs a, Geom g, DstPlan p) {
+    using T = x_real_t<LOAD>;
+    using V = cplx_t<T>;
     constexpr int TP = ct_tp(N);
     constexpr int G = ct_groups(N);
-    extern __shared__ double2 smem2[];
-    double2* tw = smem2;
-    double* sn = reinterpret_cast<double*>(smem2 + ct_tw_count(N));
-    double2* bufs = reinterpret_cast<double2*>(reinterpret_cast<char*>(smem2) + tables_bytes<N>());
-    stage_tables<N>(tw, sn, p);  // constant tables: before the dependency wait
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tw = reinterpret_cast<V*>(smem_raw);
+    T* sn = reinterpret_cast<T*>(tw + ct_tw_count(N));
+    V* bufs = reinterpret_cast<V*>(smem_raw + tables_bytes<N, T>());
+    stage_tables<N, T>(tw, sn, tabs_of<T>(p));  // constant tables: before the dependency wait
     cp_async_wait();
     __syncthreads();
     pdl_wait();
     pdl_trigger();
     const int gid = threadIdx.x / TP, tid = threadIdx.x % TP;
-    double2* buf = bufs + gid * ct_buf(N);
+    V* buf = bufs + gid * ct_buf(N);
+    constexpr bool RES = x_res<LOAD>();
     const int la = a.line0 + 2 * (blockIdx.x * G + gid);
     if (la >= a.line1) return;  // the whole group leaves together
     const bool hasb = (la + 1) < a.line1;
     const int y = blockIdx.y;
     const int P = g.P, n1 = g.n1, n2 = g.n2;
-    const double* ra = a.in + a.in_map.off(y) + (long long)la * P;
-    const double* rb = ra + P;
+    const long long ioff = a.in_map.off(y) + (long long)la * P;
 
     CoarseBC cb;
     cb.rc = nullptr; cb.P = P; cb.nx = g.nx; cb.ny = g.ny;
-    if (LOAD == XLOAD_BC && a.coarse) cb.rc = a.coarse + a.coarse_map.off(y);
+    if ((LOAD == XLOAD_BC || LOAD == XLOAD_RES_LAP) && a.coarse) cb.rc = a.coarse + a.coarse_map.off(y);
+    const double* xg = (LOAD == XLOAD_RES_LAP || LOAD == XLOAD_RES_A) ? a.aux + a.aux_map.off(y) : nullptr;
 
     // apply_bc!(r, get_bc!(coarse), 1.0) (mg-utils.jl:43-60) in the reference's
     // order: bottom row, top row, left column, right column.
@@ -366,27 +433,106 @@ __global__ void __launch_bounds__((N <= 1024 ? 128 : 256)) dst_x_kernel(XPassArg
         if (i == n1 - 1) v += cb.right(j + 1);
         return v;
     };
-    auto load = [&](int i) -> double2 {
-        double va = ra[i];
-        double vb = hasb ? rb[i] : 0.0;
-        if (LOAD == XLOAD_BC && cb.rc) {
-            va = with_bc(va, i, la);
-            if (hasb) vb = with_bc(vb, i, la + 1);
+    // Residual loads: the group stages x̃ rows la-1 … la+2 (zero outside the
+    // slab) and b rows la, la+1 in shared memory, rows of stride N doubles.
+    double* rs = RES ? reinterpret_cast<double*>(smem_raw + x_res_off<N, LOAD>()) + (size_t)gid * 6 * N : nullptr;
+    if constexpr (RES) {
+        const double* bin = static_cast<const double*>(a.in) + a.in_map.off(y);
+#pragma unroll 1
+        for (int r = 0; r < 6; ++r) {
+            const int j = r < 4 ? la - 1 + r : la + r - 4;
+            const bool valid = j >= 0 && j < n2 && (r != 5 || hasb);
+            const double* src = (r < 4 ? xg : bin) + (long long)j * P;
+            double* dst = rs + r * N;
+            for (int i = 2 * tid; i < n1; i += 2 * TP) {
+                if (valid) {
+                    if (i + 1 < n1) cp_async16(dst + i, src + i);
+                    else cp_async8(dst + i, src + i);
+                } else {
+                    dst[i] = 0.0;
+                    if (i + 1 < n1) dst[i + 1] = 0.0;
+                }
+            }
         }
-        return make_double2(va, vb);
+        cp_async_wait();
+        gsync<TP>(gid);
+    }
+    // L x̃ at (i, la + r) = 4 x̃ − Σ neighbours, zero beyond the slab edges
+    // (r = 0, 1; staged row 1 + r)
+    auto lap = [&](int i, int r) -> double {
+        const double* c = rs + (1 + r) * N + i;
+        double nb = 0.0;
+        if (i > 0) nb += c[-1];
+        if (i + 1 < n1) nb += c[1];
+        nb += c[-N];
+        nb += c[N];
+        return 4.0 * c[0] - nb;
     };
-    dst_pair<N, TP>(buf, tw, sn, tid, gid, load, [&](int o, double2 v) { buf[ct_pad(o)] = v; });
-    gsync<TP>(gid);
-    double* oa = a.out + a.out_map.off(y) + (long long)la * P;
-    double* ob = oa + P;
-    for (int o = tid; o < n1; o += TP) {
-        const double2 v = buf[ct_pad(o)];
-        if (EMIT == XEMIT_STORE) {
-            oa[o] = v.x;
-            if (hasb) ob[o] = v.y;
+    auto line_val = [&](const double* row, int i, int j) -> double {
+        double v = row[i];
+        if constexpr (LOAD == XLOAD_BC) {
+            if (cb.rc) v = with_bc(v, i, j);
+        }
+        return v;
+    };
+    auto res_val = [&](int i, int r) -> double {
+        double v = rs[(4 + r) * N + i];
+        if constexpr (LOAD == XLOAD_RES_LAP) {
+            if (cb.rc) v = with_bc(v, i, la + r);
+            v -= lap(i, r);
         } else {
-            oa[o] -= v.x;
-            if (hasb) ob[o] -= v.y;
+            v -= rs[(1 + r) * N + i] + a.cA * lap(i, r);
+        }
+        return v;
+    };
+    auto load = [&](int i) -> V {
+        if constexpr (LOAD == XLOAD_F32) {
+            const float* ra = static_cast<const float*>(a.in) + ioff;
+            return V{ra[i], hasb ? ra[i + P] : 0.0f};
+        } else if constexpr (RES) {
+            return V{(T)res_val(i, 0), hasb ? (T)res_val(i, 1) : T(0)};
+        } else {
+            const double* ra = static_cast<const double*>(a.in) + ioff;
+            const double va = line_val(ra, i, la);
+            const double vb = hasb ? line_val(ra + P, i, la + 1) : 0.0;
+            return V{(T)va, (T)vb};
+        }
+    };
+    dst_pair<N, TP, T>(buf, tw, sn, tid, gid, load, [&](int o, V v) { buf[ct_pad(o)] = v; });
+    gsync<TP>(gid);
+    const long long ooff = a.out_map.off(y) + (long long)la * P;
+    for (int o = tid; o < n1; o += TP) {
+        const V v = buf[ct_pad(o)];
+        if constexpr (EMIT == XEMIT_F32) {
+            float* oa = static_cast<float*>(a.out) + ooff;
+            oa[o] = (float)v.x;
+            if (hasb) oa[o + P] = (float)v.y;
+        } else {
+            double* oa = static_cast<double*>(a.out) + ooff;
+            if constexpr (EMIT == XEMIT_STORE) {
+                oa[o] = v.x;
+                if (hasb) oa[o + P] = v.y;
+            } else if constexpr (EMIT == XEMIT_SUB) {
+                oa[o] -= v.x;
+                if (hasb) oa[o + P] -= v.y;
+            } else if constexpr (EMIT == XEMIT_ADD) {
+                oa[o] += (double)v.x;
+                if (hasb) oa[o + P] += (double)v.y;
+            } else if constexpr (EMIT == XEMIT_ADD_FROM) {
+                const double* xa = a.aux + a.aux_map.off(y) + (long long)la * P;
+                oa[o] = xa[o] + (double)v.x;
+                if (hasb) oa[o + P] = xa[o + P] + (double)v.y;
+            } else {  // XEMIT_ACC_SUB
+                double* xa = a.aux + a.aux_map.off(y) + (long long)la * P;
+                const double pa = xa[o] + (double)v.x;
+                xa[o] = pa;
+                oa[o] -= pa;
+                if (hasb) {
+                    const double pb = xa[o + P] + (double)v.y;
+                    xa[o + P] = pb;
+                    oa[o + P] -= pb;
+                }
+            }
         }
     }
 }
@@ -399,41 +545,44 @@ template <int N>
 __host__ __device__ constexpr int y_groups() { return ct_groups(N); }
 template <int N>
 __host__ __device__ constexpr int y_tile_w() { return 2 * y_groups<N>(); }
-template <int N>
+__host__ __device__ constexpr int round4(int n) { return ((n + 3) / 4) * 4; }
+template <int N, class T>
 __host__ __device__ constexpr size_t y_smem_bytes(int n2) {
-    return tables_bytes<N>() + (size_t)(((n2 + 1) / 2) * 2) * sizeof(double) +  // cos(π(j+1)/ny)
-           (size_t)(((n2 * (y_tile_w<N>() + 1) + 1) / 2) * 2) * sizeof(double) +
-           (size_t)y_groups<N>() * ct_buf(N) * sizeof(double2);
+    return tables_bytes<N, T>() + (size_t)round4(n2) * sizeof(T) +  // spectral table of y
+           (size_t)round4(n2 * (y_tile_w<N>() + 1)) * sizeof(T) +
+           (size_t)y_groups<N>() * ct_buf(N) * sizeof(cplx_t<T>);
 }
 
-template <int N>
+template <int N, class T>
 __global__ void __launch_bounds__((N <= 1024 ? 128 : 256), (N <= 512 ? 5 : 1))
-    dst_y_kernel(double* data, SlabMap map, Geom g, DstPlan p, const double* __restrict__ cx, SpecParams sp) {
+    dst_y_kernel(T* data, SlabMap map, Geom g, DstPlan p, const T* __restrict__ cx, SpecParams sp) {
+    using V = cplx_t<T>;
     constexpr int TP = ct_tp(N);
     constexpr int TW = y_tile_w<N>();
     constexpr int TWp = TW + 1;
-    extern __shared__ double2 smem2[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P = g.P, n1 = g.n1, n2 = g.n2;
-    double2* tw = smem2;
-    double* sn = reinterpret_cast<double*>(smem2 + ct_tw_count(N));
-    double* cyv = reinterpret_cast<double*>(reinterpret_cast<char*>(smem2) + tables_bytes<N>());
-    double* tile = cyv + ((n2 + 1) / 2) * 2;
-    const int tile_d = ((n2 * TWp + 1) / 2) * 2;
+    const Tabs<T> tb = tabs_of<T>(p);
+    V* tw = reinterpret_cast<V*>(smem_raw);
+    T* sn = reinterpret_cast<T*>(tw + ct_tw_count(N));
+    T* cyv = reinterpret_cast<T*>(smem_raw + tables_bytes<N, T>());
+    T* tile = cyv + round4(n2);
+    const int tile_d = round4(n2 * TWp);
     const int gid = threadIdx.x / TP, tid = threadIdx.x % TP;
-    double2* buf = reinterpret_cast<double2*>(tile + tile_d) + gid * ct_buf(N);
+    V* buf = reinterpret_cast<V*>(tile + tile_d) + gid * ct_buf(N);
     const int i0 = blockIdx.x * TW;
-    double* base = data + map.off(blockIdx.y);
+    T* base = data + map.off(blockIdx.y);
     const int lev = map.level(blockIdx.y);
 
-    stage_tables<N>(tw, sn, p);  // constant tables: before the dependency wait
-    for (int j = threadIdx.x; j < n2; j += blockDim.x) cp_async8(cyv + j, p.c + j);
+    stage_tables<N, T>(tw, sn, tb);  // constant tables: before the dependency wait
+    for (int j = threadIdx.x; j < n2; j += blockDim.x) cp_async<sizeof(T)>(cyv + j, tb.c + j);
     pdl_wait();
     pdl_trigger();
     for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
         const int j = idx / TW, c = idx - j * TW;
         const int i = i0 + c;
-        if (i < n1) cp_async8(tile + j * TWp + c, base + (long long)j * P + i);
-        else tile[j * TWp + c] = 0.0;
+        if (i < n1) cp_async<sizeof(T)>(tile + j * TWp + c, base + (long long)j * P + i);
+        else tile[j * TWp + c] = T(0);
     }
     cp_async_wait();
     __syncthreads();
@@ -442,37 +591,55 @@ __global__ void __launch_bounds__((N <= 1024 ? 128 : 256), (N <= 512 ? 5 : 1))
     const int ia = i0 + ca;
     if (ia < n1) {
         const bool hasb = ia + 1 < n1;
-        auto load = [&](int m) -> double2 { return make_double2(tile[m * TWp + ca], tile[m * TWp + ca + 1]); };
-        auto emit = [&](int o, double2 v) {
+        auto load = [&](int m) -> V { return V{tile[m * TWp + ca], tile[m * TWp + ca + 1]}; };
+        auto emit = [&](int o, V v) {
             tile[o * TWp + ca] = v.x;
             tile[o * TWp + ca + 1] = v.y;
         };
-        // w ./= M ; w .*= scale  with Λ = -2 (cos(π i/nx) + cos(π j/ny) - 2)
         auto divide = [&]() {
-            const double cxa = __ldg(&cx[ia]);
-            const double cxb = hasb ? __ldg(&cx[ia + 1]) : 0.0;
-            const double den = sp.den[lev];
-            for (int o = tid; o < n2; o += TP) {
-                const double c2 = cyv[o];
-                const double la = -2.0 * ((cxa + c2) - 2.0);
-                const double lb = -2.0 * ((cxb + c2) - 2.0);
-                double Ma, Mb;
-                if (sp.mode == SPEC_DELTA) {
-                    Ma = la;
-                    Mb = lb;
-                } else {
-                    Ma = 1.0 + la * sp.dt / den;
-                    Mb = 1.0 + lb * sp.dt / den;
+            if constexpr (std::is_same<T, double>::value) {
+                // w ./= M ; w .*= scale  with Λ = -2 (cos(π i/nx) + cos(π j/ny) - 2)
+                // (laplacian.jl:173-197, 217-227)
+                const double cxa = __ldg(&cx[ia]);
+                const double cxb = hasb ? __ldg(&cx[ia + 1]) : 0.0;
+                const double den = sp.den[lev];
+                for (int o = tid; o < n2; o += TP) {
+                    const double c2 = cyv[o];
+                    const double la = -2.0 * ((cxa + c2) - 2.0);
+                    const double lb = -2.0 * ((cxb + c2) - 2.0);
+                    double Ma, Mb;
+                    if (sp.mode == SPEC_DELTA) {
+                        Ma = la;
+                        Mb = lb;
+                    } else {
+                        Ma = 1.0 + la * sp.dt / den;
+                        Mb = 1.0 + lb * sp.dt / den;
+                    }
+                    tile[o * TWp + ca] = (tile[o * TWp + ca] * nr_rcp(Ma)) * sp.scale;
+                    tile[o * TWp + ca + 1] = hasb ? (tile[o * TWp + ca + 1] * nr_rcp(Mb)) * sp.scale : 0.0;
                 }
-                tile[o * TWp + ca] = (tile[o * TWp + ca] * nr_rcp(Ma)) * sp.scale;
-                tile[o * TWp + ca + 1] = hasb ? (tile[o * TWp + ca + 1] * nr_rcp(Mb)) * sp.scale : 0.0;
+            } else {
+                // the same divisor from Λ = a_x(i) + a_y(j), a(k) = 4 sin²(πk/(2n)):
+                // no cancellation for the smallest eigenvalues in FP32
+                const float axa = __ldg(&cx[ia]);
+                const float axb = hasb ? __ldg(&cx[ia + 1]) : 0.0f;
+                const float kf = (sp.mode == SPEC_DELTA) ? 0.0f : (float)(sp.dt / sp.den[lev]);
+                const float sc = (float)sp.scale;
+                for (int o = tid; o < n2; o += TP) {
+                    const float la = axa + cyv[o];
+                    const float lb = axb + cyv[o];
+                    const float Ma = (sp.mode == SPEC_DELTA) ? la : fmaf(la, kf, 1.0f);
+                    const float Mb = (sp.mode == SPEC_DELTA) ? lb : fmaf(lb, kf, 1.0f);
+                    tile[o * TWp + ca] = tile[o * TWp + ca] * (__frcp_rn(Ma) * sc);
+                    tile[o * TWp + ca + 1] = hasb ? tile[o * TWp + ca + 1] * (__frcp_rn(Mb) * sc) : 0.0f;
+                }
             }
         };
-        dst_pair<N, TP>(buf, tw, sn, tid, gid, load, emit);
+        dst_pair<N, TP, T>(buf, tw, sn, tid, gid, load, emit);
         gsync<TP>(gid);
         divide();
         gsync<TP>(gid);
-        dst_pair<N, TP>(buf, tw, sn, tid, gid, load, emit);
+        dst_pair<N, TP, T>(buf, tw, sn, tid, gid, load, emit);
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
@@ -493,28 +660,44 @@ cudaError_t launch_x_n(const Geom& g, const DstPlan& px, const XPassArgs& a, cud
     if (lines <= 0 || a.nslabs <= 0) return cudaSuccess;
     const int pairs = (lines + 1) / 2;
     dim3 grid((pairs + G - 1) / G, a.nslabs);
-    const size_t smem = tables_bytes<N>() + (size_t)G * ct_buf(N) * sizeof(double2);
+    const size_t smem = x_smem_bytes<N, LOAD>();
     return launch_k(dst_x_kernel<N, LOAD, EMIT>, grid, dim3(G * TP), smem, st, a, g, px);
 }
 
-template <int N>
-cudaError_t launch_x_t(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {
-    if (a.load == XLOAD_BC)
-        return a.emit == XEMIT_SUB ? launch_x_n<N, XLOAD_BC, XEMIT_SUB>(g, px, a, st)
-                                   : launch_x_n<N, XLOAD_BC, XEMIT_STORE>(g, px, a, st);
-    return a.emit == XEMIT_SUB ? launch_x_n<N, XLOAD_PLAIN, XEMIT_SUB>(g, px, a, st)
-                               : launch_x_n<N, XLOAD_PLAIN, XEMIT_STORE>(g, px, a, st);
-}
+// The (load, emit) pairs the library uses: FP64 solves, and the three passes
+// of an FP32 refinement correction.
+#define IBPM_X_COMBOS(X)                                                                  \
+    X(XLOAD_PLAIN, XEMIT_STORE) X(XLOAD_PLAIN, XEMIT_SUB) X(XLOAD_BC, XEMIT_STORE)       \
+    X(XLOAD_BC, XEMIT_SUB) X(XLOAD_F32, XEMIT_F32) X(XLOAD_RES_LAP, XEMIT_F32)           \
+    X(XLOAD_RES_A, XEMIT_F32) X(XLOAD_F32, XEMIT_ADD) X(XLOAD_F32, XEMIT_ADD_FROM)       \
+    X(XLOAD_F32, XEMIT_ACC_SUB)
 
 template <int N>
-cudaError_t launch_y_t(const Geom& g, const DstPlan& py, const DstPlan& px, double* data, SlabMap map, int nslabs,
+cudaError_t launch_x_t(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {
+#define IBPM_X_DISPATCH(L, E) \
+    if (a.load == L && a.emit == E) return launch_x_n<N, L, E>(g, px, a, st);
+    IBPM_X_COMBOS(IBPM_X_DISPATCH)
+#undef IBPM_X_DISPATCH
+    return cudaErrorInvalidValue;
+}
+
+template <int N, class T>
+cudaError_t launch_y_n(const Geom& g, const DstPlan& py, const DstPlan& px, void* data, SlabMap map, int nslabs,
                        const SpecParams& sp, cudaStream_t st) {
     constexpr int TW = y_tile_w<N>();
-    const size_t smem = y_smem_bytes<N>(g.n2);
+    const size_t smem = y_smem_bytes<N, T>(g.n2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     dim3 grid((g.n1 + TW - 1) / TW, nslabs);
     const int threads = y_groups<N>() * ct_tp(N);
-    return launch_k(dst_y_kernel<N>, grid, dim3(threads), smem, st, data, map, g, py, px.c, sp);
+    return launch_k(dst_y_kernel<N, T>, grid, dim3(threads), smem, st, static_cast<T*>(data), map, g, py,
+                    static_cast<const T*>(tabs_of<T>(px).c), sp);
+}
+
+template <int N>
+cudaError_t launch_y_t(const Geom& g, const DstPlan& py, const DstPlan& px, void* data, SlabMap map, int nslabs,
+                       const SpecParams& sp, cudaStream_t st) {
+    return sp.f32 ? launch_y_n<N, float>(g, py, px, data, map, nslabs, sp, st)
+                  : launch_y_n<N, double>(g, py, px, data, map, nslabs, sp, st);
 }
 
 template <class K>
@@ -528,11 +711,12 @@ cudaError_t smem_attrs(K kernel) {
 template <int N>
 cudaError_t attr_t() {
     cudaError_t e;
-    if ((e = smem_attrs(dst_x_kernel<N, XLOAD_PLAIN, XEMIT_STORE>))) return e;
-    if ((e = smem_attrs(dst_x_kernel<N, XLOAD_PLAIN, XEMIT_SUB>))) return e;
-    if ((e = smem_attrs(dst_x_kernel<N, XLOAD_BC, XEMIT_STORE>))) return e;
-    if ((e = smem_attrs(dst_x_kernel<N, XLOAD_BC, XEMIT_SUB>))) return e;
-    return smem_attrs(dst_y_kernel<N>);
+#define IBPM_X_ATTR(L, E) \
+    if ((e = smem_attrs(dst_x_kernel<N, L, E>))) return e;
+    IBPM_X_COMBOS(IBPM_X_ATTR)
+#undef IBPM_X_ATTR
+    if ((e = smem_attrs(dst_y_kernel<N, double>))) return e;
+    return smem_attrs(dst_y_kernel<N, float>);
 }
 
 }  // namespace dstk
@@ -543,7 +727,7 @@ cudaError_t attr_t() {
     cudaError_t dst_x_##N(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {         \
         return dstk::launch_x_t<N>(g, px, a, st);                                                          \
     }                                                                                                      \
-    cudaError_t dst_y_##N(const Geom& g, const DstPlan& py, const DstPlan& px, double* d, SlabMap m, int n, \
+    cudaError_t dst_y_##N(const Geom& g, const DstPlan& py, const DstPlan& px, void* d, SlabMap m, int n,   \
                           const SpecParams& sp, cudaStream_t st) {                                         \
         return dstk::launch_y_t<N>(g, py, px, d, m, n, sp, st);                                            \
     }                                                                                                      \

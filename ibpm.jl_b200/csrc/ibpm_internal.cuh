@@ -115,6 +115,16 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+template <int B> __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    static_assert(B == 4 || B == 8 || B == 16, "cp.async copies 4, 8 or 16 bytes");
+    if constexpr (B == 4) cp_async4(smem, gmem);
+    else if constexpr (B == 8) cp_async8(smem, gmem);
+    else cp_async16(smem, gmem);
+}
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 bool pdl_enabled();
@@ -155,13 +165,19 @@ struct DstPlan {
     double2* W;          // device: per-stage FFT twiddles (stage-contiguous, ≤ N entries)
     double* s;           // device: sin(π m/N), m < N
     double* c;           // device: cos(π (k+1)/N), k < N-1 (Laplacian eigenvalues)
+    // the same tables rounded to FP32, for the FP32 transforms
+    float2* W32;
+    float* s32;
+    float* a32;          // 2 (1 − cos(π (k+1)/N)) = 4 sin²(π (k+1)/(2N)), free of cancellation
 };
+// Doubles in the table block of one length (FP64 tables, then FP32 tables).
+inline long long dst_table_doubles(int N) { return 6LL * N; }
 
 bool dst_supported(int N);
 int dst_plan_create(DstPlan* p, int N, cudaStream_t st);  // 0 on success
 cudaError_t dst_init_attributes(int N);
-// Fill the 4N-double table block of length N in caller-provided device memory
-// and view it as a plan.
+// Fill the table block of length N (dst_table_doubles(N) doubles) in
+// caller-provided device memory and view it as a plan.
 cudaError_t dst_tables_build(int N, double* base, cudaStream_t st);
 DstPlan dst_plan_at(double* base, int N);
 // Error text returned by ibpm_last_error(NULL).
@@ -174,19 +190,35 @@ void dst_plan_destroy(DstPlan* p);
 enum SpecMode { SPEC_DELTA = 0, SPEC_AINV = 1 };
 struct SpecParams {
     int mode;
+    int f32;             // data and transforms in FP32 (the refinement correction)
     double scale;        // 1 / (4 nx ny)
     double dt;
     double den[8];       // 2 Re hc² per level
 };
 
 // x-direction DST-I of every line of the slabs selected by `map` over lines
-// [line0, line1).  Load/emit variants:
-enum XLoad { XLOAD_PLAIN = 0, XLOAD_BC = 1 };   // BC: add apply_bc!(·, get_bc!(coarser), 1)
-enum XEmit { XEMIT_STORE = 0, XEMIT_SUB = 1 };  // SUB: out ← out − value
+// [line0, line1).  The load mode fixes how the input line is formed and the
+// precision of the transform; the emit mode how the result is stored.
+//   FP64 transforms (the reference's arithmetic):
+//     XLOAD_PLAIN    b (double)
+//     XLOAD_BC       b + apply_bc!(·, get_bc!(coarser), 1)            (mg-utils.jl:7-60)
+//   FP32 transforms (the correction of one FP64-residual refinement sweep):
+//     XLOAD_F32      b (float)
+//     XLOAD_RES_LAP  Γ + apply_bc!(get_bc!(ψ coarser)) − L ψ̃   (double → float)
+//     XLOAD_RES_A    b − (I + c L) x̃                            (double → float)
+//   with L x = 4x − Σ neighbours (zero Dirichlet edges) the operator whose
+//   inverse the DST-I solve with Λ applies, x̃ / ψ̃ the current solution (aux).
+//     XEMIT_STORE    out = v (double)       XEMIT_SUB      out −= v (double)
+//     XEMIT_F32      out = v (float)        XEMIT_ADD      out += v (double)
+//     XEMIT_ADD_FROM out = aux + v          XEMIT_ACC_SUB  aux += v; out −= aux
+enum XLoad { XLOAD_PLAIN = 0, XLOAD_BC = 1, XLOAD_F32 = 2, XLOAD_RES_LAP = 3, XLOAD_RES_A = 4 };
+enum XEmit { XEMIT_STORE = 0, XEMIT_SUB = 1, XEMIT_F32 = 2, XEMIT_ADD = 3, XEMIT_ADD_FROM = 4, XEMIT_ACC_SUB = 5 };
 struct XPassArgs {
-    const double* in; double* out;
+    const void* in; void* out;
     SlabMap in_map, out_map;
-    const double* coarse;  SlabMap coarse_map;   // XLOAD_BC: coarser-level field
+    const double* coarse;  SlabMap coarse_map;   // XLOAD_BC / RES_LAP: coarser-level field
+    double* aux; SlabMap aux_map;                // RES_*: current solution; ADD_FROM / ACC_SUB (see above)
+    double cA;                                   // XLOAD_RES_A: c = dt / (2 Re hc²)
     int nslabs, line0, line1;
     int load, emit;
 };
@@ -194,7 +226,7 @@ cudaError_t launch_dst_x(const Geom& g, const DstPlan& px, const XPassArgs& a, c
 
 // y-direction pass of a Poisson-type solve, in place on every slab selected by
 // `map`: DST-I, spectral divide (SpecParams), DST-I.
-cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px_cos, double* data, SlabMap map,
+cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px_cos, void* data, SlabMap map,
                          int nslabs, const SpecParams& sp, cudaStream_t st);
 
 // Stencil kernels (stencil.cu)
@@ -203,7 +235,8 @@ struct RhsArgs {
     const double* q;                      // state q, nq per level
     const double* Nprev;                  // nonlin from the previous step
     double* Nnew;                         // nonlin of this step
-    double* rhs;                          // right-hand side of the trial solve
+    double* rhs;                          // right-hand side of the trial solve, or
+    float* rhs_inc;                       // (when set) rhs − A Γ, the increment form
     double q0x[8], q0y[8];                // uniform base flux per level
     double fac_bc[8];                     // 0.25 dt / (Re hc²)
     double c_lap[8];                      // dt / (2 Re hc²)

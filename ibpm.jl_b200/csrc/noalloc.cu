@@ -8,7 +8,7 @@
 // side and the result buffer; the one intermediate slab of the solve and the
 // transform tables live in file-scope __device__ arrays of fixed size, which
 // every GPU that loads the library holds until the process exits
-// (2.1 MB + 32 KB).
+// (2.1 MB + 48 KB).
 #include "../../include/ibpm_gpu.h"
 #include "ibpm_internal.cuh"
 
@@ -21,7 +21,7 @@ namespace {
 
 constexpr int kMaxN = 512;                                         // nx, ny <= 512
 constexpr size_t kSlabDoubles = (size_t)(kMaxN - 1) * kMaxN;       // (ny-1) rows of pitch nx
-constexpr size_t kTableDoubles = 4 * (size_t)kMaxN;                // cos (N) + sin (N) + twiddles (<= 2N)
+constexpr size_t kTableDoubles = 6 * (size_t)kMaxN;                // FP64 + FP32 tables of one length
 
 __device__ __align__(256) double g_noalloc_slab[kSlabDoubles];
 __device__ __align__(256) double g_noalloc_tables[2 * kTableDoubles];  // x tables, then y tables

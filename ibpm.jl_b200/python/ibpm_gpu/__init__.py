@@ -38,6 +38,8 @@ IBPM_ERR_NONFINITE = -3
 IBPM_ERR_UNSUPPORTED = -4
 IBPM_ERR_NOMEM = -5
 IBPM_PREC_FP64 = 0
+IBPM_PREC_FP32_REFINED = 1
+PRECISIONS = {"fp64": IBPM_PREC_FP64, "fp32_refined": IBPM_PREC_FP32_REFINED}
 KERNEL_COUNT = 9
 
 _ERRNAMES = {IBPM_ERR_INVALID: "INVALID", IBPM_ERR_CUDA: "CUDA", IBPM_ERR_NONFINITE: "NONFINITE",
@@ -60,7 +62,7 @@ class ProblemDesc(C.Structure):
                 ("nbodies", C.c_int32), ("nb", C.c_int32),
                 ("body_npts", C.POINTER(C.c_int32)), ("xb", C.POINTER(C.c_double)),
                 ("ds", C.POINTER(C.c_double)),
-                ("precision", C.c_int32), ("device", C.c_int32)]
+                ("precision", C.c_int32), ("device", C.c_int32), ("refine_sweeps", C.c_int32)]
 
 
 _DP = C.POINTER(C.c_double)
@@ -239,10 +241,15 @@ class IBProblem:
     evaluated at t = 0 as the reference's IBState does for static bodies
     (state-types.jl:291, timestepping.jl:252-270).  The handle owns the device
     state; ``IBState`` objects are host mirrors of it.
+
+    ``precision``: "fp64" (the reference's arithmetic) or "fp32_refined"
+    (FP32 sine transforms, every Poisson-type solve corrected by
+    ``refine_sweeps`` sweeps of FP64-residual iterative refinement started
+    from the previous solution; state, stencils, Schur solve and forces FP64).
     """
 
     def __init__(self, grid, bodies, dt, Re, freestream=(1.0, 0.0, 0.0), beta=(1.5, -0.5),
-                 device=0, sync_fields=True):
+                 device=0, sync_fields=True, precision="fp64", refine_sweeps=1):
         self.lib = load_library()
         self.grid = grid
         self.bodies = list(bodies)
@@ -267,8 +274,12 @@ class IBProblem:
         d.body_npts = C.cast(self._npts, C.POINTER(C.c_int32))
         d.xb = self._xb.ctypes.data_as(_DP)
         d.ds = self._ds.ctypes.data_as(_DP)
-        d.precision = IBPM_PREC_FP64
+        if precision not in PRECISIONS:
+            raise IBPMError(IBPM_ERR_INVALID, "precision must be one of %s" % sorted(PRECISIONS))
+        self.precision = precision
+        d.precision = PRECISIONS[precision]
         d.device = device
+        d.refine_sweeps = int(refine_sweeps)
         self._desc = d
         h = C.c_void_p()
         rc = self.lib.ibpm_create(C.byref(d), C.byref(h))

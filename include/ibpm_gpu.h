@@ -35,7 +35,12 @@ extern "C" {
 #define IBPM_ERR_NOMEM       -5   /* device allocation failed                    */
 
 /* Arithmetic of the step. */
-#define IBPM_PREC_FP64        0   /* plain FP64 everywhere                        */
+#define IBPM_PREC_FP64         0  /* plain FP64 everywhere                        */
+#define IBPM_PREC_FP32_REFINED 1  /* FP32 sine transforms; FP64 state, stencils,
+                                     residuals, Schur solve and forces.  Every
+                                     Poisson-type solve is x = x̃ + S32(b − M x̃)
+                                     with the residual in FP64 and x̃ the previous
+                                     solution (iterative refinement, warm start) */
 
 typedef struct ibpm_handle ibpm_handle;
 
@@ -60,6 +65,8 @@ typedef struct ibpm_problem_desc {
     const double*  ds;         /* [nb] segment lengths                          */
     int32_t precision;         /* IBPM_PREC_*                                   */
     int32_t device;            /* CUDA device ordinal                           */
+    int32_t refine_sweeps;     /* FP32_REFINED: FP64-residual correction sweeps
+                                  per solve (0 means 1); ignored for FP64        */
 } ibpm_problem_desc;
 
 /* Library version string. */
@@ -137,7 +144,7 @@ int ibpm_sync(ibpm_handle* h);
  * `stream` (a cudaStream_t, or NULL for the legacy default stream) and the call
  * returns without waiting for it.  Limit: nx, ny <= 512 and in the supported
  * transform lengths; larger sizes return IBPM_ERR_INVALID.  The intermediate
- * slab and transform tables are file-scope device arrays (2.1 MB + 32 KB on
+ * slab and transform tables are file-scope device arrays (2.1 MB + 48 KB on
  * every GPU that loads the library, held until exit), shared by all calls:
  * calls that overlap on the GPU (other streams, other threads) race on them.
  * The first call on a device looks up their device addresses and sets kernel

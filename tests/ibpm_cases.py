@@ -13,8 +13,8 @@ CASES = {
     # single grid, a flat plate
     "sq64_mg1_plate": dict(h=0.0625, bnd=(-2.0, 2.0, -2.0, 2.0), mg=1, Re=200.0, dt=0.01,
                            bodies=[("plate", 1.0, 0.2, -0.5, 0.1, 17)], fs=(1.0, 0.0, 0.0)),
-    # BASELINE config 1: 200x200, h=0.02, 3 levels, 157-point cylinder, Re=40, dt=0.004
-    "c1": dict(h=0.02, bnd=(-1.0, 3.0, -2.0, 2.0), mg=3, Re=40.0, dt=0.004,
+    # 200x200, h=0.02, 3 levels, 157-point cylinder, Re=40, dt=0.004
+    "cyl200_mg3": dict(h=0.02, bnd=(-1.0, 3.0, -2.0, 2.0), mg=3, Re=40.0, dt=0.004,
                bodies=[("cyl", 0.5, 0.0, 0.0, 157)], fs=(1.0, 0.0, 0.0)),
 }
 

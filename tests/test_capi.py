@@ -65,3 +65,17 @@ def test_create_without_gpu_fails_loudly():
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=120)
     assert out.returncode == 0, out.stderr
     assert "ERR -2" in out.stdout
+
+
+def test_create_validates_precision_before_touching_a_device():
+    """An unknown precision mode or sweep count is rejected with
+    IBPM_ERR_INVALID by argument checking alone (no GPU needed)."""
+    import ibpm_gpu as G
+    g = G.make_grid(0.0625, (-2., 2., -2., 2.), 2)
+    body = G.make_cylinder(0.5, g.h, 0, 0, n=40)
+    with pytest.raises(G.IBPMError) as e:
+        G.IBProblem(g, [body], 0.01, 40., precision="fp32_refined", refine_sweeps=-1)
+    assert e.value.code == G.IBPM_ERR_INVALID
+    with pytest.raises(G.IBPMError) as e:
+        G.IBProblem(g, [body], 0.01, 40., precision="fp16")
+    assert e.value.code == G.IBPM_ERR_INVALID

@@ -57,14 +57,14 @@ def test_step_from_random_state(pair, nsteps):
     assert rel(cd, ocd) < TOL and rel(cl, ocl) < TOL, name
 
 
-def test_config1_500_steps():
-    """BASELINE config 1 (200x200, 3 levels, 157-point cylinder, Re=40,
+def test_cyl200_mg3_500_steps():
+    """The 200x200, 3-level, 157-point cylinder at Re=40 (h=0.02,
     dt=0.004) from rest for 500 steps: CD/CL histories and the final
     vorticity agree with the oracle to 1e-10."""
     import ibpm_gpu as G
     from oracle import ibpm_ref as R
-    op = oracle_problem("c1")
-    gp = gpu_problem("c1")
+    op = oracle_problem("cyl200_mg3")
+    gp = gpu_problem("cyl200_mg3")
     ost = R.make_state(op)
     gst = G.IBState(gp)
     cd, cl = G.advance(gst, gp, 0.0, nsteps=500)
