@@ -306,6 +306,94 @@ def measure(args, d, precision, sampler=None):
                 clocks=clocks, state_bytes=state_bytes, bodies=1)
 
 
+# The adjoint workload: a cylinder at Re = 100 on 256x256 cells x 4 levels
+# (h = 0.02, same domain), dt = 0.004, 1000 steps; J = the drag averaged over
+# the last 200 steps; start state from a seeded N(0, (1e-4)²) vorticity per
+# finest cell; a checkpoint every 50 steps.
+ADJ = dict(h=0.02, mg=4, dt=0.004, nb=157, steps=1000, window=200, k=50, sigma=1e-4, seed=11)
+ADJ_WORKLOAD = ("adjoint of mean drag (last 200 of 1000 steps), cylinder D=1 (157 pts) Re=100, 256x256 cells "
+                "x 4 levels, h=0.02, dt=0.004, N(0,1e-4) start vorticity, checkpoint every 50 steps")
+
+
+def measure_adjoint(args, d, precision="fp64"):
+    """Wall time of ibpm_adjoint_run (forward with checkpoints, recomputation,
+    adjoint sweep) against ibpm_advance over the same steps, the device time
+    of one adjoint step against one forward step, and a central-difference
+    check of ⟨∂J/∂ω, d⟩ (ε = 1e-6) through two forward runs."""
+    import ibpm_gpu as G
+    g = G.make_grid(ADJ["h"], BOUNDARY, ADJ["mg"])
+    body = G.make_cylinder(0.5, g.h, 0.0, 0.0, n=ADJ["nb"])
+    prob = G.IBProblem(g, [body], ADJ["dt"], RE, device=d.local, sync_fields=False, precision=precision)
+    rng = np.random.default_rng(ADJ["seed"])
+    w0 = ADJ["sigma"] * rng.standard_normal((g.nx - 1, g.ny - 1))
+    dirn = rng.standard_normal(w0.shape)
+    st = G.IBState(prob)
+    n = ADJ["steps"]
+
+    def start(w):
+        for a in (st.Gamma, st.q, st.psi, st.nonlin[0], st.nonlin[1], st.Fb):
+            a[...] = 0.0
+        st.Gamma[:, 0] = g.h ** 2 * w.flatten(order="F")
+        G.push_state(st, prob)
+        G.vort2flux(st, prob)
+
+    def forward(w):
+        start(w)
+        prob.sync()
+        t0 = time.perf_counter()
+        cd, _ = G.advance(st, prob, 0.0, nsteps=n)
+        return time.perf_counter() - t0, float(np.mean(cd[-ADJ["window"]:, 0]))
+
+    forward(w0)                                   # warm-up (graph capture)
+    start(w0)
+    G.adjoint_run(prob, n, ADJ["k"], ADJ["window"])
+    t_fwd, J0 = forward(w0)
+    start(w0)
+    prob.sync()
+    t0 = time.perf_counter()
+    res = G.adjoint_run(prob, n, ADJ["k"], ADJ["window"])
+    t_adj = time.perf_counter() - t0
+    eps = 1e-6
+    _, Jp = forward(w0 + eps * dirn)
+    _, Jm = forward(w0 - eps * dirn)
+    fd = (Jp - Jm) / (2 * eps)
+    ad = float(np.dot(res.grad_omega0.flatten(order="F"), dirn.flatten(order="F")))
+    fwd_ms = float(np.mean(G.bench_steps(prob, 100, flush_l2=True)[10:]))
+    adj_ms = float(np.mean(G.adjoint_bench_steps(prob, 100, flush_l2=True)[10:]))
+    prob.close()
+    return dict(J=res.J, J_forward=J0, grad_alpha=res.grad_alpha, grad_omega0=res.grad_omega0,
+                forward_s=t_fwd, adjoint_run_s=t_adj, fd=fd, ad=ad, fwd_step_ms=fwd_ms, adj_step_ms=adj_ms)
+
+
+def adjoint_block(args, d):
+    a64 = measure_adjoint(args, d, "fp64")
+    a32 = measure_adjoint(args, d, "fp32_refined")
+    gw64, gw32 = a64["grad_omega0"], a32["grad_omega0"]
+    return {
+        "workload": ADJ_WORKLOAD,
+        "metric": "adjoint/forward cost",
+        "value": (a64["adjoint_run_s"] - a64["forward_s"]) / a64["forward_s"],
+        "reverse_over_forward": (a64["adjoint_run_s"] - a64["forward_s"]) / a64["forward_s"],
+        "adjoint_over_forward": a64["adjoint_run_s"] / a64["forward_s"],
+        "note": "value = reverse_over_forward = (wall(ibpm_adjoint_run) - wall(forward run)) / wall(forward "
+                "run): the reverse sweep (recomputation from checkpoints + adjoint steps) per forward run; "
+                "adjoint_over_forward also counts the forward pass with checkpoints that any gradient needs",
+        "forward_s": a64["forward_s"], "adjoint_run_s": a64["adjoint_run_s"],
+        "adjoint_step_ms": a64["adj_step_ms"], "forward_step_ms": a64["fwd_step_ms"],
+        "adjoint_step_over_forward_step": a64["adj_step_ms"] / a64["fwd_step_ms"],
+        "J": a64["J"], "J_forward_run": a64["J_forward"],
+        "fd_check": {"eps": 1e-6, "fd": a64["fd"], "adjoint": a64["ad"],
+                     "rel_err": abs(a64["fd"] - a64["ad"]) / abs(a64["fd"])},
+        "grad_alpha": a64["grad_alpha"],
+        "fp32_refined": {"adjoint_over_forward": a32["adjoint_run_s"] / a32["forward_s"],
+                         "reverse_over_forward": (a32["adjoint_run_s"] - a32["forward_s"]) / a32["forward_s"],
+                         "J_rel_diff_vs_fp64": abs(a32["J"] - a64["J"]) / abs(a64["J"]),
+                         "grad_omega0_rel_diff_vs_fp64": float(np.max(np.abs(gw32 - gw64)) / np.max(np.abs(gw64))),
+                         "note": "checked against the FP64 gradient: a central difference with eps = 1e-6 "
+                                 "changes J by less than the refined forward run's own error"},
+    }
+
+
 def run_ours(args, d):
     K = args.steps
     sampler = ClockSampler(d.local)
@@ -374,6 +462,8 @@ def run_ours(args, d):
                         "launches_per_step": v[2] / 4.0} for k, v in prof.items()},
         "clocks": r32["clocks"],
     }
+    if not args.no_adjoint:
+        out["adjoint"] = adjoint_block(args, d)
     if d.world == 1 and not args.no_cpu:
         try:
             rate, secs = cpu_step_rate(args.cpu_steps, os.cpu_count() or 1)
@@ -396,6 +486,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     d = Dist()
     try:

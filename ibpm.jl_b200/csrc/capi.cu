@@ -46,7 +46,7 @@ struct ibpm_handle {
     double* d_xb = nullptr; double* d_ds = nullptr; int* d_bidx = nullptr; double* d_w = nullptr;
     int* d_body_start = nullptr;
     int* d_src_pts = nullptr; int* d_src_rows = nullptr; int* d_et_ptr = nullptr; int* d_et_k = nullptr;
-    int* d_et_w = nullptr;
+    int* d_et_w = nullptr; int* d_et_flux = nullptr;
     BodyDev body{};
     // per-step outputs
     double* hist = nullptr; int hist_cap = 0;
@@ -60,6 +60,28 @@ struct ibpm_handle {
     int cold = 2;                          // steps left that lack good initial guesses
     float* T32 = nullptr;                  // mg slabs of FP32 transform scratch
     double* Pp = nullptr;                  // A⁻¹C'E'F̃b of the previous step (level 1)
+    // discrete adjoint (allocated by the first ibpm_adjoint_run)
+    int adj_k = 0, adj_ncp = 0, adj_nsteps = 0;
+    double* tapeG = nullptr;               // [k][mg slabs]  Γ_n of the segment being reversed
+    double* tapeq = nullptr;               // [k][nq·mg]      q_n
+    double* ck = nullptr;                  // checkpoints (and the final state), ck_doubles each
+    long long ck_doubles = 0;
+    std::vector<int> ck_cur, ck_cold;
+    double* Gb = nullptr;                  // Γ̄ (mg slabs)
+    double* qb = nullptr;                  // q̄ (nq·mg)
+    double* Nb[2] = {nullptr, nullptr};    // N̄ (ping-pong)
+    double* Gt = nullptr;                  // Γ̄' and Γ̄s (mg slabs)
+    double* psib = nullptr;                // ψ̄ of one level
+    double* Wadj = nullptr;                // solve results of the adjoint level chain (mg slabs)
+    double* rb = nullptr;                  // r̄ = A⁻¹ Γ̄s (mg slabs)
+    double* qsb = nullptr;                 // q̄s (nq)
+    double* Ft = nullptr; double* Fbar = nullptr;
+    double* bcc = nullptr; double* bcv = nullptr;  // edge adjoints (mg·nbc each)
+    double* q0part = nullptr;              // [mg][blocks][2] + 2 (E' part)
+    double* stepw = nullptr;               // objective weight of each step
+    int* adj_n = nullptr;
+    double adj_wx = 0, adj_wy = 0;
+    cudaGraphExec_t gadj[2] = {nullptr, nullptr};
     // measurement
     int launches = 0;                      // kernel launches enqueued (counted always)
     bool prof_on = false;                  // eager profiling: events around every launch
@@ -97,8 +119,8 @@ void ibpm::set_global_error(const char* msg) { g_create_err = msg ? msg : ""; }
 
 // Kernel classes reported by ibpm_profile (order of IBPM_KERNEL_* in the header).
 static const char* kKernelNames[] = {"trial_rhs", "dst_x", "dst_y", "coarsify", "curl",
-                                     "E_gather", "binv_gemv", "stress", "proj_src"};
-enum { K_RHS = 0, K_DSTX, K_DSTY, K_COARSIFY, K_CURL, K_E, K_GEMV, K_STRESS, K_SRC, K_COUNT };
+                                     "E_gather", "binv_gemv", "stress", "proj_src", "adjoint"};
+enum { K_RHS = 0, K_DSTX, K_DSTY, K_COARSIFY, K_CURL, K_E, K_GEMV, K_STRESS, K_SRC, K_ADJ, K_COUNT };
 
 static int prof_pre(ibpm_handle* h, int label, double bytes) {
     ++h->launches;
@@ -384,11 +406,12 @@ static int build_coupling(ibpm_handle* h, const ibpm_problem_desc* d) {
                 rows[f].push_back({kk, (kk * 13 + l) * 13 + m});
             }
     }
-    std::vector<int> et_ptr, et_k, et_w;
+    std::vector<int> et_ptr, et_k, et_w, et_flux;
     std::map<int, int> row_of;
     et_ptr.push_back(0);
     for (auto& kv : rows) {
         row_of[kv.first] = (int)et_ptr.size() - 1;
+        et_flux.push_back(kv.first);
         for (auto& e : kv.second) { et_k.push_back(e.first); et_w.push_back(e.second); }
         et_ptr.push_back((int)et_k.size());
     }
@@ -416,7 +439,7 @@ static int build_coupling(ibpm_handle* h, const ibpm_problem_desc* d) {
         (rc = dalloc(h, &h->d_w, (size_t)h->nf * 169)) || (rc = dalloc(h, &h->d_body_start, h->nbodies + 1)) ||
         (rc = dalloc(h, &h->d_src_pts, src_pts.size())) || (rc = dalloc(h, &h->d_src_rows, src_rows.size())) ||
         (rc = dalloc(h, &h->d_et_ptr, et_ptr.size())) || (rc = dalloc(h, &h->d_et_k, et_k.size())) ||
-        (rc = dalloc(h, &h->d_et_w, et_w.size())))
+        (rc = dalloc(h, &h->d_et_w, et_w.size())) || (rc = dalloc(h, &h->d_et_flux, et_flux.size())))
         return rc;
     auto up = [&](void* dst, const void* src, size_t bytes) {
         return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->st);
@@ -432,12 +455,14 @@ static int build_coupling(ibpm_handle* h, const ibpm_problem_desc* d) {
     CK(up(h->d_et_ptr, et_ptr.data(), sizeof(int) * et_ptr.size()));
     CK(up(h->d_et_k, et_k.data(), sizeof(int) * et_k.size()));
     CK(up(h->d_et_w, et_w.data(), sizeof(int) * et_w.size()));
+    CK(up(h->d_et_flux, et_flux.data(), sizeof(int) * et_flux.size()));
     CK(cudaStreamSynchronize(h->st));  // host vectors go out of scope
     BodyDev& b = h->body;
     b.nb = nb; b.nf = h->nf; b.nbodies = h->nbodies;
     b.xb = h->d_xb; b.ds = h->d_ds; b.bidx = h->d_bidx; b.w = h->d_w; b.body_start = h->d_body_start;
     b.n_src = (int)src_pts.size(); b.src_pts = h->d_src_pts; b.src_rows = h->d_src_rows;
     b.et_ptr = h->d_et_ptr; b.et_k = h->d_et_k; b.et_w = h->d_et_w;
+    b.n_et_rows = (int)et_flux.size(); b.et_flux = h->d_et_flux;
     CK(launch_weights(g, d->h, d->offx, d->offy, b, h->st));
     return IBPM_OK;
 }
@@ -496,9 +521,14 @@ static void free_handle(ibpm_handle* h) {
     }
     if (h->T32) cudaFree(h->T32);
     if (h->Pp) cudaFree(h->Pp);
+    for (int p = 0; p < 2; ++p) if (h->gadj[p]) cudaGraphExecDestroy(h->gadj[p]);
+    void* adj[] = {h->tapeG, h->tapeq, h->ck, h->Gb, h->qb, h->Nb[0], h->Nb[1], h->Gt, h->psib, h->Wadj, h->rb,
+                   h->qsb, h->Ft, h->Fbar, h->bcc, h->bcv, h->q0part, h->stepw, h->adj_n};
+    for (void* p : adj) if (p) cudaFree(p);
     void* ptrs[] = {h->G[0], h->G[1], h->Nl[0], h->Nl[1], h->psi, h->q, h->qs, h->rhs, h->Gsrc, h->F, h->Fb,
                     h->Binv, h->nonlin1_shadow, h->d_xb, h->d_ds, h->d_bidx, h->d_w, h->d_body_start,
-                    h->d_src_pts, h->d_src_rows, h->d_et_ptr, h->d_et_k, h->d_et_w, h->hist, h->counter, h->status};
+                    h->d_src_pts, h->d_src_rows, h->d_et_ptr, h->d_et_k, h->d_et_w, h->d_et_flux, h->hist,
+                    h->counter, h->status};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (h->flush_buf) cudaFree(h->flush_buf);
     for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
@@ -650,8 +680,15 @@ extern "C" int ibpm_set_state(ibpm_handle* h, const double* Gamma, const double*
             for (int e = g.nu; e < g.nq; ++e)
                 if (ql[e] != ny0[l]) return fail(h, IBPM_ERR_UNSUPPORTED, "q0 must be uniform per level (y part)");
         }
-        for (int l = 0; l < g.mg; ++l) { h->q0x[l] = nx0[l]; h->q0y[l] = ny0[l]; }
-        h->graphs_ready = false;  // q0 is baked into the captured step
+        bool changed = false;
+        for (int l = 0; l < g.mg; ++l) {
+            changed |= h->q0x[l] != nx0[l] || h->q0y[l] != ny0[l];
+            h->q0x[l] = nx0[l]; h->q0y[l] = ny0[l];
+        }
+        if (changed) {  // q0 is baked into the captured step and its adjoint
+            h->graphs_ready = false;
+            for (int p = 0; p < 2; ++p) if (h->gadj[p]) { cudaGraphExecDestroy(h->gadj[p]); h->gadj[p] = nullptr; }
+        }
     }
     if (Gamma) CK(slab_copy(h, h->G[h->cur], Gamma, true));
     if (psi) CK(slab_copy(h, h->psi, psi, true));
@@ -911,6 +948,300 @@ extern "C" int ibpm_profile(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, do
     h->nonlin1_valid = false;
     for (int p = 0; p < 2; ++p) if (pexec[p]) cudaGraphExecDestroy(pexec[p]);
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Discrete adjoint: the transpose of the derivative of one step, checkpointed
+// recomputation, and the gradient of a time-averaged force objective.
+// ---------------------------------------------------------------------------
+
+// Transpose of the level chain of vort2flux! (curl.jl:425-440), finest level
+// first: ψ̄ = curl!ᵀ(q̄) + get_bc!ᵀ(edge adjoint of the finer level), Γ̄ += Δ⁻¹ψ̄
+// (Δ⁻¹ is symmetric).  q̄ is given on levels [0, qnlev), zero above.
+static int solves_T(ibpm_handle* h, const double* qbar, int qnlev, double* Gacc) {
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    const long long bs = g.S * mg;
+    const double slab = 16.0 * g.n1 * g.n2;
+    for (int lev = 0; lev < mg; ++lev) {
+        LAUNCH(K_ADJ, 8.0 * (g.nq + 2.0 * g.n1 * g.n2),
+               launch_adj_curlT(g, lev < qnlev ? qbar + (long long)lev * g.nq : nullptr,
+                                lev > 0 ? h->bcc + (long long)(lev - 1) * g.nbc : nullptr,
+                                lev > 0 ? h->Wadj + (long long)(lev - 1) * g.S : nullptr, h->psib,
+                                h->bcc + (long long)lev * g.nbc, h->st));
+        SlabMap one = levmap(g, 0, 1, g.S);
+        SlabMap m = levmap(g, lev, 1, bs);
+        XPassArgs a{};
+        a.in = h->psib; a.out = h->rhs; a.in_map = one; a.out_map = one;
+        a.nslabs = 1; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_PLAIN; a.emit = XEMIT_STORE;
+        LAUNCH(K_DSTX, slab, launch_dst_x(g, h->px, a, h->st));
+        LAUNCH(K_DSTY, slab, launch_dst_y(g, h->py, h->px, h->rhs, one, 1, spec(h, SPEC_DELTA), h->st));
+        XPassArgs c{};
+        c.in = h->rhs; c.out = Gacc; c.in_map = one; c.out_map = m; c.aux = h->Wadj; c.aux_map = m;
+        c.nslabs = 1; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_PLAIN; c.emit = XEMIT_ADD_STORE;
+        LAUNCH(K_DSTX, slab * 2.0, launch_dst_x(g, h->px, c, h->st));
+    }
+    return IBPM_OK;
+}
+
+// Transpose of the coarsify chain (curl.jl:419-421): coarsest level first.
+static int coarsify_T(ibpm_handle* h, double* Gacc) {
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    for (int lev = mg - 1; lev >= 1; --lev)
+        LAUNCH(K_ADJ, 8.0 * 2.25 * g.n1 * g.n2,
+               launch_adj_coarsifyT(g, Gacc, g.S, lev, lev + 1 <= mg - 1 ? lev + 1 : -1, h->st));
+    if (mg >= 2) LAUNCH(K_ADJ, 2.0 * g.n1 * g.n2, launch_zero_centre(g, Gacc + g.S, h->st));
+    return IBPM_OK;
+}
+
+// Adjoint of one step, from (Γ̄, q̄, N̄[par]) of the next state to those of
+// this one (N̄ into N̄[par^1]), with this step's forward (Γ_n, q_n) in tape
+// slot (*adj_n mod k) and objective weight stepw[*adj_n].
+static int enqueue_adjoint_step(ibpm_handle* h, int par) {
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    const long long bs = g.S * mg;
+    int rc;
+    // project_circ! and the final vort2flux!: Γ_{n+1} = coarsify(Γ'), q_{n+1} = curl ψ(Γ_{n+1})
+    CK(cudaMemcpyAsync(h->Gt, h->Gb, sizeof(double) * bs, cudaMemcpyDeviceToDevice, h->st));
+    if ((rc = solves_T(h, h->qb, mg, h->Gt))) return rc;
+    if ((rc = coarsify_T(h, h->Gt))) return rc;
+    // Γ' = Γs − e₁ A⁻¹₁ C'E' F̃b:  F̄t = ∂J/∂F̃b − E rot!ᵀ(A⁻¹₁ Γ̄'₁)
+    SlabMap l0 = levmap(g, 0, 1, bs);
+    if ((rc = poisson(h, h->Gt, l0, h->rhs, l0, h->rb, l0, 1, SPEC_AINV, XEMIT_STORE))) return rc;
+    LAUNCH(K_ADJ, 16.0 * 169 * h->nf,
+           launch_adj_E_rotT(g, h->body, h->rb, h->adj_wx, h->adj_wy, h->stepw, h->adj_n, h->Ft, h->st));
+    // F̃b = B⁻¹ E(qs + q0)
+    LAUNCH(K_ADJ, 8.0 * h->nf * (h->nf + 2.0), launch_gemv_t(h->Binv, h->Ft, h->Fbar, h->nf, h->st));
+    LAUNCH(K_ADJ, 8.0 * 4 * 169 * h->nf,
+           launch_adj_Et(g, h->body, h->Fbar, h->qsb, h->q0part + (long long)mg * adj_nlq_blocks(g) * 2, h->st));
+    // the trial vort2flux!: Γs ← coarsify(Γs), qs = curl ψs on level 1
+    if ((rc = solves_T(h, h->qsb, 1, h->Gt))) return rc;
+    if ((rc = coarsify_T(h, h->Gt))) return rc;
+    // get_trial_state!: r̄ = A⁻¹ Γ̄s (every level), then the products and stencils
+    SlabMap all = levmap(g, 0, mg, bs);
+    if ((rc = poisson(h, h->Gt, all, h->rhs, all, h->rb, all, mg, SPEC_AINV, XEMIT_STORE))) return rc;
+    AdjTrialArgs ta{};
+    ta.rb = h->rb; ta.Nb_in = h->Nb[par]; ta.Nb_out = h->Nb[par ^ 1];
+    ta.tapeG = h->tapeG; ta.tapeq = h->tapeq; ta.tape_gstride = bs; ta.tape_qstride = (long long)g.nq * mg;
+    ta.adj_n = h->adj_n; ta.k = h->adj_k;
+    ta.Gb = h->Gb; ta.qb = h->qb; ta.bcv = h->bcv; ta.q0part = h->q0part;
+    const RhsArgs ra = rhs_args(h, 0);
+    for (int l = 0; l < mg; ++l) {
+        ta.q0x[l] = h->q0x[l]; ta.q0y[l] = h->q0y[l];
+        ta.c_lap[l] = ra.c_lap[l]; ta.fac_bc[l] = ra.fac_bc[l]; ta.nl_scale[l] = ra.nl_scale[l];
+    }
+    ta.b1dt = ra.b1dt; ta.b2dt = ra.b2dt; ta.mg = mg;
+    LAUNCH(K_ADJ, 8.0 * (10.0 * g.n1 * g.n2 + 3.0 * g.nq) * mg, launch_adj_trial(g, ta, h->st));
+    LAUNCH(K_ADJ, 8.0, launch_adj_tick(h->adj_n, h->st));
+    return IBPM_OK;
+}
+
+static int adj_alloc(ibpm_handle* h, int k, int ncp, int nsteps) {
+    const Geom& g = h->g;
+    const long long bs = g.S * g.mg, qs = (long long)g.nq * g.mg;
+    const long long ckd = 3 * bs + qs + (h->Pp ? g.S : 0);
+    if (h->Gb && k == h->adj_k && ncp <= h->adj_ncp && nsteps <= h->adj_nsteps) return IBPM_OK;
+    for (int p = 0; p < 2; ++p) if (h->gadj[p]) { cudaGraphExecDestroy(h->gadj[p]); h->gadj[p] = nullptr; }
+    double** bufs[] = {&h->tapeG, &h->tapeq, &h->ck, &h->Gb, &h->qb, &h->Nb[0], &h->Nb[1], &h->Gt, &h->psib,
+                       &h->Wadj, &h->rb, &h->qsb, &h->Ft, &h->Fbar, &h->bcc, &h->bcv, &h->q0part, &h->stepw};
+    for (double** b : bufs) if (*b) { cudaFree(*b); *b = nullptr; }
+    if (h->adj_n) { cudaFree(h->adj_n); h->adj_n = nullptr; }
+    int rc;
+    const long long nq0 = (long long)g.mg * adj_nlq_blocks(g) * 2 + 2;
+    if ((rc = dalloc(h, &h->tapeG, (size_t)k * bs)) || (rc = dalloc(h, &h->tapeq, (size_t)k * qs)) ||
+        (rc = dalloc(h, &h->ck, (size_t)(ncp + 1) * ckd)) || (rc = dalloc(h, &h->Gb, bs)) ||
+        (rc = dalloc(h, &h->qb, qs)) || (rc = dalloc(h, &h->Nb[0], bs)) || (rc = dalloc(h, &h->Nb[1], bs)) ||
+        (rc = dalloc(h, &h->Gt, bs)) || (rc = dalloc(h, &h->psib, g.S)) || (rc = dalloc(h, &h->Wadj, bs)) ||
+        (rc = dalloc(h, &h->rb, bs)) || (rc = dalloc(h, &h->qsb, g.nq)) || (rc = dalloc(h, &h->Ft, h->nf)) ||
+        (rc = dalloc(h, &h->Fbar, h->nf)) || (rc = dalloc(h, &h->bcc, (size_t)g.mg * g.nbc)) ||
+        (rc = dalloc(h, &h->bcv, (size_t)g.mg * g.nbc)) || (rc = dalloc(h, &h->q0part, nq0)) ||
+        (rc = dalloc(h, &h->stepw, nsteps)) || (rc = dalloc(h, &h->adj_n, 1)))
+        return rc;
+    // slab pitch padding, the untouched flux rows of q̄s and unused edge
+    // entries must read as zero
+    for (double* p : {h->psib, h->Wadj, h->rb, h->Gt, h->Gb, h->Nb[0], h->Nb[1]})
+        CK(cudaMemsetAsync(p, 0, sizeof(double) * (p == h->psib ? g.S : bs), h->st));
+    CK(cudaMemsetAsync(h->qsb, 0, sizeof(double) * g.nq, h->st));
+    CK(cudaMemsetAsync(h->bcv, 0, sizeof(double) * g.mg * g.nbc, h->st));
+    h->adj_k = k; h->adj_ncp = ncp; h->adj_nsteps = nsteps; h->ck_doubles = ckd;
+    h->ck_cur.assign(ncp + 1, 0);
+    h->ck_cold.assign(ncp + 1, 0);
+    return IBPM_OK;
+}
+
+// Checkpoint slot c <-> the state that a step reads: Γ, q, N_{n-1} of the
+// current parity, ψ and the refined mode's projection guess.
+static int ck_copy(ibpm_handle* h, int c, bool save) {
+    const Geom& g = h->g;
+    const long long bs = g.S * g.mg, qs = (long long)g.nq * g.mg;
+    double* base = h->ck + (long long)c * h->ck_doubles;
+    if (!save) { h->cur = h->ck_cur[c]; h->cold = h->ck_cold[c]; }
+    struct { double* dev; long long n; } f[5] = {{h->G[h->cur], bs}, {h->q, qs}, {h->Nl[h->cur], bs}, {h->psi, bs},
+                                                 {h->Pp, h->Pp ? g.S : 0}};
+    long long off = 0;
+    for (auto& x : f) {
+        if (!x.n) continue;
+        if (save) CK(cudaMemcpyAsync(base + off, x.dev, sizeof(double) * x.n, cudaMemcpyDeviceToDevice, h->st));
+        else CK(cudaMemcpyAsync(x.dev, base + off, sizeof(double) * x.n, cudaMemcpyDeviceToDevice, h->st));
+        off += x.n;
+    }
+    if (save) { h->ck_cur[c] = h->cur; h->ck_cold[c] = h->cold; }
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkpoint, const ibpm_objective* obj,
+                                double* J, double* grad_Gamma0, double* grad_q0, double* grad_omega0,
+                                double* grad_alpha) {
+    if (!h || !obj || nsteps < 1 || k_checkpoint < 1) return IBPM_ERR_INVALID;
+    if (obj->window < 1 || obj->window > nsteps) return fail(h, IBPM_ERR_INVALID, "objective window must be in 1..nsteps");
+    CK(cudaSetDevice(h->device));
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    const long long bs = g.S * mg, qs = (long long)g.nq * mg;
+    const int k = std::min(k_checkpoint, nsteps);
+    const int ncp = (nsteps + k - 1) / k;
+    int rc = ensure_graphs(h, std::max(std::max(1024, h->hist_cap), k));
+    if (rc) return rc;
+    if ((rc = adj_alloc(h, k, ncp, nsteps))) return rc;
+    h->adj_wx = obj->w_cd * 2.0 * h->h / h->dt;  // CD_j = 2 (h/dt) Σ F̃x (timestepping.jl:330-354)
+    h->adj_wy = obj->w_cl * 2.0 * h->h / h->dt;
+    std::vector<double> w(nsteps, 0.0);
+    for (int n = nsteps - obj->window; n < nsteps; ++n) w[n] = 1.0 / obj->window;
+    CK(cudaMemcpyAsync(h->stepw, w.data(), sizeof(double) * nsteps, cudaMemcpyHostToDevice, h->st));
+    for (int p = 0; p < 2; ++p)
+        if (!h->gadj[p]) {
+            cudaGraph_t graph;
+            CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue_adjoint_step(h, p);
+            cudaError_t e = cudaStreamEndCapture(h->st, &graph);
+            if (rc) return rc;
+            if (e != cudaSuccess) return fail(h, IBPM_ERR_CUDA, std::string("adjoint capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&h->gadj[p], graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return fail(h, IBPM_ERR_CUDA, std::string("adjoint instantiate: ") + cudaGetErrorString(e));
+        }
+    // ---- forward pass with a checkpoint every k steps; J from CD/CL
+    CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
+    double Jv = 0.0;
+    std::vector<double> hb;
+    int done = 0;
+    while (done < nsteps) {
+        const int n = std::min(h->hist_cap, nsteps - done);
+        CK(cudaMemsetAsync(h->counter, 0, sizeof(int), h->st));
+        for (int s = 0; s < n; ++s) {
+            if ((done + s) % k == 0 && (rc = ck_copy(h, (done + s) / k, true))) return rc;
+            CK(launch_step(h));
+        }
+        hb.resize((size_t)n * 2 * h->nbodies);
+        CK(cudaMemcpyAsync(hb.data(), h->hist, sizeof(double) * hb.size(), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        for (int s = 0; s < n; ++s)
+            for (int j = 0; j < h->nbodies; ++j)
+                Jv += w[done + s] * (obj->w_cd * hb[((size_t)s * 2 + 0) * h->nbodies + j] +
+                                     obj->w_cl * hb[((size_t)s * 2 + 1) * h->nbodies + j]);
+        done += n;
+    }
+    if ((rc = ck_copy(h, ncp, true))) return rc;  // the final state, restored at the end
+    // ---- reverse sweep: recompute each segment into the tape, then adjoint steps
+    for (double* p : {h->Gb, h->Nb[0], h->Nb[1]}) CK(cudaMemsetAsync(p, 0, sizeof(double) * bs, h->st));
+    CK(cudaMemsetAsync(h->qb, 0, sizeof(double) * qs, h->st));
+    const long long nq0 = (long long)mg * adj_nlq_blocks(g) * 2 + 2;
+    CK(cudaMemsetAsync(h->q0part, 0, sizeof(double) * nq0, h->st));
+    const int last = nsteps - 1;
+    CK(cudaMemcpyAsync(h->adj_n, &last, sizeof(int), cudaMemcpyHostToDevice, h->st));
+    int par = 0;
+    for (int c = ncp - 1; c >= 0; --c) {
+        const int s0 = c * k, s1 = std::min(s0 + k, nsteps);
+        if ((rc = ck_copy(h, c, false))) return rc;
+        CK(cudaMemsetAsync(h->counter, 0, sizeof(int), h->st));
+        for (int n = s0; n < s1; ++n) {
+            const int slot = n % k;
+            CK(cudaMemcpyAsync(h->tapeG + slot * bs, h->G[h->cur], sizeof(double) * bs, cudaMemcpyDeviceToDevice,
+                               h->st));
+            CK(cudaMemcpyAsync(h->tapeq + slot * qs, h->q, sizeof(double) * qs, cudaMemcpyDeviceToDevice, h->st));
+            CK(launch_step(h));
+        }
+        for (int n = s1 - 1; n >= s0; --n) {
+            CK(cudaGraphLaunch(h->gadj[par], h->st));
+            par ^= 1;
+        }
+    }
+    // ---- gradients with respect to the initial state
+    CK(cudaStreamSynchronize(h->st));
+    if (J) *J = Jv;
+    auto slabs_out = [&](double* dst, const double* src) {
+        const size_t wbytes = sizeof(double) * g.n1, rows = (size_t)g.n2 * mg;
+        return cudaMemcpy2DAsync(dst, wbytes, src, sizeof(double) * g.P, wbytes, rows, cudaMemcpyDeviceToHost, h->st);
+    };
+    if (grad_Gamma0) CK(slabs_out(grad_Gamma0, h->Gb));
+    if (grad_q0) CK(cudaMemcpyAsync(grad_q0, h->qb, sizeof(double) * qs, cudaMemcpyDeviceToHost, h->st));
+    if (grad_omega0) {
+        // Γ₀ = coarsify([h²ω, 0, …]), q₀ = curl ψ(Γ₀): ω̄ = h² (coarsify!ᵀ(Γ̄₀ + solves!ᵀ(q̄₀)))₁
+        CK(cudaMemcpyAsync(h->Gt, h->Gb, sizeof(double) * bs, cudaMemcpyDeviceToDevice, h->st));
+        if ((rc = solves_T(h, h->qb, mg, h->Gt)) || (rc = coarsify_T(h, h->Gt))) return rc;
+        std::vector<double> G1((size_t)g.n1 * g.n2);
+        const size_t wbytes = sizeof(double) * g.n1;
+        CK(cudaMemcpy2DAsync(G1.data(), wbytes, h->Gt, sizeof(double) * g.P, wbytes, g.n2, cudaMemcpyDeviceToHost,
+                             h->st));
+        CK(cudaStreamSynchronize(h->st));
+        for (size_t i = 0; i < G1.size(); ++i) grad_omega0[i] = h->h * h->h * G1[i];
+    }
+    if (grad_alpha) {
+        // q0x = (Ux cos α − Uy sin α) hc, q0y = (Ux sin α + Uy cos α) hc (timestepping.jl:252-270)
+        std::vector<double> part(nq0);
+        CK(cudaMemcpyAsync(part.data(), h->q0part, sizeof(double) * nq0, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        const int nb = adj_nlq_blocks(g);
+        double d = 0.0;
+        for (int l = 0; l < mg; ++l) {
+            double sx = 0.0, sy = 0.0;
+            for (int b = 0; b < nb; ++b) { sx += part[2 * ((size_t)l * nb + b)]; sy += part[2 * ((size_t)l * nb + b) + 1]; }
+            if (l == 0) { sx += part[nq0 - 2]; sy += part[nq0 - 1]; }
+            const double hc = h->h * std::ldexp(1.0, l), a = h->incl;
+            d += sx * (-h->Ux * std::sin(a) - h->Uy * std::cos(a)) * hc;
+            d += sy * (h->Ux * std::cos(a) - h->Uy * std::sin(a)) * hc;
+        }
+        *grad_alpha = d;
+    }
+    if ((rc = ck_copy(h, ncp, false))) return rc;  // leave the handle at the final state
+    CK(cudaStreamSynchronize(h->st));
+    int hstatus = 0;
+    CK(cudaMemcpy(&hstatus, h->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hstatus) return fail(h, IBPM_ERR_NONFINITE, "CD/CL became non-finite");
+    return IBPM_OK;
+}
+
+// Time the adjoint step alone: graph replays of the adjoint of one step
+// (tape slot 0 repeatedly), CUDA events around each.
+extern "C" int ibpm_adjoint_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, double* step_ms) {
+    if (!h || nsteps < 1 || !step_ms) return IBPM_ERR_INVALID;
+    if (!h->gadj[0] || !h->gadj[1]) return fail(h, IBPM_ERR_INVALID, "no adjoint captured: run ibpm_adjoint_run first");
+    CK(cudaSetDevice(h->device));
+    if (flush_l2 && !h->flush_buf) {
+        h->flush_bytes = (size_t)512 << 20;
+        int rc = dalloc(h, (char**)&h->flush_buf, h->flush_bytes);
+        if (rc) return rc;
+    }
+    const int zero = 0;
+    std::vector<cudaEvent_t> ev(2 * nsteps);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (int s = 0; s < nsteps; ++s) {
+        CK(cudaMemcpyAsync(h->adj_n, &zero, sizeof(int), cudaMemcpyHostToDevice, h->st));
+        if (flush_l2) CK(cudaMemsetAsync(h->flush_buf, s & 0xff, h->flush_bytes, h->st));
+        CK(cudaEventRecord(ev[2 * s], h->st));
+        CK(cudaGraphLaunch(h->gadj[s & 1], h->st));
+        CK(cudaEventRecord(ev[2 * s + 1], h->st));
+    }
+    CK(cudaStreamSynchronize(h->st));
+    for (int s = 0; s < nsteps; ++s) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev[2 * s], ev[2 * s + 1]));
+        step_ms[s] = ms;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return IBPM_OK;
 }
 
 extern "C" const char* ibpm_kernel_name(int32_t k) {

@@ -522,6 +522,14 @@ __global__ void __launch_bounds__((N <= 1024 ? 128 : 256)) dst_x_kernel(XPassArg
                 const double* xa = a.aux + a.aux_map.off(y) + (long long)la * P;
                 oa[o] = xa[o] + (double)v.x;
                 if (hasb) oa[o + P] = xa[o + P] + (double)v.y;
+            } else if constexpr (EMIT == XEMIT_ADD_STORE) {
+                double* xa = a.aux + a.aux_map.off(y) + (long long)la * P;
+                oa[o] += v.x;
+                xa[o] = v.x;
+                if (hasb) {
+                    oa[o + P] += v.y;
+                    xa[o + P] = v.y;
+                }
             } else {  // XEMIT_ACC_SUB
                 double* xa = a.aux + a.aux_map.off(y) + (long long)la * P;
                 const double pa = xa[o] + (double)v.x;
@@ -670,7 +678,7 @@ cudaError_t launch_x_n(const Geom& g, const DstPlan& px, const XPassArgs& a, cud
     X(XLOAD_PLAIN, XEMIT_STORE) X(XLOAD_PLAIN, XEMIT_SUB) X(XLOAD_BC, XEMIT_STORE)       \
     X(XLOAD_BC, XEMIT_SUB) X(XLOAD_F32, XEMIT_F32) X(XLOAD_RES_LAP, XEMIT_F32)           \
     X(XLOAD_RES_A, XEMIT_F32) X(XLOAD_F32, XEMIT_ADD) X(XLOAD_F32, XEMIT_ADD_FROM)       \
-    X(XLOAD_F32, XEMIT_ACC_SUB)
+    X(XLOAD_F32, XEMIT_ACC_SUB) X(XLOAD_PLAIN, XEMIT_ADD_STORE)
 
 template <int N>
 cudaError_t launch_x_t(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {

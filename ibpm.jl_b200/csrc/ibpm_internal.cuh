@@ -212,7 +212,9 @@ struct SpecParams {
 //     XEMIT_F32      out = v (float)        XEMIT_ADD      out += v (double)
 //     XEMIT_ADD_FROM out = aux + v          XEMIT_ACC_SUB  aux += v; out −= aux
 enum XLoad { XLOAD_PLAIN = 0, XLOAD_BC = 1, XLOAD_F32 = 2, XLOAD_RES_LAP = 3, XLOAD_RES_A = 4 };
-enum XEmit { XEMIT_STORE = 0, XEMIT_SUB = 1, XEMIT_F32 = 2, XEMIT_ADD = 3, XEMIT_ADD_FROM = 4, XEMIT_ACC_SUB = 5 };
+//     XEMIT_ADD_STORE out += v; aux = v (double; the adjoint level chain)
+enum XEmit { XEMIT_STORE = 0, XEMIT_SUB = 1, XEMIT_F32 = 2, XEMIT_ADD = 3, XEMIT_ADD_FROM = 4, XEMIT_ACC_SUB = 5,
+             XEMIT_ADD_STORE = 6 };
 struct XPassArgs {
     const void* in; void* out;
     SlabMap in_map, out_map;
@@ -274,6 +276,8 @@ struct BodyDev {
     const int* et_ptr;      // CSR row pointer over touched flux points
     const int* et_k;        // CSR: force component index (0..nf-1), sorted ascending
     const int* et_w;        // CSR: index into w[]
+    int n_et_rows;          // touched flux points
+    const int* et_flux;     // [n_et_rows] level-1 flux index of each CSR row
 };
 cudaError_t launch_weights(const Geom& g, double h, double offx, double offy,
                            const BodyDev& b, cudaStream_t st);
@@ -292,5 +296,42 @@ cudaError_t launch_unit_src(const Geom& g, const BodyDev& b, int col0, int ncol,
 // partial pivoting of the row-major n×n matrix A; `work` holds 2 n² + 2 n
 // doubles and `info` one int (set to the failing column + 1 on a zero pivot).
 cudaError_t launch_gj_inverse(double* A, int n, double* work, int* info, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Discrete adjoint of the step (adjoint.cu)
+// ---------------------------------------------------------------------------
+cudaError_t launch_adj_curlT(const Geom& g, const double* qb, const double* prev_bc, const double* prev_W,
+                             double* psib, double* bc_out, cudaStream_t st);
+cudaError_t launch_adj_coarsifyT(const Geom& g, double* G, long long lstride, int lev, int zero_lev,
+                                 cudaStream_t st);
+cudaError_t launch_zero_centre(const Geom& g, double* G, cudaStream_t st);
+cudaError_t launch_adj_E_rotT(const Geom& g, const BodyDev& b, const double* W, double wx, double wy,
+                              const double* stepw, const int* adj_n, double* Ft, cudaStream_t st);
+cudaError_t launch_gemv_t(const double* A, const double* x, double* y, int n, cudaStream_t st);
+cudaError_t launch_adj_Et(const Geom& g, const BodyDev& b, const double* Fbar, double* qsb, double* acc,
+                          cudaStream_t st);
+// Trial-step adjoint: see adjoint.cu.
+struct AdjTrialArgs {
+    const double* rb;          // r̄ = A⁻¹ Γ̄s, mg slabs
+    const double* Nb_in;       // N̄ of the next state, mg slabs
+    double* Nb_out;            // N̄ of this state (β2 dt r̄)
+    const double* tapeG;       // forward Γ_n, mg slabs per tape slot
+    const double* tapeq;       // forward q_n, nq·mg per tape slot
+    long long tape_gstride, tape_qstride;
+    const int* adj_n;          // current step n (tape slot n % k)
+    int k;
+    double* Gb;                // out: Γ̄_n
+    double* qb;                // out: q̄_n (nq per level)
+    double* bcv;               // edge adjoints per level (mg·nbc)
+    double* q0part;            // per-block partial sums of Σq̄0 [block][2]
+    double q0x[8], q0y[8];
+    double c_lap[8], fac_bc[8], nl_scale[8];
+    double b1dt, b2dt;
+    int mg;
+};
+
+int adj_nlq_blocks(const Geom& g);
+cudaError_t launch_adj_trial(const Geom& g, const AdjTrialArgs& a, cudaStream_t st);
+cudaError_t launch_adj_tick(int* adj_n, cudaStream_t st);
 
 }  // namespace ibpm

@@ -11,7 +11,7 @@ module IBPMGPU
 
 using ..ibpm: ibpm, IBState, AbstractIBProblem, MultiGrid, RigidBody, Static, get_body_info
 
-export IBProblemGPU, sync!, push!
+export IBProblemGPU, sync!, push!, adjoint_run, set_vorticity!
 
 const LIB = get(ENV, "IBPM_GPU_LIB", joinpath(@__DIR__, "..", "lib", "libibpm_gpu.so"))
 
@@ -25,7 +25,17 @@ struct ProblemDesc
     nbodies::Int32; nb::Int32
     body_npts::Ptr{Int32}; xb::Ptr{Float64}; ds::Ptr{Float64}
     precision::Int32; device::Int32
+    refine_sweeps::Int32
 end
+
+# Mirror of ibpm_objective.
+struct Objective
+    window::Int32
+    w_cd::Float64
+    w_cl::Float64
+end
+
+const PRECISIONS = Dict(:fp64 => Int32(0), :fp32_refined => Int32(1))
 
 mutable struct IBProblemGPU <: AbstractIBProblem
     handle::Ptr{Cvoid}
@@ -39,16 +49,18 @@ lasterr(h) = unsafe_string(ccall((:ibpm_last_error, LIB), Cstring, (Ptr{Cvoid},)
 check(rc, h) = rc == 0 || error("libibpm_gpu error $rc: $(lasterr(h))")
 
 """
-    IBProblemGPU(grid, bodies, dt, Re; freestream, device=0, sync_fields=false)
+    IBProblemGPU(grid, bodies, dt, Re; freestream, device=0, sync_fields=false,
+                 precision=:fp64, refine_sweeps=1)
 
 GPU counterpart of `IBProblem(grid, bodies, dt, Re; freestream)`
 (src/pre-processing/problem-types.jl:188-199) for `RigidBody{Static}` bodies.
 The freestream functions are evaluated at t = 0, as IBState's base_flux! does
-for static bodies.
+for static bodies.  `precision = :fp32_refined` runs the sine transforms in
+FP32 with FP64-residual refinement of every Poisson solve.
 """
 function IBProblemGPU(grid::MultiGrid, bodies::Vector{<:RigidBody{Static}}, dt::Float64, Re::Float64;
                       freestream=(Ux=t->1.0, Uy=t->0.0, inclination=t->0.0), device::Integer=0,
-                      sync_fields::Bool=false)
+                      sync_fields::Bool=false, precision::Symbol=:fp64, refine_sweeps::Integer=1)
     nb, _ = get_body_info(bodies)
     xb = vcat([b.xb for b in bodies]...)           # (nb, 2) column-major
     ds = vcat([b.ds for b in bodies]...)
@@ -58,7 +70,8 @@ function IBProblemGPU(grid::MultiGrid, bodies::Vector{<:RigidBody{Static}}, dt::
         d = ProblemDesc(grid.nx, grid.ny, grid.mg, grid.h, grid.offx, grid.offy, Re, dt,
                         freestream.Ux(0.0), freestream.Uy(0.0), freestream.inclination(0.0),
                         (1.5, -0.5), length(bodies), sum(nb),
-                        pointer(npts), pointer(xb), pointer(ds), 0, device)
+                        pointer(npts), pointer(xb), pointer(ds), PRECISIONS[precision], device,
+                        refine_sweeps)
         rc = ccall((:ibpm_create, LIB), Cint, (Ref{ProblemDesc}, Ref{Ptr{Cvoid}}), d, h)
         check(rc, C_NULL)
     end
@@ -107,6 +120,51 @@ function ibpm.advance!(state::IBState, prob::IBProblemGPU, t::Float64)
     rc == -3 && return nothing          # IBPM_ERR_NONFINITE: CL carries the NaN
     check(rc, prob.handle)
     return nothing
+end
+
+"""
+    set_vorticity!(prob, ω)
+
+Start state from a finest-level vorticity field ω ((nx-1)×(ny-1)): Γ = h²ω on
+level 1, zero elsewhere and zero history, then vort2flux! (curl.jl:411-443)
+makes ψ and q consistent.  This is the start state whose gradient
+`adjoint_run` returns as `grad_omega0`.
+"""
+function set_vorticity!(prob::IBProblemGPU, ω::AbstractMatrix{Float64})
+    g = prob.model_grid
+    nΓ = (g.nx - 1) * (g.ny - 1)
+    Γ = zeros(nΓ, g.mg); Γ[:, 1] .= vec(ω) .* g.h^2
+    z = zeros(nΓ, g.mg)
+    rc = ccall((:ibpm_set_state, LIB), Cint,
+               (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+                Ptr{Float64}, Ptr{Float64}),
+               prob.handle, Γ, zeros(g.nq, g.mg), C_NULL, z, z, z, C_NULL)
+    check(rc, prob.handle)
+    check(ccall((:ibpm_vort2flux, LIB), Cint, (Ptr{Cvoid},), prob.handle), prob.handle)
+end
+
+"""
+    adjoint_run(prob, nsteps; k=50, window=nsteps, w_cd=1.0, w_cl=0.0)
+
+Discrete adjoint of `nsteps` steps from the device state: J = the mean over
+the last `window` steps of Σ_bodies (w_cd·CD + w_cl·CL), and its gradients
+with respect to the start state (Γ, q as independent inputs), to the
+vorticity the start state was built from (`set_vorticity!`), and to the
+freestream angle.  A checkpoint every `k` steps bounds the device memory.
+"""
+function adjoint_run(prob::IBProblemGPU, nsteps::Integer; k::Integer=50, window::Integer=nsteps,
+                     w_cd::Real=1.0, w_cl::Real=0.0)
+    g = prob.model_grid
+    nΓ = (g.nx - 1) * (g.ny - 1)
+    J = Ref(0.0); α = Ref(0.0)
+    gΓ = zeros(nΓ, g.mg); gq = zeros(g.nq, g.mg); gω = zeros(g.nx - 1, g.ny - 1)
+    obj = Objective(window, w_cd, w_cl)
+    rc = ccall((:ibpm_adjoint_run, LIB), Cint,
+               (Ptr{Cvoid}, Int32, Int32, Ref{Objective}, Ref{Float64}, Ptr{Float64}, Ptr{Float64},
+                Ptr{Float64}, Ref{Float64}),
+               prob.handle, nsteps, k, obj, J, gΓ, gq, gω, α)
+    check(rc, prob.handle)
+    return (J=J[], grad_Gamma0=gΓ, grad_q0=gq, grad_omega0=gω, grad_alpha=α[])
 end
 
 end # module

@@ -40,7 +40,7 @@ IBPM_ERR_NOMEM = -5
 IBPM_PREC_FP64 = 0
 IBPM_PREC_FP32_REFINED = 1
 PRECISIONS = {"fp64": IBPM_PREC_FP64, "fp32_refined": IBPM_PREC_FP32_REFINED}
-KERNEL_COUNT = 9
+KERNEL_COUNT = 10
 
 _ERRNAMES = {IBPM_ERR_INVALID: "INVALID", IBPM_ERR_CUDA: "CUDA", IBPM_ERR_NONFINITE: "NONFINITE",
              IBPM_ERR_UNSUPPORTED: "UNSUPPORTED", IBPM_ERR_NOMEM: "NOMEM"}
@@ -63,6 +63,12 @@ class ProblemDesc(C.Structure):
                 ("body_npts", C.POINTER(C.c_int32)), ("xb", C.POINTER(C.c_double)),
                 ("ds", C.POINTER(C.c_double)),
                 ("precision", C.c_int32), ("device", C.c_int32), ("refine_sweeps", C.c_int32)]
+
+
+class Objective(C.Structure):
+    """Mirror of ``ibpm_objective``: J = (1/window) Σ over the last ``window``
+    steps of Σ_bodies (w_cd CD + w_cl CL)."""
+    _fields_ = [("window", C.c_int32), ("w_cd", C.c_double), ("w_cl", C.c_double)]
 
 
 _DP = C.POINTER(C.c_double)
@@ -114,6 +120,10 @@ def load_library(path=None):
     lib.ibpm_bench.argtypes = [H, C.c_int32, C.c_int32, _DP]
     lib.ibpm_profile.restype = C.c_int
     lib.ibpm_profile.argtypes = [H, C.c_int32, C.c_int32, _DP, _DP, C.POINTER(C.c_int32)]
+    lib.ibpm_adjoint_run.restype = C.c_int
+    lib.ibpm_adjoint_run.argtypes = [H, C.c_int32, C.c_int32, C.POINTER(Objective), _DP, _DP, _DP, _DP, _DP]
+    lib.ibpm_adjoint_bench.restype = C.c_int
+    lib.ibpm_adjoint_bench.argtypes = [H, C.c_int32, C.c_int32, _DP]
     if path is None:
         _lib = lib
     return lib
@@ -449,3 +459,43 @@ def run_sim(t, state, prob):
     ``t``; stops (like the reference) on a non-finite lift coefficient."""
     cd, cl = advance(state, prob, t[0] if len(t) else 0.0, nsteps=len(t))
     return cd, cl
+
+
+# --------------------------------------------------------------------------
+# Discrete adjoint
+# --------------------------------------------------------------------------
+@dataclass
+class AdjointResult:
+    J: float
+    grad_Gamma0: np.ndarray     # (nΓ, mg), like state.Gamma
+    grad_q0: np.ndarray         # (nq, mg), like state.q
+    grad_omega0: np.ndarray     # (nΓ,): for a start state built from a finest-level vorticity
+    grad_alpha: float           # freestream angle
+
+
+def adjoint_run(prob, nsteps, k_checkpoint=50, window=None, w_cd=1.0, w_cl=0.0):
+    """Gradient of J = mean over the last ``window`` steps of Σ_bodies
+    (w_cd·CD + w_cl·CL) over ``nsteps`` steps of advance! from the problem's
+    current device state, by the discrete adjoint with a checkpoint every
+    ``k_checkpoint`` steps.  The device state ends at the final state of the
+    run (pull it with ``pull_state``)."""
+    lib = prob.lib
+    window = nsteps if window is None else window
+    obj = Objective(window=int(window), w_cd=float(w_cd), w_cl=float(w_cl))
+    nG, nq, mg = prob.grid.nGamma, prob.grid.nq, prob.grid.mg
+    J = C.c_double()
+    gG = np.zeros((nG, mg), order="F")
+    gq = np.zeros((nq, mg), order="F")
+    gw = np.zeros(nG)
+    ga = C.c_double()
+    prob._check(lib.ibpm_adjoint_run(prob.handle, int(nsteps), int(k_checkpoint), C.byref(obj), C.byref(J),
+                                     _ptr(gG), _ptr(gq), _ptr(gw), C.byref(ga)))
+    return AdjointResult(J=J.value, grad_Gamma0=gG, grad_q0=gq, grad_omega0=gw, grad_alpha=ga.value)
+
+
+def adjoint_bench_steps(prob, nsteps, flush_l2=True):
+    """Device ms of the adjoint of one step, ``nsteps`` replays (after an
+    ``adjoint_run`` on the problem)."""
+    out = np.zeros(nsteps)
+    prob._check(prob.lib.ibpm_adjoint_bench(prob.handle, int(nsteps), 1 if flush_l2 else 0, _ptr(out)))
+    return out

@@ -153,6 +153,44 @@ int ibpm_sync(ibpm_handle* h);
  */
 int ibpm_lap_inv_noalloc(int32_t nx, int32_t ny, const double* rhs, double* x, void* stream);
 
+/*
+ * Objective of the discrete adjoint: the time average, over the last `window`
+ * of the steps run, of the force coefficients summed over the bodies,
+ *   J = (1/window) Σ_{n > nsteps-window} Σ_j (w_cd CD_j(n) + w_cl CL_j(n)),
+ * CD/CL those of update_stress! (timestepping.jl:330-354).
+ */
+typedef struct ibpm_objective {
+    int32_t window;
+    double  w_cd, w_cl;
+} ibpm_objective;
+
+/*
+ * Discrete adjoint of `nsteps` steps of advance! from the current state (no
+ * counterpart in the reference, which has the forward step and a linearised
+ * problem, problem-types.jl:47-87).  The forward run stores a checkpoint of
+ * the state every `k_checkpoint` steps; the reverse sweep recomputes each
+ * segment from its checkpoint and applies the transpose of the step's
+ * derivative backwards.  Outputs (any may be NULL):
+ *   J            the objective
+ *   grad_Gamma0  ∂J/∂Γ at the start, (nΓ, mg) like Γ (Γ and q as independent)
+ *   grad_q0      ∂J/∂q at the start, (nq, mg) like q
+ *   grad_omega0  ∂J/∂ω for a start state built from a finest-level vorticity
+ *                ω as Γ = coarsify([h²ω, 0, …]), (ψ, q) = vort2flux!: (nΓ, 1)
+ *   grad_alpha   ∂J/∂α, α the freestream angle of the uniform base flux
+ * The handle is left at the final state of the run, as after ibpm_advance.
+ * Device memory: k tape entries (Γ and q) and nsteps/k checkpoints.
+ */
+int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkpoint,
+                     const ibpm_objective* obj, double* J, double* grad_Gamma0,
+                     double* grad_q0, double* grad_omega0, double* grad_alpha);
+
+/*
+ * Device time of the adjoint of one step (after an ibpm_adjoint_run), for
+ * measurement: `nsteps` graph replays, one CUDA-event pair each, L2 flushed
+ * between replays when flush_l2 != 0.  step_ms receives nsteps values.
+ */
+int ibpm_adjoint_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, double* step_ms);
+
 /* Page-locked host memory for state mirrors (faster get/set_state); NULL on
  * failure.  No counterpart in the reference (Julia arrays are pageable). */
 void* ibpm_host_alloc(int64_t bytes);
@@ -162,8 +200,8 @@ int ibpm_host_free(void* p);
  * @elapsed around run_sim!, src/ibpm.jl:71) ---------------------------- */
 
 /* Kernel classes reported by ibpm_profile. */
-#define IBPM_KERNEL_COUNT 9  /* trial_rhs, dst_x, dst_y, coarsify, curl, E_gather,
-                                binv_gemv, stress, proj_src */
+#define IBPM_KERNEL_COUNT 10 /* trial_rhs, dst_x, dst_y, coarsify, curl, E_gather,
+                                binv_gemv, stress, proj_src, adjoint */
 
 /* Name of kernel class k (0 <= k < IBPM_KERNEL_COUNT). */
 const char* ibpm_kernel_name(int32_t k);
