@@ -394,6 +394,93 @@ def adjoint_block(args, d):
     }
 
 
+# The batch workload: 64 independent static-body simulations, 16 each of
+# nx = ny in {128, 192, 256, 384} (h = 4/nx, domain [-1, 3] x [-2, 2]), 3 to 5
+# levels, Re uniform in [40, 200], cylinders (D = 1, ≈ 1 point per h) or NACA
+# 4-digit sections (chord 1, thickness uniform in [0.08, 0.18], angle of
+# attack uniform in [0, 15] deg about the leading edge, max panel ≈ h), dt =
+# 0.2 h, FP32-refined; all drawn from one seed.
+BATCH = dict(n=64, sizes=(128, 192, 256, 384), seed=5, steps=200)
+BATCH_WORKLOAD = ("64 independent simulations: nx=ny in {128,192,256,384} x16, h=4/nx, 3-5 levels, Re U[40,200], "
+                  "cylinders or NACA 4-digit (t U[0.08,0.18], aoa U[0,15] deg), dt=0.2h, fp32_refined")
+
+
+def naca_body(G, t, aoa, h):
+    """A NACA 00xx section (chord 1, rotated by aoa about its leading edge)
+    with boundary points ≈ h apart along the outline: the cosine-spaced
+    outline of make_naca crowds points far closer than h at the leading edge
+    and brings the two surfaces within h of each other near the trailing
+    edge, which makes the Schur complement nearly singular.  The outline is
+    sampled at uniform arc length h, dropping points closer than 0.75 h to
+    one already kept (CD/CL do not depend on ds: it cancels in
+    update_stress!)."""
+    dense = G.make_naca(0.0, 4001, t, chord=1.0, aoa=aoa, pivot=(0.0, 0.0)).xb
+    seg = np.sqrt(np.sum(np.diff(dense, axis=0) ** 2, axis=1))
+    s = np.concatenate([[0.0], np.cumsum(seg)])
+    n = max(8, int(round(s[-1] / h)))
+    targets = np.linspace(0.0, s[-1], n, endpoint=False)
+    pts = np.stack([np.interp(targets, s, dense[:, 0]), np.interp(targets, s, dense[:, 1])], axis=1)
+    keep = []
+    for p in pts:
+        if all(np.hypot(*(p - q)) >= 0.75 * h for q in keep):
+            keep.append(p)
+    xb = np.array(keep)
+    return G.RigidBody(xb=xb, ds=np.full(len(xb), s[-1] / len(xb)))
+
+
+def batch_specs(G, seed=BATCH["seed"]):
+    import math
+    rng = np.random.default_rng(seed)
+    specs = []
+    for nx in [s for s in BATCH["sizes"] for _ in range(BATCH["n"] // len(BATCH["sizes"]))]:
+        h = 4.0 / nx
+        mg = int(rng.integers(3, 6))
+        Re = float(rng.uniform(40.0, 200.0))
+        g = G.make_grid(h, (-1.0, 3.0, -2.0, 2.0), mg)
+        if rng.random() < 0.5:
+            body = G.make_cylinder(0.5, g.h, 0.0, 0.0, n=int(math.floor(math.pi / g.h)))
+        else:
+            t = float(rng.uniform(0.08, 0.18))
+            aoa = math.radians(float(rng.uniform(0.0, 15.0)))
+            body = naca_body(G, t, aoa, g.h)
+        specs.append(dict(grid=g, bodies=[body], dt=0.2 * g.h, Re=Re, precision="fp32_refined"))
+    return specs
+
+
+def batch_block(args, d):
+    """Batch throughput: Σ_members nx·ny·mg per step over the device time of
+    one batch step (graph launch, L2 flushed between steps), with the tuned
+    lane count and with one lane (the members one after another)."""
+    import ibpm_gpu as G
+    specs = batch_specs(G)
+    t0 = time.perf_counter()
+    b = G.Batch(specs, lanes=0, device=d.local)
+    setup_s = time.perf_counter() - t0
+    cells = sum(sp["grid"].nx * sp["grid"].ny * sp["grid"].mg for sp in specs)
+    K = BATCH["steps"]
+    b.advance(3)
+    tuned = b.lanes
+    ms = b.bench_steps(K, flush_l2=True)
+    t_tuned = float(np.sum(ms)) / 1e3
+    b.set_lanes(1)
+    b.advance(2)
+    ms1 = b.bench_steps(K, flush_l2=True)
+    t_seq = float(np.sum(ms1)) / 1e3
+    t0 = time.perf_counter()
+    forces = b.advance(K)
+    e2e_s = time.perf_counter() - t0
+    finite = all(np.all(np.isfinite(f[0])) for f in forces)
+    b.close()
+    return {"workload": BATCH_WORKLOAD, "metric": METRIC, "value": cells * K / t_tuned, "unit": METRIC,
+            "steps": K, "lanes": tuned, "ms_per_batch_step": 1e3 * t_tuned / K,
+            "one_lane": {"value": cells * K / t_seq, "ms_per_batch_step": 1e3 * t_seq / K},
+            "speedup_over_one_lane": t_seq / t_tuned,
+            "e2e": {"value": cells * K / e2e_s, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 16.0 * len(specs),
+                    "note": "ibpm_batch_advance of K steps, CD/CL of every member returned to the host"},
+            "setup_s": setup_s, "cells_per_step": cells, "forces_finite": finite}
+
+
 def run_ours(args, d):
     K = args.steps
     sampler = ClockSampler(d.local)
@@ -464,6 +551,11 @@ def run_ours(args, d):
     }
     if not args.no_adjoint:
         out["adjoint"] = adjoint_block(args, d)
+    if not args.no_batch:
+        try:
+            out["batch"] = batch_block(args, d)
+        except Exception as e:  # reported, not fatal: the headline line still prints
+            out["batch"] = {"workload": BATCH_WORKLOAD, "error": str(e)[:300]}
     if d.world == 1 and not args.no_cpu:
         try:
             rate, secs = cpu_step_rate(args.cpu_steps, os.cpu_count() or 1)
@@ -487,6 +579,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     d = Dist()
     try:

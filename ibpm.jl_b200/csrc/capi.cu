@@ -60,6 +60,8 @@ struct ibpm_handle {
     int cold = 2;                          // steps left that lack good initial guesses
     float* T32 = nullptr;                  // mg slabs of FP32 transform scratch
     double* Pp = nullptr;                  // A⁻¹C'E'F̃b of the previous step (level 1)
+    bool cluster = false;                  // level solves in one cluster launch (cluster_solve.cuh)
+    float* D32 = nullptr;                  // mg slabs: each level's last FP32 correction
     // discrete adjoint (allocated by the first ibpm_adjoint_run)
     int adj_k = 0, adj_ncp = 0, adj_nsteps = 0;
     double* tapeG = nullptr;               // [k][mg slabs]  Γ_n of the segment being reversed
@@ -119,8 +121,10 @@ void ibpm::set_global_error(const char* msg) { g_create_err = msg ? msg : ""; }
 
 // Kernel classes reported by ibpm_profile (order of IBPM_KERNEL_* in the header).
 static const char* kKernelNames[] = {"trial_rhs", "dst_x", "dst_y", "coarsify", "curl",
-                                     "E_gather", "binv_gemv", "stress", "proj_src", "adjoint"};
-enum { K_RHS = 0, K_DSTX, K_DSTY, K_COARSIFY, K_CURL, K_E, K_GEMV, K_STRESS, K_SRC, K_ADJ, K_COUNT };
+                                     "E_gather", "binv_gemv", "stress", "proj_src", "adjoint",
+                                     "resid", "level_solve"};
+enum { K_RHS = 0, K_DSTX, K_DSTY, K_COARSIFY, K_CURL, K_E, K_GEMV, K_STRESS, K_SRC, K_ADJ, K_RESID, K_LSOLVE,
+       K_COUNT };
 
 static int prof_pre(ibpm_handle* h, int label, double bytes) {
     ++h->launches;
@@ -319,6 +323,43 @@ static int correction32(ibpm_handle* h, int load, const double* b, const double*
     return IBPM_OK;
 }
 
+// FP64 residual of the levels [lev0, lev0 + nlev) into T32: RESID_LAP with the
+// coarser ψ's edge terms, or RESID_A with c of each level.
+static int resid(ibpm_handle* h, int mode, const double* b, const double* x, int lev0, int nlev, bool one_slab_src) {
+    const Geom& g = h->g;
+    const long long bs = g.S * g.mg;
+    ResidArgs a{};
+    a.b = b; a.bmap = one_slab_src ? levmap(g, 0, 1, g.S) : levmap(g, lev0, nlev, bs);
+    a.x = x; a.xmap = one_slab_src ? levmap(g, 0, 1, g.S) : levmap(g, lev0, nlev, bs);
+    a.coarse = mode == RESID_LAP ? h->psi : nullptr; a.cmap = levmap(g, lev0 + 1, nlev, bs);
+    a.r = h->T32; a.rmap = levmap(g, lev0, nlev, bs);
+    for (int l = 0; l < 8; ++l) a.cA[l] = c_lap(h, l);
+    a.mode = mode; a.mg = g.mg;
+    // the source slab of RESID_A is level 1's: its level index must read as lev0
+    if (one_slab_src) { a.bmap.lev0 = 0; a.bmap.lstride = 0; a.xmap.lstride = 0; }
+    LAUNCH(K_RESID, (8.0 * 2 + 4.0) * g.n1 * g.n2 * nlev, launch_resid(g, a, nlev, h->st));
+    return IBPM_OK;
+}
+
+// One cluster launch: the FP32 correction of level `lev` from T32, emitted as
+// ψ += d (dstore/dc for the level chain) or P += d; Γ −= P.
+static int level_solve(ibpm_handle* h, int lev, int mode, int emit, double* out, double* aux, bool chain) {
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    const long long bs = g.S * mg;
+    ClusterSolveArgs a{};
+    a.r = h->T32; a.rmap = levmap(g, lev, 1, bs);
+    a.dc = (chain && lev < mg - 1) ? h->D32 : nullptr; a.dcmap = levmap(g, lev + 1, 1, bs);
+    a.out = out; a.out_map = (emit == XEMIT_ACC_SUB || out != h->Pp) ? levmap(g, lev, 1, bs) : levmap(g, 0, 1, g.S);
+    a.aux = aux; a.aux_map = levmap(g, 0, 1, g.S);
+    a.dstore = (chain && lev > 0) ? h->D32 : nullptr; a.dstore_map = levmap(g, lev, 1, bs);
+    a.sp = spec(h, mode, 1);
+    a.emit = emit;
+    LAUNCH(K_LSOLVE, (4.0 + 16.0 + (a.dstore ? 4.0 : 0.0) + (emit == XEMIT_ACC_SUB ? 16.0 : 0.0)) * g.n1 * g.n2,
+           launch_cluster_solve(g, h->px, a, 1, h->st));
+    return IBPM_OK;
+}
+
 // vort2flux! with every level's Δ⁻¹ solve refined from the ψ in h->psi.
 static int vort2flux_refined(ibpm_handle* h, double* G, int nsw, double* q, int qnlev) {
     const Geom& g = h->g;
@@ -327,11 +368,25 @@ static int vort2flux_refined(ibpm_handle* h, double* G, int nsw, double* q, int 
     for (int lev = 1; lev < mg; ++lev)
         LAUNCH(K_COARSIFY, 8.0 * 1.25 * g.n1 * g.n2,
                launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), 1, h->st));
-    for (int lev = mg - 1; lev >= 0; --lev) {
-        const double* coarse = (lev < mg - 1) ? h->psi : nullptr;
-        for (int s = 0; s < nsw; ++s) {
-            int rc = correction32(h, XLOAD_RES_LAP, G, coarse, h->psi, 0.0, lev, XEMIT_ADD, h->psi);
-            if (rc) return rc;
+    int rc;
+    if (h->cluster && nsw == 1) {
+        // every level's residual against the present ψ at once; each level's
+        // solve then adds the edge terms of the coarser level's correction
+        if ((rc = resid(h, RESID_LAP, G, h->psi, 0, mg, false))) return rc;
+        for (int lev = mg - 1; lev >= 0; --lev)
+            if ((rc = level_solve(h, lev, SPEC_DELTA, XEMIT_ADD, h->psi, nullptr, true))) return rc;
+    } else if (h->cluster) {
+        for (int lev = mg - 1; lev >= 0; --lev)
+            for (int s = 0; s < nsw; ++s) {
+                if ((rc = resid(h, RESID_LAP, G, h->psi, lev, 1, false))) return rc;
+                if ((rc = level_solve(h, lev, SPEC_DELTA, XEMIT_ADD, h->psi, nullptr, false))) return rc;
+            }
+    } else {
+        for (int lev = mg - 1; lev >= 0; --lev) {
+            const double* coarse = (lev < mg - 1) ? h->psi : nullptr;
+            for (int s = 0; s < nsw; ++s) {
+                if ((rc = correction32(h, XLOAD_RES_LAP, G, coarse, h->psi, 0.0, lev, XEMIT_ADD, h->psi))) return rc;
+            }
         }
     }
     CurlArgs ca{};
@@ -365,8 +420,14 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
     // --- project_circ!: P = A⁻¹ C'E' F̃b refined from the previous P; Γ[1] −= P
     LAUNCH(K_SRC, 8.0 * 4 * 169 * h->nf, launch_proj_src(g, h->body, h->Fb, h->Gsrc, h->st));
     for (int s = 0; s < nsw; ++s) {
-        rc = correction32(h, XLOAD_RES_A, h->Gsrc, nullptr, h->Pp, c_lap(h, 0), 0,
-                          s + 1 < nsw ? XEMIT_ADD : XEMIT_ACC_SUB, s + 1 < nsw ? h->Pp : Gnew);
+        const bool last = s + 1 == nsw;
+        if (h->cluster) {
+            if ((rc = resid(h, RESID_A, h->Gsrc, h->Pp, 0, 1, true))) return rc;
+            rc = level_solve(h, 0, SPEC_AINV, last ? XEMIT_ACC_SUB : XEMIT_ADD, last ? Gnew : h->Pp, h->Pp, false);
+        } else {
+            rc = correction32(h, XLOAD_RES_A, h->Gsrc, nullptr, h->Pp, c_lap(h, 0), 0,
+                              last ? XEMIT_ACC_SUB : XEMIT_ADD, last ? Gnew : h->Pp);
+        }
         if (rc) return rc;
     }
     // --- vort2flux!(state.ψ, state.q, state.Γ)
@@ -521,6 +582,7 @@ static void free_handle(ibpm_handle* h) {
     }
     if (h->T32) cudaFree(h->T32);
     if (h->Pp) cudaFree(h->Pp);
+    if (h->D32) cudaFree(h->D32);
     for (int p = 0; p < 2; ++p) if (h->gadj[p]) cudaGraphExecDestroy(h->gadj[p]);
     void* adj[] = {h->tapeG, h->tapeq, h->ck, h->Gb, h->qb, h->Nb[0], h->Nb[1], h->Gt, h->psib, h->Wadj, h->rb,
                    h->qsb, h->Ft, h->Fbar, h->bcc, h->bcv, h->q0part, h->stepw, h->adj_n};
@@ -611,6 +673,15 @@ static int create_impl(ibpm_handle* h, const ibpm_problem_desc* d) {
         if ((rc = dalloc(h, &h->T32, slabs)) || (rc = dalloc(h, &h->Pp, g.S))) return rc;
         CK(cudaMemsetAsync(h->T32, 0, sizeof(float) * slabs, h->st));
         CK(cudaMemsetAsync(h->Pp, 0, sizeof(double) * g.S, h->st));
+        // one-launch level solves where the level fits a cluster (IBPM_CLUSTER=1); three passes otherwise
+        const char* nc = getenv("IBPM_CLUSTER");
+        if ((nc && nc[0] == '1') && cluster_solve_supported(g.nx, g.ny) &&
+            cluster_init_attributes(g.nx) == cudaSuccess) {
+            if ((rc = dalloc(h, &h->D32, slabs))) return rc;
+            CK(cudaMemsetAsync(h->D32, 0, sizeof(float) * slabs, h->st));
+            h->cluster = true;
+        }
+        cudaGetLastError();  // a device that cannot place the cluster leaves its error here
     }
     if ((rc = build_coupling(h, d))) return rc;
     if ((rc = build_binv(h))) return rc;
@@ -1238,6 +1309,331 @@ extern "C" int ibpm_adjoint_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_
     for (int s = 0; s < nsteps; ++s) {
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ev[2 * s], ev[2 * s + 1]));
+        step_ms[s] = ms;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return IBPM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batches of independent simulations.  Each member is an ordinary handle;
+// one step of the batch is one graph launch whose branches are the members'
+// steps, spread over `lanes` concurrent streams (members of one lane run one
+// after another).  Small grids leave most of the GPU idle when run alone;
+// run side by side they fill it.  The lane count is picked by timing.
+// ---------------------------------------------------------------------------
+struct ibpm_batch {
+    int device = 0;
+    std::vector<ibpm_handle*> m;
+    cudaStream_t st = nullptr;                 // the batch stream (fork/join point)
+    std::vector<cudaStream_t> lane_st;
+    std::vector<cudaEvent_t> ev;               // fork + one join event per lane
+    int lanes = 0;
+    int cur = 0;                               // parity shared by the members
+    int cold = 2;
+    cudaGraphExec_t g[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cold][parity]
+    int hist_cap = 0;
+    std::vector<double> cd, cl;                // [member][step][body] of the last advance
+    std::vector<int> off;                      // member offsets into cd/cl
+    int last_steps = 0;
+    std::string err;
+};
+
+static int bfail(ibpm_batch* b, int code, const std::string& msg) {
+    b->err = msg;
+    return code;
+}
+
+#define BCK(call)                                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) return bfail(b, IBPM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Zero the state of a handle, as after create.
+static int reset_state(ibpm_handle* h) {
+    const Geom& g = h->g;
+    const size_t slabs = (size_t)g.S * g.mg;
+    for (double* p : {h->G[0], h->G[1], h->Nl[0], h->Nl[1], h->psi, h->nonlin1_shadow})
+        CK(cudaMemsetAsync(p, 0, sizeof(double) * slabs, h->st));
+    CK(cudaMemsetAsync(h->q, 0, sizeof(double) * g.nq * g.mg, h->st));
+    CK(cudaMemsetAsync(h->Fb, 0, sizeof(double) * h->nf, h->st));
+    if (h->Pp) CK(cudaMemsetAsync(h->Pp, 0, sizeof(double) * g.S, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->cur = 0;
+    h->cold = 2;
+    h->nonlin1_valid = false;
+    return IBPM_OK;
+}
+
+static void batch_free_graphs(ibpm_batch* b) {
+    for (auto& row : b->g)
+        for (auto& x : row)
+            if (x) { cudaGraphExecDestroy(x); x = nullptr; }
+}
+
+// Capture the batch step of parity p (cold: the refined members' first steps).
+static int batch_capture(ibpm_batch* b, int lanes, int p, bool cold, cudaGraphExec_t* out) {
+    cudaGraph_t graph;
+    BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaEventRecord(b->ev[0], b->st);
+    int rc = IBPM_OK;
+    for (int l = 0; l < lanes && e == cudaSuccess && rc == IBPM_OK; ++l) {
+        e = cudaStreamWaitEvent(b->lane_st[l], b->ev[0], 0);
+        for (size_t i = l; i < b->m.size() && e == cudaSuccess && rc == IBPM_OK; i += lanes) {
+            ibpm_handle* h = b->m[i];
+            cudaStream_t own = h->st;
+            h->st = b->lane_st[l];                 // the member's launches join lane l
+            rc = enqueue_step(h, p, cold);
+            h->st = own;
+            if (rc) b->err = "member " + std::to_string(i) + ": " + h->err;
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(b->ev[1 + l], b->lane_st[l]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, b->ev[1 + l], 0);
+    }
+    cudaError_t ee = cudaStreamEndCapture(b->st, &graph);
+    if (rc) return rc;
+    if (e != cudaSuccess || ee != cudaSuccess)
+        return bfail(b, IBPM_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(e != cudaSuccess ? e : ee));
+    e = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return bfail(b, IBPM_ERR_CUDA, std::string("batch instantiate: ") + cudaGetErrorString(e));
+    return IBPM_OK;
+}
+
+static int batch_graphs(ibpm_batch* b, int lanes) {
+    batch_free_graphs(b);
+    bool any_refined = false;
+    for (auto* h : b->m) any_refined |= h->prec == IBPM_PREC_FP32_REFINED;
+    for (int c = 0; c < (any_refined ? 2 : 1); ++c)
+        for (int p = 0; p < 2; ++p) {
+            int rc = batch_capture(b, lanes, p, c == 1, &b->g[c][p]);
+            if (rc) return rc;
+        }
+    b->lanes = lanes;
+    return IBPM_OK;
+}
+
+static cudaError_t batch_step(ibpm_batch* b) {
+    cudaGraphExec_t ge = (b->cold > 0 && b->g[1][b->cur]) ? b->g[1][b->cur] : b->g[0][b->cur];
+    if (b->cold > 0) --b->cold;
+    const cudaError_t e = cudaGraphLaunch(ge, b->st);
+    b->cur ^= 1;
+    for (auto* h : b->m) { h->cur = b->cur; h->cold = b->cold; h->nonlin1_valid = false; }
+    return e;
+}
+
+static void batch_destroy_impl(ibpm_batch* b) {
+    if (!b) return;
+    if (b->st) cudaStreamSynchronize(b->st);
+    batch_free_graphs(b);
+    for (auto* h : b->m) { if (h) { cudaStreamSynchronize(h->st); free_handle(h); } }
+    for (auto s : b->lane_st) cudaStreamDestroy(s);
+    for (auto e : b->ev) cudaEventDestroy(e);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+// Time `steps` batch steps for each candidate lane count (powers of two up to
+// the member count); keep the fastest.  The members are reset afterwards.
+static int batch_tune(ibpm_batch* b, int steps) {
+    const int n = (int)b->m.size();
+    std::vector<int> cand;
+    for (int l = 1; l < n; l *= 2) cand.push_back(l);
+    cand.push_back(n);
+    double best = 1e300;
+    int best_l = n;
+    cudaEvent_t e0, e1;
+    BCK(cudaEventCreate(&e0));
+    BCK(cudaEventCreate(&e1));
+    int rc = IBPM_OK;
+    for (int l : cand) {
+        if ((rc = batch_graphs(b, l))) break;
+        for (int s = 0; s < 2 && rc == IBPM_OK; ++s)
+            if (batch_step(b) != cudaSuccess) rc = bfail(b, IBPM_ERR_CUDA, "batch tuning step failed");
+        if (rc) break;
+        cudaEventRecord(e0, b->st);
+        for (int s = 0; s < steps && rc == IBPM_OK; ++s)
+            if (batch_step(b) != cudaSuccess) rc = bfail(b, IBPM_ERR_CUDA, "batch tuning step failed");
+        cudaEventRecord(e1, b->st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) { rc = bfail(b, IBPM_ERR_CUDA, "batch tuning sync failed"); break; }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) { best = ms; best_l = l; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    for (auto* h : b->m)
+        if ((rc = reset_state(h))) return bfail(b, rc, h->err);
+    b->cur = 0;
+    b->cold = 2;
+    return batch_graphs(b, best_l);
+}
+
+extern "C" int ibpm_batch_create(int32_t n, const ibpm_problem_desc* descs, int32_t lanes, ibpm_batch** out) {
+    if (!out || !descs || n < 1) { g_create_err = "batch: n >= 1 descriptions and an output pointer are required"; return IBPM_ERR_INVALID; }
+    *out = nullptr;
+    if (lanes < 0 || lanes > n) { g_create_err = "batch: lanes must be in 0..n (0 = tune)"; return IBPM_ERR_INVALID; }
+    ibpm_batch* b = new ibpm_batch();
+    b->device = descs[0].device;
+    for (int i = 0; i < n; ++i) {
+        if (descs[i].device != b->device) {
+            g_create_err = "batch: all members must be on one device";
+            batch_destroy_impl(b);
+            return IBPM_ERR_INVALID;
+        }
+        ibpm_handle* h = nullptr;
+        int rc = ibpm_create(&descs[i], &h);
+        if (rc) {
+            g_create_err = "batch member " + std::to_string(i) + ": " + g_create_err;
+            batch_destroy_impl(b);
+            return rc;
+        }
+        b->m.push_back(h);
+    }
+    int rc = IBPM_OK;
+    auto done = [&](int code) {
+        if (code) { g_create_err = b->err; batch_destroy_impl(b); return code; }
+        *out = b;
+        return IBPM_OK;
+    };
+    if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess)
+        return done(bfail(b, IBPM_ERR_CUDA, "batch stream"));
+    b->lane_st.resize(n);
+    b->ev.resize(n + 1);
+    for (int i = 0; i < n; ++i)
+        if (cudaStreamCreateWithFlags(&b->lane_st[i], cudaStreamNonBlocking) != cudaSuccess)
+            return done(bfail(b, IBPM_ERR_CUDA, "batch lane stream"));
+    for (auto& e : b->ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            return done(bfail(b, IBPM_ERR_CUDA, "batch event"));
+    b->hist_cap = 1024;
+    for (auto* h : b->m)
+        if ((rc = ensure_graphs(h, b->hist_cap))) return done(bfail(b, rc, h->err));
+    b->off.assign(n + 1, 0);
+    for (int i = 0; i < n; ++i) b->off[i + 1] = b->off[i] + b->m[i]->nbodies;
+    rc = lanes == 0 ? batch_tune(b, 8) : batch_graphs(b, lanes);
+    return done(rc);
+}
+
+extern "C" int ibpm_batch_destroy(ibpm_batch* b) {
+    if (!b) return IBPM_ERR_INVALID;
+    cudaSetDevice(b->device);
+    batch_destroy_impl(b);
+    return IBPM_OK;
+}
+
+extern "C" ibpm_handle* ibpm_batch_member(ibpm_batch* b, int32_t i) {
+    if (!b || i < 0 || i >= (int)b->m.size()) return nullptr;
+    return b->m[i];
+}
+
+extern "C" int ibpm_batch_lanes(const ibpm_batch* b) { return b ? b->lanes : IBPM_ERR_INVALID; }
+
+extern "C" int ibpm_batch_set_lanes(ibpm_batch* b, int32_t lanes) {
+    if (!b || lanes < 1 || lanes > (int)b->m.size()) return IBPM_ERR_INVALID;
+    BCK(cudaSetDevice(b->device));
+    BCK(cudaStreamSynchronize(b->st));
+    return batch_graphs(b, lanes);
+}
+
+extern "C" const char* ibpm_batch_last_error(const ibpm_batch* b) {
+    return b ? b->err.c_str() : g_create_err.c_str();
+}
+
+// Check that no member was stepped, or had its state replaced, on its own.
+static int batch_sync_members(ibpm_batch* b) {
+    for (size_t i = 0; i < b->m.size(); ++i) {
+        ibpm_handle* h = b->m[i];
+        if (h->cur != b->cur)
+            return bfail(b, IBPM_ERR_INVALID, "member " + std::to_string(i) +
+                                                  " was advanced on its own: batch members must step together");
+        if (!h->graphs_ready)  // a changed base flux
+            return bfail(b, IBPM_ERR_UNSUPPORTED, "member " + std::to_string(i) + " changed its base flux");
+        b->cold = std::max(b->cold, h->cold);      // set_state on a member re-arms its first steps
+    }
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_batch_advance(ibpm_batch* b, int32_t nsteps) {
+    if (!b || nsteps < 0) return IBPM_ERR_INVALID;
+    BCK(cudaSetDevice(b->device));
+    int rc = batch_sync_members(b);
+    if (rc) return rc;
+    const int n = (int)b->m.size();
+    b->cd.assign((size_t)nsteps * b->off[n], 0.0);
+    b->cl.assign((size_t)nsteps * b->off[n], 0.0);
+    b->last_steps = nsteps;
+    for (auto* h : b->m) BCK(cudaMemsetAsync(h->status, 0, sizeof(int), b->st));
+    std::vector<double> hb;
+    int done = 0;
+    while (done < nsteps) {
+        const int k = std::min(b->hist_cap, nsteps - done);
+        for (auto* h : b->m) BCK(cudaMemsetAsync(h->counter, 0, sizeof(int), b->st));
+        for (int s = 0; s < k; ++s) BCK(batch_step(b));
+        for (int i = 0; i < n; ++i) {
+            ibpm_handle* h = b->m[i];
+            hb.resize((size_t)k * 2 * h->nbodies);
+            BCK(cudaMemcpyAsync(hb.data(), h->hist, sizeof(double) * hb.size(), cudaMemcpyDeviceToHost, b->st));
+            BCK(cudaStreamSynchronize(b->st));
+            for (int s = 0; s < k; ++s)
+                for (int j = 0; j < h->nbodies; ++j) {
+                    const size_t o = ((size_t)(done + s)) * b->off[n] + b->off[i] + j;
+                    b->cd[o] = hb[((size_t)s * 2 + 0) * h->nbodies + j];
+                    b->cl[o] = hb[((size_t)s * 2 + 1) * h->nbodies + j];
+                }
+        }
+        done += k;
+    }
+    BCK(cudaStreamSynchronize(b->st));
+    for (size_t i = 0; i < b->m.size(); ++i) {
+        int hs = 0;
+        BCK(cudaMemcpy(&hs, b->m[i]->status, sizeof(int), cudaMemcpyDeviceToHost));
+        if (hs) return bfail(b, IBPM_ERR_NONFINITE, "member " + std::to_string(i) + ": CD/CL became non-finite");
+    }
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_batch_get_forces(const ibpm_batch* b, int32_t i, double* CD, double* CL) {
+    if (!b || i < 0 || i >= (int)b->m.size()) return IBPM_ERR_INVALID;
+    const int nb = b->m[i]->nbodies, tot = b->off.back();
+    for (int s = 0; s < b->last_steps; ++s)
+        for (int j = 0; j < nb; ++j) {
+            if (CD) CD[(size_t)s * nb + j] = b->cd[(size_t)s * tot + b->off[i] + j];
+            if (CL) CL[(size_t)s * nb + j] = b->cl[(size_t)s * tot + b->off[i] + j];
+        }
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_batch_bench(ibpm_batch* b, int32_t nsteps, int32_t flush_l2, double* step_ms) {
+    if (!b || nsteps < 1 || !step_ms) return IBPM_ERR_INVALID;
+    BCK(cudaSetDevice(b->device));
+    int rc = batch_sync_members(b);
+    if (rc) return rc;
+    ibpm_handle* h0 = b->m[0];
+    if (flush_l2 && !h0->flush_buf) {
+        h0->flush_bytes = (size_t)512 << 20;
+        if ((rc = dalloc(h0, (char**)&h0->flush_buf, h0->flush_bytes))) return bfail(b, rc, h0->err);
+    }
+    std::vector<cudaEvent_t> ev(2 * nsteps);
+    for (auto& e : ev) BCK(cudaEventCreate(&e));
+    int done = 0;
+    while (done < nsteps) {
+        const int k = std::min(b->hist_cap, nsteps - done);
+        for (auto* h : b->m) BCK(cudaMemsetAsync(h->counter, 0, sizeof(int), b->st));
+        for (int s = 0; s < k; ++s) {
+            if (flush_l2) BCK(cudaMemsetAsync(h0->flush_buf, (done + s) & 0xff, h0->flush_bytes, b->st));
+            BCK(cudaEventRecord(ev[2 * (done + s)], b->st));
+            BCK(batch_step(b));
+            BCK(cudaEventRecord(ev[2 * (done + s) + 1], b->st));
+        }
+        done += k;
+    }
+    BCK(cudaStreamSynchronize(b->st));
+    for (int s = 0; s < nsteps; ++s) {
+        float ms = 0;
+        BCK(cudaEventElapsedTime(&ms, ev[2 * s], ev[2 * s + 1]));
         step_ms[s] = ms;
     }
     for (auto& e : ev) cudaEventDestroy(e);

@@ -498,10 +498,39 @@ __global__ void __launch_bounds__((N <= 1024 ? 128 : 256)) dst_x_kernel(XPassArg
             return V{(T)va, (T)vb};
         }
     };
+    // Stores that read what they update: fetch those values before the
+    // transform, so their latency overlaps it (each thread owns the same
+    // columns o = tid + k·TP of both lines throughout).
+    constexpr int EO = (N - 1 + TP - 1) / TP;
+    constexpr bool READ_OUT = (EMIT == XEMIT_SUB || EMIT == XEMIT_ADD || EMIT == XEMIT_ADD_STORE ||
+                               EMIT == XEMIT_ACC_SUB);
+    constexpr bool READ_AUX = (EMIT == XEMIT_ADD_FROM || EMIT == XEMIT_ACC_SUB);
+    const long long ooff = a.out_map.off(y) + (long long)la * P;
+    double po[EO][2], px[EO][2];
+    if constexpr (READ_OUT || READ_AUX) {
+        const double* oa = static_cast<const double*>(a.out) + ooff;
+        const double* xa = READ_AUX ? a.aux + a.aux_map.off(y) + (long long)la * P : nullptr;
+#pragma unroll
+        for (int k = 0; k < EO; ++k) {
+            const int o = tid + k * TP;
+            if (o < n1) {
+                if constexpr (READ_OUT) {
+                    po[k][0] = oa[o];
+                    po[k][1] = hasb ? oa[o + P] : 0.0;
+                }
+                if constexpr (READ_AUX) {
+                    px[k][0] = xa[o];
+                    px[k][1] = hasb ? xa[o + P] : 0.0;
+                }
+            }
+        }
+    }
     dst_pair<N, TP, T>(buf, tw, sn, tid, gid, load, [&](int o, V v) { buf[ct_pad(o)] = v; });
     gsync<TP>(gid);
-    const long long ooff = a.out_map.off(y) + (long long)la * P;
-    for (int o = tid; o < n1; o += TP) {
+#pragma unroll
+    for (int k = 0; k < EO; ++k) {
+        const int o = tid + k * TP;
+        if (o >= n1) break;
         const V v = buf[ct_pad(o)];
         if constexpr (EMIT == XEMIT_F32) {
             float* oa = static_cast<float*>(a.out) + ooff;
@@ -513,32 +542,31 @@ __global__ void __launch_bounds__((N <= 1024 ? 128 : 256)) dst_x_kernel(XPassArg
                 oa[o] = v.x;
                 if (hasb) oa[o + P] = v.y;
             } else if constexpr (EMIT == XEMIT_SUB) {
-                oa[o] -= v.x;
-                if (hasb) oa[o + P] -= v.y;
+                oa[o] = po[k][0] - v.x;
+                if (hasb) oa[o + P] = po[k][1] - v.y;
             } else if constexpr (EMIT == XEMIT_ADD) {
-                oa[o] += (double)v.x;
-                if (hasb) oa[o + P] += (double)v.y;
+                oa[o] = po[k][0] + (double)v.x;
+                if (hasb) oa[o + P] = po[k][1] + (double)v.y;
             } else if constexpr (EMIT == XEMIT_ADD_FROM) {
-                const double* xa = a.aux + a.aux_map.off(y) + (long long)la * P;
-                oa[o] = xa[o] + (double)v.x;
-                if (hasb) oa[o + P] = xa[o + P] + (double)v.y;
+                oa[o] = px[k][0] + (double)v.x;
+                if (hasb) oa[o + P] = px[k][1] + (double)v.y;
             } else if constexpr (EMIT == XEMIT_ADD_STORE) {
                 double* xa = a.aux + a.aux_map.off(y) + (long long)la * P;
-                oa[o] += v.x;
+                oa[o] = po[k][0] + v.x;
                 xa[o] = v.x;
                 if (hasb) {
-                    oa[o + P] += v.y;
+                    oa[o + P] = po[k][1] + v.y;
                     xa[o + P] = v.y;
                 }
             } else {  // XEMIT_ACC_SUB
                 double* xa = a.aux + a.aux_map.off(y) + (long long)la * P;
-                const double pa = xa[o] + (double)v.x;
+                const double pa = px[k][0] + (double)v.x;
                 xa[o] = pa;
-                oa[o] -= pa;
+                oa[o] = po[k][0] - pa;
                 if (hasb) {
-                    const double pb = xa[o + P] + (double)v.y;
+                    const double pb = px[k][1] + (double)v.y;
                     xa[o + P] = pb;
-                    oa[o + P] -= pb;
+                    oa[o + P] = po[k][1] - pb;
                 }
             }
         }

@@ -226,6 +226,38 @@ struct XPassArgs {
 };
 cudaError_t launch_dst_x(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st);
 
+// One FP32 correction solve of a whole square level in one cluster launch
+// (cluster_solve.cuh): r → x-DST, y-DST, divide, y-DST, x-DST → emit.
+//   XEMIT_ADD      out += d (and dstore = d, FP32, when set)
+//   XEMIT_ACC_SUB  aux += d; out −= aux
+struct ClusterSolveArgs {
+    const float* r; SlabMap rmap;        // FP32 right-hand side (a refinement residual)
+    const float* dc; SlabMap dcmap;      // FP32 correction of the coarser level: its edge terms are added, or null
+    double* out; SlabMap out_map;
+    double* aux; SlabMap aux_map;
+    float* dstore; SlabMap dstore_map;
+    SpecParams sp;
+    int emit;
+};
+bool cluster_solve_supported(int nx, int ny);
+cudaError_t cluster_init_attributes(int N);  // cudaErrorNotSupported when the device cannot place the cluster
+cudaError_t launch_cluster_solve(const Geom& g, const DstPlan& p, const ClusterSolveArgs& a, int nslabs,
+                                 cudaStream_t st);
+
+// FP64 residual of a refinement sweep, stored in FP32 (stencil.cu):
+//   RESID_LAP  r = b + apply_bc!(get_bc!(coarse)) − L x    (vort2flux! levels)
+//   RESID_A    r = b − (x + c L x)                         (A⁻¹ solves)
+enum ResidMode { RESID_LAP = 0, RESID_A = 1 };
+struct ResidArgs {
+    const double* b; SlabMap bmap;
+    const double* x; SlabMap xmap;
+    const double* coarse; SlabMap cmap;  // RESID_LAP: coarser-level ψ, or null
+    float* r; SlabMap rmap;
+    double cA[8];                         // RESID_A: dt / (2 Re hc²) per level
+    int mode, mg;
+};
+cudaError_t launch_resid(const Geom& g, const ResidArgs& a, int nslabs, cudaStream_t st);
+
 // y-direction pass of a Poisson-type solve, in place on every slab selected by
 // `map`: DST-I, spectral divide (SpecParams), DST-I.
 cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px_cos, void* data, SlabMap map,

@@ -40,7 +40,7 @@ IBPM_ERR_NOMEM = -5
 IBPM_PREC_FP64 = 0
 IBPM_PREC_FP32_REFINED = 1
 PRECISIONS = {"fp64": IBPM_PREC_FP64, "fp32_refined": IBPM_PREC_FP32_REFINED}
-KERNEL_COUNT = 10
+KERNEL_COUNT = 12
 
 _ERRNAMES = {IBPM_ERR_INVALID: "INVALID", IBPM_ERR_CUDA: "CUDA", IBPM_ERR_NONFINITE: "NONFINITE",
              IBPM_ERR_UNSUPPORTED: "UNSUPPORTED", IBPM_ERR_NOMEM: "NOMEM"}
@@ -120,6 +120,24 @@ def load_library(path=None):
     lib.ibpm_bench.argtypes = [H, C.c_int32, C.c_int32, _DP]
     lib.ibpm_profile.restype = C.c_int
     lib.ibpm_profile.argtypes = [H, C.c_int32, C.c_int32, _DP, _DP, C.POINTER(C.c_int32)]
+    lib.ibpm_batch_create.restype = C.c_int
+    lib.ibpm_batch_create.argtypes = [C.c_int32, C.POINTER(ProblemDesc), C.c_int32, C.POINTER(H)]
+    lib.ibpm_batch_destroy.restype = C.c_int
+    lib.ibpm_batch_destroy.argtypes = [H]
+    lib.ibpm_batch_member.restype = H
+    lib.ibpm_batch_member.argtypes = [H, C.c_int32]
+    lib.ibpm_batch_lanes.restype = C.c_int
+    lib.ibpm_batch_lanes.argtypes = [H]
+    lib.ibpm_batch_set_lanes.restype = C.c_int
+    lib.ibpm_batch_set_lanes.argtypes = [H, C.c_int32]
+    lib.ibpm_batch_last_error.restype = C.c_char_p
+    lib.ibpm_batch_last_error.argtypes = [H]
+    lib.ibpm_batch_advance.restype = C.c_int
+    lib.ibpm_batch_advance.argtypes = [H, C.c_int32]
+    lib.ibpm_batch_get_forces.restype = C.c_int
+    lib.ibpm_batch_get_forces.argtypes = [H, C.c_int32, _DP, _DP]
+    lib.ibpm_batch_bench.restype = C.c_int
+    lib.ibpm_batch_bench.argtypes = [H, C.c_int32, C.c_int32, _DP]
     lib.ibpm_adjoint_run.restype = C.c_int
     lib.ibpm_adjoint_run.argtypes = [H, C.c_int32, C.c_int32, C.POINTER(Objective), _DP, _DP, _DP, _DP, _DP]
     lib.ibpm_adjoint_bench.restype = C.c_int
@@ -274,6 +292,15 @@ class IBProblem:
         self._xb = np.ascontiguousarray(xb.T.reshape(-1))      # column-major (nb, 2)
         self._ds = np.ascontiguousarray(np.concatenate([b.ds for b in self.bodies]).astype(np.float64))
         self._npts = (C.c_int32 * len(self.bodies))(*[b.xb.shape[0] for b in self.bodies])
+        d = self._desc_of(grid, ev, beta, precision, device, refine_sweeps)
+        h = C.c_void_p()
+        rc = self.lib.ibpm_create(C.byref(d), C.byref(h))
+        if rc != IBPM_OK:
+            raise IBPMError(rc, self.lib.ibpm_last_error(None).decode())
+        self.handle = h
+        self._owns = True
+
+    def _desc_of(self, grid, ev, beta, precision, device, refine_sweeps):
         d = ProblemDesc()
         d.nx, d.ny, d.mg = grid.nx, grid.ny, grid.mg
         d.h, d.offx, d.offy = grid.h, grid.offx, grid.offy
@@ -291,11 +318,7 @@ class IBProblem:
         d.device = device
         d.refine_sweeps = int(refine_sweeps)
         self._desc = d
-        h = C.c_void_p()
-        rc = self.lib.ibpm_create(C.byref(d), C.byref(h))
-        if rc != IBPM_OK:
-            raise IBPMError(rc, self.lib.ibpm_last_error(None).decode())
-        self.handle = h
+        return d
 
     def _check(self, rc):
         if rc != IBPM_OK:
@@ -303,7 +326,8 @@ class IBProblem:
 
     def close(self):
         if getattr(self, "handle", None):
-            self.lib.ibpm_destroy(self.handle)
+            if getattr(self, "_owns", True):
+                self.lib.ibpm_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
@@ -499,3 +523,93 @@ def adjoint_bench_steps(prob, nsteps, flush_l2=True):
     out = np.zeros(nsteps)
     prob._check(prob.lib.ibpm_adjoint_bench(prob.handle, int(nsteps), 1 if flush_l2 else 0, _ptr(out)))
     return out
+
+
+# --------------------------------------------------------------------------
+# Batches of independent simulations
+# --------------------------------------------------------------------------
+class Batch:
+    """Many independent simulations advanced together: one CUDA-graph launch
+    per step whose branches are the members' steps over ``lanes`` concurrent
+    streams (``lanes=0`` picks the count by timing).  ``members`` are
+    IBProblem-like objects for push_state / pull_state / vort2flux; step them
+    only through the batch.  ``specs`` is a list of dicts with the IBProblem
+    arguments (grid, bodies, dt, Re and optionally freestream, beta,
+    precision, refine_sweeps)."""
+
+    def __init__(self, specs, lanes=0, device=0):
+        self.lib = load_library()
+        self.members = []
+        descs = (ProblemDesc * len(specs))()
+        keep = []
+        for i, sp_ in enumerate(specs):
+            m = IBProblem.__new__(IBProblem)
+            m.lib = self.lib
+            m.grid = sp_["grid"]
+            m.bodies = list(sp_["bodies"])
+            m.dt = float(sp_["dt"])
+            m.Re = float(sp_["Re"])
+            fs = sp_.get("freestream", (1.0, 0.0, 0.0))
+            ev = tuple(f(0.0) if callable(f) else float(f) for f in fs)
+            m.freestream = ev
+            m.sync_fields = sp_.get("sync_fields", False)
+            xb = np.concatenate([b.xb for b in m.bodies], axis=0)
+            m.nb = xb.shape[0]
+            m.nf = 2 * m.nb
+            m._xb = np.ascontiguousarray(xb.T.reshape(-1))
+            m._ds = np.ascontiguousarray(np.concatenate([b.ds for b in m.bodies]).astype(np.float64))
+            m._npts = (C.c_int32 * len(m.bodies))(*[b.xb.shape[0] for b in m.bodies])
+            m.Re = float(sp_["Re"])
+            d = m._desc_of(m.grid, ev, sp_.get("beta", (1.5, -0.5)), sp_.get("precision", "fp64"), device,
+                           sp_.get("refine_sweeps", 1))
+            descs[i] = d
+            keep.append(m)
+            self.members.append(m)
+        h = C.c_void_p()
+        rc = self.lib.ibpm_batch_create(len(specs), descs, int(lanes), C.byref(h))
+        if rc != IBPM_OK:
+            raise IBPMError(rc, self.lib.ibpm_batch_last_error(None).decode())
+        self.handle = h
+        for i, m in enumerate(self.members):
+            m.handle = C.c_void_p(self.lib.ibpm_batch_member(h, i))
+            m._owns = False
+
+    def _check(self, rc):
+        if rc != IBPM_OK:
+            raise IBPMError(rc, self.lib.ibpm_batch_last_error(self.handle).decode())
+
+    @property
+    def lanes(self):
+        return self.lib.ibpm_batch_lanes(self.handle)
+
+    def set_lanes(self, lanes):
+        self._check(self.lib.ibpm_batch_set_lanes(self.handle, int(lanes)))
+
+    def advance(self, nsteps=1):
+        """Advance every member; returns per-member (CD, CL) histories (nsteps, nbodies)."""
+        self._check(self.lib.ibpm_batch_advance(self.handle, int(nsteps)))
+        out = []
+        for i, m in enumerate(self.members):
+            cd = np.zeros((nsteps, len(m.bodies)))
+            cl = np.zeros((nsteps, len(m.bodies)))
+            self._check(self.lib.ibpm_batch_get_forces(self.handle, i, _ptr(cd), _ptr(cl)))
+            out.append((cd, cl))
+        return out
+
+    def bench_steps(self, nsteps, flush_l2=True):
+        out = np.zeros(nsteps)
+        self._check(self.lib.ibpm_batch_bench(self.handle, int(nsteps), 1 if flush_l2 else 0, _ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            for m in self.members:
+                m.handle = None
+            self.lib.ibpm_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

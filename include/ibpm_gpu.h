@@ -191,6 +191,33 @@ int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkpoint,
  */
 int ibpm_adjoint_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, double* step_ms);
 
+/*
+ * Batches of independent simulations (no counterpart in the reference, which
+ * runs one problem per IBProblem).  Members may differ in grid size, levels,
+ * Reynolds number, time step, bodies and precision; each is an ordinary
+ * handle (ibpm_batch_member) whose state is set and read with
+ * ibpm_set_state / ibpm_get_state.  One batch step is one CUDA-graph launch
+ * whose branches are the members' steps spread over `lanes` concurrent
+ * streams; lanes = 0 picks the lane count by timing a few steps of each
+ * power of two up to n (the members are reset to their created state
+ * afterwards).  Members must be stepped through the batch only.
+ */
+typedef struct ibpm_batch ibpm_batch;
+int ibpm_batch_create(int32_t n, const ibpm_problem_desc* descs, int32_t lanes, ibpm_batch** out);
+int ibpm_batch_destroy(ibpm_batch* b);
+ibpm_handle* ibpm_batch_member(ibpm_batch* b, int32_t i);
+/* Lane count in use; set it explicitly (1 … n; the state is kept). */
+int ibpm_batch_lanes(const ibpm_batch* b);
+int ibpm_batch_set_lanes(ibpm_batch* b, int32_t lanes);
+/* Text of the last error of the batch (or of the last failed create if b is NULL). */
+const char* ibpm_batch_last_error(const ibpm_batch* b);
+/* Advance every member by nsteps steps of advance! (timestepping.jl:35-67). */
+int ibpm_batch_advance(ibpm_batch* b, int32_t nsteps);
+/* CD/CL histories of member i over the last ibpm_batch_advance, [nsteps][nbodies_i]. */
+int ibpm_batch_get_forces(const ibpm_batch* b, int32_t i, double* CD, double* CL);
+/* Device time of each of nsteps batch steps (CUDA events; L2 flushed between steps if flush_l2). */
+int ibpm_batch_bench(ibpm_batch* b, int32_t nsteps, int32_t flush_l2, double* step_ms);
+
 /* Page-locked host memory for state mirrors (faster get/set_state); NULL on
  * failure.  No counterpart in the reference (Julia arrays are pageable). */
 void* ibpm_host_alloc(int64_t bytes);
@@ -200,8 +227,9 @@ int ibpm_host_free(void* p);
  * @elapsed around run_sim!, src/ibpm.jl:71) ---------------------------- */
 
 /* Kernel classes reported by ibpm_profile. */
-#define IBPM_KERNEL_COUNT 10 /* trial_rhs, dst_x, dst_y, coarsify, curl, E_gather,
-                                binv_gemv, stress, proj_src, adjoint */
+#define IBPM_KERNEL_COUNT 12 /* trial_rhs, dst_x, dst_y, coarsify, curl, E_gather,
+                                binv_gemv, stress, proj_src, adjoint, resid,
+                                level_solve */
 
 /* Name of kernel class k (0 <= k < IBPM_KERNEL_COUNT). */
 const char* ibpm_kernel_name(int32_t k);

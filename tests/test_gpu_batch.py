@@ -1,0 +1,62 @@
+"""Batches of independent simulations (ibpm_batch_*, through the C ABI): a
+member of a batch computes exactly what the same problem computes on its own
+handle — the batch only runs the members' steps side by side."""
+import numpy as np
+import pytest
+
+from ibpm_cases import CASES, build_bodies, oracle_problem, random_state, to_gpu_state
+
+pytestmark = pytest.mark.gpu
+MEMBERS = [("sq64_mg3", "fp64"), ("rect64x32_mg2_two", "fp64"), ("sq64_mg1_plate", "fp32_refined"),
+           ("sq64_mg3", "fp32_refined")]
+NSTEPS = 20
+
+
+def _spec(name, prec):
+    import ibpm_gpu as G
+    c = CASES[name]
+    g = G.make_grid(c["h"], c["bnd"], c["mg"])
+    return dict(grid=g, bodies=build_bodies(G, c["bodies"], g.h), dt=c["dt"], Re=c["Re"], freestream=c["fs"],
+                precision=prec)
+
+
+def _start(m, name, seed):
+    import ibpm_gpu as G
+    ost = random_state(oracle_problem(name), seed=seed)
+    st = G.IBState(m)
+    to_gpu_state(ost, st)
+    G.push_state(st, m)
+
+
+@pytest.mark.parametrize("lanes", [0, 1])
+def test_batch_members_match_single_runs(lanes):
+    import ibpm_gpu as G
+    specs = [_spec(n, p) for n, p in MEMBERS]
+    batch = G.Batch(specs, lanes=lanes)
+    assert 1 <= batch.lanes <= len(MEMBERS)
+    for i, (name, _) in enumerate(MEMBERS):
+        _start(batch.members[i], name, seed=30 + i)
+    forces = batch.advance(NSTEPS)
+    for i, (name, prec) in enumerate(MEMBERS):
+        sp = specs[i]
+        solo = G.IBProblem(sp["grid"], sp["bodies"], sp["dt"], sp["Re"], freestream=sp["freestream"],
+                           precision=prec, sync_fields=False)
+        _start(solo, name, seed=30 + i)
+        st = G.IBState(solo)
+        cd, cl = G.advance(st, solo, 0.0, nsteps=NSTEPS)
+        G.pull_state(st, solo)
+        bst = G.IBState(batch.members[i])
+        assert np.array_equal(forces[i][0], cd) and np.array_equal(forces[i][1], cl), (name, prec)
+        assert np.array_equal(bst.Gamma, st.Gamma) and np.array_equal(bst.q, st.q), (name, prec)
+        solo.close()
+    batch.close()
+
+
+def test_batch_rejects_members_stepped_alone():
+    import ibpm_gpu as G
+    batch = G.Batch([_spec("sq64_mg3", "fp64"), _spec("sq64_mg1_plate", "fp64")], lanes=2)
+    st = G.IBState(batch.members[0])
+    G.advance(st, batch.members[0], 0.0, nsteps=1)
+    with pytest.raises(G.IBPMError):
+        batch.advance(1)
+    batch.close()
