@@ -61,6 +61,11 @@ struct ibpm_handle {
     float* T32 = nullptr;                  // mg slabs of FP32 transform scratch
     double* Pp = nullptr;                  // A⁻¹C'E'F̃b of the previous step (level 1)
     bool cluster = false;                  // level solves in one cluster launch (cluster_solve.cuh)
+    // linearised problem (ibpm_set_base_state): base Γ, base q, base flux
+    bool lin = false;
+    double* GB = nullptr;
+    double* qB = nullptr;
+    double q0Bx[8] = {0}, q0By[8] = {0};
     float* D32 = nullptr;                  // mg slabs: each level's last FP32 correction
     // discrete adjoint (allocated by the first ibpm_adjoint_run)
     int adj_k = 0, adj_ncp = 0, adj_nsteps = 0;
@@ -226,6 +231,10 @@ static RhsArgs rhs_args(const ibpm_handle* h, int p) {
         ra.nl_scale[l] = 1.0 / (4.0 * (hc * hc));
     }
     ra.b1dt = h->beta[0] * h->dt; ra.b2dt = h->beta[1] * h->dt; ra.mg = g.mg;
+    if (h->lin) {
+        ra.GB = h->GB; ra.qB = h->qB;
+        for (int l = 0; l < g.mg; ++l) { ra.q0Bx[l] = h->q0Bx[l]; ra.q0By[l] = h->q0By[l]; }
+    }
     return ra;
 }
 
@@ -583,6 +592,8 @@ static void free_handle(ibpm_handle* h) {
     if (h->T32) cudaFree(h->T32);
     if (h->Pp) cudaFree(h->Pp);
     if (h->D32) cudaFree(h->D32);
+    if (h->GB) cudaFree(h->GB);
+    if (h->qB) cudaFree(h->qB);
     for (int p = 0; p < 2; ++p) if (h->gadj[p]) cudaGraphExecDestroy(h->gadj[p]);
     void* adj[] = {h->tapeG, h->tapeq, h->ck, h->Gb, h->qb, h->Nb[0], h->Nb[1], h->Gt, h->psib, h->Wadj, h->rb,
                    h->qsb, h->Ft, h->Fbar, h->bcc, h->bcv, h->q0part, h->stepw, h->adj_n};
@@ -779,6 +790,34 @@ extern "C" int ibpm_set_state(ibpm_handle* h, const double* Gamma, const double*
         if (h->Pp) CK(cudaMemsetAsync(h->Pp, 0, sizeof(double) * g.S, h->st));
         CK(cudaStreamSynchronize(h->st));
     }
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_set_base_state(ibpm_handle* h, const double* Gamma_B, const double* q_B) {
+    if (!h || !Gamma_B || !q_B) return IBPM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    const Geom& g = h->g;
+    const size_t slabs = (size_t)g.S * g.mg;
+    if (!h->GB) {
+        int rc;
+        if ((rc = dalloc(h, &h->GB, slabs)) || (rc = dalloc(h, &h->qB, (size_t)g.nq * g.mg))) return rc;
+        CK(cudaMemsetAsync(h->GB, 0, sizeof(double) * slabs, h->st));
+    }
+    CK(slab_copy(h, h->GB, Gamma_B, true));
+    CK(cudaMemcpyAsync(h->qB, q_B, sizeof(double) * g.nq * g.mg, cudaMemcpyHostToDevice, h->st));
+    if (!h->lin) {
+        // the base state carries the problem's base flux; the perturbation's is
+        // zero (base_flux! of a LinearizedIBProblem, timestepping.jl:236-250)
+        for (int l = 0; l < g.mg; ++l) {
+            h->q0Bx[l] = h->q0x[l]; h->q0By[l] = h->q0y[l];
+            h->q0x[l] = 0.0; h->q0y[l] = 0.0;
+        }
+        h->lin = true;
+    }
+    h->graphs_ready = false;
+    for (int p = 0; p < 2; ++p) if (h->gadj[p]) { cudaGraphExecDestroy(h->gadj[p]); h->gadj[p] = nullptr; }
+    h->cold = 2;
+    CK(cudaStreamSynchronize(h->st));
     return IBPM_OK;
 }
 
@@ -1167,6 +1206,7 @@ extern "C" int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkp
                                 double* grad_alpha) {
     if (!h || !obj || nsteps < 1 || k_checkpoint < 1) return IBPM_ERR_INVALID;
     if (obj->window < 1 || obj->window > nsteps) return fail(h, IBPM_ERR_INVALID, "objective window must be in 1..nsteps");
+    if (h->lin) return fail(h, IBPM_ERR_UNSUPPORTED, "the adjoint is of the nonlinear step, not of a linearised problem");
     CK(cudaSetDevice(h->device));
     const Geom& g = h->g;
     const int mg = g.mg;

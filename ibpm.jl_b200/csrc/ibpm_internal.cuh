@@ -277,6 +277,10 @@ struct RhsArgs {
     double nl_scale[8];                   // 1 / (4 hc²)
     double b1dt, b2dt;                    // β1 dt, β2 dt
     int mg;
+    // linearised problem (set: GB non-null): base Γ, base q and its base flux
+    const double* GB;
+    const double* qB;
+    double q0Bx[8], q0By[8];
 };
 cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st);
 

@@ -17,6 +17,12 @@ namespace ibpm {
 // through two DSTs with the eigenvalues 1 − Λ c (laplacian.jl:229-232), whose
 // eigenvectors are exactly the DST-I basis.
 // ---------------------------------------------------------------------------
+// LIN: the linearised problem's term (nonlinear.jl:45-65, 144-163),
+//   N = C'(DP(Q, ΓB) + DP(QB, Γ)) / (4 hc²),
+// Q the face sums of q without base flux, QB those of the base state with its
+// base flux, both products using this state's edge values ¼ get_bc!(Γ[l+1])
+// (the reference passes the perturbation's Γbc to the ΓB product too).
+template <bool LIN>
 __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
     pdl_wait();
     pdl_trigger();
@@ -53,8 +59,37 @@ __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
         return -1.0 * (QxJ(I + 1, J) * Ge(I, J - 1) + QxJ(I, J) * Ge(I - 1, J - 1));
     };
     const int i = i0 + 1, j = j0 + 1;  // Julia Γ index
-    // C' fq (rot!, curl.jl:300-312) scaled by 1/(4 hc²)
-    const double N = ((fqxJ(i + 1, j) - fqxJ(i + 1, j + 1)) + (fqyJ(i + 1, j + 1) - fqyJ(i, j + 1))) * a.nl_scale[lev];
+    double N;
+    if constexpr (!LIN) {
+        // C' fq (rot!, curl.jl:300-312) scaled by 1/(4 hc²)
+        N = ((fqxJ(i + 1, j) - fqxJ(i + 1, j + 1)) + (fqyJ(i + 1, j + 1) - fqyJ(i, j + 1))) * a.nl_scale[lev];
+    } else {
+        const double* GB = a.GB + a.Gmap.off(lev);
+        const double* qB = a.qB + (long long)lev * g.nq;
+        const double* qBy = qB + g.nu;
+        const double q0Bx = a.q0Bx[lev], q0By = a.q0By[lev];
+        auto GeB = [&](int vi, int vj) -> double {   // base Γ, this state's edge values
+            if (vj == 0 || vj == ny || vi == 0 || vi == nx) return Ge(vi, vj);
+            return GB[(long long)(vj - 1) * P + (vi - 1)];
+        };
+        auto QxL = [&](int I, int J) -> double { return qxJ(I, J) + qxJ(I, J - 1); };
+        auto QyL = [&](int I, int J) -> double { return qyJ(I, J) + qyJ(I - 1, J); };
+        auto QBx = [&](int I, int J) -> double {
+            return ((qB[(I - 1) + (long long)(J - 1) * (nx + 1)] + q0Bx) + qB[(I - 1) + (long long)(J - 2) * (nx + 1)]) + q0Bx;
+        };
+        auto QBy = [&](int I, int J) -> double {
+            return ((qBy[(I - 1) + (long long)(J - 1) * nx] + q0By) + qBy[(I - 2) + (long long)(J - 1) * nx]) + q0By;
+        };
+        auto fx = [&](int I, int J) -> double {
+            return (QyL(I, J + 1) * GeB(I - 1, J) + QyL(I, J) * GeB(I - 1, J - 1)) +
+                   (QBy(I, J + 1) * Ge(I - 1, J) + QBy(I, J) * Ge(I - 1, J - 1));
+        };
+        auto fy = [&](int I, int J) -> double {
+            return -1.0 * (QxL(I + 1, J) * GeB(I, J - 1) + QxL(I, J) * GeB(I - 1, J - 1)) +
+                   -1.0 * (QBx(I + 1, J) * Ge(I, J - 1) + QBx(I, J) * Ge(I - 1, J - 1));
+        };
+        N = ((fx(i + 1, j) - fx(i + 1, j + 1)) + (fy(i + 1, j + 1) - fy(i, j + 1))) * a.nl_scale[lev];
+    }
 
     // explicit viscous operator
     const double gc = G[(long long)j0 * P + i0];
@@ -89,7 +124,8 @@ __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
 cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st) {
     dim3 blk(32, 8);
     dim3 grid((g.n1 + 31) / 32, (g.n2 + 7) / 8, a.mg);
-    return launch_k(trial_rhs_kernel, grid, blk, 0, st, a, g);
+    return a.GB ? launch_k(trial_rhs_kernel<true>, grid, blk, 0, st, a, g)
+                : launch_k(trial_rhs_kernel<false>, grid, blk, 0, st, a, g);
 }
 
 // ---------------------------------------------------------------------------

@@ -98,6 +98,8 @@ def load_library(path=None):
                                C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     lib.ibpm_set_state.restype = C.c_int
     lib.ibpm_set_state.argtypes = [H] + [_DP] * 7
+    lib.ibpm_set_base_state.restype = C.c_int
+    lib.ibpm_set_base_state.argtypes = [H, _DP, _DP]
     lib.ibpm_get_state.restype = C.c_int
     lib.ibpm_get_state.argtypes = [H] + [_DP] * 7
     lib.ibpm_advance.restype = C.c_int
@@ -336,6 +338,14 @@ class IBProblem:
         except Exception:
             pass
 
+    def set_base_state(self, base):
+        """LinearizedIBProblem(base, prob, dt) (problem-types.jl:47-87): step the
+        linearisation about the host state ``base`` (its Γ and q; the base flux
+        is the problem's) from now on.  The state's own q0 becomes zero."""
+        G = np.asfortranarray(base.Gamma, dtype=np.float64)
+        q = np.asfortranarray(base.q, dtype=np.float64)
+        self._check(self.lib.ibpm_set_base_state(self.handle, _ptr(G), _ptr(q)))
+
     def binv(self):
         """prob.Binv (laplacian.jl:274) as an (nf, nf) array."""
         out = np.empty((self.nf, self.nf), order="F")
@@ -361,6 +371,50 @@ class IBState:
         self.CD = np.zeros(len(prob.bodies))
         self.CL = np.zeros(len(prob.bodies))
         pull_state(self, prob)
+
+    # The vector space of states (state-types.jl:57-155): scaling and sums act
+    # on Γ, q, ψ and the nonlinear terms; the inner product is that of q (the
+    # kinetic energy), as Krylov stability runs use it
+    # (benchmarks/cyl40_stability/run_krylov.jl:30-42).
+    _VEC = ("Gamma", "q", "psi")
+
+    def copy(self):
+        """copy!(similar(v), v): a host mirror with every field copied."""
+        w = IBState.__new__(IBState)
+        for name in ("q", "q0", "Gamma", "psi", "Fb", "CD", "CL"):
+            setattr(w, name, np.array(getattr(self, name), order="F"))
+        w.nonlin = [np.array(a, order="F") for a in self.nonlin]
+        return w
+
+    def rmul(self, alpha):
+        """rmul!(v, α): v ← α v in place."""
+        for name in self._VEC:
+            getattr(self, name)[...] *= alpha
+        for a in self.nonlin:
+            a *= alpha
+        return self
+
+    def axpby(self, alpha, v, beta):
+        """axpby!(α, v, β, w) with w = self: w ← α v + β w, evaluated as the
+        reference does, (β/α w + v) α."""
+        self.rmul(beta / alpha)
+        for name in self._VEC:
+            getattr(self, name)[...] += getattr(v, name)
+        for a, b in zip(self.nonlin, v.nonlin):
+            a += b
+        return self.rmul(alpha)
+
+    def axpy(self, alpha, v):
+        """axpy!(α, v, w) with w = self: w ← α v + w."""
+        return self.axpby(alpha, v, 1.0)
+
+    def dot(self, other):
+        """dot(v, w) = dot(v.q, w.q)."""
+        return float(np.vdot(self.q, other.q))
+
+    def norm(self):
+        """norm(v) = norm(v.q)."""
+        return float(np.linalg.norm(self.q))
 
 
 class PinnedArray:

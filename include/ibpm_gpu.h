@@ -103,6 +103,18 @@ int ibpm_set_state(ibpm_handle* h, const double* Gamma, const double* q,
                    const double* q0, const double* psi, const double* nonlin1,
                    const double* nonlin2, const double* Fb);
 
+/*
+ * Turn the handle into LinearizedIBProblem(base_state, prob, dt)
+ * (problem-types.jl:47-87): from now on ibpm_advance steps the linearisation
+ * about the base state (Γ_B (nΓ, mg), q_B (nq, mg), with the problem's base
+ * flux), whose nonlinear term is C'(Q⊗Γ_B + Q_B⊗Γ)/(4hc²) (nonlinear.jl:45-65,
+ * 144-163); the state's own base flux becomes zero (timestepping.jl:236-250).
+ * May be called again to change the base state.  The adjoint
+ * (ibpm_adjoint_run) is that of the nonlinear step and refuses a linearised
+ * handle.
+ */
+int ibpm_set_base_state(ibpm_handle* h, const double* Gamma_B, const double* q_B);
+
 /* Copy the state out (NULL pointers are skipped). */
 int ibpm_get_state(ibpm_handle* h, double* Gamma, double* q, double* q0,
                    double* psi, double* nonlin1, double* nonlin2, double* Fb);

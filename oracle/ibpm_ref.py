@@ -534,6 +534,9 @@ class IBProblem:
     E: object = field(init=False)
     B: np.ndarray = field(init=False, default=None)
     Binv: np.ndarray = field(init=False, default=None)
+    # LinearizedIBProblem (problem-types.jl:47-87): base Γ and averaged base
+    # flux QB per level, or None for the nonlinear problem
+    base: tuple = field(init=False, default=None)
 
     def __post_init__(self):
         g = self.grid
@@ -631,9 +634,24 @@ class IBState:
                        self.Fb.copy(), self.CD.copy(), self.CL.copy())
 
 
+def linearize(prob, base_state):
+    """LinearizedIBProblem(base_state, base_prob, dt) (problem-types.jl:65-86):
+    the same model and matrices, with ΓB = base Γ and QB = avg_flux of the
+    base state INCLUDING its base flux (the IBProblem avg_flux,
+    problem-types.jl:78-83).  Returns a shallow copy of ``prob``."""
+    import copy
+    lp = copy.copy(prob)
+    QBx, QBy = avg_flux(base_state.qx, base_state.qy, base_state.q0x, base_state.q0y, prob.grid)
+    lp.base = (base_state.Gamma.copy(), QBx, QBy)
+    return lp
+
+
 def base_flux(prob, t=0.0):
-    """timestepping.jl:252-270 (InertialMotion): uniform q0 per level."""
+    """timestepping.jl:252-270 (InertialMotion): uniform q0 per level; zero
+    for a linearized problem (timestepping.jl:236-250)."""
     g = prob.grid
+    if prob.base is not None:
+        return np.zeros((g.mg, g.nx + 1, g.ny)), np.zeros((g.mg, g.nx, g.ny + 1))
     a = prob.inclination
     q0x = np.zeros((g.mg, g.nx + 1, g.ny))
     q0y = np.zeros((g.mg, g.nx, g.ny + 1))
@@ -677,8 +695,13 @@ def get_trial_state(state, prob):
             fac = 0.25 * dt / (prob.Re * hc ** 2)
             apply_bc(rhsbc, bc, fac, g)
         bc = bc * 0.25                                        # nonlinear.jl:183
-        N1[lev] = nonlinear(state.Gamma[lev], state.qx[lev], state.qy[lev],
-                            state.q0x[lev], state.q0y[lev], bc, hc, g)
+        if prob.base is None:
+            N1[lev] = nonlinear(state.Gamma[lev], state.qx[lev], state.qy[lev],
+                                state.q0x[lev], state.q0y[lev], bc, hc, g)
+        else:                                                 # nonlinear.jl:45-65,144-163
+            GB, QBx, QBy = prob.base
+            N1[lev] = nonlinear_linearized(state.Gamma[lev], state.qx[lev], state.qy[lev],
+                                           GB[lev], QBx[lev], QBy[lev], bc, hc, g)
         state.nonlin[0][lev] = N1[lev]
         rhs = a_level(state.Gamma[lev], prob, lev)            # :111
         for n, b in enumerate(prob.beta):                     # :113-115

@@ -106,3 +106,57 @@ def test_single_grid_cylinder_known_answer():
     assert abs(cd[-1, 0] / ref - 1) < 1e-6
     assert np.min(np.abs(cd[900:, 0] / ref - 1)) < 2e-8
     assert np.all(np.abs(cl[:, 0]) < 1e-7)           # symmetric flow: lift at round-off level
+
+
+def test_linearized_step_is_linear():
+    """The LinearizedIBProblem step (problem-types.jl:47-87) on a single grid is
+    linear in the perturbation state: step(a x + b y) = a step(x) + b step(y).
+    (With nested grids it is not quite: the reference hands the perturbation's
+    edge values ¼ get_bc!(Γ[l+1]) to the product with the base Γ too,
+    nonlinear.jl:144-163, which adds a term quadratic in the perturbation.)"""
+    import numpy as np
+    from ibpm_cases import oracle_problem, random_state
+    from oracle import ibpm_ref as R
+    prob = oracle_problem("sq64_mg1_plate")
+    base = random_state(prob, seed=1)
+    lp = R.linearize(prob, base)
+    def pert(seed):
+        st = random_state(prob, seed=seed)
+        st.q0x[...] = 0.0
+        st.q0y[...] = 0.0
+        return st
+    x, y = pert(2), pert(3)
+    z = x.copy()
+    a, b = 0.7, -1.3
+    z.Gamma = a * x.Gamma + b * y.Gamma
+    z.qx, z.qy = a * x.qx + b * y.qx, a * x.qy + b * y.qy
+    z.nonlin = [a * x.nonlin[k] + b * y.nonlin[k] for k in range(2)]
+    for st in (x, y, z):
+        R.advance(st, lp)
+    assert np.max(np.abs(z.Gamma - (a * x.Gamma + b * y.Gamma))) <= 1e-12 * np.max(np.abs(z.Gamma))
+    assert abs(z.CD[0] - (a * x.CD[0] + b * y.CD[0])) <= 1e-12 * max(abs(z.CD[0]), 1e-30) + 1e-15
+
+
+def test_state_vector_space():
+    """IBState arithmetic of the host mirror (state-types.jl:57-155)."""
+    import numpy as np
+    import ibpm_gpu as G
+    rng = np.random.default_rng(0)
+
+    def st():
+        s = G.IBState.__new__(G.IBState)
+        s.q, s.q0 = rng.standard_normal((30, 2)), np.zeros((30, 2))
+        s.Gamma, s.psi = rng.standard_normal((12, 2)), rng.standard_normal((12, 2))
+        s.nonlin = [rng.standard_normal((12, 2)), rng.standard_normal((12, 2))]
+        s.Fb, s.CD, s.CL = np.zeros((4, 1)), np.zeros(1), np.zeros(1)
+        return s
+    v, w = st(), st()
+    w0 = w.copy()
+    w.axpby(2.0, v, 3.0)
+    for name in ("Gamma", "q", "psi"):
+        assert np.allclose(getattr(w, name), 2.0 * getattr(v, name) + 3.0 * getattr(w0, name), rtol=1e-14)
+    assert np.allclose(w.nonlin[1], 2.0 * v.nonlin[1] + 3.0 * w0.nonlin[1], rtol=1e-14)
+    assert np.isclose(v.dot(w0), float(np.sum(v.q * w0.q)))
+    assert np.isclose(v.norm(), np.sqrt(v.dot(v)))
+    u = v.copy().rmul(0.0)
+    assert not np.any(u.Gamma) and not np.any(u.q)
