@@ -71,8 +71,10 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // E (regT!, interface-coupling.jl:122-133) on (q + q0): one warp per force
 // component and batch member.  F[bt*F_bstride + kk*F_kstride].
+// A moving grid's base flux (MovingFlux, level 1) replaces the uniform q0x, q0y.
 __global__ void E_kernel(BodyDev b, Geom g, const double* __restrict__ q, long long q_stride, int nbatch,
-                         double q0x, double q0y, double* F, long long F_bstride, long long F_kstride) {
+                         double q0x, double q0y, double* F, long long F_bstride, long long F_kstride,
+                         MovingFlux mv) {
     pdl_wait();
     pdl_trigger();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -83,13 +85,16 @@ __global__ void E_kernel(BodyDev b, Geom g, const double* __restrict__ q, long l
     const double* qq = q + (long long)bt * q_stride;
     const int bx = b.bidx[k], by = b.bidx[b.nb + k];
     const double* w = b.w + (long long)kk * 169;
+    const double* mrow = mv.tab ? moving_row(mv) : nullptr;
     double acc = 0.0;
     for (int t = lane; t < 169; t += 32) {
         const int l = t / 13, m = t % 13;
         const int I = bx + l - 6, J = by + m - 6;
         double qv;
-        if (comp == 0) qv = qq[(I - 1) + (long long)(J - 1) * (g.nx + 1)] + q0x;
-        else qv = qq[g.nu + (I - 1) + (long long)(J - 1) * g.nx] + q0y;
+        if (comp == 0)
+            qv = qq[(I - 1) + (long long)(J - 1) * (g.nx + 1)] + (mrow ? moving_q0x(mv, mrow, J, g.ny, mv.h) : q0x);
+        else
+            qv = qq[g.nu + (I - 1) + (long long)(J - 1) * g.nx] + (mrow ? moving_q0y(mv, mrow, I, g.nx, mv.h) : q0y);
         acc += w[t] * qv;
     }
     acc = warp_sum(acc);
@@ -97,14 +102,15 @@ __global__ void E_kernel(BodyDev b, Geom g, const double* __restrict__ q, long l
 }
 
 cudaError_t launch_E(const Geom& g, const BodyDev& b, const double* q, long long q_stride, int nbatch,
-                     double q0x, double q0y, double* F, long long F_stride, cudaStream_t st) {
+                     double q0x, double q0y, double* F, long long F_stride, cudaStream_t st,
+                     const MovingFlux& mv) {
     // F_stride > 0: batch stride with unit component stride; F_stride < 0:
     // component stride |F_stride| with unit batch stride (columns of B).
     const long long bs = F_stride > 0 ? F_stride : 1;
     const long long ks = F_stride > 0 ? 1 : -F_stride;
     const long long warps = (long long)b.nf * nbatch;
     const int blocks = (int)((warps * 32 + 255) / 256);
-    return launch_k(E_kernel, dim3(blocks), dim3(256), 0, st, b, g, q, q_stride, nbatch, q0x, q0y, F, bs, ks);
+    return launch_k(E_kernel, dim3(blocks), dim3(256), 0, st, b, g, q, q_stride, nbatch, q0x, q0y, F, bs, ks, mv);
 }
 
 // y = A x, A row-major n×n: one warp per row (F̃b .= Binv*F̃b, timestepping.jl:160).

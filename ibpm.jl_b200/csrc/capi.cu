@@ -67,6 +67,11 @@ struct ibpm_handle {
     double* qB = nullptr;
     double q0Bx[8] = {0}, q0By[8] = {0};
     float* D32 = nullptr;                  // mg slabs: each level's last FP32 correction
+    // moving grid (ibpm_set_moving_grid): per-step (Ω, Ux0, Uy0) rows indexed by `counter`
+    bool moving = false;
+    double mv_xc = 0, mv_yc = 0;
+    double mv_last[3] = {0, 0, 0};         // the row of the last step run (or of t = 0)
+    double* mtab = nullptr; int mtab_cap = 0;
     // discrete adjoint (allocated by the first ibpm_adjoint_run)
     int adj_k = 0, adj_ncp = 0, adj_nsteps = 0;
     double* tapeG = nullptr;               // [k][mg slabs]  Γ_n of the segment being reversed
@@ -218,6 +223,26 @@ static double c_lap(const ibpm_handle* h, int lev) {
     return h->dt / (2.0 * h->Re * (hc * hc));  // laplacian.jl:225
 }
 
+// The moving grid's base flux for the kernels, or none (uniform q0x, q0y).
+static MovingFlux mv_of(const ibpm_handle* h) {
+    MovingFlux m;
+    if (!h->moving) return m;
+    m.tab = h->mtab; m.step = h->counter;
+    m.h = h->h; m.offx = h->offx; m.offy = h->offy; m.xc = h->mv_xc; m.yc = h->mv_yc;
+    return m;
+}
+
+// (Ω, Ux0, Uy0) of base_flux! for a MovingGrid (timestepping.jl:283-296) from
+// the motion's U, V, θ, θ̇ at the step's t and the problem's free stream.
+static void moving_rates(const ibpm_handle* h, const double* m, double* r) {
+    const double U = m[0], V = m[1], a = -m[2];
+    double Ux0 = U * std::cos(a) - V * std::sin(a);
+    double Uy0 = U * std::sin(a) + V * std::cos(a);
+    Ux0 += h->Ux * std::cos(h->incl) - h->Uy * std::sin(h->incl);
+    Uy0 += h->Ux * std::sin(h->incl) + h->Uy * std::cos(h->incl);
+    r[0] = -m[3]; r[1] = Ux0; r[2] = Uy0;
+}
+
 static RhsArgs rhs_args(const ibpm_handle* h, int p) {
     const Geom& g = h->g;
     RhsArgs ra{};
@@ -231,6 +256,7 @@ static RhsArgs rhs_args(const ibpm_handle* h, int p) {
         ra.nl_scale[l] = 1.0 / (4.0 * (hc * hc));
     }
     ra.b1dt = h->beta[0] * h->dt; ra.b2dt = h->beta[1] * h->dt; ra.mg = g.mg;
+    ra.mv = mv_of(h);
     if (h->lin) {
         ra.GB = h->GB; ra.qB = h->qB;
         for (int l = 0; l < g.mg; ++l) { ra.q0Bx[l] = h->q0Bx[l]; ra.q0By[l] = h->q0By[l]; }
@@ -281,7 +307,7 @@ static int enqueue_step_fp64(ibpm_handle* h, int p) {
     rc = vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->qs, 0, 0, 1);  // only the level-1 trial flux is read
     if (rc) return rc;
     // --- boundary_forces! (timestepping.jl:154-163) and update_stress! (:330-354)
-    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st));
+    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h)));
     LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
     LAUNCH(K_STRESS, 8.0 * 3 * h->nb,
            launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
@@ -422,7 +448,7 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
     rc = vort2flux_refined(h, Gnew, nsw, h->qs, 1);  // only the level-1 trial flux is read
     if (rc) return rc;
     // --- boundary_forces! and update_stress! (FP64)
-    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st));
+    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h)));
     LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
     LAUNCH(K_STRESS, 8.0 * 3 * h->nb,
            launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
@@ -592,6 +618,7 @@ static void free_handle(ibpm_handle* h) {
     if (h->T32) cudaFree(h->T32);
     if (h->Pp) cudaFree(h->Pp);
     if (h->D32) cudaFree(h->D32);
+    if (h->mtab) cudaFree(h->mtab);
     if (h->GB) cudaFree(h->GB);
     if (h->qB) cudaFree(h->qB);
     for (int p = 0; p < 2; ++p) if (h->gadj[p]) cudaGraphExecDestroy(h->gadj[p]);
@@ -751,7 +778,7 @@ extern "C" int ibpm_set_state(ibpm_handle* h, const double* Gamma, const double*
     if (!h) return IBPM_ERR_INVALID;
     CK(cudaSetDevice(h->device));
     const Geom& g = h->g;
-    if (q0) {
+    if (q0 && !h->moving) {  // a moving grid's q0 is recomputed at every step (timestepping.jl:41-43)
         double nx0[8], ny0[8];
         for (int l = 0; l < g.mg; ++l) {
             const double* ql = q0 + (size_t)l * g.nq;
@@ -833,13 +860,45 @@ extern "C" int ibpm_get_state(ibpm_handle* h, double* Gamma, double* q, double* 
     if (nonlin1) CK(slab_copy(h, nonlin1, h->nonlin1_valid ? h->nonlin1_shadow : h->Nl[h->cur], false));
     if (Fb) CK(cudaMemcpyAsync(Fb, h->Fb, sizeof(double) * h->nf, cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
-    if (q0) {
+    if (q0 && h->moving) {
+        // the base flux of the last step's motion row, by the device's formula
+        const double* r = h->mv_last;
+        for (int l = 0; l < g.mg; ++l) {
+            const double hc = h->h * std::ldexp(1.0, l);
+            double* ql = q0 + (size_t)l * g.nq;
+            for (int j = 1; j <= g.ny; ++j) {
+                const double y = (((j - 0.5) - 0.5 * g.ny) * hc + (0.5 * g.ny) * h->h) - h->offy;
+                const double v = (y - h->mv_yc) * (-hc * r[0]) + hc * r[1];
+                for (int i = 0; i <= g.nx; ++i) ql[i + (size_t)(j - 1) * (g.nx + 1)] = v;
+            }
+            for (int i = 1; i <= g.nx; ++i) {
+                const double x = (((i - 0.5) - 0.5 * g.nx) * hc + (0.5 * g.nx) * h->h) - h->offx;
+                const double v = (x - h->mv_xc) * (hc * r[0]) + hc * r[2];
+                for (int j = 0; j <= g.ny; ++j) ql[g.nu + (i - 1) + (size_t)j * g.nx] = v;
+            }
+        }
+    } else if (q0) {
         for (int l = 0; l < g.mg; ++l) {
             double* ql = q0 + (size_t)l * g.nq;
             for (int e = 0; e < g.nu; ++e) ql[e] = h->q0x[l];
             for (int e = g.nu; e < g.nq; ++e) ql[e] = h->q0y[l];
         }
     }
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_set_moving_grid(ibpm_handle* h, double xc, double yc, const double* motion0) {
+    if (!h || !motion0) return IBPM_ERR_INVALID;
+    if (h->nbodies != 1) return fail(h, IBPM_ERR_UNSUPPORTED, "a moving grid carries exactly one body");
+    if (h->lin) return fail(h, IBPM_ERR_UNSUPPORTED, "a linearised problem has no moving-grid base flux");
+    if (!std::isfinite(xc) || !std::isfinite(yc)) return fail(h, IBPM_ERR_INVALID, "xc and yc must be finite");
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->st));
+    h->moving = true;
+    h->mv_xc = xc; h->mv_yc = yc;
+    moving_rates(h, motion0, h->mv_last);
+    h->graphs_ready = false;  // the step now reads the per-step rows
+    for (int p = 0; p < 2; ++p) if (h->gadj[p]) { cudaGraphExecDestroy(h->gadj[p]); h->gadj[p] = nullptr; }
     return IBPM_OK;
 }
 
@@ -851,6 +910,15 @@ static int ensure_graphs(ibpm_handle* h, int cap) {
         int rc = dalloc(h, &h->hist, (size_t)cap * 2 * h->nbodies);
         if (rc) return rc;
         h->hist_cap = cap;
+    }
+    if (h->moving && h->mtab_cap < h->hist_cap) {
+        if (h->mtab) cudaFree(h->mtab);
+        h->mtab = nullptr;
+        h->mtab_cap = 0;
+        int rc = dalloc(h, &h->mtab, (size_t)h->hist_cap * 3);
+        if (rc) return rc;
+        CK(cudaMemsetAsync(h->mtab, 0, sizeof(double) * 3 * h->hist_cap, h->st));
+        h->mtab_cap = h->hist_cap;
     }
     const int nkind = h->prec == IBPM_PREC_FP32_REFINED ? 2 : 1;
     for (int kind = 0; kind < nkind; ++kind)
@@ -885,9 +953,9 @@ static cudaError_t launch_step(ibpm_handle* h) {
     return e;
 }
 
-extern "C" int ibpm_advance(ibpm_handle* h, double t, int32_t nsteps, double* CD_out, double* CL_out) {
-    (void)t;
-    if (!h || nsteps < 0) return IBPM_ERR_INVALID;
+// Steps of ibpm_advance and ibpm_advance_moving; `motion` (moving grid only)
+// holds each step's U, V, θ, θ̇.
+static int advance_impl(ibpm_handle* h, int32_t nsteps, const double* motion, double* CD_out, double* CL_out) {
     if (nsteps == 0) return IBPM_OK;
     CK(cudaSetDevice(h->device));
     const int cap = std::max(1024, std::min(nsteps, 4096));
@@ -898,6 +966,14 @@ extern "C" int ibpm_advance(ibpm_handle* h, double t, int32_t nsteps, double* CD
     int done = 0;
     while (done < nsteps) {
         const int n = std::min(h->hist_cap, nsteps - done);
+        if (motion) {
+            // this chunk's rows; the copy is ordered after the previous chunk's steps
+            std::vector<double> rows((size_t)3 * n);
+            for (int s = 0; s < n; ++s) moving_rates(h, motion + 4 * (size_t)(done + s), &rows[3 * (size_t)s]);
+            CK(cudaMemcpyAsync(h->mtab, rows.data(), sizeof(double) * rows.size(), cudaMemcpyHostToDevice, h->st));
+            CK(cudaStreamSynchronize(h->st));
+            std::copy(rows.end() - 3, rows.end(), h->mv_last);
+        }
         CK(cudaMemsetAsync(h->counter, 0, sizeof(int), h->st));
         for (int s = 0; s < n; ++s) CK(launch_step(h));
         h->nonlin1_valid = false;
@@ -918,6 +994,22 @@ extern "C" int ibpm_advance(ibpm_handle* h, double t, int32_t nsteps, double* CD
     CK(cudaStreamSynchronize(h->st));
     if (hstatus) return fail(h, IBPM_ERR_NONFINITE, "CD/CL became non-finite");
     return IBPM_OK;
+}
+
+extern "C" int ibpm_advance(ibpm_handle* h, double t, int32_t nsteps, double* CD_out, double* CL_out) {
+    (void)t;
+    if (!h || nsteps < 0) return IBPM_ERR_INVALID;
+    if (h->moving) return fail(h, IBPM_ERR_INVALID, "a moving grid needs each step's motion: use ibpm_advance_moving");
+    return advance_impl(h, nsteps, nullptr, CD_out, CL_out);
+}
+
+extern "C" int ibpm_advance_moving(ibpm_handle* h, int32_t nsteps, const double* motion, double* CD_out,
+                                   double* CL_out) {
+    if (!h || nsteps < 0 || (nsteps > 0 && !motion)) return IBPM_ERR_INVALID;
+    if (!h->moving) return fail(h, IBPM_ERR_INVALID, "not a moving grid: call ibpm_set_moving_grid first");
+    for (int64_t e = 0; e < 4 * (int64_t)nsteps; ++e)
+        if (!std::isfinite(motion[e])) return fail(h, IBPM_ERR_INVALID, "motion values must be finite");
+    return advance_impl(h, nsteps, motion, CD_out, CL_out);
 }
 
 extern "C" int ibpm_vort2flux(ibpm_handle* h) {
@@ -1207,6 +1299,7 @@ extern "C" int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkp
     if (!h || !obj || nsteps < 1 || k_checkpoint < 1) return IBPM_ERR_INVALID;
     if (obj->window < 1 || obj->window > nsteps) return fail(h, IBPM_ERR_INVALID, "objective window must be in 1..nsteps");
     if (h->lin) return fail(h, IBPM_ERR_UNSUPPORTED, "the adjoint is of the nonlinear step, not of a linearised problem");
+    if (h->moving) return fail(h, IBPM_ERR_UNSUPPORTED, "the adjoint is of the static-body step, not of a moving grid");
     CK(cudaSetDevice(h->device));
     const Geom& g = h->g;
     const int mg = g.mg;
@@ -1422,6 +1515,10 @@ static int batch_capture(ibpm_batch* b, int lanes, int p, bool cold, cudaGraphEx
         e = cudaStreamWaitEvent(b->lane_st[l], b->ev[0], 0);
         for (size_t i = l; i < b->m.size() && e == cudaSuccess && rc == IBPM_OK; i += lanes) {
             ibpm_handle* h = b->m[i];
+            if (h->moving) {
+                rc = bfail(b, IBPM_ERR_UNSUPPORTED, "member " + std::to_string(i) + " is a moving grid (not batched)");
+                break;
+            }
             cudaStream_t own = h->st;
             h->st = b->lane_st[l];                 // the member's launches join lane l
             rc = enqueue_step(h, p, cold);

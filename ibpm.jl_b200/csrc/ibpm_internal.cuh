@@ -263,6 +263,31 @@ cudaError_t launch_resid(const Geom& g, const ResidArgs& a, int nslabs, cudaStre
 cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px_cos, void* data, SlabMap map,
                          int nslabs, const SpecParams& sp, cudaStream_t st);
 
+// Base flux of a moving grid (base_flux!, timestepping.jl:273-318): on level
+// spacing hc, q0x = YY·(−hc Ω) + hc Ux0 at every x-flux of row J and
+// q0y = XX·(hc Ω) + hc Uy0 at every y-flux of column I, with the face
+// coordinates of models.jl:145-152, YY = ((J − ½ − ny/2) hc + (ny/2) h − offy) − yc
+// and XX likewise in x.  (Ω, Ux0, Uy0) of the running step are row *step of
+// `tab`, `step` being the per-step counter the force kernel advances.  The
+// reference evaluates these without fused multiply-adds; so does this.
+struct MovingFlux {
+    const double* tab = nullptr;   // [steps][3]: Ω, Ux0, Uy0; nullptr: uniform base flux
+    const int* step = nullptr;
+    double h = 0, offx = 0, offy = 0, xc = 0, yc = 0;
+};
+
+__device__ __forceinline__ const double* moving_row(const MovingFlux& m) { return m.tab + 3 * (*m.step); }
+
+// q0 of x-flux row J (1-based) and of y-flux column I (1-based) on spacing hc
+__device__ __forceinline__ double moving_q0x(const MovingFlux& m, const double* r, int J, int ny, double hc) {
+    const double y = __dadd_rn(__dadd_rn(__dmul_rn((J - 0.5) - 0.5 * ny, hc), __dmul_rn(0.5 * ny, m.h)), -m.offy);
+    return __dadd_rn(__dmul_rn(__dadd_rn(y, -m.yc), __dmul_rn(-hc, r[0])), __dmul_rn(hc, r[1]));
+}
+__device__ __forceinline__ double moving_q0y(const MovingFlux& m, const double* r, int I, int nx, double hc) {
+    const double x = __dadd_rn(__dadd_rn(__dmul_rn((I - 0.5) - 0.5 * nx, hc), __dmul_rn(0.5 * nx, m.h)), -m.offx);
+    return __dadd_rn(__dmul_rn(__dadd_rn(x, -m.xc), __dmul_rn(hc, r[0])), __dmul_rn(hc, r[2]));
+}
+
 // Stencil kernels (stencil.cu)
 struct RhsArgs {
     const double* G; SlabMap Gmap;        // state Γ (all levels)
@@ -281,6 +306,7 @@ struct RhsArgs {
     const double* GB;
     const double* qB;
     double q0Bx[8], q0By[8];
+    MovingFlux mv;                        // moving grid: per-face q0 replaces q0x/q0y
 };
 cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st);
 
@@ -319,7 +345,7 @@ cudaError_t launch_weights(const Geom& g, double h, double offx, double offy,
                            const BodyDev& b, cudaStream_t st);
 cudaError_t launch_E(const Geom& g, const BodyDev& b, const double* q, long long q_stride,
                      int nbatch, double q0x, double q0y, double* F, long long F_stride,
-                     cudaStream_t st);
+                     cudaStream_t st, const MovingFlux& mv = MovingFlux{});
 cudaError_t launch_gemv(const double* A, const double* x, double* y, int n, cudaStream_t st);
 cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double dt,
                           double* hist, int* counter, int* status, cudaStream_t st);

@@ -35,6 +35,10 @@ __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
     const double* q = a.q + (long long)lev * g.nq;
     const double* qy = q + g.nu;
     const double q0x = a.q0x[lev], q0y = a.q0y[lev];
+    // moving grid: the base flux varies along y on x-faces and along x on y-faces
+    const bool mov = a.mv.tab != nullptr;
+    const double* mrow = mov ? moving_row(a.mv) : nullptr;
+    const double hc = mov ? ldexp(a.mv.h, lev) : 0.0;
 
     CoarseBC cb;
     cb.rc = (lev < a.mg - 1) ? a.G + a.Gmap.off(lev + 1) : nullptr;
@@ -51,8 +55,10 @@ __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
     auto qxJ = [&](int I, int J) -> double { return q[(I - 1) + (long long)(J - 1) * (nx + 1)]; };
     auto qyJ = [&](int I, int J) -> double { return qy[(I - 1) + (long long)(J - 1) * nx]; };
     // avg_flux (nonlinear.jl:17-38)
-    auto QxJ = [&](int I, int J) -> double { return ((qxJ(I, J) + q0x) + qxJ(I, J - 1)) + q0x; };
-    auto QyJ = [&](int I, int J) -> double { return ((qyJ(I, J) + q0y) + qyJ(I - 1, J)) + q0y; };
+    auto q0xJ = [&](int J) -> double { return mov ? moving_q0x(a.mv, mrow, J, ny, hc) : q0x; };
+    auto q0yI = [&](int I) -> double { return mov ? moving_q0y(a.mv, mrow, I, nx, hc) : q0y; };
+    auto QxJ = [&](int I, int J) -> double { return ((qxJ(I, J) + q0xJ(J)) + qxJ(I, J - 1)) + q0xJ(J - 1); };
+    auto QyJ = [&](int I, int J) -> double { return ((qyJ(I, J) + q0yI(I)) + qyJ(I - 1, J)) + q0yI(I - 1); };
     // direct_product_loops! (nonlinear.jl:73-114)
     auto fqxJ = [&](int I, int J) -> double { return QyJ(I, J + 1) * Ge(I - 1, J) + QyJ(I, J) * Ge(I - 1, J - 1); };
     auto fqyJ = [&](int I, int J) -> double {

@@ -2,6 +2,7 @@
 #
 # Binds libibpm_gpu.so (include/ibpm_gpu.h) with ccall and adds
 #     advance!(state::ibpm.IBState, prob::IBProblemGPU, t::Float64)
+# for static bodies and for one body on a MovingGrid
 # so callers of the reference's advance! (src/timestepping/timestepping.jl:35-67),
 # run_sim! (src/ibpm.jl:90-106) included, run unchanged.  The GPU owns the
 # state between calls; `prob.sync_fields = true` copies Γ, ψ, q and the
@@ -9,7 +10,8 @@
 # and F̃b come back and `sync!(state, prob)` pulls the fields on demand.
 module IBPMGPU
 
-using ..ibpm: ibpm, IBState, AbstractIBProblem, MultiGrid, RigidBody, Static, get_body_info
+using ..ibpm: ibpm, IBState, AbstractIBProblem, MultiGrid, RigidBody, Static, MovingGrid, MotionType,
+              get_body_info
 
 export IBProblemGPU, sync!, push!, adjoint_run, set_vorticity!
 
@@ -43,6 +45,7 @@ mutable struct IBProblemGPU <: AbstractIBProblem
     nbodies::Int
     dt::Float64
     sync_fields::Bool
+    motion::Union{Nothing, MovingGrid}
 end
 
 lasterr(h) = unsafe_string(ccall((:ibpm_last_error, LIB), Cstring, (Ptr{Cvoid},), h))
@@ -53,12 +56,14 @@ check(rc, h) = rc == 0 || error("libibpm_gpu error $rc: $(lasterr(h))")
                  precision=:fp64, refine_sweeps=1)
 
 GPU counterpart of `IBProblem(grid, bodies, dt, Re; freestream)`
-(src/pre-processing/problem-types.jl:188-199) for `RigidBody{Static}` bodies.
-The freestream functions are evaluated at t = 0, as IBState's base_flux! does
-for static bodies.  `precision = :fp32_refined` runs the sine transforms in
-FP32 with FP64-residual refinement of every Poisson solve.
+(src/pre-processing/problem-types.jl:188-199) for `RigidBody{Static}` bodies,
+or one `RigidBody{MovingGrid}` (its base flux is recomputed from the motion at
+every step's t, timestepping.jl:41-43, 273-318).  The freestream functions are
+evaluated at t = 0, as IBState's base_flux! does for static bodies.
+`precision = :fp32_refined` runs the sine transforms in FP32 with
+FP64-residual refinement of every Poisson solve.
 """
-function IBProblemGPU(grid::MultiGrid, bodies::Vector{<:RigidBody{Static}}, dt::Float64, Re::Float64;
+function IBProblemGPU(grid::MultiGrid, bodies::Vector{<:RigidBody}, dt::Float64, Re::Float64;
                       freestream=(Ux=t->1.0, Uy=t->0.0, inclination=t->0.0), device::Integer=0,
                       sync_fields::Bool=false, precision::Symbol=:fp64, refine_sweeps::Integer=1)
     nb, _ = get_body_info(bodies)
@@ -75,13 +80,25 @@ function IBProblemGPU(grid::MultiGrid, bodies::Vector{<:RigidBody{Static}}, dt::
         rc = ccall((:ibpm_create, LIB), Cint, (Ref{ProblemDesc}, Ref{Ptr{Cvoid}}), d, h)
         check(rc, C_NULL)
     end
-    p = IBProblemGPU(h[], grid, length(bodies), dt, sync_fields)
+    mt = MotionType(bodies)
+    motion = mt == MovingGrid ? bodies[1].motion : nothing
+    mt == Static || mt == MovingGrid || error("IBProblemGPU: bodies must be Static or one MovingGrid")
+    p = IBProblemGPU(h[], grid, length(bodies), dt, sync_fields, motion)
     finalizer(p) do x
         x.handle == C_NULL || ccall((:ibpm_destroy, LIB), Cint, (Ptr{Cvoid},), x.handle)
         x.handle = C_NULL
     end
+    if motion !== nothing
+        # rotation about the IBModel's (0, 0), as IBProblem builds it (models.jl:127-153)
+        rc = ccall((:ibpm_set_moving_grid, LIB), Cint, (Ptr{Cvoid}, Float64, Float64, Ptr{Float64}),
+                   p.handle, 0.0, 0.0, motion_row(motion, 0.0))
+        check(rc, p.handle)
+    end
     return p
 end
+
+"U, V, θ, θ̇ of a MovingGrid at t (motion-types.jl:40-48)."
+motion_row(m::MovingGrid, t::Float64) = Float64[m.U(t), m.V(t), m.θ(t), m.θ̇(t)]
 
 "Copy every IBState field to the device (the reference's column-major layouts)."
 function push!(state::IBState, prob::IBProblemGPU)
@@ -112,8 +129,13 @@ the loop.
 """
 function ibpm.advance!(state::IBState, prob::IBProblemGPU, t::Float64)
     cd = zeros(prob.nbodies); cl = zeros(prob.nbodies)
-    rc = ccall((:ibpm_advance, LIB), Cint, (Ptr{Cvoid}, Float64, Int32, Ptr{Float64}, Ptr{Float64}),
-               prob.handle, t, 1, cd, cl)
+    rc = if prob.motion === nothing
+        ccall((:ibpm_advance, LIB), Cint, (Ptr{Cvoid}, Float64, Int32, Ptr{Float64}, Ptr{Float64}),
+              prob.handle, t, 1, cd, cl)
+    else
+        ccall((:ibpm_advance_moving, LIB), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+              prob.handle, 1, motion_row(prob.motion, t), cd, cl)
+    end
     state.CD .= cd
     state.CL .= cl
     prob.sync_fields && sync!(state, prob)

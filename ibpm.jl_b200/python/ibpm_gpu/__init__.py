@@ -8,6 +8,7 @@ with the same names and argument meanings:
                                        src/structure-domain/sample-bodies.jl:17-134
 * ``IBProblem(grid, bodies, dt, Re, freestream=...)``
                                        src/pre-processing/problem-types.jl:188-199
+* ``MovingGrid(U, V, theta, theta_dot)`` src/structure-domain/motion-types.jl:40-48
 * ``IBState(prob)``                    src/pre-processing/state-types.jl:271-293
 * ``advance(state, prob, t)``          advance!(state, prob, t), src/timestepping/timestepping.jl:35-67
 * ``vort2flux(state, prob)``           vort2flux!(ψ, q, Γ, model, mg), src/fluid-operators/curl.jl:411-443
@@ -104,6 +105,10 @@ def load_library(path=None):
     lib.ibpm_get_state.argtypes = [H] + [_DP] * 7
     lib.ibpm_advance.restype = C.c_int
     lib.ibpm_advance.argtypes = [H, C.c_double, C.c_int32, _DP, _DP]
+    lib.ibpm_set_moving_grid.restype = C.c_int
+    lib.ibpm_set_moving_grid.argtypes = [H, C.c_double, C.c_double, _DP]
+    lib.ibpm_advance_moving.restype = C.c_int
+    lib.ibpm_advance_moving.argtypes = [H, C.c_int32, _DP, _DP, _DP]
     lib.ibpm_vort2flux.restype = C.c_int
     lib.ibpm_vort2flux.argtypes = [H]
     lib.ibpm_get_binv.restype = C.c_int
@@ -200,13 +205,34 @@ def make_grid(h, boundary, mg=1):
 
 
 @dataclass
+class MovingGrid:
+    """MovingGrid (motion-types.jl:40-48): the grid moves with the body.  U, V
+    are the lab-frame free stream, theta the body frame's angular position
+    (minus the aerodynamic pitch) and theta_dot its rate: callables of t.
+    xc, yc are kept for parity; the reference's IBProblem takes the rotational
+    flux about the IBModel's (0, 0) (models.jl:127-153), and so does this."""
+    U: object
+    V: object
+    theta: object
+    theta_dot: object
+    xc: float = 0.0
+    yc: float = 0.0
+
+    def row(self, t):
+        """(U, V, θ, θ̇) at t."""
+        return (float(self.U(t)), float(self.V(t)), float(self.theta(t)), float(self.theta_dot(t)))
+
+
+@dataclass
 class RigidBody:
-    """RigidBody{Static} (body-types.jl:10-16): points xb (nb, 2) and ds (nb,)."""
+    """RigidBody (body-types.jl:10-16): points xb (nb, 2), ds (nb,) and the
+    motion (None: Static; or a MovingGrid)."""
     xb: np.ndarray
     ds: np.ndarray
+    motion: object = None
 
 
-def make_cylinder(r, h, x0, y0, n=0):
+def make_cylinder(r, h, x0, y0, n=0, motion=None):
     """sample-bodies.jl:42-65 (n = 0 chooses ds ≈ 2h)."""
     if n == 0:
         n = int(math.floor(2 * math.pi * r / h / 2))
@@ -214,10 +240,10 @@ def make_cylinder(r, h, x0, y0, n=0):
     xhat = r * np.cos(spt)
     yhat = r * np.sin(spt)
     ds = math.sqrt((xhat[1] - xhat[0]) ** 2 + (yhat[1] - yhat[0]) ** 2)
-    return RigidBody(xb=np.stack([xhat + x0, yhat + y0], axis=1), ds=np.full(n, ds))
+    return RigidBody(xb=np.stack([xhat + x0, yhat + y0], axis=1), ds=np.full(n, ds), motion=motion)
 
 
-def make_plate(L, alpha, h, x0, y0, n=0):
+def make_plate(L, alpha, h, x0, y0, n=0, motion=None):
     """sample-bodies.jl:17-33 (n = 0 chooses ds ≈ 2h)."""
     if n == 0:
         n = int(math.floor(L / h / 2)) + 1
@@ -225,10 +251,10 @@ def make_plate(L, alpha, h, x0, y0, n=0):
     xhat = spt * math.cos(-alpha)
     yhat = spt * math.sin(-alpha)
     ds = math.sqrt((xhat[1] - xhat[0]) ** 2 + (yhat[1] - yhat[0]) ** 2)
-    return RigidBody(xb=np.stack([xhat + x0, yhat + y0], axis=1), ds=np.full(n, ds))
+    return RigidBody(xb=np.stack([xhat + x0, yhat + y0], axis=1), ds=np.full(n, ds), motion=motion)
 
 
-def make_naca(x0, N, t, m=0.0, p=0.0, chord=1.0, aoa=0.0, pivot=(0.0, 0.0)):
+def make_naca(x0, N, t, m=0.0, p=0.0, chord=1.0, aoa=0.0, pivot=(0.0, 0.0), motion=None):
     """sample-bodies.jl:72-134 with a real thickness ``t``, chord scale and a
     rotation by ``aoa`` (rad, nose up) about ``pivot``; panel midpoints and
     lengths as the reference."""
@@ -258,7 +284,8 @@ def make_naca(x0, N, t, m=0.0, p=0.0, chord=1.0, aoa=0.0, pivot=(0.0, 0.0)):
         X = xe[:, 0] - pivot[0]
         Y = xe[:, 1] - pivot[1]
         xe = np.stack([c * X - s * Y + pivot[0], s * X + c * Y + pivot[1]], axis=1)
-    return RigidBody(xb=(xe[1:] + xe[:-1]) / 2.0, ds=np.sqrt(np.sum((xe[1:] - xe[:-1]) ** 2, axis=1)))
+    return RigidBody(xb=(xe[1:] + xe[:-1]) / 2.0, ds=np.sqrt(np.sum((xe[1:] - xe[:-1]) ** 2, axis=1)),
+                     motion=motion)
 
 
 # --------------------------------------------------------------------------
@@ -276,6 +303,11 @@ class IBProblem:
     (FP32 sine transforms, every Poisson-type solve corrected by
     ``refine_sweeps`` sweeps of FP64-residual iterative refinement started
     from the previous solution; state, stencils, Schur solve and forces FP64).
+
+    A body whose ``motion`` is a ``MovingGrid`` (one body only, models.jl:137)
+    makes every ``advance`` recompute the base flux from the motion at each
+    step's t (timestepping.jl:41-43, 273-318); the free stream is then added
+    to the motion's (the reference's default free stream is zero).
     """
 
     def __init__(self, grid, bodies, dt, Re, freestream=(1.0, 0.0, 0.0), beta=(1.5, -0.5),
@@ -301,6 +333,14 @@ class IBProblem:
             raise IBPMError(rc, self.lib.ibpm_last_error(None).decode())
         self.handle = h
         self._owns = True
+        moving = [b.motion for b in self.bodies if isinstance(b.motion, MovingGrid)]
+        self.motion = moving[0] if moving else None
+        if self.motion is not None:
+            if len(self.bodies) != 1:
+                self.close()
+                raise IBPMError(IBPM_ERR_UNSUPPORTED, "a moving grid carries exactly one body")
+            m0 = np.array(self.motion.row(0.0))
+            self._check(self.lib.ibpm_set_moving_grid(self.handle, 0.0, 0.0, _ptr(m0)))
 
     def _desc_of(self, grid, ev, beta, precision, device, refine_sweeps):
         d = ProblemDesc()
@@ -509,14 +549,25 @@ def push_state(state, prob, fields=("Gamma", "q", "q0", "psi", "nonlin", "Fb")):
 
 
 def advance(state, prob, t=0.0, nsteps=1):
-    """advance!(state, prob, t) — ``nsteps`` steps on the device.  Returns the
+    """advance!(state, prob, t) — ``nsteps`` steps on the device at times
+    t, t + dt, … (or at the times of ``t`` when it is an array).  Returns the
     (nsteps, nbodies) CD and CL histories; state.CD/CL hold the last row.
     Fields are copied back when ``prob.sync_fields`` is set."""
     nbod = len(prob.bodies)
+    ts = np.atleast_1d(np.asarray(t, dtype=np.float64))
+    if ts.size > 1 or np.ndim(t) == 1:
+        nsteps = ts.size
     cd = np.zeros((nsteps, nbod))
     cl = np.zeros((nsteps, nbod))
-    rc = prob.lib.ibpm_advance(prob.handle, float(t), int(nsteps), cd.ctypes.data_as(_DP),
-                               cl.ctypes.data_as(_DP))
+    if getattr(prob, "motion", None) is not None:
+        if ts.size != nsteps:
+            ts = ts[0] + prob.dt * np.arange(nsteps)
+        rows = np.ascontiguousarray([prob.motion.row(tk) for tk in ts], dtype=np.float64).reshape(-1)
+        rc = prob.lib.ibpm_advance_moving(prob.handle, int(nsteps), _ptr(rows), cd.ctypes.data_as(_DP),
+                                          cl.ctypes.data_as(_DP))
+    else:
+        rc = prob.lib.ibpm_advance(prob.handle, float(ts[0]) if ts.size else 0.0, int(nsteps),
+                                   cd.ctypes.data_as(_DP), cl.ctypes.data_as(_DP))
     if nsteps:
         state.CD[:] = cd[-1]
         state.CL[:] = cl[-1]
@@ -535,7 +586,7 @@ def vort2flux(state, prob):
 def run_sim(t, state, prob):
     """run_sim! of src/ibpm.jl:90-106 without logging: one step per entry of
     ``t``; stops (like the reference) on a non-finite lift coefficient."""
-    cd, cl = advance(state, prob, t[0] if len(t) else 0.0, nsteps=len(t))
+    cd, cl = advance(state, prob, np.asarray(t, dtype=np.float64), nsteps=len(t))
     return cd, cl
 
 
@@ -601,6 +652,9 @@ class Batch:
             m.lib = self.lib
             m.grid = sp_["grid"]
             m.bodies = list(sp_["bodies"])
+            if any(isinstance(b.motion, MovingGrid) for b in m.bodies):
+                raise IBPMError(IBPM_ERR_UNSUPPORTED, "member %d: a moving grid is not batched" % i)
+            m.motion = None
             m.dt = float(sp_["dt"])
             m.Re = float(sp_["Re"])
             fs = sp_.get("freestream", (1.0, 0.0, 0.0))

@@ -96,6 +96,7 @@ int ibpm_sizes(const ibpm_handle* h, int64_t* nGamma, int64_t* nq, int32_t* mg,
  * layouts are IBState's (state-types.jl:253-268).  q0 must be uniform per
  * level and component, as base_flux! makes it for static bodies
  * (timestepping.jl:252-270); anything else returns IBPM_ERR_UNSUPPORTED.
+ * On a moving grid q0 is ignored: every step recomputes it.
  * q is stored as given: the next step's nonlinear term reads it, as the
  * reference does, even if it is not the curl of ψ.
  */
@@ -131,6 +132,37 @@ int ibpm_get_state(ibpm_handle* h, double* Gamma, double* q, double* q0,
  */
 int ibpm_advance(ibpm_handle* h, double t, int32_t nsteps, double* CD_out,
                  double* CL_out);
+
+/*
+ * Make the handle's single body move with the grid: MovingGrid(U, V, θ, θ̇)
+ * (structure-domain/motion-types.jl:40-48), the motion type for which
+ * advance! recomputes the base flux at the start of every step
+ * (timestepping.jl:41-43) as base_flux! does (timestepping.jl:273-318):
+ *   Ω = −θ̇(t), α = −θ(t),
+ *   Ux0 = U cos α − V sin α + (Ux cos i − Uy sin i),
+ *   Uy0 = U sin α + V cos α + (Ux sin i + Uy cos i)   (Ux, Uy, i: the desc's
+ *                                                      free stream),
+ *   q0 = hc (−Ω (y − yc) + Ux0) on x-fluxes, hc (Ω (x − xc) + Uy0) on y-fluxes,
+ * (x, y) the face centres of each level (pre-processing/models.jl:135-153).
+ * xc, yc are the IBModel keywords of that file (IBProblem leaves them 0).
+ * motion0 = {U, V, θ, θ̇} at t = 0 sets the q0 reported before the first step
+ * (IBState(prob) calls base_flux! at t = 0, state-types.jl:45).  The bodies'
+ * E, B⁻¹ and the step are those of the static case (timestepping.jl:154-163,
+ * 361-372).  Refused (IBPM_ERR_UNSUPPORTED) for more than one body
+ * (models.jl:137) and for a linearised handle.  From then on the handle steps
+ * only through ibpm_advance_moving; the adjoint and batches refuse it.
+ */
+int ibpm_set_moving_grid(ibpm_handle* h, double xc, double yc, const double* motion0);
+
+/*
+ * ibpm_advance for a moving grid: step k uses motion[4k .. 4k+3] = {U, V, θ,
+ * θ̇} evaluated at that step's t (the reference's advance!(state, prob, t[k])
+ * evaluates the motion's functions at t[k]).  Outputs as ibpm_advance; the
+ * forces are in the body (grid) frame, as the reference's state.CD/CL.
+ * ibpm_get_state's q0 is then the base flux of the last step.
+ */
+int ibpm_advance_moving(ibpm_handle* h, int32_t nsteps, const double* motion,
+                        double* CD_out, double* CL_out);
 
 /*
  * vort2flux!(state.ψ, state.q, state.Γ, model, mg) (curl.jl:411-443): make ψ

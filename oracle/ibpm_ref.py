@@ -16,6 +16,8 @@ relative to the IBPM.jl project root):
 * ``src/fluid-operators/nonlinear.jl:17-201``    ``avg_flux``, ``direct_product!``, ``nonlinear!``
 * ``src/interface-coupling/interface-coupling.jl:6-137`` ``δh``, ``setup_reg`` (E, E')
 * ``src/timestepping/timestepping.jl:35-354``    ``advance!`` and its helpers
+  (``base_flux!`` of a ``MovingGrid``: ``:273-318``)
+* ``src/structure-domain/motion-types.jl:40-48`` ``MovingGrid``
 * ``src/pre-processing/{models,problem-types,state-types}.jl`` state/problem layout
 * ``src/structure-domain/sample-bodies.jl:17-134`` plate, cylinder, NACA bodies
 
@@ -517,6 +519,50 @@ def make_naca(x0, N, t, m=0.0, p=0.0, chord=1.0, aoa=0.0, pivot=(0.0, 0.0)):
 # Problem, state and the time step
 # --------------------------------------------------------------------------
 @dataclass
+class MovingGrid:
+    """MovingGrid (motion-types.jl:40-48): the grid moves with the body; the
+    lab-frame free stream (U(t), V(t)) and the body frame's angular position
+    θ(t) (minus the aerodynamic pitch) and rate θ̇(t), all callables of t."""
+    U: object
+    V: object
+    theta: object
+    theta_dot: object
+    xc: float = 0.0
+    yc: float = 0.0
+
+
+def moving_grid_coords(g, xc, yc):
+    """models.jl:135-153: per level, y − yc of every x-flux row (YY, shape
+    (mg, ny)) and x − xc of every y-flux column (XX, shape (mg, nx)); the
+    reference stores them expanded to every flux point."""
+    XX = np.zeros((g.mg, g.nx))
+    YY = np.zeros((g.mg, g.ny))
+    for lev in range(g.mg):
+        hc = g.hc(lev)
+        y = ((np.arange(1, g.ny + 1) - 0.5) - g.ny / 2) * hc + (g.ny / 2) * g.h - g.offy
+        YY[lev] = y - yc
+        x = ((np.arange(1, g.nx + 1) - 0.5) - g.nx / 2) * hc + (g.nx / 2) * g.h - g.offx
+        XX[lev] = x - xc
+    return XX, YY
+
+
+def moving_grid_rates(prob, t):
+    """The scalars of base_flux! for a MovingGrid (timestepping.jl:283-296):
+    Ω = −θ̇(t) and the body-frame translation (Ux0, Uy0) of the motion's free
+    stream rotated by α = −θ(t), plus the problem's own free stream."""
+    m = prob.motion
+    Om = -m.theta_dot(t)
+    a = -m.theta(t)
+    U, V = m.U(t), m.V(t)
+    Ux0 = U * math.cos(a) - V * math.sin(a)
+    Uy0 = U * math.sin(a) + V * math.cos(a)
+    af = prob.inclination
+    Ux0 += prob.Ux * math.cos(af) - prob.Uy * math.sin(af)
+    Uy0 += prob.Ux * math.sin(af) + prob.Uy * math.cos(af)
+    return Om, Ux0, Uy0
+
+
+@dataclass
 class IBProblem:
     """problem-types.jl:182-200 + models.jl:27-159 for Static bodies."""
     grid: MultiGrid
@@ -537,6 +583,12 @@ class IBProblem:
     # LinearizedIBProblem (problem-types.jl:47-87): base Γ and averaged base
     # flux QB per level, or None for the nonlinear problem
     base: tuple = field(init=False, default=None)
+    # the bodies' motion: None (Static) or a MovingGrid; xc, yc are the
+    # IBModel keywords (models.jl:127-129), which IBProblem never sets, so the
+    # rotational flux is taken about (0, 0) whatever MovingGrid.xc/yc say
+    motion: object = None
+    xc: float = 0.0
+    yc: float = 0.0
 
     def __post_init__(self):
         g = self.grid
@@ -550,6 +602,9 @@ class IBProblem:
         if self.build_binv:
             self.B = build_B(self)
             self.Binv = np.linalg.inv(self.B)     # laplacian.jl:274 (LAPACK getrf/getri)
+        if isinstance(self.motion, MovingGrid):
+            assert len(self.bodies) == 1          # models.jl:137, timestepping.jl:277
+            self.XX, self.YY = moving_grid_coords(g, self.xc, self.yc)
 
     @property
     def nb(self):
@@ -648,10 +703,21 @@ def linearize(prob, base_state):
 
 def base_flux(prob, t=0.0):
     """timestepping.jl:252-270 (InertialMotion): uniform q0 per level; zero
-    for a linearized problem (timestepping.jl:236-250)."""
+    for a linearized problem (timestepping.jl:236-250); for a MovingGrid
+    (:273-318) solid-body rotation plus translation,
+    q0x = YY·(−hc Ω) + hc Ux0 and q0y = XX·(hc Ω) + hc Uy0 on each level."""
     g = prob.grid
     if prob.base is not None:
         return np.zeros((g.mg, g.nx + 1, g.ny)), np.zeros((g.mg, g.nx, g.ny + 1))
+    if isinstance(prob.motion, MovingGrid):
+        Om, Ux0, Uy0 = moving_grid_rates(prob, t)
+        q0x = np.zeros((g.mg, g.nx + 1, g.ny))
+        q0y = np.zeros((g.mg, g.nx, g.ny + 1))
+        for lev in range(g.mg):
+            hc = g.hc(lev)
+            q0x[lev] = prob.YY[lev][None, :] * ((-hc) * Om) + hc * Ux0
+            q0y[lev] = prob.XX[lev][:, None] * (hc * Om) + hc * Uy0
+        return q0x, q0y
     a = prob.inclination
     q0x = np.zeros((g.mg, g.nx + 1, g.ny))
     q0y = np.zeros((g.mg, g.nx, g.ny + 1))
@@ -730,8 +796,11 @@ def update_stress(state, prob):
 
 
 def advance(state, prob, t=0.0):
-    """advance!(state, prob, t) for a Static body, timestepping.jl:35-67."""
+    """advance!(state, prob, t) for a Static body or a MovingGrid,
+    timestepping.jl:35-67."""
     g = prob.grid
+    if isinstance(prob.motion, MovingGrid):                              # :41-43
+        state.q0x, state.q0y = base_flux(prob, t)
     Gs, qsx, qsy = get_trial_state(state, prob)                          # :52
     F = E_apply(qsx[0] + state.q0x[0], qsy[0] + state.q0y[0], prob)      # :154-159
     state.Fb = prob.Binv @ F                                             # :160
@@ -743,12 +812,13 @@ def advance(state, prob, t=0.0):
     return state
 
 
-def run(prob, state, nsteps, dt=None, record=True):
-    """Advance ``nsteps`` steps; returns (CD, CL) histories (nsteps, nbodies)."""
+def run(prob, state, nsteps, dt=None, record=True, t0=0.0):
+    """Advance ``nsteps`` steps at t = t0 + k dt; returns (CD, CL) histories
+    (nsteps, nbodies)."""
     cd = np.zeros((nsteps, len(prob.bodies)))
     cl = np.zeros((nsteps, len(prob.bodies)))
     for k in range(nsteps):
-        advance(state, prob, k * prob.dt)
+        advance(state, prob, t0 + k * prob.dt)
         cd[k] = state.CD
         cl[k] = state.CL
     return cd, cl

@@ -1,0 +1,64 @@
+"""Extract the golden force history of the reference's moving-grid pitch
+manoeuvre (IBPM.jl ``benchmarks/eldredge/pitch_maneuver.jl``, which wrote
+``benchmarks/eldredge/results/force_jl2.mat``) into ``eldredge_pitch.json``.
+
+The .mat file is MATLAB v7.3 (an HDF5 file after a 512-byte header) holding
+three float64 vectors of 10 001 entries, t, CL and CD (lab frame), stored
+contiguously.  h5py is not available, so the vectors are read at their data
+offset and identified by content: t is 0:1e-3:10, CD starts at the steady
+flat-plate drag (≈ 0.394) and CL near zero.  Every 10th entry is kept.
+
+Run from the repository root with the reference tree present:
+    python tests/golden/make_eldredge_golden.py
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+SRC = "/root/reference/benchmarks/eldredge/results/force_jl2.mat"
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "eldredge_pitch.json")
+N = 10001
+OFFSET = 2560   # first byte of the contiguous data blocks
+KEEP = 10
+
+
+def main(src=SRC):
+    raw = open(src, "rb").read()
+    if not raw.startswith(b"MATLAB 7.3 MAT-file") or raw[512:520] != b"\x89HDF\r\n\x1a\n":
+        sys.exit("not a MATLAB v7.3 (HDF5) file: %s" % src)
+    blocks = np.frombuffer(raw, dtype="<f8", count=3 * N, offset=OFFSET).reshape(3, N)
+    tref = np.arange(N) * 1e-3
+    it = [k for k in range(3) if np.abs(blocks[k] - tref).max() < 1e-12]
+    icd = [k for k in range(3) if abs(blocks[k][0] - 0.394) < 1e-3]
+    icl = [k for k in range(3) if abs(blocks[k][0]) < 1e-5 and k not in it]
+    if len(it) != 1 or len(icd) != 1 or len(icl) != 1 or len({it[0], icd[0], icl[0]}) != 3:
+        sys.exit("could not identify t, CL and CD")
+    t, cl, cd = blocks[it[0]], blocks[icl[0]], blocks[icd[0]]
+    if not (np.all(np.isfinite(cl)) and np.all(np.isfinite(cd))):
+        sys.exit("non-finite force history")
+    sel = np.arange(0, N, KEEP)
+    doc = {
+        "source": "IBPM.jl benchmarks/eldredge/results/force_jl2.mat (pitch_maneuver.jl, MovingGrid)",
+        "setup": {
+            "boundary": [-1.5, 6.5, -2.0, 2.0], "h": 0.02, "mg": 5, "Re": 100.0,
+            "plate": {"L": 1.0, "alpha": 0.0, "x0": 0.0, "y0": 0.0, "n": 51},
+            "steady": {"dt": 1e-2, "steps": 10001, "freestream": [1.0, 0.0, 0.0]},
+            "pitch": {"dt": 1e-3, "steps": N, "a": 11.0, "t1234": [1.0, 3.0, 4.0, 6.0],
+                      "alpha_max_deg": 45.0, "U": 1.0},
+        },
+        "steady_cd_published": {"julia": 0.39415052, "fortran": 0.39415060,
+                                "where": "benchmarks/eldredge/README.md:25-26"},
+        "step_stride": KEEP,
+        "t": [float(v) for v in t[sel]],
+        "CL_lab": [float(v) for v in cl[sel]],
+        "CD_lab": [float(v) for v in cd[sel]],
+    }
+    with open(OUT, "w") as f:
+        json.dump(doc, f, indent=0)
+    print("wrote %s (%d samples)" % (OUT, sel.size))
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])
