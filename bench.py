@@ -481,6 +481,89 @@ def batch_block(args, d):
             "setup_s": setup_s, "cells_per_step": cells, "forces_finite": finite}
 
 
+# The reference's moving-grid benchmark (benchmarks/eldredge): a flat plate
+# (L = 1, 51 points) on 400x200 cells x 5 levels, h = 0.02, Re = 100; the
+# steady boundary layer (dt = 0.01, 10 001 steps) and from it the
+# pitch-up/hold/down manoeuvre (dt = 1e-3, 10 001 steps, a = 11,
+# t1..t4 = 1, 3, 4, 6, 45 degrees).  The reference reports 1098 s for the
+# manoeuvre (benchmarks/eldredge/README.md:40-44, its own hardware).
+ELDREDGE_WORKLOAD = ("Eldredge pitch manoeuvre, MovingGrid flat plate (51 pts) Re=100, 400x200 cells x 5 levels, "
+                     "h=0.02, dt=1e-3, 10001 steps from the steady boundary layer (dt=1e-2, 10001 steps)")
+ELDREDGE_REF_S = 1098.0
+GOLDEN_ELDREDGE = os.path.join(ROOT, "tests", "golden", "eldredge_pitch.json")
+
+
+def eldredge_motion():
+    """θ(t), θ̇(t) of benchmarks/eldredge/pitch_maneuver.jl:11-20."""
+    import math
+    a, t1, t2, t3, t4 = 11.0, 1.0, 3.0, 4.0, 6.0
+    amax = 45 * math.pi / 180
+
+    def G(t):
+        return np.log(np.cosh(a * (t - t1)) * np.cosh(a * (t - t4)) / (np.cosh(a * (t - t2)) * np.cosh(a * (t - t3))))
+
+    gmax = float(np.max(G(np.arange(10001) * 1e-3)))
+    ch, th = math.cosh, math.tanh
+
+    def theta(t):   # scalar form of -amax G(t) / gmax (the host evaluates it every step)
+        return -amax * math.log(ch(a * (t - t1)) * ch(a * (t - t4)) / (ch(a * (t - t2)) * ch(a * (t - t3)))) / gmax
+
+    def theta_dot(t):
+        return -amax * (a * (th(a * (t - t1)) - th(a * (t - t2)) - th(a * (t - t3)) + th(a * (t - t4)))) / gmax
+
+    return theta, theta_dot
+
+
+def eldredge_block(args, d):
+    """The manoeuvre end to end through the public API (advance with the
+    motion evaluated on the host every step, CD/CL returned), FP64, wall clock
+    after the steady start state is computed; lab-frame CL/CD against the
+    reference's own history (tests/golden/eldredge_pitch.json)."""
+    import ibpm_gpu as G
+    g = G.make_grid(0.02, (-1.5, 6.5, -2.0, 2.0), 5)
+    steady = G.IBProblem(g, [G.make_plate(1.0, 0.0, g.h, 0.0, 0.0, n=51)], 1e-2, 100.0,
+                         freestream=(1.0, 0.0, 0.0), device=d.local, sync_fields=False)
+    st = G.IBState(steady)
+    t0 = time.perf_counter()
+    cd_s, _ = G.advance(st, steady, np.arange(10001) * 1e-2)
+    steady_s = time.perf_counter() - t0
+    G.pull_state(st, steady)
+    steady.close()
+    theta, theta_dot = eldredge_motion()
+    mot = G.MovingGrid(U=lambda t: 1.0, V=lambda t: 0.0, theta=theta, theta_dot=theta_dot)
+    pitch = G.IBProblem(g, [G.make_plate(1.0, 0.0, g.h, 0.0, 0.0, n=51, motion=mot)], 1e-3, 100.0,
+                        freestream=(0.0, 0.0, 0.0), device=d.local, sync_fields=False)
+    G.push_state(st, pitch)
+    t = np.arange(10001) * 1e-3
+    t0 = time.perf_counter()
+    F1, F2 = G.advance(st, pitch, t)
+    wall = time.perf_counter() - t0
+    pitch.close()
+    th = np.array([theta(tk) for tk in t])
+    CD = F1[:, 0] * np.cos(th) - F2[:, 0] * np.sin(th)
+    CL = F1[:, 0] * np.sin(th) + F2[:, 0] * np.cos(th)
+    out = {"workload": ELDREDGE_WORKLOAD, "precision": "fp64", "steps": 10001, "seconds": wall,
+           "steps_per_s": 10001 / wall, "level_cell_steps_per_s": 400 * 200 * 5 * 10001 / wall,
+           "steady_start_seconds": steady_s, "steady_cd": float(cd_s[-1, 0]),
+           "reference_published_seconds": ELDREDGE_REF_S,
+           "reference_published_note": "Julia, body-fixed (MovingGrid) formulation, on the reference's own "
+                                       "hardware (benchmarks/eldredge/README.md:40-44); not measured here",
+           "timing": "wall clock around one advance call of 10001 steps: host evaluation of the motion, "
+                     "one graph replay per step, per-step CD/CL returned"}
+    try:
+        with open(GOLDEN_ELDREDGE) as f:
+            gold = json.load(f)
+        k = gold["step_stride"]
+        gcl, gcd = np.array(gold["CL_lab"]), np.array(gold["CD_lab"])
+        out["vs_reference_history"] = {
+            "cl_max_err_rel_to_peak": float(np.max(np.abs(CL[::k] - gcl)) / np.max(np.abs(gcl))),
+            "cd_max_err_rel_to_peak": float(np.max(np.abs(CD[::k] - gcd)) / np.max(np.abs(gcd))),
+            "source": gold["source"]}
+    except OSError as e:
+        out["vs_reference_history"] = {"error": str(e)[:200]}
+    return out
+
+
 def run_ours(args, d):
     K = args.steps
     sampler = ClockSampler(d.local)
@@ -551,6 +634,11 @@ def run_ours(args, d):
     }
     if not args.no_adjoint:
         out["adjoint"] = adjoint_block(args, d)
+    if not args.no_eldredge:
+        try:
+            out["eldredge"] = eldredge_block(args, d)
+        except Exception as e:  # reported, not fatal
+            out["eldredge"] = {"workload": ELDREDGE_WORKLOAD, "error": str(e)[:300]}
     if not args.no_batch:
         try:
             out["batch"] = batch_block(args, d)
@@ -580,6 +668,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-eldredge", action="store_true")
     args = ap.parse_args()
     d = Dist()
     try:

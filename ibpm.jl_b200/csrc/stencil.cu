@@ -22,7 +22,8 @@ namespace ibpm {
 // Q the face sums of q without base flux, QB those of the base state with its
 // base flux, both products using this state's edge values ¼ get_bc!(Γ[l+1])
 // (the reference passes the perturbation's Γbc to the ΓB product too).
-template <bool LIN>
+// MOV: a moving grid's per-face base flux (MovingFlux) instead of q0x, q0y.
+template <bool LIN, bool MOV>
 __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
     pdl_wait();
     pdl_trigger();
@@ -36,9 +37,8 @@ __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
     const double* qy = q + g.nu;
     const double q0x = a.q0x[lev], q0y = a.q0y[lev];
     // moving grid: the base flux varies along y on x-faces and along x on y-faces
-    const bool mov = a.mv.tab != nullptr;
-    const double* mrow = mov ? moving_row(a.mv) : nullptr;
-    const double hc = mov ? ldexp(a.mv.h, lev) : 0.0;
+    const double* mrow = MOV ? moving_row(a.mv) : nullptr;
+    const double hc = MOV ? ldexp(a.mv.h, lev) : 0.0;
 
     CoarseBC cb;
     cb.rc = (lev < a.mg - 1) ? a.G + a.Gmap.off(lev + 1) : nullptr;
@@ -55,8 +55,14 @@ __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
     auto qxJ = [&](int I, int J) -> double { return q[(I - 1) + (long long)(J - 1) * (nx + 1)]; };
     auto qyJ = [&](int I, int J) -> double { return qy[(I - 1) + (long long)(J - 1) * nx]; };
     // avg_flux (nonlinear.jl:17-38)
-    auto q0xJ = [&](int J) -> double { return mov ? moving_q0x(a.mv, mrow, J, ny, hc) : q0x; };
-    auto q0yI = [&](int I) -> double { return mov ? moving_q0y(a.mv, mrow, I, nx, hc) : q0y; };
+    auto q0xJ = [&](int J) -> double {
+        if constexpr (MOV) return moving_q0x(a.mv, mrow, J, ny, hc);
+        else return q0x;
+    };
+    auto q0yI = [&](int I) -> double {
+        if constexpr (MOV) return moving_q0y(a.mv, mrow, I, nx, hc);
+        else return q0y;
+    };
     auto QxJ = [&](int I, int J) -> double { return ((qxJ(I, J) + q0xJ(J)) + qxJ(I, J - 1)) + q0xJ(J - 1); };
     auto QyJ = [&](int I, int J) -> double { return ((qyJ(I, J) + q0yI(I)) + qyJ(I - 1, J)) + q0yI(I - 1); };
     // direct_product_loops! (nonlinear.jl:73-114)
@@ -130,8 +136,9 @@ __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
 cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st) {
     dim3 blk(32, 8);
     dim3 grid((g.n1 + 31) / 32, (g.n2 + 7) / 8, a.mg);
-    return a.GB ? launch_k(trial_rhs_kernel<true>, grid, blk, 0, st, a, g)
-                : launch_k(trial_rhs_kernel<false>, grid, blk, 0, st, a, g);
+    if (a.GB) return launch_k(trial_rhs_kernel<true, false>, grid, blk, 0, st, a, g);
+    if (a.mv.tab) return launch_k(trial_rhs_kernel<false, true>, grid, blk, 0, st, a, g);
+    return launch_k(trial_rhs_kernel<false, false>, grid, blk, 0, st, a, g);
 }
 
 // ---------------------------------------------------------------------------
