@@ -233,6 +233,62 @@ cudaError_t launch_adj_E_rotT(const Geom& g, const BodyDev& b, const double* W, 
     return launch_k(adj_E_rotT_kernel, dim3(blocks), dim3(256), 0, st, b, g, W, wx, wy, stepw, adj_n, Ft);
 }
 
+// Position gradient of one adjoint step (the derivation is in the note above
+// launch_dweights): one warp per body point, both force components and both
+// coordinates; lanes stride the 13×13 window, warp sums in a fixed order, so
+// the accumulation is deterministic.  C r̄ is rot!ᵀ of r̄₁, as in adj_E_rotT.
+__global__ void adj_xb_kernel(BodyDev b, Geom g, AdjXbArgs a) {
+    pdl_wait();
+    pdl_trigger();
+    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (p >= b.nb) return;
+    const int nx = g.nx, ny = g.ny, P = g.P;
+    const int slot = (*a.adj_n) % a.k;
+    const double* Fn = a.tapeFb + (long long)slot * b.nf;
+    const double* q1 = a.tapeq1 + (long long)slot * g.nq;
+    const int bx = b.bidx[p], by = b.bidx[b.nb + p];
+    auto Wv = [&](int i, int j) -> double { return a.rb1[(long long)j * P + i]; };
+    double gx = 0.0, gy = 0.0;
+    for (int comp = 0; comp < 2; ++comp) {
+        const int kk = comp * b.nb + p;
+        const double fbar = a.Fbar[kk], fn = Fn[kk];
+        const double* wd = a.wd + (long long)kk * 338;
+        for (int t = lane; t < 169; t += 32) {
+            const int l = t / 13, m = t % 13;
+            const int I = bx + l - 7, J = by + m - 7;   // 0-based flux indices
+            double u, cr = 0.0;
+            if (comp == 0) {
+                u = q1[I + (long long)J * (nx + 1)] + a.q0x;
+                if (I >= 1 && I <= nx - 1) {
+                    if (J <= ny - 2) cr += Wv(I - 1, J);
+                    if (J >= 1) cr -= Wv(I - 1, J - 1);
+                }
+            } else {
+                u = q1[g.nu + I + (long long)J * nx] + a.q0y;
+                if (J >= 1 && J <= ny - 1) {
+                    if (I >= 1) cr += Wv(I - 1, J - 1);
+                    if (I <= nx - 2) cr -= Wv(I, J - 1);
+                }
+            }
+            const double v = fbar * u - fn * cr;
+            gx += wd[t] * v;
+            gy += wd[169 + t] * v;
+        }
+    }
+    gx = warp_sum_d(gx);
+    gy = warp_sum_d(gy);
+    if (lane == 0) {
+        a.gxb[p] += gx;
+        a.gxb[b.nb + p] += gy;
+    }
+}
+
+cudaError_t launch_adj_xb(const Geom& g, const BodyDev& b, const AdjXbArgs& a, cudaStream_t st) {
+    const int blocks = (b.nb * 32 + 255) / 256;
+    return launch_k(adj_xb_kernel, dim3(blocks), dim3(256), 0, st, b, g, a);
+}
+
 // y = Aᵀ x, A row-major n×n (the transpose of F̃b = B⁻¹ F): 32 columns per
 // block, the rows split over 8 warps, partial sums added in a fixed order.
 __global__ void gemv_t_kernel(const double* __restrict__ A, const double* __restrict__ x, double* y, int n) {

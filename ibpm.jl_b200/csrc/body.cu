@@ -38,6 +38,67 @@ __device__ double delta_h(double rf, double rb, double dr) {
     return 0.0;
 }
 
+// ∂δh(rf, rb, dr)/∂rb: −sign(rf − rb)/dr times the r1-derivative of the same
+// rounded-coefficient pieces (d asin(√3/2 (2r1 − c))/dr1 = √3/√(1 − ¾(2r1 − c)²),
+// d √p/dr1 = p'/(2√p)).  At r = 0 the pieces' derivative is ~1e-9 (not exactly
+// zero with rounded coefficients); the sign factor makes it 0 there.
+__device__ double delta_h_db(double rf, double rb, double dr) {
+    const double d = rf - rb;
+    const double r1 = fabs(d) / dr, r2 = r1 * r1, r3 = r2 * r1;
+    const double s3 = sqrt(3.0);
+    double f;
+    if (r1 <= 1.0) {
+        const double u = 2.0 * r1 - 1.0;
+        const double a5 = asin(0.5 * s3 * u), a8 = sqrt(1.0 - 12.0 * r2 + 12.0 * r1);
+        const double da5 = s3 / sqrt(1.0 - 0.75 * u * u), da8 = (6.0 - 12.0 * r1) / a8;
+        f = 4 * 4.166666667e-2 * r3 + 3 * (-0.1388888889 + 3.472222222e-2 * a8) * r2 + 3.472222222e-2 * da8 * r3 +
+            2 * (-7.121664902e-2 - 5.208333333e-2 * a8 + 0.2405626122 * a5) * r1 +
+            (-5.208333333e-2 * da8 + 0.2405626122 * da5) * r2 + (-.2405626122 * a5 - 0.3792313933 + 0.1012731481 * a8) +
+            (-.2405626122 * da5 + 0.1012731481 * da8) * r1 + 8.0187537413e-2 * da5 - 4.195601852e-2 * da8;
+    } else if (r1 <= 2.0) {
+        const double u = 2.0 * r1 - 3.0;
+        const double a6 = asin(0.5 * s3 * u), a9 = sqrt(-23.0 + 36.0 * r1 - 12.0 * r2);
+        const double da6 = s3 / sqrt(1.0 - 0.75 * u * u), da9 = (18.0 - 12.0 * r1) / a9;
+        f = -4 * 6.250000000e-2 * r3 + 3 * (0.4861111111 - 1.736111111e-2 * a9) * r2 - 1.736111111e-2 * da9 * r3 +
+            2 * (-1.143175026 + 7.812500000e-2 * a9 - 0.1202813061 * a6) * r1 +
+            (7.812500000e-2 * da9 - 0.1202813061 * da6) * r2 + (0.8751991178 + 0.3608439183 * a6 - 0.1548032407 * a9) +
+            (0.3608439183 * da6 - 0.1548032407 * da9) * r1 - 0.2806563809 * da6 + 0.1150173611 * da9;
+    } else if (r1 <= 3.0) {
+        const double u = 2.0 * r1 - 5.0;
+        const double a1 = asin(0.5 * u * s3), a7 = sqrt(-71.0 - 12.0 * r2 + 60.0 * r1);
+        const double da1 = s3 / sqrt(1.0 - 0.75 * u * u), da7 = (30.0 - 12.0 * r1) / a7;
+        f = 4 * 2.083333333e-2 * r3 + 3 * (3.472222222e-3 * a7 - 0.2638888889) * r2 + 3.472222222e-3 * da7 * r3 +
+            2 * (1.214391675 - 2.604166667e-2 * a7 + 2.405626122e-2 * a1) * r1 +
+            (-2.604166667e-2 * da7 + 2.405626122e-2 * da1) * r2 +
+            (-0.1202813061 * a1 - 2.449273192 + 7.262731481e-2 * a7) + (-0.1202813061 * da1 + 7.262731481e-2 * da7) * r1 +
+            0.1523563211 * da1 - 7.306134259e-2 * da7;
+    } else {
+        return 0.0;
+    }
+    const double sg = d > 0.0 ? 1.0 : (d < 0.0 ? -1.0 : 0.0);
+    return -sg * f / dr;
+}
+
+// Position derivatives of the weights: wd[kk][0][l][m] = ∂w/∂xb_k and
+// wd[kk][1][l][m] = ∂w/∂yb_k for the weights of weights_kernel below.
+__global__ void dweights_kernel(BodyDev b, double h, double offx, double offy, double* wd) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b.nf * 169) return;
+    const int kk = t / 169, lm = t % 169, l = lm / 13, m = lm % 13;
+    const int comp = kk / b.nb, k = kk % b.nb;
+    const double xk = b.xb[k], yk = b.xb[b.nb + k];
+    const double x = h * (double)((b.bidx[k] - 1) + (l - 6)) - offx + (comp == 1 ? h / 2 : 0.0);
+    const double y = h * (double)((b.bidx[b.nb + k] - 1) + (m - 6)) - offy + (comp == 0 ? h / 2 : 0.0);
+    wd[(long long)kk * 338 + lm] = delta_h_db(x, xk, h) * delta_h(y, yk, h);
+    wd[(long long)kk * 338 + 169 + lm] = delta_h(x, xk, h) * delta_h_db(y, yk, h);
+}
+
+cudaError_t launch_dweights(double h, double offx, double offy, const BodyDev& b, double* wd, cudaStream_t st) {
+    const int n = b.nf * 169;
+    dweights_kernel<<<(n + 255) / 256, 256, 0, st>>>(b, h, offx, offy, wd);
+    return cudaGetLastError();
+}
+
 // w[kk][l][m], kk = comp·nb + k: weight of flux point (bidx + l − 6, bidx + m − 6)
 // for body point k (interface-coupling.jl:89-96).
 __global__ void weights_kernel(BodyDev b, double h, double offx, double offy) {

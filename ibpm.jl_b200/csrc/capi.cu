@@ -94,6 +94,14 @@ struct ibpm_handle {
     int* adj_n = nullptr;
     double adj_wx = 0, adj_wy = 0;
     cudaGraphExec_t gadj[2] = {nullptr, nullptr};
+    // body-point position gradient (ibpm_adjoint_run with grad_xb)
+    bool adj_xb = false;                   // requested by the current run
+    bool gadj_xb = false;                  // the captured adjoint graphs include it
+    double* wd = nullptr;                  // [nf][2][169] position derivatives of the weights
+    double* tapeFb = nullptr;              // [k][nf]  F̃b of each step of the segment
+    double* tapeq1 = nullptr;              // [k][nq]  level-1 q after each step
+    double* gxb = nullptr;                 // (nb, 2) accumulator
+    int xb_k = 0;
     // measurement
     int launches = 0;                      // kernel launches enqueued (counted always)
     bool prof_on = false;                  // eager profiling: events around every launch
@@ -623,7 +631,8 @@ static void free_handle(ibpm_handle* h) {
     if (h->qB) cudaFree(h->qB);
     for (int p = 0; p < 2; ++p) if (h->gadj[p]) cudaGraphExecDestroy(h->gadj[p]);
     void* adj[] = {h->tapeG, h->tapeq, h->ck, h->Gb, h->qb, h->Nb[0], h->Nb[1], h->Gt, h->psib, h->Wadj, h->rb,
-                   h->qsb, h->Ft, h->Fbar, h->bcc, h->bcv, h->q0part, h->stepw, h->adj_n};
+                   h->qsb, h->Ft, h->Fbar, h->bcc, h->bcv, h->q0part, h->stepw, h->adj_n, h->wd, h->tapeFb,
+                   h->tapeq1, h->gxb};
     for (void* p : adj) if (p) cudaFree(p);
     void* ptrs[] = {h->G[0], h->G[1], h->Nl[0], h->Nl[1], h->psi, h->q, h->qs, h->rhs, h->Gsrc, h->F, h->Fb,
                     h->Binv, h->nonlin1_shadow, h->d_xb, h->d_ds, h->d_bidx, h->d_w, h->d_body_start,
@@ -1235,8 +1244,42 @@ static int enqueue_adjoint_step(ibpm_handle* h, int par) {
         ta.c_lap[l] = ra.c_lap[l]; ta.fac_bc[l] = ra.fac_bc[l]; ta.nl_scale[l] = ra.nl_scale[l];
     }
     ta.b1dt = ra.b1dt; ta.b2dt = ra.b2dt; ta.mg = mg;
+    if (h->adj_xb) {
+        // ∂J/∂xb of this step: F̄ · ∂E[q_{n+1,1} + q0] − F̃_n · ∂E[C r̄₁]
+        AdjXbArgs xa{};
+        xa.wd = h->wd; xa.Fbar = h->Fbar; xa.tapeFb = h->tapeFb; xa.tapeq1 = h->tapeq1;
+        xa.adj_n = h->adj_n; xa.k = h->adj_k; xa.q0x = h->q0x[0]; xa.q0y = h->q0y[0];
+        xa.rb1 = h->rb; xa.gxb = h->gxb;
+        LAUNCH(K_ADJ, 8.0 * (4.0 * 169 * h->nf + 2.0 * h->nf), launch_adj_xb(g, h->body, xa, h->st));
+    }
     LAUNCH(K_ADJ, 8.0 * (10.0 * g.n1 * g.n2 + 3.0 * g.nq) * mg, launch_adj_trial(g, ta, h->st));
     LAUNCH(K_ADJ, 8.0, launch_adj_tick(h->adj_n, h->st));
+    return IBPM_OK;
+}
+
+// Buffers of the position gradient for segments of k steps (the adjoint graphs
+// hold their pointers: reallocation drops them).
+static int xb_alloc(ibpm_handle* h, int k) {
+    if (!h->wd) {
+        int rc = dalloc(h, &h->wd, (size_t)h->nf * 338);
+        if (rc) return rc;
+        CK(launch_dweights(h->h, h->offx, h->offy, h->body, h->wd, h->st));
+    }
+    if (!h->gxb) {
+        int rc = dalloc(h, &h->gxb, h->nf);
+        if (rc) return rc;
+    }
+    if (h->xb_k < k) {
+        for (int p = 0; p < 2; ++p) if (h->gadj[p]) { cudaGraphExecDestroy(h->gadj[p]); h->gadj[p] = nullptr; }
+        if (h->tapeFb) cudaFree(h->tapeFb);
+        if (h->tapeq1) cudaFree(h->tapeq1);
+        h->tapeFb = h->tapeq1 = nullptr;
+        h->xb_k = 0;
+        int rc;
+        if ((rc = dalloc(h, &h->tapeFb, (size_t)k * h->nf)) || (rc = dalloc(h, &h->tapeq1, (size_t)k * h->g.nq)))
+            return rc;
+        h->xb_k = k;
+    }
     return IBPM_OK;
 }
 
@@ -1295,7 +1338,7 @@ static int ck_copy(ibpm_handle* h, int c, bool save) {
 
 extern "C" int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkpoint, const ibpm_objective* obj,
                                 double* J, double* grad_Gamma0, double* grad_q0, double* grad_omega0,
-                                double* grad_alpha) {
+                                double* grad_alpha, double* grad_xb) {
     if (!h || !obj || nsteps < 1 || k_checkpoint < 1) return IBPM_ERR_INVALID;
     if (obj->window < 1 || obj->window > nsteps) return fail(h, IBPM_ERR_INVALID, "objective window must be in 1..nsteps");
     if (h->lin) return fail(h, IBPM_ERR_UNSUPPORTED, "the adjoint is of the nonlinear step, not of a linearised problem");
@@ -1309,6 +1352,10 @@ extern "C" int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkp
     int rc = ensure_graphs(h, std::max(std::max(1024, h->hist_cap), k));
     if (rc) return rc;
     if ((rc = adj_alloc(h, k, ncp, nsteps))) return rc;
+    h->adj_xb = grad_xb != nullptr;
+    if (h->adj_xb && (rc = xb_alloc(h, k))) return rc;
+    if (h->gadj_xb != h->adj_xb)  // the captured adjoint step must match the request
+        for (int p = 0; p < 2; ++p) if (h->gadj[p]) { cudaGraphExecDestroy(h->gadj[p]); h->gadj[p] = nullptr; }
     h->adj_wx = obj->w_cd * 2.0 * h->h / h->dt;  // CD_j = 2 (h/dt) Σ F̃x (timestepping.jl:330-354)
     h->adj_wy = obj->w_cl * 2.0 * h->h / h->dt;
     std::vector<double> w(nsteps, 0.0);
@@ -1325,6 +1372,7 @@ extern "C" int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkp
             e = cudaGraphInstantiate(&h->gadj[p], graph, 0);
             cudaGraphDestroy(graph);
             if (e != cudaSuccess) return fail(h, IBPM_ERR_CUDA, std::string("adjoint instantiate: ") + cudaGetErrorString(e));
+            h->gadj_xb = h->adj_xb;
         }
     // ---- forward pass with a checkpoint every k steps; J from CD/CL
     CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
@@ -1353,6 +1401,7 @@ extern "C" int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkp
     CK(cudaMemsetAsync(h->qb, 0, sizeof(double) * qs, h->st));
     const long long nq0 = (long long)mg * adj_nlq_blocks(g) * 2 + 2;
     CK(cudaMemsetAsync(h->q0part, 0, sizeof(double) * nq0, h->st));
+    if (h->adj_xb) CK(cudaMemsetAsync(h->gxb, 0, sizeof(double) * h->nf, h->st));
     const int last = nsteps - 1;
     CK(cudaMemcpyAsync(h->adj_n, &last, sizeof(int), cudaMemcpyHostToDevice, h->st));
     int par = 0;
@@ -1366,6 +1415,12 @@ extern "C" int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkp
                                h->st));
             CK(cudaMemcpyAsync(h->tapeq + slot * qs, h->q, sizeof(double) * qs, cudaMemcpyDeviceToDevice, h->st));
             CK(launch_step(h));
+            if (h->adj_xb) {  // what the position gradient reads: F̃b and the level-1 q the step produced
+                CK(cudaMemcpyAsync(h->tapeFb + (long long)slot * h->nf, h->Fb, sizeof(double) * h->nf,
+                                   cudaMemcpyDeviceToDevice, h->st));
+                CK(cudaMemcpyAsync(h->tapeq1 + (long long)slot * g.nq, h->q, sizeof(double) * g.nq,
+                                   cudaMemcpyDeviceToDevice, h->st));
+            }
         }
         for (int n = s1 - 1; n >= s0; --n) {
             CK(cudaGraphLaunch(h->gadj[par], h->st));
@@ -1409,6 +1464,7 @@ extern "C" int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkp
         }
         *grad_alpha = d;
     }
+    if (grad_xb) CK(cudaMemcpyAsync(grad_xb, h->gxb, sizeof(double) * h->nf, cudaMemcpyDeviceToHost, h->st));
     if ((rc = ck_copy(h, ncp, false))) return rc;  // leave the handle at the final state
     CK(cudaStreamSynchronize(h->st));
     int hstatus = 0;

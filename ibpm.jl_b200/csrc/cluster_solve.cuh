@@ -130,8 +130,8 @@ __global__ void __launch_bounds__(cs_threads<N>(), 1) cluster_solve_kernel(Clust
             }
             return V{u, w};
         };
-        dst_pair<N, TP, float>(buf, tw, sn, tid, gid, load, [&](int o, V v) { buf[ct_pad(o)] = v; });
-        gsync<TP>(gid);
+        dst_pair<N, TP, cs_groups<N>(), float>(buf, tw, sn, tid, gid, load, [&](int o, V v) { buf[ct_pad(o)] = v; });
+        gsync<TP, cs_groups<N>()>(gid);
         for (int idx = tid; idx < 2 * CS_CLUSTER * NQ; idx += TP) {
             const int pr = idx / (CS_CLUSTER * NQ), rem = idx % (CS_CLUSTER * NQ);
             const int d = rem / NQ, q = rem % NQ;
@@ -161,8 +161,8 @@ __global__ void __launch_bounds__(cs_threads<N>(), 1) cluster_solve_kernel(Clust
                 tile[o * TPITCH + ca] = v.x;
                 tile[o * TPITCH + ca + 1] = v.y;
             };
-            dst_pair<N, TP, float>(buf, tw, sn, tid, gid, load, emit);
-            gsync<TP>(gid);
+            dst_pair<N, TP, cs_groups<N>(), float>(buf, tw, sn, tid, gid, load, emit);
+            gsync<TP, cs_groups<N>()>(gid);
             const float axa = __ldg(&tb.c[ia]);
             const float axb = hasb ? __ldg(&tb.c[ia + 1]) : 0.0f;
             const float kf = (a.sp.mode == SPEC_DELTA) ? 0.0f : (float)(a.sp.dt / a.sp.den[lev]);
@@ -174,8 +174,8 @@ __global__ void __launch_bounds__(cs_threads<N>(), 1) cluster_solve_kernel(Clust
                 tile[o * TPITCH + ca] *= __frcp_rn(M0) * sc;
                 tile[o * TPITCH + ca + 1] = hasb ? tile[o * TPITCH + ca + 1] * (__frcp_rn(M1) * sc) : 0.0f;
             }
-            gsync<TP>(gid);
-            dst_pair<N, TP, float>(buf, tw, sn, tid, gid, load, emit);
+            gsync<TP, cs_groups<N>()>(gid);
+            dst_pair<N, TP, cs_groups<N>(), float>(buf, tw, sn, tid, gid, load, emit);
         }
     }
     cl.sync();
@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(cs_threads<N>(), 1) cluster_solve_kernel(Clust
             if (c0 + 2 < N && 4 * q + 2 < R) row[2] = v.z;
             if (c0 + 3 < N && 4 * q + 3 < R) row[3] = v.w;
         }
-        gsync<TP>(gid);
+        gsync<TP, cs_groups<N>()>(gid);
         constexpr int EO = (N - 1 + TP - 1) / TP;
         const long long ooff = a.out_map.off(y) + (long long)la * P;
         double* oa = a.out + ooff;
@@ -212,8 +212,8 @@ __global__ void __launch_bounds__(cs_threads<N>(), 1) cluster_solve_kernel(Clust
             }
         }
         auto load = [&](int i) -> V { return V{st[i], vb ? st[N + i] : 0.0f}; };
-        dst_pair<N, TP, float>(buf, tw, sn, tid, gid, load, [&](int o, V v) { buf[ct_pad(o)] = v; });
-        gsync<TP>(gid);
+        dst_pair<N, TP, cs_groups<N>(), float>(buf, tw, sn, tid, gid, load, [&](int o, V v) { buf[ct_pad(o)] = v; });
+        gsync<TP, cs_groups<N>()>(gid);
         float* ds = a.dstore ? a.dstore + a.dstore_map.off(y) + (long long)la * P : nullptr;
 #pragma unroll
         for (int k = 0; k < EO; ++k) {

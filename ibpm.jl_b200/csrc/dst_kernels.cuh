@@ -13,11 +13,16 @@
 // carries the odd harmonics as a running sum, the antisymmetric part the even
 // ones).  Re Y is line a, Im Y is line b.
 //
-// The FFT is a mixed-radix (8, 5, 4, 3, 2) Stockham transform, run in place in
-// shared memory by one "group" of TP = N/8 threads (at least one warp): each
-// stage reads all its inputs into registers, synchronises the group, then
-// writes.  N is a template parameter, so every stride, radix and loop bound is
-// a compile-time constant.  Shared-memory indices are padded by one element
+// The FFT is a mixed-radix Stockham transform, run in place in shared memory
+// by one "group" of TP threads (at least one warp): each stage reads all its
+// inputs into registers, synchronises the group, then writes.  Below N = 1024
+// the plan takes radices (4, 5, 3, 2) with TP = N/4, so each thread holds one
+// radix-4 butterfly per stage: a single slab is a few hundred line pairs, too
+// little work to fill the GPU, and the time of a launch is the length of each
+// thread's dependent chain, which the wider group halves against radix 8.
+// From N = 1024 on (enough line pairs to fill the GPU) the plan is radices
+// (8, 5, 4, 3, 2) with TP = N/8.  N is a template parameter, so every stride,
+// radix and loop bound is a compile-time constant.  Shared-memory indices are padded by one element
 // every eight (pad(i) = i + i/8) so the stride-8 writes of the first stage are
 // free of bank conflicts.
 #pragma once
@@ -29,9 +34,10 @@
 namespace ibpm {
 namespace dstk {
 
+__host__ __device__ constexpr bool ct_fine(int N) { return N < 1024; }
 __host__ __device__ constexpr int ct_radix(int N, int s) {
     int n = N, idx = 0;
-    const int rs[5] = {8, 5, 4, 3, 2};
+    const int rs[5] = {ct_fine(N) ? 4 : 8, 5, ct_fine(N) ? 3 : 4, ct_fine(N) ? 2 : 3, ct_fine(N) ? 8 : 2};
     for (int i = 0; i < 5; ++i) {
         while (n % rs[i] == 0) {
             if (idx == s) return rs[i];
@@ -43,13 +49,13 @@ __host__ __device__ constexpr int ct_radix(int N, int s) {
 }
 __host__ __device__ constexpr int ct_nstages(int N) {
     int n = N, s = 0;
-    const int rs[5] = {8, 5, 4, 3, 2};
+    const int rs[5] = {ct_fine(N) ? 4 : 8, 5, ct_fine(N) ? 3 : 4, ct_fine(N) ? 2 : 3, ct_fine(N) ? 8 : 2};
     for (int i = 0; i < 5; ++i)
         while (n % rs[i] == 0) { n /= rs[i]; ++s; }
     return n == 1 ? s : -1;
 }
 __host__ __device__ constexpr int ct_tp(int N) {
-    int t = ((N / 8 + 31) / 32) * 32;
+    int t = (((ct_fine(N) ? N / 4 : N / 8) + 31) / 32) * 32;
     return t < 32 ? 32 : t;
 }
 __host__ __device__ constexpr int ct_pad(int i) { return i + (i >> 3); }
@@ -72,7 +78,7 @@ __host__ __device__ constexpr int ct_tw_off(int N, int S) {
     return off;
 }
 __host__ __device__ constexpr int ct_tw_count(int N) { return ct_tw_off(N, ct_nstages(N)); }
-// Groups (line pairs) per CTA: 128-thread CTAs for N <= 1024.
+// Groups (line pairs) per CTA of the x-pass: up to 128 threads, or one group.
 __host__ __device__ constexpr int ct_groups(int N) { return ct_tp(N) >= 128 ? 1 : 128 / ct_tp(N); }
 
 // Complex arithmetic for both precisions (V = double2 or float2).
@@ -175,15 +181,16 @@ template <class T> struct dft_t<8, T> {
     }
 };
 
-// Synchronise the TP threads of group `gid` (named barrier 1 + gid when the
-// group spans several warps).
+// Synchronise the TP threads of group `gid` of the G groups of a CTA (named
+// barrier 1 + gid when the group spans several warps).
 // The barrier id is an immediate in each branch, so ptxas reserves only the
 // barriers a kernel can use (a run-time id reserves all sixteen, which caps
 // the resident blocks per SM).
-template <int TP> __device__ __forceinline__ void gsync(int gid) {
+template <int TP, int G> __device__ __forceinline__ void gsync(int gid) {
+    static_assert(G >= 1 && (TP == 32 || G <= 4), "at most four multi-warp groups per CTA");
     if constexpr (TP == 32) {
         __syncwarp();
-    } else if constexpr (TP >= 128) {
+    } else if constexpr (G == 1) {
         asm volatile("bar.sync 1, %0;" ::"n"(TP) : "memory");
     } else {
         switch (gid) {
@@ -195,7 +202,7 @@ template <int TP> __device__ __forceinline__ void gsync(int gid) {
     }
 }
 
-template <int N, int TP, int R, int Ns, int TWOFF, class T>
+template <int N, int TP, int G, int R, int Ns, int TWOFF, class T>
 __device__ __forceinline__ void fft_stage(cplx_t<T>* buf, const cplx_t<T>* W, int tid, int gid) {
     using V = cplx_t<T>;
     constexpr int nb = N / R;
@@ -210,7 +217,7 @@ __device__ __forceinline__ void fft_stage(cplx_t<T>* buf, const cplx_t<T>* W, in
             for (int r = 0; r < R; ++r) v[q][r] = buf[ct_pad(b + r * nb)];
         }
     }
-    gsync<TP>(gid);
+    gsync<TP, G>(gid);
 #pragma unroll
     for (int q = 0; q < QM; ++q) {
         const int b = tid + q * TP;
@@ -226,15 +233,15 @@ __device__ __forceinline__ void fft_stage(cplx_t<T>* buf, const cplx_t<T>* W, in
             for (int r = 0; r < R; ++r) buf[ct_pad(base + r * Ns)] = v[q][r];
         }
     }
-    gsync<TP>(gid);
+    gsync<TP, G>(gid);
 }
 
-template <int N, int TP, int S, int Ns, class T>
+template <int N, int TP, int G, int S, int Ns, class T>
 __device__ __forceinline__ void fft_stages(cplx_t<T>* buf, const cplx_t<T>* W, int tid, int gid) {
     if constexpr (S < ct_nstages(N)) {
         constexpr int R = ct_radix(N, S);
-        fft_stage<N, TP, R, Ns, ct_tw_off(N, S), T>(buf, W, tid, gid);
-        fft_stages<N, TP, S + 1, Ns * R, T>(buf, W, tid, gid);
+        fft_stage<N, TP, G, R, Ns, ct_tw_off(N, S), T>(buf, W, tid, gid);
+        fft_stages<N, TP, G, S + 1, Ns * R, T>(buf, W, tid, gid);
     }
 }
 
@@ -279,7 +286,7 @@ __device__ __forceinline__ float2 shfl_up2(float2 v, int off) {
 
 // Exclusive prefix sum of one complex value per thread over the TP threads of
 // a group.
-template <int TP, class V>
+template <int TP, int G, class V>
 __device__ __forceinline__ V group_excl_scan(V v, int tid, int gid, V* scratch) {
     const int lane = tid & 31, w = tid >> 5;
     V inc = v;
@@ -292,7 +299,7 @@ __device__ __forceinline__ V group_excl_scan(V v, int tid, int gid, V* scratch) 
     if (lane == 0) ex = V{0, 0};
     if constexpr (TP > 32) {
         if (lane == 31) scratch[w] = inc;
-        gsync<TP>(gid);
+        gsync<TP, G>(gid);
         V base = V{0, 0};
         for (int u = 0; u < w; ++u) base = cadd(base, scratch[u]);
         ex = cadd(base, ex);
@@ -303,7 +310,7 @@ __device__ __forceinline__ V group_excl_scan(V v, int tid, int gid, V* scratch) 
 // Post-processing: from Z (in buf) produce the N-1 outputs of both lines and
 // hand them to emit(o, (a_o, b_o)).  All reads of buf precede every emit, so
 // emit may write into buf.
-template <int N, int TP, class T, class Emit>
+template <int N, int TP, int G, class T, class Emit>
 __device__ __forceinline__ void dst_post(cplx_t<T>* buf, int tid, int gid, cplx_t<T>* scratch, Emit emit) {
     using V = cplx_t<T>;
     constexpr int half = N >> 1;
@@ -330,8 +337,8 @@ __device__ __forceinline__ void dst_post(cplx_t<T>* buf, int tid, int gid, cplx_
             D[t] = tot;
         }
     }
-    const V ex = group_excl_scan<TP>(tot, tid, gid, scratch);
-    gsync<TP>(gid);
+    const V ex = group_excl_scan<TP, G>(tot, tid, gid, scratch);
+    gsync<TP, G>(gid);
 #pragma unroll
     for (int t = 0; t < C; ++t) {
         const int k = k0 + t;
@@ -343,13 +350,13 @@ __device__ __forceinline__ void dst_post(cplx_t<T>* buf, int tid, int gid, cplx_
 }
 
 // One DST-I of a line pair: load → pre → FFT → post → emit.
-template <int N, int TP, class T, class Load, class Emit>
+template <int N, int TP, int G, class T, class Load, class Emit>
 __device__ __forceinline__ void dst_pair(cplx_t<T>* buf, const cplx_t<T>* W, const T* s, int tid, int gid,
                                          Load load, Emit emit) {
     dst_pre<N, TP, T>(buf, s, tid, load);
-    gsync<TP>(gid);
-    fft_stages<N, TP, 0, 1, T>(buf, W, tid, gid);
-    dst_post<N, TP, T>(buf, tid, gid, buf + ct_pad(N), emit);
+    gsync<TP, G>(gid);
+    fft_stages<N, TP, G, 0, 1, T>(buf, W, tid, gid);
+    dst_post<N, TP, G, T>(buf, tid, gid, buf + ct_pad(N), emit);
 }
 
 // Tables of one precision: stage twiddles, sin(π m/N) and the spectral table
@@ -395,7 +402,7 @@ __host__ __device__ constexpr size_t x_smem_bytes() {
 }
 
 template <int N, int LOAD, int EMIT>
-__global__ void __launch_bounds__((N <= 1024 ? 128 : 256)) dst_x_kernel(XPassArgs a, Geom g, DstPlan p) {
+__global__ void __launch_bounds__(ct_groups(N) * ct_tp(N)) dst_x_kernel(XPassArgs a, Geom g, DstPlan p) {
     using T = x_real_t<LOAD>;
     using V = cplx_t<T>;
     constexpr int TP = ct_tp(N);
@@ -455,7 +462,7 @@ __global__ void __launch_bounds__((N <= 1024 ? 128 : 256)) dst_x_kernel(XPassArg
             }
         }
         cp_async_wait();
-        gsync<TP>(gid);
+        gsync<TP, G>(gid);
     }
     // L x̃ at (i, la + r) = 4 x̃ − Σ neighbours, zero beyond the slab edges
     // (r = 0, 1; staged row 1 + r)
@@ -525,8 +532,8 @@ __global__ void __launch_bounds__((N <= 1024 ? 128 : 256)) dst_x_kernel(XPassArg
             }
         }
     }
-    dst_pair<N, TP, T>(buf, tw, sn, tid, gid, load, [&](int o, V v) { buf[ct_pad(o)] = v; });
-    gsync<TP>(gid);
+    dst_pair<N, TP, G, T>(buf, tw, sn, tid, gid, load, [&](int o, V v) { buf[ct_pad(o)] = v; });
+    gsync<TP, G>(gid);
 #pragma unroll
     for (int k = 0; k < EO; ++k) {
         const int o = tid + k * TP;
@@ -577,8 +584,12 @@ __global__ void __launch_bounds__((N <= 1024 ? 128 : 256)) dst_x_kernel(XPassArg
 // y-pass of a Poisson-type solve on a tile of TW = 2G columns (all rows)
 // staged in shared memory, in place: DST-I, spectral divide, DST-I.
 // ---------------------------------------------------------------------------
+// Groups of the y-pass: at least two with the fine plan, so that a CTA reads
+// tiles four columns wide.
 template <int N>
-__host__ __device__ constexpr int y_groups() { return ct_groups(N); }
+__host__ __device__ constexpr int y_groups() { return (ct_fine(N) && ct_groups(N) < 2) ? 2 : ct_groups(N); }
+template <int N>
+__host__ __device__ constexpr int y_threads() { return y_groups<N>() * ct_tp(N); }
 template <int N>
 __host__ __device__ constexpr int y_tile_w() { return 2 * y_groups<N>(); }
 __host__ __device__ constexpr int round4(int n) { return ((n + 3) / 4) * 4; }
@@ -590,10 +601,11 @@ __host__ __device__ constexpr size_t y_smem_bytes(int n2) {
 }
 
 template <int N, class T>
-__global__ void __launch_bounds__((N <= 1024 ? 128 : 256), (N <= 512 ? 5 : 1))
+__global__ void __launch_bounds__(y_threads<N>(), (!ct_fine(N) || N > 512) ? 1 : (y_threads<N>() <= 128 ? 5 : 2))
     dst_y_kernel(T* data, SlabMap map, Geom g, DstPlan p, const T* __restrict__ cx, SpecParams sp) {
     using V = cplx_t<T>;
     constexpr int TP = ct_tp(N);
+    constexpr int G = y_groups<N>();
     constexpr int TW = y_tile_w<N>();
     constexpr int TWp = TW + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -671,11 +683,11 @@ __global__ void __launch_bounds__((N <= 1024 ? 128 : 256), (N <= 512 ? 5 : 1))
                 }
             }
         };
-        dst_pair<N, TP, T>(buf, tw, sn, tid, gid, load, emit);
-        gsync<TP>(gid);
+        dst_pair<N, TP, G, T>(buf, tw, sn, tid, gid, load, emit);
+        gsync<TP, G>(gid);
         divide();
-        gsync<TP>(gid);
-        dst_pair<N, TP, T>(buf, tw, sn, tid, gid, load, emit);
+        gsync<TP, G>(gid);
+        dst_pair<N, TP, G, T>(buf, tw, sn, tid, gid, load, emit);
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
@@ -724,7 +736,7 @@ cudaError_t launch_y_n(const Geom& g, const DstPlan& py, const DstPlan& px, void
     const size_t smem = y_smem_bytes<N, T>(g.n2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     dim3 grid((g.n1 + TW - 1) / TW, nslabs);
-    const int threads = y_groups<N>() * ct_tp(N);
+    const int threads = y_threads<N>();
     return launch_k(dst_y_kernel<N, T>, grid, dim3(threads), smem, st, static_cast<T*>(data), map, g, py,
                     static_cast<const T*>(tabs_of<T>(px).c), sp);
 }

@@ -395,5 +395,21 @@ struct AdjTrialArgs {
 int adj_nlq_blocks(const Geom& g);
 cudaError_t launch_adj_trial(const Geom& g, const AdjTrialArgs& a, cudaStream_t st);
 cudaError_t launch_adj_tick(int* adj_n, cudaStream_t st);
+// Body-point position gradient (body.cu, adjoint.cu): derivative weights
+// wd[nf][2][169] once, then per adjoint step
+//   gxb[p] += Σ_{kk ∈ {p, nb+p}} ∇_p [ F̄_kk (E(q_{n+1,1} + q0))_kk − F̃_n,kk (E C r̄₁)_kk ]
+// with F̃_n and q_{n+1,1} read from tape slot (*adj_n) % k.
+cudaError_t launch_dweights(double h, double offx, double offy, const BodyDev& b, double* wd, cudaStream_t st);
+struct AdjXbArgs {
+    const double* wd;
+    const double* Fbar;        // F̄ = B⁻ᵀ F̃̄ of this step
+    const double* tapeFb;      // [k][nf]
+    const double* tapeq1;      // [k][nq]: level-1 q after each step
+    const int* adj_n; int k;
+    double q0x, q0y;           // level-1 base flux
+    const double* rb1;         // r̄ on level 1 (one slab)
+    double* gxb;               // (nb, 2) column-major accumulator
+};
+cudaError_t launch_adj_xb(const Geom& g, const BodyDev& b, const AdjXbArgs& a, cudaStream_t st);
 
 }  // namespace ibpm

@@ -166,27 +166,32 @@ function set_vorticity!(prob::IBProblemGPU, ω::AbstractMatrix{Float64})
 end
 
 """
-    adjoint_run(prob, nsteps; k=50, window=nsteps, w_cd=1.0, w_cl=0.0)
+    adjoint_run(prob, nsteps; k=50, window=nsteps, w_cd=1.0, w_cl=0.0, want_xb=false)
 
 Discrete adjoint of `nsteps` steps from the device state: J = the mean over
 the last `window` steps of Σ_bodies (w_cd·CD + w_cl·CL), and its gradients
 with respect to the start state (Γ, q as independent inputs), to the
-vorticity the start state was built from (`set_vorticity!`), and to the
-freestream angle.  A checkpoint every `k` steps bounds the device memory.
+vorticity the start state was built from (`set_vorticity!`), to the
+freestream angle and (`want_xb`) to the body-point positions, an (nb, 2)
+matrix like `body.xb`.  A checkpoint every `k` steps bounds the device memory.
 """
 function adjoint_run(prob::IBProblemGPU, nsteps::Integer; k::Integer=50, window::Integer=nsteps,
-                     w_cd::Real=1.0, w_cl::Real=0.0)
+                     w_cd::Real=1.0, w_cl::Real=0.0, want_xb::Bool=false)
     g = prob.model_grid
     nΓ = (g.nx - 1) * (g.ny - 1)
     J = Ref(0.0); α = Ref(0.0)
     gΓ = zeros(nΓ, g.mg); gq = zeros(g.nq, g.mg); gω = zeros(g.nx - 1, g.ny - 1)
+    nf = Ref{Int32}(0)
+    check(ccall((:ibpm_sizes, LIB), Cint, (Ptr{Cvoid}, Ptr{Int64}, Ptr{Int64}, Ptr{Int32}, Ref{Int32}, Ptr{Int32}),
+                prob.handle, C_NULL, C_NULL, C_NULL, nf, C_NULL), prob.handle)
+    gx = want_xb ? zeros(nf[] ÷ 2, 2) : nothing
     obj = Objective(window, w_cd, w_cl)
     rc = ccall((:ibpm_adjoint_run, LIB), Cint,
                (Ptr{Cvoid}, Int32, Int32, Ref{Objective}, Ref{Float64}, Ptr{Float64}, Ptr{Float64},
-                Ptr{Float64}, Ref{Float64}),
-               prob.handle, nsteps, k, obj, J, gΓ, gq, gω, α)
+                Ptr{Float64}, Ref{Float64}, Ptr{Float64}),
+               prob.handle, nsteps, k, obj, J, gΓ, gq, gω, α, gx === nothing ? C_NULL : gx)
     check(rc, prob.handle)
-    return (J=J[], grad_Gamma0=gΓ, grad_q0=gq, grad_omega0=gω, grad_alpha=α[])
+    return (J=J[], grad_Gamma0=gΓ, grad_q0=gq, grad_omega0=gω, grad_alpha=α[], grad_xb=gx)
 end
 
 end # module

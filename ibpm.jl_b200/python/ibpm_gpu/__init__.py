@@ -146,7 +146,7 @@ def load_library(path=None):
     lib.ibpm_batch_bench.restype = C.c_int
     lib.ibpm_batch_bench.argtypes = [H, C.c_int32, C.c_int32, _DP]
     lib.ibpm_adjoint_run.restype = C.c_int
-    lib.ibpm_adjoint_run.argtypes = [H, C.c_int32, C.c_int32, C.POINTER(Objective), _DP, _DP, _DP, _DP, _DP]
+    lib.ibpm_adjoint_run.argtypes = [H, C.c_int32, C.c_int32, C.POINTER(Objective), _DP, _DP, _DP, _DP, _DP, _DP]
     lib.ibpm_adjoint_bench.restype = C.c_int
     lib.ibpm_adjoint_bench.argtypes = [H, C.c_int32, C.c_int32, _DP]
     if path is None:
@@ -600,13 +600,15 @@ class AdjointResult:
     grad_q0: np.ndarray         # (nq, mg), like state.q
     grad_omega0: np.ndarray     # (nΓ,): for a start state built from a finest-level vorticity
     grad_alpha: float           # freestream angle
+    grad_xb: np.ndarray = None  # (nb, 2): body-point positions (when asked for)
 
 
-def adjoint_run(prob, nsteps, k_checkpoint=50, window=None, w_cd=1.0, w_cl=0.0):
+def adjoint_run(prob, nsteps, k_checkpoint=50, window=None, w_cd=1.0, w_cl=0.0, want_xb=False):
     """Gradient of J = mean over the last ``window`` steps of Σ_bodies
     (w_cd·CD + w_cl·CL) over ``nsteps`` steps of advance! from the problem's
     current device state, by the discrete adjoint with a checkpoint every
-    ``k_checkpoint`` steps.  The device state ends at the final state of the
+    ``k_checkpoint`` steps; with ``want_xb`` also with respect to the
+    body-point positions.  The device state ends at the final state of the
     run (pull it with ``pull_state``)."""
     lib = prob.lib
     window = nsteps if window is None else window
@@ -617,9 +619,10 @@ def adjoint_run(prob, nsteps, k_checkpoint=50, window=None, w_cd=1.0, w_cl=0.0):
     gq = np.zeros((nq, mg), order="F")
     gw = np.zeros(nG)
     ga = C.c_double()
+    gx = np.zeros((prob.nb, 2), order="F") if want_xb else None
     prob._check(lib.ibpm_adjoint_run(prob.handle, int(nsteps), int(k_checkpoint), C.byref(obj), C.byref(J),
-                                     _ptr(gG), _ptr(gq), _ptr(gw), C.byref(ga)))
-    return AdjointResult(J=J.value, grad_Gamma0=gG, grad_q0=gq, grad_omega0=gw, grad_alpha=ga.value)
+                                     _ptr(gG), _ptr(gq), _ptr(gw), C.byref(ga), _ptr(gx)))
+    return AdjointResult(J=J.value, grad_Gamma0=gG, grad_q0=gq, grad_omega0=gw, grad_alpha=ga.value, grad_xb=gx)
 
 
 def adjoint_bench_steps(prob, nsteps, flush_l2=True):

@@ -221,12 +221,20 @@ typedef struct ibpm_objective {
  *   grad_omega0  ∂J/∂ω for a start state built from a finest-level vorticity
  *                ω as Γ = coarsify([h²ω, 0, …]), (ψ, q) = vort2flux!: (nΓ, 1)
  *   grad_alpha   ∂J/∂α, α the freestream angle of the uniform base flux
+ *   grad_xb      ∂J/∂xb, the body-point positions, (nb, 2) column-major like
+ *                desc.xb (ds held fixed); B = E M E' is differentiated with E
  * The handle is left at the final state of the run, as after ibpm_advance.
- * Device memory: k tape entries (Γ and q) and nsteps/k checkpoints.
+ * Device memory: k tape entries (Γ and q; with grad_xb also F̃b and the
+ * level-1 q of each step) and nsteps/k checkpoints.
+ * The smoothed delta of interface-coupling.jl:24-61 jumps by up to ~3e-9 at
+ * |r| = h, 2h, 3h (rounded coefficients); grad_xb is the derivative of the
+ * pieces, so finite differences agree with it where no grid sample sits at
+ * such a distance (a body point on a grid line puts samples exactly there).
  */
 int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkpoint,
                      const ibpm_objective* obj, double* J, double* grad_Gamma0,
-                     double* grad_q0, double* grad_omega0, double* grad_alpha);
+                     double* grad_q0, double* grad_omega0, double* grad_alpha,
+                     double* grad_xb);
 
 /*
  * Device time of the adjoint of one step (after an ibpm_adjoint_run), for

@@ -22,7 +22,15 @@ flux that vort2flux! made from Γ_n):
   5. Γ_{n+1} = coarsify(Γ'); q_{n+1} = curl ψ_{n+1}; N_n kept      (vort2flux!)
 
 Everything but the product in the nonlinear term is linear with fixed
-coefficients, so the adjoint of a step needs only (Γ_n, q_n).  The spectral
+coefficients, so the adjoint of a step needs only (Γ_n, q_n).
+
+Body-point positions xb enter through E (steps 3 and 4) and through
+B = E M E' (M: C'-source on level 1 → A⁻¹₁ → vort2flux! → level-1 flux,
+laplacian.jl:143-169).  With F̄ = B⁻ᵀ F̃̄ and r̄ = A⁻¹ Γ̄s (both formed by the
+adjoint step anyway) the position gradient of a step is
+  ∂J/∂xb += F̄ · ∂E/∂xb [q_{n+1,1} + q0]  −  F̃_n · ∂E/∂xb [C r̄₁]
+because q_{n+1,1} = qs − M E'F̃ (so E(qs + q0) − B F̃ = E(q_{n+1,1} + q0)),
+and C A⁻¹ Γ̄s₁ = C W + Mᵀ E' F̄ collects the E' and B terms of step 4.  The spectral
 solves S diag(1/M) S·scale are symmetric (S, the 2-D DST-I matrix, is), and
 so is the stencil A; B⁻¹ is not (B is not symmetric), so its transpose is
 applied.  E' is the transpose of E (the same weights).
@@ -252,11 +260,13 @@ def cd_weights(prob):
     return w
 
 
-def adjoint_step(prob, Gn, qxn, qyn, q0x, q0y, Gb1, qxb1, qyb1, Nb1, Fbar):
+def adjoint_step(prob, Gn, qxn, qyn, q0x, q0y, Gb1, qxb1, qyb1, Nb1, Fbar, xb_terms=None):
     """Adjoint of one ``ibpm_ref.advance`` from the state (Gn, qn) at the start
     of the step.  Inputs: the adjoints of the next state (Γ̄, q̄, N̄) and the
     direct sensitivity F̄ of the objective to this step's F̃b.  Returns the
-    adjoints of this step's state and the per-level sums Σq̄0x, Σq̄0y."""
+    adjoints of this step's state and the per-level sums Σq̄0x, Σq̄0y; with
+    ``xb_terms`` = (F̃_n, qx_{n+1} level 1, qy_{n+1} level 1) also this step's
+    contribution to ∂J/∂xb, shape (nb, 2)."""
     g = prob.grid
     mg = g.mg
     dt = prob.dt
@@ -282,6 +292,11 @@ def adjoint_step(prob, Gn, qxn, qyn, q0x, q0y, Gb1, qxb1, qyb1, Nb1, Fbar):
     coarsify_T(Gsb, g)
     # 1: the trial solve of every level
     rb = np.stack([R.ainv_level(Gsb[l], prob, l) for l in range(mg)])
+    gxb = None
+    if xb_terms is not None:
+        Fn, qx1, qy1 = xb_terms
+        cx, cy = rot_T(rb[0], g)
+        gxb = R.dE_T(prob, Fb_, qx1 + q0x[0], qy1 + q0y[0]) - R.dE_T(prob, Fn, cx, cy)
     Gb = np.zeros_like(Gn)
     qxo = np.zeros_like(qxn)
     qyo = np.zeros_like(qyn)
@@ -303,6 +318,8 @@ def adjoint_step(prob, Gn, qxn, qyn, q0x, q0y, Gb1, qxb1, qyb1, Nb1, Fbar):
         if lev < mg - 1:
             fac = 0.25 * dt / (prob.Re * hc ** 2)
             Gb[lev + 1] += get_bc_T(0.25 * bcb + apply_bc_T(rb[lev], fac, g), g)
+    if xb_terms is not None:
+        return Gb, qxo, qyo, Nbo, q0xb, q0yb, gxb
     return Gb, qxo, qyo, Nbo, q0xb, q0yb
 
 
@@ -329,37 +346,60 @@ def mean_drag_gradient(prob, state, nsteps, window, k=50):
     Returns (J, Γ̄_0, q̄_0x, q̄_0y, Σq̄0x[lev], Σq̄0y[lev]): the gradient of J
     with respect to the initial Γ, q (the nonlinear history enters through
     N_{-1} = state.nonlin) and the uniform base flux of every level."""
+    return mean_force_gradient(prob, state, nsteps, window, k)
+
+
+def force_weights(prob, w_cd, w_cl):
+    """∂(Σ_bodies w_cd CD + w_cl CL)/∂F̃b (update_stress!, timestepping.jl:330-354)."""
+    w = np.zeros(prob.nf)
+    w[:prob.nb] = w_cd * 2.0 * prob.grid.h / prob.dt
+    w[prob.nb:] = w_cl * 2.0 * prob.grid.h / prob.dt
+    return w
+
+
+def mean_force_gradient(prob, state, nsteps, window, k=50, w_cd=1.0, w_cl=0.0, want_xb=False):
+    """J = (1/window) Σ_{n > nsteps-window} Σ_bodies (w_cd CD_n + w_cl CL_n);
+    as mean_drag_gradient, and with ``want_xb`` the gradient with respect to
+    the body-point positions (nb, 2) appended to the result."""
     g = prob.grid
     st = state.copy()
     ckpt = {}
     J = 0.0
-    w = cd_weights(prob)
+    w = force_weights(prob, w_cd, w_cl)
     n0 = nsteps - window
     for n in range(nsteps):
         if n % k == 0:
             ckpt[n] = _snapshot(st)
         R.advance(st, prob)
         if n >= n0:
-            J += float(np.sum(st.CD)) / window
+            J += float(np.sum(w_cd * st.CD + w_cl * st.CL)) / window
     Gb = np.zeros_like(st.Gamma)
     qxb = np.zeros_like(st.qx)
     qyb = np.zeros_like(st.qy)
     Nb = np.zeros_like(st.Gamma)
     q0xb = np.zeros(g.mg)
     q0yb = np.zeros(g.mg)
+    gxb = np.zeros((prob.nb, 2))
     for s in sorted(ckpt, reverse=True):
         e = min(s + k, nsteps)
         _restore(st, ckpt[s])
         tape = []
         for n in range(s, e):
-            tape.append((st.Gamma.copy(), st.qx.copy(), st.qy.copy()))
+            Gn, qxn, qyn = st.Gamma.copy(), st.qx.copy(), st.qy.copy()
             R.advance(st, prob)
+            tape.append((Gn, qxn, qyn, st.Fb.copy(), st.qx[0].copy(), st.qy[0].copy()))
         for n in range(e - 1, s - 1, -1):
-            Gn, qxn, qyn = tape[n - s]
+            Gn, qxn, qyn, Fn, qx1, qy1 = tape[n - s]
             Fbar = w / window if n >= n0 else np.zeros(prob.nf)
-            Gb, qxb, qyb, Nb, sx, sy = adjoint_step(prob, Gn, qxn, qyn, st.q0x, st.q0y, Gb, qxb, qyb, Nb, Fbar)
+            out = adjoint_step(prob, Gn, qxn, qyn, st.q0x, st.q0y, Gb, qxb, qyb, Nb, Fbar,
+                               xb_terms=(Fn, qx1, qy1) if want_xb else None)
+            Gb, qxb, qyb, Nb, sx, sy = out[:6]
+            if want_xb:
+                gxb += out[6]
             q0xb += sx
             q0yb += sy
+    if want_xb:
+        return J, Gb, qxb, qyb, q0xb, q0yb, gxb
     return J, Gb, qxb, qyb, q0xb, q0yb
 
 

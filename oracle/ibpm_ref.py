@@ -386,6 +386,97 @@ def delta_h(rf, rb, dr):
     return out
 
 
+def delta_h_db(rf, rb, dr):
+    """∂δh(rf, rb, dr)/∂rb for delta_h above: −sign(rf − rb)/dr times the
+    derivative in r1 = |rf − rb|/dr of the same rounded-coefficient pieces,
+    with d asin(√3/2 (2r1 − c))/dr1 = √3 / √(1 − ¾ (2r1 − c)²) and
+    d √p(r1)/dr1 = p'(r1) / (2 √p(r1))."""
+    d = np.asarray(rf, dtype=np.float64) - rb
+    r1 = np.abs(d) / dr
+    r2 = r1 * r1
+    r3 = r2 * r1
+    out = np.zeros_like(r1)
+    m1 = r1 <= 1.0
+    m2 = (~m1) & (r1 <= 2.0)
+    m3 = (~m1) & (~m2) & (r1 <= 3.0)
+    s3 = np.sqrt(3.0)
+    if np.any(m1):
+        x1, x2, x3 = r1[m1], r2[m1], r3[m1]
+        u = 2.0 * x1 - 1.0
+        a5 = np.arcsin(0.5 * s3 * u)
+        a8 = np.sqrt(1.0 - 12.0 * x2 + 12.0 * x1)
+        da5 = s3 / np.sqrt(1.0 - 0.75 * u * u)
+        da8 = (6.0 - 12.0 * x1) / a8
+        out[m1] = (4 * 4.166666667e-2 * x3 + 3 * (-0.1388888889 + 3.472222222e-2 * a8) * x2
+                   + 3.472222222e-2 * da8 * x3
+                   + 2 * (-7.121664902e-2 - 5.208333333e-2 * a8 + 0.2405626122 * a5) * x1
+                   + (-5.208333333e-2 * da8 + 0.2405626122 * da5) * x2
+                   + (-.2405626122 * a5 - 0.3792313933 + 0.1012731481 * a8)
+                   + (-.2405626122 * da5 + 0.1012731481 * da8) * x1
+                   + 8.0187537413e-2 * da5 - 4.195601852e-2 * da8)
+    if np.any(m2):
+        x1, x2, x3 = r1[m2], r2[m2], r3[m2]
+        u = 2.0 * x1 - 3.0
+        a6 = np.arcsin(0.5 * s3 * u)
+        a9 = np.sqrt(-23.0 + 36.0 * x1 - 12.0 * x2)
+        da6 = s3 / np.sqrt(1.0 - 0.75 * u * u)
+        da9 = (18.0 - 12.0 * x1) / a9
+        out[m2] = (-4 * 6.250000000e-2 * x3 + 3 * (0.4861111111 - 1.736111111e-2 * a9) * x2
+                   - 1.736111111e-2 * da9 * x3
+                   + 2 * (-1.143175026 + 7.812500000e-2 * a9 - 0.1202813061 * a6) * x1
+                   + (7.812500000e-2 * da9 - 0.1202813061 * da6) * x2
+                   + (0.8751991178 + 0.3608439183 * a6 - 0.1548032407 * a9)
+                   + (0.3608439183 * da6 - 0.1548032407 * da9) * x1
+                   - 0.2806563809 * da6 + 0.1150173611 * da9)
+    if np.any(m3):
+        x1, x2, x3 = r1[m3], r2[m3], r3[m3]
+        u = 2.0 * x1 - 5.0
+        a1 = np.arcsin(0.5 * u * s3)
+        a7 = np.sqrt(-71.0 - 12.0 * x2 + 60.0 * x1)
+        da1 = s3 / np.sqrt(1.0 - 0.75 * u * u)
+        da7 = (30.0 - 12.0 * x1) / a7
+        out[m3] = (4 * 2.083333333e-2 * x3 + 3 * (3.472222222e-3 * a7 - 0.2638888889) * x2
+                   + 3.472222222e-3 * da7 * x3
+                   + 2 * (1.214391675 - 2.604166667e-2 * a7 + 2.405626122e-2 * a1) * x1
+                   + (-2.604166667e-2 * da7 + 2.405626122e-2 * da1) * x2
+                   + (-0.1202813061 * a1 - 2.449273192 + 7.262731481e-2 * a7)
+                   + (-0.1202813061 * da1 + 7.262731481e-2 * da7) * x1
+                   + 0.1523563211 * da1 - 7.306134259e-2 * da7)
+    return -np.sign(d) * out / dr
+
+
+def dE_T(prob, c, qx1, qy1):
+    """The position derivative of E contracted with force weights ``c`` (nf,)
+    and a level-1 flux v = (qx1, qy1): for every body point p,
+    G[p] = Σ_{k ∈ {p, nb+p}} c_k ∂(E v)_k/∂xb_p, shape (nb, 2).  The window
+    indices (body_idx) are piecewise constant in xb and the weights vanish at
+    the window's edge, so only the δh factors are differentiated."""
+    g = prob.grid
+    h = g.h
+    nb = prob.nb
+    s = np.arange(-SUPP, SUPP + 1)
+    out = np.zeros((nb, 2))
+    for k in range(nb):
+        xk, yk = prob.xb[k]
+        bx, by = prob.body_idx[k]
+        x = h * (bx - 1 + s) - g.offx
+        y = h * (by - 1 + s) - g.offy
+        I = bx + s - 1                      # 0-based flux indices
+        J = by + s - 1
+        vx = qx1[np.ix_(I, J)]
+        vy = qy1[np.ix_(I, J)]
+        # x-force: qx points at (x, y + h/2); y-force: qy points at (x + h/2, y)
+        dx1, dy1 = delta_h_db(x, xk, h), delta_h_db(y + h / 2, yk, h)
+        fx1, fy1 = delta_h(x, xk, h), delta_h(y + h / 2, yk, h)
+        dx2, dy2 = delta_h_db(x + h / 2, xk, h), delta_h_db(y, yk, h)
+        fx2, fy2 = delta_h(x + h / 2, xk, h), delta_h(y, yk, h)
+        out[k, 0] = (c[k] * np.sum(dx1[:, None] * fy1[None, :] * vx)
+                     + c[nb + k] * np.sum(dx2[:, None] * fy2[None, :] * vy))
+        out[k, 1] = (c[k] * np.sum(fx1[:, None] * dy1[None, :] * vx)
+                     + c[nb + k] * np.sum(fx2[:, None] * dy2[None, :] * vy))
+    return out
+
+
 SUPP = 6
 
 

@@ -143,3 +143,85 @@ def _with_angle(prob, alpha):
     p = copy.copy(prob)
     p.inclination = alpha
     return p
+
+
+# Finite differences in xb: the reference's δh (rounded coefficients) jumps by
+# up to ~3e-9 at |r| = h, 2h, 3h, and a body point on a grid line puts grid
+# samples exactly there, so the bodies are first moved off the grid lines.
+OFF = np.array([0.01234, -0.00711])
+
+
+def _with_xb(prob, xb):
+    """The same problem with body points moved to ``xb`` (E and B rebuilt)."""
+    bodies, t0 = [], 0
+    for b in prob.bodies:
+        n = b.xb.shape[0]
+        bodies.append(R.Body(xb=xb[t0:t0 + n].copy(), ds=b.ds.copy()))
+        t0 += n
+    return R.IBProblem(grid=prob.grid, bodies=bodies, dt=prob.dt, Re=prob.Re, Ux=prob.Ux, Uy=prob.Uy,
+                       inclination=prob.inclination)
+
+
+def test_delta_derivative_matches_central_differences():
+    h = 0.0625
+    rb = 0.0313
+    rf = rb + h * np.linspace(-3.2, 3.2, 4001)
+    eps = 1e-7
+    fd = (R.delta_h(rf, rb + eps, h) - R.delta_h(rf, rb - eps, h)) / (2 * eps)
+    an = R.delta_h_db(rf, rb, h)
+    r1 = np.abs(rf - rb) / h
+    away = np.abs(r1 - np.round(r1)) > 1e-4      # the rounded coefficients leave ~1e-9 jumps at r = h, 2h, 3h
+    assert np.max(np.abs(fd - an)[away]) <= 1e-7 * np.max(np.abs(an))
+
+
+def test_step_position_adjoint_matches_central_differences(prob):
+    """One step: the xb part of the step adjoint against central differences of
+    ⟨adjoint weights, step outputs⟩ with E and B rebuilt at moved points."""
+    prob = _with_xb(prob, prob.xb + OFF)
+    rng = np.random.default_rng(13)
+    st = random_state(prob, seed=8)
+    Gb1 = rng.standard_normal(st.Gamma.shape)
+    qxb1, qyb1 = rng.standard_normal(st.qx.shape), rng.standard_normal(st.qy.shape)
+    Nb1 = rng.standard_normal(st.Gamma.shape)
+    Fbar = rng.standard_normal(prob.nf)
+    dx = rng.standard_normal(prob.xb.shape)
+    eps = 1e-6 * prob.grid.h
+
+    def phi(s):
+        p = _with_xb(prob, prob.xb + s * dx)
+        x = st.copy()
+        R.advance(x, p)
+        return _dot((Gb1, x.Gamma), (qxb1, x.qx), (qyb1, x.qy), (Nb1, x.nonlin[1]), (Fbar, x.Fb))
+    fd = (phi(eps) - phi(-eps)) / (2 * eps)
+    x = st.copy()
+    R.advance(x, prob)
+    out = A.adjoint_step(prob, st.Gamma, st.qx, st.qy, st.q0x, st.q0y, Gb1, qxb1, qyb1, Nb1, Fbar,
+                         xb_terms=(x.Fb, x.qx[0], x.qy[0]))
+    ad = float(np.sum(out[6] * dx))
+    print("step d/dxb: fd %.12e adjoint %.12e" % (fd, ad))
+    assert abs(fd - ad) <= 1e-6 * abs(fd)
+
+
+def test_mean_lift_position_gradient_matches_finite_differences():
+    """∂J/∂xb of the mean total lift over the last 6 of 16 steps (two bodies,
+    an inclined free stream, seeded state; checkpoint every 4 steps) along a
+    random direction of all body points, against central differences with E
+    and B rebuilt at the moved points."""
+    prob2 = oracle_problem("rect64x32_mg2_two")
+    prob2 = _with_xb(prob2, prob2.xb + OFF)
+    rng = np.random.default_rng(21)
+    st = random_state(prob2, seed=9)
+    nsteps, window = 16, 6
+    J, *_, gxb = A.mean_force_gradient(prob2, st, nsteps, window, k=4, w_cd=0.0, w_cl=1.0, want_xb=True)
+    dx = rng.standard_normal(prob2.xb.shape)
+    eps = 1e-6 * prob2.grid.h
+
+    def J_of(s):
+        p = _with_xb(prob2, prob2.xb + s * dx)
+        _, cl = R.run(p, st.copy(), nsteps)
+        return float(np.mean(np.sum(cl[-window:], axis=1)))
+    assert abs(J - J_of(0.0)) <= 1e-12 * abs(J)
+    fd = (J_of(eps) - J_of(-eps)) / (2 * eps)
+    ad = float(np.sum(gxb * dx))
+    print("dJ/dxb: fd %.12e adjoint %.12e" % (fd, ad))
+    assert abs(fd - ad) <= 1e-5 * abs(fd)

@@ -55,25 +55,8 @@ def test_adjoint_matches_oracle(name):
 
 
 def _oracle_gradient(A, prob, state, w_cd, w_cl):
-    """mean_drag_gradient generalised to the weights (w_cd, w_cl): the force
-    weights of the objective enter only through the step's F̃b sensitivity."""
-    saved = A.cd_weights
-
-    def weights(p):
-        w = np.zeros(p.nf)
-        w[:p.nb] = w_cd * 2.0 * p.grid.h / p.dt
-        w[p.nb:] = w_cl * 2.0 * p.grid.h / p.dt
-        return w
-    A.cd_weights = weights
-    try:
-        out = A.mean_drag_gradient(prob, state, NSTEPS, WINDOW, k=K)
-    finally:
-        A.cd_weights = saved
-    # J from the oracle run itself (mean_drag_gradient sums CD only)
-    st = state.copy()
-    cd, cl = __import__("oracle.ibpm_ref", fromlist=["run"]).run(prob, st, NSTEPS)
-    J = float(np.mean(np.sum(w_cd * cd[-WINDOW:] + w_cl * cl[-WINDOW:], axis=1)))
-    return (J,) + out[1:]
+    """The oracle's gradient of the mean of Σ(w_cd CD + w_cl CL) over the window."""
+    return A.mean_force_gradient(prob, state, NSTEPS, WINDOW, k=K, w_cd=w_cd, w_cl=w_cl)
 
 
 def test_adjoint_matches_gpu_finite_differences():
@@ -132,3 +115,95 @@ def test_refined_adjoint_close_to_fp64():
         gp.close()
     assert abs(out[1].J - out[0].J) <= 1e-6 * abs(out[0].J)
     assert rel(out[1].grad_omega0, out[0].grad_omega0) < 1e-5
+
+
+# Body-point positions.  Bodies are moved off the grid lines first: the
+# reference's smoothed delta jumps by ~1e-9 at |r| = h, 2h, 3h, which finite
+# differences would pick up where grid samples sit exactly at those distances.
+OFF = np.array([0.01234, -0.00711])
+
+
+def _pair_xb(name, seed):
+    """Oracle and GPU problems of case ``name`` with the bodies moved by OFF,
+    both started from the same seeded random state."""
+    import ibpm_gpu as G
+    from oracle import ibpm_ref as R
+    from ibpm_cases import CASES, build_bodies, random_state, to_gpu_state
+    c = CASES[name]
+    og = R.make_grid(c["h"], c["bnd"], c["mg"])
+    ob = build_bodies(R, c["bodies"], og.h)
+    for b in ob:
+        b.xb = b.xb + OFF
+    Ux, Uy, a = c["fs"]
+    op = R.IBProblem(grid=og, bodies=ob, dt=c["dt"], Re=c["Re"], Ux=Ux, Uy=Uy, inclination=a)
+    ost = random_state(op, seed=seed)
+    gp = _gpu_with_xb(name, np.concatenate([b.xb for b in ob]))
+    gst = G.IBState(gp)
+    to_gpu_state(ost, gst)
+    G.push_state(gst, gp)
+    return op, ost, gp, gst
+
+
+def _gpu_with_xb(name, xb):
+    import ibpm_gpu as G
+    from ibpm_cases import CASES, build_bodies
+    c = CASES[name]
+    g = G.make_grid(c["h"], c["bnd"], c["mg"])
+    bodies, t0 = build_bodies(G, c["bodies"], g.h), 0
+    for b in bodies:
+        n = b.xb.shape[0]
+        b.xb = xb[t0:t0 + n].copy()
+        t0 += n
+    return G.IBProblem(g, bodies, c["dt"], c["Re"], freestream=c["fs"])
+
+
+def test_position_gradient_matches_oracle():
+    """∂J/∂xb of the mean total lift (two bodies, inclined free stream) against
+    the oracle's position adjoint, itself checked by central differences."""
+    import ibpm_gpu as G
+    from oracle import ibpm_adjoint as A
+    op, ost, gp, _ = _pair_xb("rect64x32_mg2_two", seed=9)
+    res = G.adjoint_run(gp, 16, 4, 6, w_cd=0.3, w_cl=1.0, want_xb=True)
+    J, *_, gxb = A.mean_force_gradient(op, ost, 16, 6, k=4, w_cd=0.3, w_cl=1.0, want_xb=True)
+    assert abs(res.J - J) <= 1e-11 * abs(J)
+    assert rel(res.grad_xb, gxb) < 1e-9
+    # asking for it leaves the other gradients as they were
+    op2, ost2, gp2, _ = _pair_xb("rect64x32_mg2_two", seed=9)
+    res2 = G.adjoint_run(gp2, 16, 4, 6, w_cd=0.3, w_cl=1.0)
+    assert np.array_equal(res2.grad_Gamma0, res.grad_Gamma0) and res2.grad_xb is None
+    gp.close()
+    gp2.close()
+
+
+def test_position_gradient_matches_gpu_finite_differences():
+    """The mean total lift over the last 10 of 30 steps, its gradient with
+    respect to all body-point positions along 8 seeded unit-variance
+    directions against central differences of the GPU forward run
+    (E and B⁻¹ rebuilt on the device for each moved body), ε = 1e-5 h.  The
+    bound scales with ‖∇J‖‖d‖: a direction nearly orthogonal to the gradient
+    has a small projection whose finite difference is mostly round-off (the
+    oracle's own differences show the same, 4e-6 of such a projection)."""
+    import ibpm_gpu as G
+    from ibpm_cases import to_gpu_state
+    op, ost, gp, _ = _pair_xb("sq64_mg3", seed=12)
+    nsteps, window = 30, 10
+    res = G.adjoint_run(gp, nsteps, 10, window, w_cd=0.0, w_cl=1.0, want_xb=True)
+    xb0 = op.xb.copy()
+    eps = 1e-5 * op.grid.h
+
+    def J(xb):
+        p = _gpu_with_xb("sq64_mg3", xb)
+        st = G.IBState(p)
+        to_gpu_state(ost, st)
+        G.push_state(st, p)
+        _, cl = G.advance(st, p, 0.0, nsteps=nsteps)
+        p.close()
+        return float(np.mean(np.sum(cl[-window:], axis=1)))
+    assert abs(J(xb0) - res.J) <= 1e-12 * abs(res.J)
+    rng = np.random.default_rng(2024)
+    for _ in range(8):
+        d = rng.standard_normal(xb0.shape)
+        fd = (J(xb0 + eps * d) - J(xb0 - eps * d)) / (2 * eps)
+        ad = float(np.sum(res.grad_xb * d))
+        assert abs(fd - ad) <= 1e-6 * np.linalg.norm(res.grad_xb) * np.linalg.norm(d), (fd, ad)
+    gp.close()

@@ -80,7 +80,9 @@ def test_moving_grid_refined_matches_oracle():
 
 def test_non_rotating_moving_grid_is_the_static_problem():
     """MovingGrid(U, V, θ ≡ −i, θ̇ ≡ 0) without a free stream of its own steps
-    bitwise as the static problem in the free stream (U, V, i)."""
+    as the static problem in the free stream (U, V, i): the same base flux to
+    the bit, the same step to rounding (the moving form is its own kernel
+    instantiation, whose multiply-adds the compiler may fuse differently)."""
     import ibpm_gpu as G
     c = CASES["sq64_mg3"]
     U, V, inc = 1.0, 0.2, 0.15
@@ -93,8 +95,8 @@ def test_non_rotating_moving_grid_is_the_static_problem():
     assert np.array_equal(sm.q0, ss.q0)
     cdm, clm = G.advance(sm, pm, 0.0, nsteps=20)
     cds, cls = G.advance(ss, ps, 0.0, nsteps=20)
-    assert np.array_equal(cdm, cds) and np.array_equal(clm, cls)
-    assert np.array_equal(sm.Gamma, ss.Gamma) and np.array_equal(sm.q, ss.q)
+    assert rel(cdm, cds) < 1e-13 and rel(clm, cls) < 1e-13
+    assert rel(sm.Gamma, ss.Gamma) < 1e-13 and rel(sm.q, ss.q) < 1e-13
     pm.close()
     ps.close()
 
