@@ -133,9 +133,11 @@ __device__ __forceinline__ double warp_sum(double v) {
 // E (regT!, interface-coupling.jl:122-133) on (q + q0): one warp per force
 // component and batch member.  F[bt*F_bstride + kk*F_kstride].
 // A moving grid's base flux (MovingFlux, level 1) replaces the uniform q0x, q0y.
+// Moving bodies: F −= ub·h, the body-point velocity term of boundary_forces!
+// (timestepping.jl:174-186), when ub is set.
 __global__ void E_kernel(BodyDev b, Geom g, const double* __restrict__ q, long long q_stride, int nbatch,
                          double q0x, double q0y, double* F, long long F_bstride, long long F_kstride,
-                         MovingFlux mv) {
+                         MovingFlux mv, const double* __restrict__ ub, double hub) {
     pdl_wait();
     pdl_trigger();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -159,19 +161,21 @@ __global__ void E_kernel(BodyDev b, Geom g, const double* __restrict__ q, long l
         acc += w[t] * qv;
     }
     acc = warp_sum(acc);
+    if (ub) acc = acc - ub[kk] * hub;
     if (lane == 0) F[(long long)bt * F_bstride + (long long)kk * F_kstride] = acc;
 }
 
 cudaError_t launch_E(const Geom& g, const BodyDev& b, const double* q, long long q_stride, int nbatch,
                      double q0x, double q0y, double* F, long long F_stride, cudaStream_t st,
-                     const MovingFlux& mv) {
+                     const MovingFlux& mv, const double* ub, double hub) {
     // F_stride > 0: batch stride with unit component stride; F_stride < 0:
     // component stride |F_stride| with unit batch stride (columns of B).
     const long long bs = F_stride > 0 ? F_stride : 1;
     const long long ks = F_stride > 0 ? 1 : -F_stride;
     const long long warps = (long long)b.nf * nbatch;
     const int blocks = (int)((warps * 32 + 255) / 256);
-    return launch_k(E_kernel, dim3(blocks), dim3(256), 0, st, b, g, q, q_stride, nbatch, q0x, q0y, F, bs, ks, mv);
+    return launch_k(E_kernel, dim3(blocks), dim3(256), 0, st, b, g, q, q_stride, nbatch, q0x, q0y, F, bs, ks, mv, ub,
+                    hub);
 }
 
 // y = A x, A row-major n×n: one warp per row (F̃b .= Binv*F̃b, timestepping.jl:160).
@@ -289,6 +293,105 @@ __global__ void unit_src_kernel(BodyDev b, Geom g, int col0, int ncol, double* G
     // Γ[i-1, j-1] = (qx[i, j-1] − qx[i, j]) + (qy[i, j] − qy[i-1, j]), (i, j) = (gi+1, gj+1)
     const double v = (qx(gi + 1, gj) - qx(gi + 1, gj + 1)) + (qy(gi + 1, gj + 1) - qy(gi, gj + 1));
     G[(long long)r * bstride + (long long)(gj - 1) * g.P + (gi - 1)] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Bodies moved by a MotionFunction (move_body!, move-body-utils.jl:86-133):
+// point p of body j at the step's row r = (x, y, cos θ, sin θ, ẋ, ẏ, θ̇) of the
+// motion table is xb = (x, y) + Rx x0, ub = (ẋ, ẏ) + Ru x0 with
+// Rx = [c −s; s c], Ru = θ̇ [−s −c; c −s], evaluated in the reference's order
+// without fused multiply-adds; body_idx = floor((xb + off)/h)
+// (interface-coupling.jl:86-87).  A point whose 13×13 window would leave the
+// finest grid sets bit 4 of the status word and is clamped inside, so that no
+// later kernel reads outside the grid.  The bounding box of the windows'
+// centres (min/max body_idx) is accumulated for the projection source.
+// ---------------------------------------------------------------------------
+__global__ void kinematics_kernel(BodyDev b, Geom g, const double* __restrict__ x0, const double* __restrict__ tab,
+                                  const int* __restrict__ step, double h, double offx, double offy, double* xb,
+                                  int* bidx, double* ub, int* bbox, int* status) {
+    pdl_wait();
+    pdl_trigger();
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= b.nb) return;
+    int j = 0;
+    while (j + 1 < b.nbodies && p >= b.body_start[j + 1]) ++j;
+    const double* r = tab + ((long long)(*step) * b.nbodies + j) * 8;
+    const double X = x0[p], Y = x0[b.nb + p];
+    const double c = r[2], s = r[3], thd = r[6];
+    const double xp = __dadd_rn(r[0], __dadd_rn(__dmul_rn(c, X), __dmul_rn(-s, Y)));
+    const double yp = __dadd_rn(r[1], __dadd_rn(__dmul_rn(s, X), __dmul_rn(c, Y)));
+    xb[p] = xp;
+    xb[b.nb + p] = yp;
+    ub[p] = __dadd_rn(r[4], __dadd_rn(__dmul_rn(__dmul_rn(thd, -s), X), __dmul_rn(__dmul_rn(thd, -c), Y)));
+    ub[b.nb + p] = __dadd_rn(r[5], __dadd_rn(__dmul_rn(__dmul_rn(thd, c), X), __dmul_rn(__dmul_rn(thd, -s), Y)));
+    int bx = (int)floor((xp + offx) / h), by = (int)floor((yp + offy) / h);
+    if (!(bx - 6 >= 1 && bx + 6 <= g.nx && by - 6 >= 1 && by + 6 <= g.ny)) {
+        atomicOr(status, 4);
+        bx = min(max(bx, 7), g.nx - 6);
+        by = min(max(by, 7), g.ny - 6);
+    }
+    bidx[p] = bx;
+    bidx[b.nb + p] = by;
+    atomicMin(&bbox[0], bx);
+    atomicMin(&bbox[1], by);
+    atomicMax(&bbox[2], bx);
+    atomicMax(&bbox[3], by);
+}
+
+cudaError_t launch_kinematics(const Geom& g, const BodyDev& b, const double* x0, const double* tab, const int* step,
+                              double h, double offx, double offy, double* xb, int* bidx, double* ub, int* bbox,
+                              int* status, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(bbox, 0x7f, 2 * sizeof(int), st);   // min slots: a large positive int
+    if (e == cudaSuccess) e = cudaMemsetAsync(bbox + 2, 0x80, 2 * sizeof(int), st);  // max slots: a large negative one
+    if (e != cudaSuccess) return e;
+    return launch_k(kinematics_kernel, dim3((b.nb + 127) / 128), dim3(128), 0, st, b, g, x0, tab, step, h, offx, offy,
+                    xb, bidx, ub, bbox, status);
+}
+
+// C'E'F̃b on the level-1 slab for moving bodies, every Γ point in gather form:
+// each regularised flux sums w·F̃b over the body points whose window holds it,
+// in ascending point order (reg!, interface-coupling.jl:99-119), then
+// Γ[i-1, j-1] = (qx[i, j-1] − qx[i, j]) + (qy[i, j] − qy[i-1, j]) (rot!).
+// Points outside the windows' bounding box are written 0.
+__global__ void proj_src_moving_kernel(BodyDev b, Geom g, const double* __restrict__ Fb, const int* __restrict__ bbox,
+                                       double* Gsrc) {
+    pdl_wait();
+    pdl_trigger();
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)g.n1 * g.n2) return;
+    const int i0 = (int)(t % g.n1), j0 = (int)(t / g.n1);
+    const int i = i0 + 2, j = j0 + 2;  // Julia indices of the fluxes around Γ[i0+1, j0+1]
+    double v = 0.0;
+    if (i + 1 >= bbox[0] - 6 && i - 1 <= bbox[2] + 6 && j + 1 >= bbox[1] - 6 && j - 1 <= bbox[3] + 6) {
+        auto flux = [&](int comp, int I, int J) -> double {
+            double q = 0.0;
+            for (int k = 0; k < b.nb; ++k) {
+                const int l = I - b.bidx[k] + 6, m = J - b.bidx[b.nb + k] + 6;
+                if (l >= 0 && l < 13 && m >= 0 && m < 13) {
+                    const int kk = comp * b.nb + k;
+                    q = __dadd_rn(q, __dmul_rn(b.w[(long long)kk * 169 + l * 13 + m], Fb[kk]));
+                }
+            }
+            return q;
+        };
+        v = (flux(0, i, j - 1) - flux(0, i, j)) + (flux(1, i, j) - flux(1, i - 1, j));
+    }
+    Gsrc[(long long)j0 * g.P + i0] = v;
+}
+
+cudaError_t launch_proj_src_moving(const Geom& g, const BodyDev& b, const double* Fb, const int* bbox, double* Gsrc,
+                                   cudaStream_t st) {
+    const long long n = (long long)g.n1 * g.n2;
+    return launch_k(proj_src_moving_kernel, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, st, b, g, Fb, bbox, Gsrc);
+}
+
+__global__ void info_to_status_kernel(const int* info, int* status) {
+    if (*info) atomicOr(status, 2);
+}
+
+cudaError_t launch_info_to_status(const int* info, int* status, cudaStream_t st) {
+    info_to_status_kernel<<<1, 1, 0, st>>>(info, status);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_unit_src(const Geom& g, const BodyDev& b, int col0, int ncol, double* G, long long bstride,

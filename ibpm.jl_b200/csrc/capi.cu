@@ -72,6 +72,14 @@ struct ibpm_handle {
     double mv_xc = 0, mv_yc = 0;
     double mv_last[3] = {0, 0, 0};         // the row of the last step run (or of t = 0)
     double* mtab = nullptr; int mtab_cap = 0;
+    // moving bodies (ibpm_set_motion_function): per-step rows (x, y, cos θ, sin θ, ẋ, ẏ, θ̇, ·) per body
+    bool bodies_moving = false;
+    double* d_x0 = nullptr;                // reference points (nb, 2)
+    double* d_ub = nullptr;                // body-point velocities (nb, 2)
+    int* d_bbox = nullptr;                 // min/max body_idx of the step
+    double* btab = nullptr; int btab_cap = 0;
+    double *bGB = nullptr, *bPB = nullptr, *bQB = nullptr, *bwork = nullptr;  // per-step B rebuild
+    int* binfo = nullptr;
     // discrete adjoint (allocated by the first ibpm_adjoint_run)
     int adj_k = 0, adj_ncp = 0, adj_nsteps = 0;
     double* tapeG = nullptr;               // [k][mg slabs]  Γ_n of the segment being reversed
@@ -251,6 +259,13 @@ static void moving_rates(const ibpm_handle* h, const double* m, double* r) {
     r[0] = -m[3]; r[1] = Ux0; r[2] = Uy0;
 }
 
+// C'E'F̃b on level 1: the sorted segmented reduction of fixed bodies, or the
+// gather form for bodies that move.
+static cudaError_t proj_src(ibpm_handle* h) {
+    if (h->bodies_moving) return launch_proj_src_moving(h->g, h->body, h->Fb, h->d_bbox, h->Gsrc, h->st);
+    return launch_proj_src(h->g, h->body, h->Fb, h->Gsrc, h->st);
+}
+
 static RhsArgs rhs_args(const ibpm_handle* h, int p) {
     const Geom& g = h->g;
     RhsArgs ra{};
@@ -315,12 +330,13 @@ static int enqueue_step_fp64(ibpm_handle* h, int p) {
     rc = vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->qs, 0, 0, 1);  // only the level-1 trial flux is read
     if (rc) return rc;
     // --- boundary_forces! (timestepping.jl:154-163) and update_stress! (:330-354)
-    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h)));
+    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h),
+                    h->bodies_moving ? h->d_ub : nullptr, h->h));
     LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
     LAUNCH(K_STRESS, 8.0 * 3 * h->nb,
            launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
     // --- project_circ! (timestepping.jl:204-223): Γ = Γs − A⁻¹ C'E' F̃b on level 1
-    LAUNCH(K_SRC, 8.0 * 4 * 169 * h->nf, launch_proj_src(g, h->body, h->Fb, h->Gsrc, h->st));
+    LAUNCH(K_SRC, 8.0 * 4 * 169 * h->nf, proj_src(h));
     SlabMap one = levmap(g, 0, 1);
     rc = poisson(h, h->Gsrc, one, h->rhs, one, Gnew, one, 1, SPEC_AINV, XEMIT_SUB);
     if (rc) return rc;
@@ -456,12 +472,13 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
     rc = vort2flux_refined(h, Gnew, nsw, h->qs, 1);  // only the level-1 trial flux is read
     if (rc) return rc;
     // --- boundary_forces! and update_stress! (FP64)
-    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h)));
+    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h),
+                    h->bodies_moving ? h->d_ub : nullptr, h->h));
     LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
     LAUNCH(K_STRESS, 8.0 * 3 * h->nb,
            launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
     // --- project_circ!: P = A⁻¹ C'E' F̃b refined from the previous P; Γ[1] −= P
-    LAUNCH(K_SRC, 8.0 * 4 * 169 * h->nf, launch_proj_src(g, h->body, h->Fb, h->Gsrc, h->st));
+    LAUNCH(K_SRC, 8.0 * 4 * 169 * h->nf, proj_src(h));
     for (int s = 0; s < nsw; ++s) {
         const bool last = s + 1 == nsw;
         if (h->cluster) {
@@ -477,7 +494,42 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
     return vort2flux_refined(h, Gnew, nsw, h->q, mg);
 }
 
+// update_bodies! for MotionFunction bodies (timestepping.jl:386-398): move the
+// points to this step's row of the motion table, recompute body_idx and the
+// weights of E, and rebuild B⁻¹ from B_times! (laplacian.jl:143-169) by the
+// batched unit-source solves of the setup and the device Gauss–Jordan
+// inverse.  The reference solves with B by conjugate gradients to reltol
+// 1e-12 instead (laplacian.jl:123-141); here B⁻¹ is exact to round-off.
+static int enqueue_body_update(ibpm_handle* h) {
+    const Geom& g = h->g;
+    const int nf = h->nf;
+    LAUNCH(K_E, 8.0 * 12 * h->nb,
+           launch_kinematics(g, h->body, h->d_x0, h->btab, h->counter, h->h, h->offx, h->offy, h->d_xb, h->d_bidx,
+                             h->d_ub, h->d_bbox, h->status, h->st));
+    LAUNCH(K_E, 8.0 * 169 * h->nf, launch_weights(g, h->h, h->offx, h->offy, h->body, h->st));
+    const int chunk = std::min(nf, kBChunk);
+    const long long bstride = g.S * g.mg;
+    for (int c0 = 0; c0 < nf; c0 += chunk) {
+        const int R = std::min(chunk, nf - c0);
+        CK(cudaMemsetAsync(h->bGB, 0, sizeof(double) * bstride * R, h->st));
+        LAUNCH(K_SRC, 8.0 * 196 * R, launch_unit_src(g, h->body, c0, R, h->bGB, bstride, h->st));
+        SlabMap l0 = levmap(g, 0, 1, bstride);
+        int rc = poisson(h, h->bGB, l0, h->bGB, l0, h->bGB, l0, R, SPEC_AINV, XEMIT_STORE);
+        if (rc) return rc;
+        rc = vort2flux(h, h->bGB, h->bPB, bstride, R, h->bQB, g.nq, 0, 1);
+        if (rc) return rc;
+        LAUNCH(K_E, 16.0 * 169 * R, launch_E(g, h->body, h->bQB, g.nq, R, 0.0, 0.0, h->Binv + c0, -(long long)nf, h->st));
+    }
+    LAUNCH(K_GEMV, 8.0 * 4.0 * nf * nf, launch_gj_inverse(h->Binv, nf, h->bwork, h->binfo, h->st));
+    LAUNCH(K_GEMV, 8.0, launch_info_to_status(h->binfo, h->status, h->st));
+    return IBPM_OK;
+}
+
 static int enqueue_step(ibpm_handle* h, int p, bool cold = false) {
+    if (h->bodies_moving) {
+        int rc = enqueue_body_update(h);
+        if (rc) return rc;
+    }
     if (h->prec == IBPM_PREC_FP32_REFINED) return enqueue_step_refined(h, p, cold ? h->sweeps + 1 : h->sweeps);
     return enqueue_step_fp64(h, p);
 }
@@ -627,6 +679,9 @@ static void free_handle(ibpm_handle* h) {
     if (h->Pp) cudaFree(h->Pp);
     if (h->D32) cudaFree(h->D32);
     if (h->mtab) cudaFree(h->mtab);
+    for (void* p : {(void*)h->d_x0, (void*)h->d_ub, (void*)h->d_bbox, (void*)h->btab, (void*)h->bGB, (void*)h->bPB,
+                    (void*)h->bQB, (void*)h->bwork, (void*)h->binfo})
+        if (p) cudaFree(p);
     if (h->GB) cudaFree(h->GB);
     if (h->qB) cudaFree(h->qB);
     for (int p = 0; p < 2; ++p) if (h->gadj[p]) cudaGraphExecDestroy(h->gadj[p]);
@@ -900,6 +955,7 @@ extern "C" int ibpm_set_moving_grid(ibpm_handle* h, double xc, double yc, const 
     if (!h || !motion0) return IBPM_ERR_INVALID;
     if (h->nbodies != 1) return fail(h, IBPM_ERR_UNSUPPORTED, "a moving grid carries exactly one body");
     if (h->lin) return fail(h, IBPM_ERR_UNSUPPORTED, "a linearised problem has no moving-grid base flux");
+    if (h->bodies_moving) return fail(h, IBPM_ERR_UNSUPPORTED, "the bodies already move (MotionFunction)");
     if (!std::isfinite(xc) || !std::isfinite(yc)) return fail(h, IBPM_ERR_INVALID, "xc and yc must be finite");
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->st));
@@ -919,6 +975,15 @@ static int ensure_graphs(ibpm_handle* h, int cap) {
         int rc = dalloc(h, &h->hist, (size_t)cap * 2 * h->nbodies);
         if (rc) return rc;
         h->hist_cap = cap;
+    }
+    if (h->bodies_moving && h->btab_cap < h->hist_cap) {
+        if (h->btab) cudaFree(h->btab);
+        h->btab = nullptr;
+        h->btab_cap = 0;
+        int rc = dalloc(h, &h->btab, (size_t)h->hist_cap * h->nbodies * 8);
+        if (rc) return rc;
+        CK(cudaMemsetAsync(h->btab, 0, sizeof(double) * h->hist_cap * h->nbodies * 8, h->st));
+        h->btab_cap = h->hist_cap;
     }
     if (h->moving && h->mtab_cap < h->hist_cap) {
         if (h->mtab) cudaFree(h->mtab);
@@ -962,8 +1027,9 @@ static cudaError_t launch_step(ibpm_handle* h) {
     return e;
 }
 
-// Steps of ibpm_advance and ibpm_advance_moving; `motion` (moving grid only)
-// holds each step's U, V, θ, θ̇.
+// Steps of ibpm_advance, ibpm_advance_moving and ibpm_advance_bodies;
+// `motion` holds each step's U, V, θ, θ̇ (moving grid) or, per body, x, y, θ,
+// ẋ, ẏ, θ̇ (moving bodies).
 static int advance_impl(ibpm_handle* h, int32_t nsteps, const double* motion, double* CD_out, double* CL_out) {
     if (nsteps == 0) return IBPM_OK;
     CK(cudaSetDevice(h->device));
@@ -975,7 +1041,19 @@ static int advance_impl(ibpm_handle* h, int32_t nsteps, const double* motion, do
     int done = 0;
     while (done < nsteps) {
         const int n = std::min(h->hist_cap, nsteps - done);
-        if (motion) {
+        if (motion && h->bodies_moving) {
+            // (x, y, cos θ, sin θ, ẋ, ẏ, θ̇, 0) per body and step (TangentSE2, move-body-utils.jl:70-84)
+            std::vector<double> rows((size_t)8 * n * h->nbodies);
+            for (int s = 0; s < n; ++s)
+                for (int j = 0; j < h->nbodies; ++j) {
+                    const double* m = motion + 6 * ((size_t)(done + s) * h->nbodies + j);
+                    double* r = &rows[8 * ((size_t)s * h->nbodies + j)];
+                    r[0] = m[0]; r[1] = m[1]; r[2] = std::cos(m[2]); r[3] = std::sin(m[2]);
+                    r[4] = m[3]; r[5] = m[4]; r[6] = m[5]; r[7] = 0.0;
+                }
+            CK(cudaMemcpyAsync(h->btab, rows.data(), sizeof(double) * rows.size(), cudaMemcpyHostToDevice, h->st));
+            CK(cudaStreamSynchronize(h->st));
+        } else if (motion) {
             // this chunk's rows; the copy is ordered after the previous chunk's steps
             std::vector<double> rows((size_t)3 * n);
             for (int s = 0; s < n; ++s) moving_rates(h, motion + 4 * (size_t)(done + s), &rows[3 * (size_t)s]);
@@ -1001,6 +1079,8 @@ static int advance_impl(ibpm_handle* h, int32_t nsteps, const double* motion, do
     int hstatus = 0;
     CK(cudaMemcpyAsync(&hstatus, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
+    if (hstatus & 4) return fail(h, IBPM_ERR_INVALID, "a moving body's regularisation stencil left the finest grid");
+    if (hstatus & 2) return fail(h, IBPM_ERR_NONFINITE, "the Schur complement B of the moved bodies is singular");
     if (hstatus) return fail(h, IBPM_ERR_NONFINITE, "CD/CL became non-finite");
     return IBPM_OK;
 }
@@ -1009,7 +1089,55 @@ extern "C" int ibpm_advance(ibpm_handle* h, double t, int32_t nsteps, double* CD
     (void)t;
     if (!h || nsteps < 0) return IBPM_ERR_INVALID;
     if (h->moving) return fail(h, IBPM_ERR_INVALID, "a moving grid needs each step's motion: use ibpm_advance_moving");
+    if (h->bodies_moving)
+        return fail(h, IBPM_ERR_INVALID, "moving bodies need each step's motion: use ibpm_advance_bodies");
     return advance_impl(h, nsteps, nullptr, CD_out, CL_out);
+}
+
+extern "C" int ibpm_set_motion_function(ibpm_handle* h) {
+    if (!h) return IBPM_ERR_INVALID;
+    if (h->lin) return fail(h, IBPM_ERR_UNSUPPORTED, "a linearised problem has fixed bodies");
+    if (h->moving) return fail(h, IBPM_ERR_UNSUPPORTED, "the grid already moves with the body (MovingGrid)");
+    if (h->bodies_moving) return IBPM_OK;
+    CK(cudaSetDevice(h->device));
+    const Geom& g = h->g;
+    const int nf = h->nf, chunk = std::min(nf, kBChunk);
+    const long long bstride = g.S * g.mg;
+    int rc;
+    if ((rc = dalloc(h, &h->d_x0, 2 * h->nb)) || (rc = dalloc(h, &h->d_ub, 2 * h->nb)) ||
+        (rc = dalloc(h, &h->d_bbox, 4)) || (rc = dalloc(h, &h->bGB, (size_t)bstride * chunk)) ||
+        (rc = dalloc(h, &h->bPB, (size_t)bstride * chunk)) || (rc = dalloc(h, &h->bQB, (size_t)g.nq * chunk)) ||
+        (rc = dalloc(h, &h->bwork, (size_t)2 * nf * nf + 2 * nf)) || (rc = dalloc(h, &h->binfo, 1)))
+        return rc;
+    // the reference configuration x0 is the body as created (RigidBody.x0)
+    CK(cudaMemcpyAsync(h->d_x0, h->d_xb, sizeof(double) * 2 * h->nb, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaMemsetAsync(h->d_ub, 0, sizeof(double) * 2 * h->nb, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->bodies_moving = true;
+    h->graphs_ready = false;
+    for (int p = 0; p < 2; ++p) if (h->gadj[p]) { cudaGraphExecDestroy(h->gadj[p]); h->gadj[p] = nullptr; }
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_advance_bodies(ibpm_handle* h, int32_t nsteps, const double* motion, double* CD_out,
+                                   double* CL_out) {
+    if (!h || nsteps < 0 || (nsteps > 0 && !motion)) return IBPM_ERR_INVALID;
+    if (!h->bodies_moving) return fail(h, IBPM_ERR_INVALID, "bodies are fixed: call ibpm_set_motion_function first");
+    for (int64_t e = 0; e < 6 * (int64_t)nsteps * h->nbodies; ++e)
+        if (!std::isfinite(motion[e])) return fail(h, IBPM_ERR_INVALID, "motion values must be finite");
+    return advance_impl(h, nsteps, motion, CD_out, CL_out);
+}
+
+extern "C" int ibpm_get_body_points(ibpm_handle* h, double* xb, double* ub) {
+    if (!h) return IBPM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    if (xb) CK(cudaMemcpyAsync(xb, h->d_xb, sizeof(double) * 2 * h->nb, cudaMemcpyDeviceToHost, h->st));
+    if (ub) {
+        if (h->bodies_moving) CK(cudaMemcpyAsync(ub, h->d_ub, sizeof(double) * 2 * h->nb, cudaMemcpyDeviceToHost, h->st));
+        else std::fill(ub, ub + 2 * h->nb, 0.0);
+    }
+    CK(cudaStreamSynchronize(h->st));
+    return IBPM_OK;
 }
 
 extern "C" int ibpm_advance_moving(ibpm_handle* h, int32_t nsteps, const double* motion, double* CD_out,
@@ -1342,7 +1470,8 @@ extern "C" int ibpm_adjoint_run(ibpm_handle* h, int32_t nsteps, int32_t k_checkp
     if (!h || !obj || nsteps < 1 || k_checkpoint < 1) return IBPM_ERR_INVALID;
     if (obj->window < 1 || obj->window > nsteps) return fail(h, IBPM_ERR_INVALID, "objective window must be in 1..nsteps");
     if (h->lin) return fail(h, IBPM_ERR_UNSUPPORTED, "the adjoint is of the nonlinear step, not of a linearised problem");
-    if (h->moving) return fail(h, IBPM_ERR_UNSUPPORTED, "the adjoint is of the static-body step, not of a moving grid");
+    if (h->moving || h->bodies_moving)
+        return fail(h, IBPM_ERR_UNSUPPORTED, "the adjoint is of the static-body step, not of moving bodies or grids");
     CK(cudaSetDevice(h->device));
     const Geom& g = h->g;
     const int mg = g.mg;
@@ -1571,8 +1700,8 @@ static int batch_capture(ibpm_batch* b, int lanes, int p, bool cold, cudaGraphEx
         e = cudaStreamWaitEvent(b->lane_st[l], b->ev[0], 0);
         for (size_t i = l; i < b->m.size() && e == cudaSuccess && rc == IBPM_OK; i += lanes) {
             ibpm_handle* h = b->m[i];
-            if (h->moving) {
-                rc = bfail(b, IBPM_ERR_UNSUPPORTED, "member " + std::to_string(i) + " is a moving grid (not batched)");
+            if (h->moving || h->bodies_moving) {
+                rc = bfail(b, IBPM_ERR_UNSUPPORTED, "member " + std::to_string(i) + " moves (not batched)");
                 break;
             }
             cudaStream_t own = h->st;

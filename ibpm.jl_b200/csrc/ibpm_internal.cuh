@@ -345,7 +345,16 @@ cudaError_t launch_weights(const Geom& g, double h, double offx, double offy,
                            const BodyDev& b, cudaStream_t st);
 cudaError_t launch_E(const Geom& g, const BodyDev& b, const double* q, long long q_stride,
                      int nbatch, double q0x, double q0y, double* F, long long F_stride,
-                     cudaStream_t st, const MovingFlux& mv = MovingFlux{});
+                     cudaStream_t st, const MovingFlux& mv = MovingFlux{}, const double* ub = nullptr,
+                     double hub = 0.0);
+// Moving bodies (MotionFunction): kinematics from the step's motion-table row,
+// the projection source in gather form, and the singular-B flag.
+cudaError_t launch_kinematics(const Geom& g, const BodyDev& b, const double* x0, const double* tab, const int* step,
+                              double h, double offx, double offy, double* xb, int* bidx, double* ub, int* bbox,
+                              int* status, cudaStream_t st);
+cudaError_t launch_proj_src_moving(const Geom& g, const BodyDev& b, const double* Fb, const int* bbox, double* Gsrc,
+                                   cudaStream_t st);
+cudaError_t launch_info_to_status(const int* info, int* status, cudaStream_t st);
 cudaError_t launch_gemv(const double* A, const double* x, double* y, int n, cudaStream_t st);
 cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double dt,
                           double* hist, int* counter, int* status, cudaStream_t st);

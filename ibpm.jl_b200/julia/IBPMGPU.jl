@@ -2,7 +2,7 @@
 #
 # Binds libibpm_gpu.so (include/ibpm_gpu.h) with ccall and adds
 #     advance!(state::ibpm.IBState, prob::IBProblemGPU, t::Float64)
-# for static bodies and for one body on a MovingGrid
+# for static bodies, one body on a MovingGrid, and MotionFunction bodies
 # so callers of the reference's advance! (src/timestepping/timestepping.jl:35-67),
 # run_sim! (src/ibpm.jl:90-106) included, run unchanged.  The GPU owns the
 # state between calls; `prob.sync_fields = true` copies Γ, ψ, q and the
@@ -10,8 +10,8 @@
 # and F̃b come back and `sync!(state, prob)` pulls the fields on demand.
 module IBPMGPU
 
-using ..ibpm: ibpm, IBState, AbstractIBProblem, MultiGrid, RigidBody, Static, MovingGrid, MotionType,
-              get_body_info
+using ..ibpm: ibpm, IBState, AbstractIBProblem, MultiGrid, RigidBody, Static, MovingGrid, MotionFunction,
+              MotionType, get_body_info
 
 export IBProblemGPU, sync!, push!, adjoint_run, set_vorticity!
 
@@ -46,6 +46,7 @@ mutable struct IBProblemGPU <: AbstractIBProblem
     dt::Float64
     sync_fields::Bool
     motion::Union{Nothing, MovingGrid}
+    body_motions::Union{Nothing, Vector{MotionFunction}}
 end
 
 lasterr(h) = unsafe_string(ccall((:ibpm_last_error, LIB), Cstring, (Ptr{Cvoid},), h))
@@ -82,11 +83,17 @@ function IBProblemGPU(grid::MultiGrid, bodies::Vector{<:RigidBody}, dt::Float64,
     end
     mt = MotionType(bodies)
     motion = mt == MovingGrid ? bodies[1].motion : nothing
-    mt == Static || mt == MovingGrid || error("IBProblemGPU: bodies must be Static or one MovingGrid")
-    p = IBProblemGPU(h[], grid, length(bodies), dt, sync_fields, motion)
+    body_motions = mt == MotionFunction ? MotionFunction[b.motion for b in bodies] : nothing
+    mt in (Static, MovingGrid, MotionFunction) ||
+        error("IBProblemGPU: bodies must be Static, one MovingGrid, or all MotionFunction")
+    p = IBProblemGPU(h[], grid, length(bodies), dt, sync_fields, motion, body_motions)
     finalizer(p) do x
         x.handle == C_NULL || ccall((:ibpm_destroy, LIB), Cint, (Ptr{Cvoid},), x.handle)
         x.handle = C_NULL
+    end
+    if body_motions !== nothing
+        # the points as created are x0; E and B⁻¹ are rebuilt on the device every step
+        check(ccall((:ibpm_set_motion_function, LIB), Cint, (Ptr{Cvoid},), p.handle), p.handle)
     end
     if motion !== nothing
         # rotation about the IBModel's (0, 0), as IBProblem builds it (models.jl:127-153)
@@ -99,6 +106,10 @@ end
 
 "U, V, θ, θ̇ of a MovingGrid at t (motion-types.jl:40-48)."
 motion_row(m::MovingGrid, t::Float64) = Float64[m.U(t), m.V(t), m.θ(t), m.θ̇(t)]
+
+"x, y, θ, ẋ, ẏ, θ̇ of a MotionFunction at t (get_transformation, move-body-utils.jl:70-84)."
+motion_row(m::MotionFunction, t::Float64) =
+    Float64[m.xc[1](t), m.xc[2](t), m.xc[3](t), m.uc[1](t), m.uc[2](t), m.uc[3](t)]
 
 "Copy every IBState field to the device (the reference's column-major layouts)."
 function push!(state::IBState, prob::IBProblemGPU)
@@ -129,7 +140,11 @@ the loop.
 """
 function ibpm.advance!(state::IBState, prob::IBProblemGPU, t::Float64)
     cd = zeros(prob.nbodies); cl = zeros(prob.nbodies)
-    rc = if prob.motion === nothing
+    rc = if prob.body_motions !== nothing
+        rows = reduce(vcat, [motion_row(m, t) for m in prob.body_motions])
+        ccall((:ibpm_advance_bodies, LIB), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+              prob.handle, 1, rows, cd, cl)
+    elseif prob.motion === nothing
         ccall((:ibpm_advance, LIB), Cint, (Ptr{Cvoid}, Float64, Int32, Ptr{Float64}, Ptr{Float64}),
               prob.handle, t, 1, cd, cl)
     else

@@ -9,6 +9,7 @@ with the same names and argument meanings:
 * ``IBProblem(grid, bodies, dt, Re, freestream=...)``
                                        src/pre-processing/problem-types.jl:188-199
 * ``MovingGrid(U, V, theta, theta_dot)`` src/structure-domain/motion-types.jl:40-48
+* ``MotionFunction(xc, uc)``            src/structure-domain/motion-types.jl:13-17
 * ``IBState(prob)``                    src/pre-processing/state-types.jl:271-293
 * ``advance(state, prob, t)``          advance!(state, prob, t), src/timestepping/timestepping.jl:35-67
 * ``vort2flux(state, prob)``           vort2flux!(ψ, q, Γ, model, mg), src/fluid-operators/curl.jl:411-443
@@ -109,6 +110,12 @@ def load_library(path=None):
     lib.ibpm_set_moving_grid.argtypes = [H, C.c_double, C.c_double, _DP]
     lib.ibpm_advance_moving.restype = C.c_int
     lib.ibpm_advance_moving.argtypes = [H, C.c_int32, _DP, _DP, _DP]
+    lib.ibpm_set_motion_function.restype = C.c_int
+    lib.ibpm_set_motion_function.argtypes = [H]
+    lib.ibpm_advance_bodies.restype = C.c_int
+    lib.ibpm_advance_bodies.argtypes = [H, C.c_int32, _DP, _DP, _DP]
+    lib.ibpm_get_body_points.restype = C.c_int
+    lib.ibpm_get_body_points.argtypes = [H, _DP, _DP]
     lib.ibpm_vort2flux.restype = C.c_int
     lib.ibpm_vort2flux.argtypes = [H]
     lib.ibpm_get_binv.restype = C.c_int
@@ -224,6 +231,20 @@ class MovingGrid:
 
 
 @dataclass
+class MotionFunction:
+    """MotionFunction (motion-types.jl:13-17): the body's points as created are
+    its reference configuration, moved rigidly by xc(t) = (x, y, θ) with
+    velocity uc(t) = (ẋ, ẏ, θ̇), each a triple of callables
+    (move_body!, move-body-utils.jl:86-133)."""
+    xc: tuple
+    uc: tuple
+
+    def row(self, t):
+        """(x, y, θ, ẋ, ẏ, θ̇) at t."""
+        return tuple(float(f(t)) for f in self.xc) + tuple(float(f(t)) for f in self.uc)
+
+
+@dataclass
 class RigidBody:
     """RigidBody (body-types.jl:10-16): points xb (nb, 2), ds (nb,) and the
     motion (None: Static; or a MovingGrid)."""
@@ -307,7 +328,9 @@ class IBProblem:
     A body whose ``motion`` is a ``MovingGrid`` (one body only, models.jl:137)
     makes every ``advance`` recompute the base flux from the motion at each
     step's t (timestepping.jl:41-43, 273-318); the free stream is then added
-    to the motion's (the reference's default free stream is zero).
+    to the motion's (the reference's default free stream is zero).  Bodies
+    whose motions are all ``MotionFunction``s move every step, with E and B⁻¹
+    rebuilt on the device (timestepping.jl:386-398).
     """
 
     def __init__(self, grid, bodies, dt, Re, freestream=(1.0, 0.0, 0.0), beta=(1.5, -0.5),
@@ -335,6 +358,14 @@ class IBProblem:
         self._owns = True
         moving = [b.motion for b in self.bodies if isinstance(b.motion, MovingGrid)]
         self.motion = moving[0] if moving else None
+        mfs = [b.motion for b in self.bodies if isinstance(b.motion, MotionFunction)]
+        self.body_motions = None
+        if mfs:
+            if len(mfs) != len(self.bodies) or self.motion is not None:
+                self.close()
+                raise IBPMError(IBPM_ERR_UNSUPPORTED, "either every body has a MotionFunction or none")
+            self.body_motions = mfs
+            self._check(self.lib.ibpm_set_motion_function(self.handle))
         if self.motion is not None:
             if len(self.bodies) != 1:
                 self.close()
@@ -559,7 +590,14 @@ def advance(state, prob, t=0.0, nsteps=1):
         nsteps = ts.size
     cd = np.zeros((nsteps, nbod))
     cl = np.zeros((nsteps, nbod))
-    if getattr(prob, "motion", None) is not None:
+    if getattr(prob, "body_motions", None):
+        if ts.size != nsteps:
+            ts = ts[0] + prob.dt * np.arange(nsteps)
+        rows = np.ascontiguousarray([[m.row(tk) for m in prob.body_motions] for tk in ts],
+                                    dtype=np.float64).reshape(-1)
+        rc = prob.lib.ibpm_advance_bodies(prob.handle, int(nsteps), _ptr(rows), cd.ctypes.data_as(_DP),
+                                          cl.ctypes.data_as(_DP))
+    elif getattr(prob, "motion", None) is not None:
         if ts.size != nsteps:
             ts = ts[0] + prob.dt * np.arange(nsteps)
         rows = np.ascontiguousarray([prob.motion.row(tk) for tk in ts], dtype=np.float64).reshape(-1)
@@ -575,6 +613,15 @@ def advance(state, prob, t=0.0, nsteps=1):
         pull_state(state, prob)
     prob._check(rc)
     return cd, cl
+
+
+def body_points(prob):
+    """The body points and their velocities after the last step (state.xb and
+    the bodies' ub), each (nb, 2)."""
+    xb = np.zeros((prob.nb, 2), order="F")
+    ub = np.zeros((prob.nb, 2), order="F")
+    prob._check(prob.lib.ibpm_get_body_points(prob.handle, _ptr(xb), _ptr(ub)))
+    return xb, ub
 
 
 def vort2flux(state, prob):
@@ -655,9 +702,10 @@ class Batch:
             m.lib = self.lib
             m.grid = sp_["grid"]
             m.bodies = list(sp_["bodies"])
-            if any(isinstance(b.motion, MovingGrid) for b in m.bodies):
-                raise IBPMError(IBPM_ERR_UNSUPPORTED, "member %d: a moving grid is not batched" % i)
+            if any(b.motion is not None for b in m.bodies):
+                raise IBPMError(IBPM_ERR_UNSUPPORTED, "member %d: moving bodies or grids are not batched" % i)
             m.motion = None
+            m.body_motions = None
             m.dt = float(sp_["dt"])
             m.Re = float(sp_["Re"])
             fs = sp_.get("freestream", (1.0, 0.0, 0.0))

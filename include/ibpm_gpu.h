@@ -165,6 +165,38 @@ int ibpm_advance_moving(ibpm_handle* h, int32_t nsteps, const double* motion,
                         double* CD_out, double* CL_out);
 
 /*
+ * Make every body move with a MotionFunction (structure-domain/motion-types.jl:
+ * 13-17): the body's points as created are its reference configuration x0,
+ * and at the start of each step, as update_bodies! does
+ * (timestepping.jl:386-398, move_body! move-body-utils.jl:86-133),
+ *   xb = (x, y) + Rx x0,  ub = (ẋ, ẏ) + Ru x0,
+ *   Rx = [cos θ  −sin θ; sin θ  cos θ],  Ru = θ̇ [−sin θ  −cos θ; cos θ  −sin θ],
+ * then E and B⁻¹ are rebuilt for the moved points and the step solves
+ * B F̃b = E(qs + q0) − ub·h (boundary_forces!, timestepping.jl:174-186).  The
+ * reference applies B⁻¹ by conjugate gradients to reltol 1e-12
+ * (laplacian.jl:123-141); here B is rebuilt on the device every step and
+ * inverted exactly (to round-off).  Refused for a linearised handle or a
+ * moving grid; the adjoint and batches refuse such a handle.  A step whose
+ * moved point's 13×13 stencil would leave the finest grid ends the call with
+ * IBPM_ERR_INVALID.
+ */
+int ibpm_set_motion_function(ibpm_handle* h);
+
+/*
+ * ibpm_advance for MotionFunction bodies: step k uses, for body j,
+ * motion[6 (k nbodies + j) .. +5] = {x, y, θ, ẋ, ẏ, θ̇} evaluated at that
+ * step's t (get_transformation, move-body-utils.jl:70-84).  Outputs as
+ * ibpm_advance (lab-frame forces).
+ */
+int ibpm_advance_bodies(ibpm_handle* h, int32_t nsteps, const double* motion,
+                        double* CD_out, double* CL_out);
+
+/* The body points and their velocities as of the last step (state.xb and the
+ * bodies' ub), (nb, 2) column-major each; either may be NULL.  Fixed bodies
+ * report their points and zero velocities. */
+int ibpm_get_body_points(ibpm_handle* h, double* xb, double* ub);
+
+/*
  * vort2flux!(state.ψ, state.q, state.Γ, model, mg) (curl.jl:411-443): make ψ
  * and q consistent with Γ (coarsifies Γ into the coarse-level centres first).
  */

@@ -18,6 +18,9 @@ relative to the IBPM.jl project root):
 * ``src/timestepping/timestepping.jl:35-354``    ``advance!`` and its helpers
   (``base_flux!`` of a ``MovingGrid``: ``:273-318``)
 * ``src/structure-domain/motion-types.jl:40-48`` ``MovingGrid``
+* ``src/structure-domain/motion-types.jl:13-17``, ``move-body-utils.jl:86-133``,
+  ``timestepping.jl:174-186, 386-398`` ``MotionFunction`` bodies (E and B⁻¹
+  rebuilt every step)
 * ``src/pre-processing/{models,problem-types,state-types}.jl`` state/problem layout
 * ``src/structure-domain/sample-bodies.jl:17-134`` plate, cylinder, NACA bodies
 
@@ -622,6 +625,27 @@ class MovingGrid:
     yc: float = 0.0
 
 
+@dataclass
+class MotionFunction:
+    """MotionFunction (motion-types.jl:13-17): the body's reference points x0
+    move rigidly with the frame xc(t) = (x, y, θ) and velocity
+    uc(t) = (ẋ, ẏ, θ̇), each a triple of callables."""
+    xc: tuple
+    uc: tuple
+
+
+def rigid_motion(m, x0, t):
+    """move_body! for a MotionFunction (move-body-utils.jl:86-133): xb = pos +
+    Rx x0 and ub = vel + Ru x0 with Rx = [c −s; s c], Ru = θ̇ [−s −c; c −s]."""
+    x, y, th = (float(f(t)) for f in m.xc)
+    xd, yd, thd = (float(f(t)) for f in m.uc)
+    c, s = math.cos(th), math.sin(th)
+    X, Y = x0[:, 0], x0[:, 1]
+    xb = np.stack([x + (c * X + (-s) * Y), y + (s * X + c * Y)], axis=1)
+    ub = np.stack([xd + ((thd * (-s)) * X + (thd * (-c)) * Y), yd + ((thd * c) * X + (thd * (-s)) * Y)], axis=1)
+    return xb, ub
+
+
 def moving_grid_coords(g, xc, yc):
     """models.jl:135-153: per level, y − yc of every x-flux row (YY, shape
     (mg, ny)) and x − xc of every y-flux column (XX, shape (mg, nx)); the
@@ -696,6 +720,35 @@ class IBProblem:
         if isinstance(self.motion, MovingGrid):
             assert len(self.bodies) == 1          # models.jl:137, timestepping.jl:277
             self.XX, self.YY = moving_grid_coords(g, self.xc, self.yc)
+        if self.moving_bodies:
+            assert len(self.motion) == len(self.bodies)
+            self.x0 = [b.xb.copy() for b in self.bodies]  # the reference configuration
+            self.ub = np.zeros((self.nb, 2))
+
+    @property
+    def moving_bodies(self):
+        """Every body carries a MotionFunction (MotionType(bodies), move-body-utils.jl:19-26)."""
+        return isinstance(self.motion, (list, tuple)) and all(isinstance(m, MotionFunction) for m in self.motion)
+
+    def move_bodies(self, t):
+        """update_bodies! for MotionFunction bodies (timestepping.jl:386-398): move
+        every body to t, then rebuild E and B⁻¹.  The reference solves with B by
+        conjugate gradients to reltol 1e-12 (laplacian.jl:123-141); here B⁻¹ is
+        the exact inverse of the rebuilt B, as for static bodies."""
+        xbs, ubs = [], []
+        for m, x0 in zip(self.motion, self.x0):
+            xb, ub = rigid_motion(m, x0, t)
+            xbs.append(xb)
+            ubs.append(ub)
+        self.xb = np.concatenate(xbs, axis=0)
+        self.ub = np.concatenate(ubs, axis=0)
+        for b, xb in zip(self.bodies, xbs):
+            b.xb = xb
+        self.E, self.body_idx = setup_reg(self.grid, self.xb)
+        self.ET = self.E.T.tocsr()
+        if self.build_binv:
+            self.B = build_B(self)
+            self.Binv = np.linalg.inv(self.B)
 
     @property
     def nb(self):
@@ -890,10 +943,14 @@ def advance(state, prob, t=0.0):
     """advance!(state, prob, t) for a Static body or a MovingGrid,
     timestepping.jl:35-67."""
     g = prob.grid
+    if prob.moving_bodies:                                               # :39
+        prob.move_bodies(t)
     if isinstance(prob.motion, MovingGrid):                              # :41-43
         state.q0x, state.q0y = base_flux(prob, t)
     Gs, qsx, qsy = get_trial_state(state, prob)                          # :52
     F = E_apply(qsx[0] + state.q0x[0], qsy[0] + state.q0y[0], prob)      # :154-159
+    if prob.moving_bodies:                                               # :174-186: E(qs + q0) − ub·h
+        F = F - np.concatenate([prob.ub[:, 0], prob.ub[:, 1]]) * g.h
     state.Fb = prob.Binv @ F                                             # :160
     update_stress(state, prob)                                           # :57
     state.Gamma = Gs.copy()                                              # :216

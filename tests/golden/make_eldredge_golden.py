@@ -1,6 +1,9 @@
-"""Extract the golden force history of the reference's moving-grid pitch
-manoeuvre (IBPM.jl ``benchmarks/eldredge/pitch_maneuver.jl``, which wrote
-``benchmarks/eldredge/results/force_jl2.mat``) into ``eldredge_pitch.json``.
+"""Extract the golden force histories of the reference's pitch manoeuvre
+(IBPM.jl ``benchmarks/eldredge``) into ``eldredge_pitch.json`` (moving grid:
+``pitch_maneuver.jl`` wrote ``results/force_jl2.mat``) and
+``eldredge_pitch_motion.json`` (moving body: ``pitch_maneuver_motion.jl`` wrote
+``results/force_jl1.mat``; its run covered 10 000 of the 10 001 steps, the
+last entry is zero and is dropped).
 
 The .mat file is MATLAB v7.3 (an HDF5 file after a 512-byte header) holding
 three float64 vectors of 10 001 entries, t, CL and CD (lab frame), stored
@@ -17,14 +20,16 @@ import sys
 
 import numpy as np
 
-SRC = "/root/reference/benchmarks/eldredge/results/force_jl2.mat"
-OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "eldredge_pitch.json")
-N = 10001
+RESULTS = "/root/reference/benchmarks/eldredge/results"
+HERE = os.path.dirname(os.path.abspath(__file__))
+FILES = (("force_jl2.mat", "eldredge_pitch.json", "pitch_maneuver.jl, MovingGrid", 10001),
+         ("force_jl1.mat", "eldredge_pitch_motion.json", "pitch_maneuver_motion.jl, MotionFunction", 10000))
+N = 10001       # entries stored per vector
 OFFSET = 2560   # first byte of the contiguous data blocks
 KEEP = 10
 
 
-def main(src=SRC):
+def extract(src, out, what, nkeep):
     raw = open(src, "rb").read()
     if not raw.startswith(b"MATLAB 7.3 MAT-file") or raw[512:520] != b"\x89HDF\r\n\x1a\n":
         sys.exit("not a MATLAB v7.3 (HDF5) file: %s" % src)
@@ -35,17 +40,17 @@ def main(src=SRC):
     icl = [k for k in range(3) if abs(blocks[k][0]) < 1e-5 and k not in it]
     if len(it) != 1 or len(icd) != 1 or len(icl) != 1 or len({it[0], icd[0], icl[0]}) != 3:
         sys.exit("could not identify t, CL and CD")
-    t, cl, cd = blocks[it[0]], blocks[icl[0]], blocks[icd[0]]
-    if not (np.all(np.isfinite(cl)) and np.all(np.isfinite(cd))):
-        sys.exit("non-finite force history")
-    sel = np.arange(0, N, KEEP)
+    t, cl, cd = blocks[it[0]][:nkeep], blocks[icl[0]][:nkeep], blocks[icd[0]][:nkeep]
+    if not (np.all(np.isfinite(cl)) and np.all(np.isfinite(cd))) or cd[-1] == 0.0:
+        sys.exit("non-finite or incomplete force history")
+    sel = np.arange(0, nkeep, KEEP)
     doc = {
-        "source": "IBPM.jl benchmarks/eldredge/results/force_jl2.mat (pitch_maneuver.jl, MovingGrid)",
+        "source": "IBPM.jl benchmarks/eldredge/results/%s (%s)" % (os.path.basename(src), what),
         "setup": {
             "boundary": [-1.5, 6.5, -2.0, 2.0], "h": 0.02, "mg": 5, "Re": 100.0,
             "plate": {"L": 1.0, "alpha": 0.0, "x0": 0.0, "y0": 0.0, "n": 51},
             "steady": {"dt": 1e-2, "steps": 10001, "freestream": [1.0, 0.0, 0.0]},
-            "pitch": {"dt": 1e-3, "steps": N, "a": 11.0, "t1234": [1.0, 3.0, 4.0, 6.0],
+            "pitch": {"dt": 1e-3, "steps": nkeep, "a": 11.0, "t1234": [1.0, 3.0, 4.0, 6.0],
                       "alpha_max_deg": 45.0, "U": 1.0},
         },
         "steady_cd_published": {"julia": 0.39415052, "fortran": 0.39415060,
@@ -55,10 +60,15 @@ def main(src=SRC):
         "CL_lab": [float(v) for v in cl[sel]],
         "CD_lab": [float(v) for v in cd[sel]],
     }
-    with open(OUT, "w") as f:
+    with open(out, "w") as f:
         json.dump(doc, f, indent=0)
-    print("wrote %s (%d samples)" % (OUT, sel.size))
+    print("wrote %s (%d samples)" % (out, sel.size))
+
+
+def main():
+    for name, out, what, nkeep in FILES:
+        extract(os.path.join(RESULTS, name), os.path.join(HERE, out), what, nkeep)
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    main()
