@@ -17,6 +17,14 @@ using namespace ibpm;
 
 #define IBPM_VERSION_STR "ibpm_gpu 0.1.0 (sm_100a, FP64)"
 
+// FP32_REFINED: steps after create or set_state that run one more correction
+// sweep per solve.  The first lacks good initial guesses (ψ and the previous
+// projection may not belong to the state); the next ones follow an impulsive
+// start, whose per-step changes are orders of magnitude above the later ones
+// (on the 512² × 5-level cylinder the largest one-sweep force errors fall in
+// the first six steps).
+static const int kColdSteps = 8;
+
 struct ibpm_handle {
     int device = 0;
     cudaStream_t st = nullptr;
@@ -57,7 +65,7 @@ struct ibpm_handle {
     // FP32_REFINED
     int prec = IBPM_PREC_FP64;
     int sweeps = 1;                        // correction sweeps per solve
-    int cold = 2;                          // steps left that lack good initial guesses
+    int cold = kColdSteps;                 // steps left that lack good initial guesses
     float* T32 = nullptr;                  // mg slabs of FP32 transform scratch
     double* Pp = nullptr;                  // A⁻¹C'E'F̃b of the previous step (level 1)
     bool cluster = false;                  // level solves in one cluster launch (cluster_solve.cuh)
@@ -877,7 +885,7 @@ extern "C" int ibpm_set_state(ibpm_handle* h, const double* Gamma, const double*
         // the refined mode's hidden initial guess of the projection solve is
         // cleared, so results depend only on the state given (ψ is the other
         // guess; it is part of the state)
-        h->cold = 2;
+        h->cold = kColdSteps;
         if (h->Pp) CK(cudaMemsetAsync(h->Pp, 0, sizeof(double) * g.S, h->st));
         CK(cudaStreamSynchronize(h->st));
     }
@@ -907,7 +915,7 @@ extern "C" int ibpm_set_base_state(ibpm_handle* h, const double* Gamma_B, const 
     }
     h->graphs_ready = false;
     for (int p = 0; p < 2; ++p) if (h->gadj[p]) { cudaGraphExecDestroy(h->gadj[p]); h->gadj[p] = nullptr; }
-    h->cold = 2;
+    h->cold = kColdSteps;
     CK(cudaStreamSynchronize(h->st));
     return IBPM_OK;
 }
@@ -1014,11 +1022,9 @@ static int ensure_graphs(ibpm_handle* h, int cap) {
     return IBPM_OK;
 }
 
-// Queue one step from the current parity.  In FP32_REFINED mode the first two
-// steps after create or set_state run one more correction sweep per solve:
-// the initial guesses of the first (ψ, the previous projection) may not belong
-// to the state, and those of the second come from a step whose changes can be
-// orders of magnitude larger (an impulsive start).
+// Queue one step from the current parity.  In FP32_REFINED mode the first
+// kColdSteps steps after create or set_state run one more correction sweep
+// per solve (see kColdSteps).
 static cudaError_t launch_step(ibpm_handle* h) {
     cudaGraphExec_t ge = (h->cold > 0 && h->gcold[h->cur]) ? h->gcold[h->cur] : h->gexec[h->cur];
     if (h->cold > 0) --h->cold;
@@ -1648,7 +1654,7 @@ struct ibpm_batch {
     std::vector<cudaEvent_t> ev;               // fork + one join event per lane
     int lanes = 0;
     int cur = 0;                               // parity shared by the members
-    int cold = 2;
+    int cold = kColdSteps;
     cudaGraphExec_t g[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cold][parity]
     int hist_cap = 0;
     std::vector<double> cd, cl;                // [member][step][body] of the last advance
@@ -1679,7 +1685,7 @@ static int reset_state(ibpm_handle* h) {
     if (h->Pp) CK(cudaMemsetAsync(h->Pp, 0, sizeof(double) * g.S, h->st));
     CK(cudaStreamSynchronize(h->st));
     h->cur = 0;
-    h->cold = 2;
+    h->cold = kColdSteps;
     h->nonlin1_valid = false;
     return IBPM_OK;
 }
