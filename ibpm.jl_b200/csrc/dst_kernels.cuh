@@ -584,29 +584,33 @@ __global__ void __launch_bounds__(ct_groups(N) * ct_tp(N)) dst_x_kernel(XPassArg
 // y-pass of a Poisson-type solve on a tile of TW = 2G columns (all rows)
 // staged in shared memory, in place: DST-I, spectral divide, DST-I.
 // ---------------------------------------------------------------------------
-// Groups of the y-pass: at least two with the fine plan, so that a CTA reads
-// tiles four columns wide.
-template <int N>
-__host__ __device__ constexpr int y_groups() { return (ct_fine(N) && ct_groups(N) < 2) ? 2 : ct_groups(N); }
-template <int N>
-__host__ __device__ constexpr int y_threads() { return y_groups<N>() * ct_tp(N); }
-template <int N>
-__host__ __device__ constexpr int y_tile_w() { return 2 * y_groups<N>(); }
+// Groups (column pairs) per CTA of the y-pass.  FP32 passes take one group
+// (more CTAs for a single slab: the refined step's y-passes are single-slab
+// and latency-bound); FP64 passes keep at least two with the fine plan, so a
+// CTA reads tiles of four 8-byte columns.
+template <int N, class T>
+__host__ __device__ constexpr int y_groups() {
+    return (std::is_same<T, double>::value && ct_fine(N) && ct_groups(N) < 2) ? 2 : ct_groups(N);
+}
+template <int N, class T>
+__host__ __device__ constexpr int y_threads() { return y_groups<N, T>() * ct_tp(N); }
+template <int N, class T>
+__host__ __device__ constexpr int y_tile_w() { return 2 * y_groups<N, T>(); }
 __host__ __device__ constexpr int round4(int n) { return ((n + 3) / 4) * 4; }
 template <int N, class T>
 __host__ __device__ constexpr size_t y_smem_bytes(int n2) {
     return tables_bytes<N, T>() + (size_t)round4(n2) * sizeof(T) +  // spectral table of y
-           (size_t)round4(n2 * (y_tile_w<N>() + 1)) * sizeof(T) +
-           (size_t)y_groups<N>() * ct_buf(N) * sizeof(cplx_t<T>);
+           (size_t)round4(n2 * (y_tile_w<N, T>() + 1)) * sizeof(T) +
+           (size_t)y_groups<N, T>() * ct_buf(N) * sizeof(cplx_t<T>);
 }
 
 template <int N, class T>
-__global__ void __launch_bounds__(y_threads<N>(), (!ct_fine(N) || N > 512) ? 1 : (y_threads<N>() <= 128 ? 5 : 2))
+__global__ void __launch_bounds__(y_threads<N, T>(), (!ct_fine(N) || N > 512) ? 1 : (y_threads<N, T>() <= 128 ? 5 : 2))
     dst_y_kernel(T* data, SlabMap map, Geom g, DstPlan p, const T* __restrict__ cx, SpecParams sp) {
     using V = cplx_t<T>;
     constexpr int TP = ct_tp(N);
-    constexpr int G = y_groups<N>();
-    constexpr int TW = y_tile_w<N>();
+    constexpr int G = y_groups<N, T>();
+    constexpr int TW = y_tile_w<N, T>();
     constexpr int TWp = TW + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P = g.P, n1 = g.n1, n2 = g.n2;
@@ -732,11 +736,11 @@ cudaError_t launch_x_t(const Geom& g, const DstPlan& px, const XPassArgs& a, cud
 template <int N, class T>
 cudaError_t launch_y_n(const Geom& g, const DstPlan& py, const DstPlan& px, void* data, SlabMap map, int nslabs,
                        const SpecParams& sp, cudaStream_t st) {
-    constexpr int TW = y_tile_w<N>();
+    constexpr int TW = y_tile_w<N, T>();
     const size_t smem = y_smem_bytes<N, T>(g.n2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     dim3 grid((g.n1 + TW - 1) / TW, nslabs);
-    const int threads = y_threads<N>();
+    const int threads = y_threads<N, T>();
     return launch_k(dst_y_kernel<N, T>, grid, dim3(threads), smem, st, static_cast<T*>(data), map, g, py,
                     static_cast<const T*>(tabs_of<T>(px).c), sp);
 }
