@@ -605,7 +605,9 @@ __host__ __device__ constexpr size_t y_smem_bytes(int n2) {
 }
 
 template <int N, class T>
-__global__ void __launch_bounds__(y_threads<N, T>(), (!ct_fine(N) || N > 512) ? 1 : (y_threads<N, T>() <= 128 ? 5 : 2))
+// (3 resident 256-thread CTAs per SM keep the FP64 pass at 80 registers without
+// spills: the five-slab trial solve's y-pass then needs 1.4 waves instead of 2.2)
+__global__ void __launch_bounds__(y_threads<N, T>(), (!ct_fine(N) || N > 512) ? 1 : (y_threads<N, T>() <= 128 ? 5 : 3))
     dst_y_kernel(T* data, SlabMap map, Geom g, DstPlan p, const T* __restrict__ cx, SpecParams sp) {
     using V = cplx_t<T>;
     constexpr int TP = ct_tp(N);
