@@ -241,30 +241,36 @@ cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double d
 }
 
 // Γsrc = C'(E' F̃b) at the Γ points whose rot! stencil touches a regularised
-// flux point (timestepping.jl:217, curl.jl:300-312).  Each flux value is the
-// sum over its sorted contributor list (ascending force component, the order
-// reg! accumulates in, interface-coupling.jl:103-107).
+// flux point (timestepping.jl:217, curl.jl:300-312): Γ = (qx₁ − qx₂) +
+// (qy₁ − qy₂) over the point's four fluxes, each flux the sum over its sorted
+// contributor list (interface-coupling.jl:103-107).  One warp per Γ point:
+// the lanes take the contributors of all four fluxes (about 50 at one point
+// per h), with the signs of rot!, and a shuffle tree adds them in a fixed
+// order, so the result is deterministic (the reference adds sequentially;
+// the two agree to round-off).
 __global__ void proj_src_kernel(BodyDev b, const double* __restrict__ Fb, double* Gsrc) {
     pdl_wait();
     pdl_trigger();
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (p >= b.n_src) return;
-    double v[4];
+    double v = 0.0;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int row = b.src_rows[4 * p + r];
+        if (row < 0) continue;
         double acc = 0.0;
-        if (row >= 0) {
-            for (int e = b.et_ptr[row]; e < b.et_ptr[row + 1]; ++e) acc += b.w[b.et_w[e]] * Fb[b.et_k[e]];
-        }
-        v[r] = acc;
+        for (int e = b.et_ptr[row] + lane; e < b.et_ptr[row + 1]; e += 32) acc += b.w[b.et_w[e]] * Fb[b.et_k[e]];
+        v += (r == 0 || r == 2) ? acc : -acc;
     }
-    Gsrc[b.src_pts[p]] = (v[0] - v[1]) + (v[2] - v[3]);
+    v = warp_sum(v);
+    if (lane == 0) Gsrc[b.src_pts[p]] = v;
 }
 
 cudaError_t launch_proj_src(const Geom& g, const BodyDev& b, const double* Fb, double* Gsrc, cudaStream_t st) {
     if (b.n_src == 0) return cudaSuccess;
-    return launch_k(proj_src_kernel, dim3((b.n_src + 127) / 128), dim3(128), 0, st, b, Fb, Gsrc);
+    const long long threads = (long long)b.n_src * 32;
+    return launch_k(proj_src_kernel, dim3((unsigned)((threads + 255) / 256)), dim3(256), 0, st, b, Fb, Gsrc);
 }
 
 // C'E' e_kk for unit forces kk = col0 + r (B_times!, laplacian.jl:318), written
