@@ -199,10 +199,8 @@ cudaError_t launch_gemv(const double* A, const double* x, double* y, int n, cuda
 // update_stress! (timestepping.jl:330-354): fb = F̃b (h/dt) ./ ds,
 // CD_j = 2 Σ ds fb_x, CL_j = 2 Σ ds fb_y, written to hist[step][2][nbodies].
 // One block; a non-finite CD/CL sets bit 0 of *status.
-__global__ void stress_kernel(BodyDev b, const double* __restrict__ Fb, double h, double dt, double* hist,
-                              int* counter, int* status) {
-    pdl_wait();
-    pdl_trigger();
+__device__ __forceinline__ void stress_block(const BodyDev& b, const double* __restrict__ Fb, double h, double dt,
+                                             double* hist, int* counter, int* status) {
     __shared__ double red[2][256];
     const int step = *counter;
     const double hdt = h / dt;
@@ -235,6 +233,13 @@ __global__ void stress_kernel(BodyDev b, const double* __restrict__ Fb, double h
     if (threadIdx.x == 0) *counter = step + 1;
 }
 
+__global__ void stress_kernel(BodyDev b, const double* __restrict__ Fb, double h, double dt, double* hist,
+                              int* counter, int* status) {
+    pdl_wait();
+    pdl_trigger();
+    stress_block(b, Fb, h, dt, hist, counter, status);
+}
+
 cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double dt, double* hist, int* counter,
                           int* status, cudaStream_t st) {
     return launch_k(stress_kernel, dim3(1), dim3(256), 0, st, b, Fb, h, dt, hist, counter, status);
@@ -248,11 +253,8 @@ cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double d
 // per h), with the signs of rot!, and a shuffle tree adds them in a fixed
 // order, so the result is deterministic (the reference adds sequentially;
 // the two agree to round-off).
-__global__ void proj_src_kernel(BodyDev b, const double* __restrict__ Fb, double* Gsrc) {
-    pdl_wait();
-    pdl_trigger();
-    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void proj_src_warp(const BodyDev& b, const double* __restrict__ Fb, double* Gsrc, int p,
+                                              int lane) {
     if (p >= b.n_src) return;
     double v = 0.0;
 #pragma unroll
@@ -267,10 +269,37 @@ __global__ void proj_src_kernel(BodyDev b, const double* __restrict__ Fb, double
     if (lane == 0) Gsrc[b.src_pts[p]] = v;
 }
 
+__global__ void proj_src_kernel(BodyDev b, const double* __restrict__ Fb, double* Gsrc) {
+    pdl_wait();
+    pdl_trigger();
+    proj_src_warp(b, Fb, Gsrc, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31);
+}
+
 cudaError_t launch_proj_src(const Geom& g, const BodyDev& b, const double* Fb, double* Gsrc, cudaStream_t st) {
     if (b.n_src == 0) return cudaSuccess;
     const long long threads = (long long)b.n_src * 32;
     return launch_k(proj_src_kernel, dim3((unsigned)((threads + 255) / 256)), dim3(256), 0, st, b, Fb, Gsrc);
+}
+
+// update_stress! and the projection source in one launch (both read only F̃b):
+// block 0 reduces CD/CL (and advances the step counter), the other blocks
+// form C'E'F̃b, one warp per Γ point.
+__global__ void stress_src_kernel(BodyDev b, const double* __restrict__ Fb, double h, double dt, double* hist,
+                                  int* counter, int* status, double* Gsrc) {
+    pdl_wait();
+    pdl_trigger();
+    if (blockIdx.x == 0) {
+        stress_block(b, Fb, h, dt, hist, counter, status);
+        return;
+    }
+    proj_src_warp(b, Fb, Gsrc, ((blockIdx.x - 1) * blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31);
+}
+
+cudaError_t launch_stress_src(const BodyDev& b, const double* Fb, double h, double dt, double* hist, int* counter,
+                              int* status, double* Gsrc, cudaStream_t st) {
+    const long long threads = (long long)b.n_src * 32;
+    const unsigned blocks = 1 + (unsigned)((threads + 255) / 256);
+    return launch_k(stress_src_kernel, dim3(blocks), dim3(256), 0, st, b, Fb, h, dt, hist, counter, status, Gsrc);
 }
 
 // C'E' e_kk for unit forces kk = col0 + r (B_times!, laplacian.jl:318), written

@@ -267,11 +267,20 @@ static void moving_rates(const ibpm_handle* h, const double* m, double* r) {
     r[0] = -m[3]; r[1] = Ux0; r[2] = Uy0;
 }
 
-// C'E'F̃b on level 1: the sorted segmented reduction of fixed bodies, or the
-// gather form for bodies that move.
-static cudaError_t proj_src(ibpm_handle* h) {
-    if (h->bodies_moving) return launch_proj_src_moving(h->g, h->body, h->Fb, h->d_bbox, h->Gsrc, h->st);
-    return launch_proj_src(h->g, h->body, h->Fb, h->Gsrc, h->st);
+// update_stress! (timestepping.jl:330-354) and the projection source C'E'F̃b
+// on level 1: for fixed bodies one launch (block 0 reduces CD/CL, the others
+// gather the sorted contributor lists); for moving bodies the stress kernel
+// and the gather form over the moved points.
+static int stress_and_src(ibpm_handle* h) {
+    if (h->bodies_moving) {
+        LAUNCH(K_STRESS, 8.0 * 3 * h->nb,
+               launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
+        LAUNCH(K_SRC, 8.0 * 4 * 169 * h->nf, launch_proj_src_moving(h->g, h->body, h->Fb, h->d_bbox, h->Gsrc, h->st));
+        return IBPM_OK;
+    }
+    LAUNCH(K_SRC, 8.0 * (4 * 169 * h->nf + 3 * h->nb),
+           launch_stress_src(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->Gsrc, h->st));
+    return IBPM_OK;
 }
 
 static RhsArgs rhs_args(const ibpm_handle* h, int p) {
@@ -341,10 +350,8 @@ static int enqueue_step_fp64(ibpm_handle* h, int p) {
     LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h),
                     h->bodies_moving ? h->d_ub : nullptr, h->h));
     LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
-    LAUNCH(K_STRESS, 8.0 * 3 * h->nb,
-           launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
     // --- project_circ! (timestepping.jl:204-223): Γ = Γs − A⁻¹ C'E' F̃b on level 1
-    LAUNCH(K_SRC, 8.0 * 4 * 169 * h->nf, proj_src(h));
+    if ((rc = stress_and_src(h))) return rc;
     SlabMap one = levmap(g, 0, 1);
     rc = poisson(h, h->Gsrc, one, h->rhs, one, Gnew, one, 1, SPEC_AINV, XEMIT_SUB);
     if (rc) return rc;
@@ -483,10 +490,8 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
     LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h),
                     h->bodies_moving ? h->d_ub : nullptr, h->h));
     LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
-    LAUNCH(K_STRESS, 8.0 * 3 * h->nb,
-           launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
     // --- project_circ!: P = A⁻¹ C'E' F̃b refined from the previous P; Γ[1] −= P
-    LAUNCH(K_SRC, 8.0 * 4 * 169 * h->nf, proj_src(h));
+    if ((rc = stress_and_src(h))) return rc;
     for (int s = 0; s < nsw; ++s) {
         const bool last = s + 1 == nsw;
         if (h->cluster) {

@@ -360,6 +360,9 @@ cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double d
                           double* hist, int* counter, int* status, cudaStream_t st);
 cudaError_t launch_proj_src(const Geom& g, const BodyDev& b, const double* Fb, double* Gsrc,
                             cudaStream_t st);
+// launch_stress and launch_proj_src in one launch (fixed bodies)
+cudaError_t launch_stress_src(const BodyDev& b, const double* Fb, double h, double dt, double* hist, int* counter,
+                              int* status, double* Gsrc, cudaStream_t st);
 cudaError_t launch_unit_src(const Geom& g, const BodyDev& b, int col0, int ncol, double* G,
                             long long bstride, cudaStream_t st);
 
