@@ -294,8 +294,7 @@ struct RhsArgs {
     const double* q;                      // state q, nq per level
     const double* Nprev;                  // nonlin from the previous step
     double* Nnew;                         // nonlin of this step
-    double* rhs;                          // right-hand side of the trial solve, or
-    float* rhs_inc;                       // (when set) rhs − A Γ, the increment form
+    double* rhs;                          // right-hand side of the trial solve
     double q0x[8], q0y[8];                // uniform base flux per level
     double fac_bc[8];                     // 0.25 dt / (Re hc²)
     double c_lap[8];                      // dt / (2 Re hc²)

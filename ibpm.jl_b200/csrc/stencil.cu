@@ -123,14 +123,7 @@ __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
     const long long o = a.Gmap.off(lev) + (long long)j0 * P + i0;
     const double Np = a.Nprev[o];
     a.Nnew[o] = N;
-    if (a.rhs_inc) {
-        // rhs − (I + cL) Γ = −2c L Γ + β1 dt N + β2 dt Nprev + rhsbc: the trial
-        // solve Γs = Γ + A⁻¹(rhs − A Γ) needs only this increment
-        const double dA = 2.0 * a.c_lap[lev] * ((((ge + gw) + gn) + gs) - 4.0 * gc);
-        a.rhs_inc[o] = (float)(((dA + a.b1dt * N) + a.b2dt * Np) + rbc);
-    } else {
-        a.rhs[o] = ((AG + a.b1dt * N) + a.b2dt * Np) + rbc;
-    }
+    a.rhs[o] = ((AG + a.b1dt * N) + a.b2dt * Np) + rbc;
 }
 
 cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st) {
