@@ -297,13 +297,14 @@ def measure(args, d, precision, sampler=None):
     G.pull_state(st, prob)
     e2e_s = d.max(time.perf_counter() - t0)
     state_bytes = 8 * (st.Gamma.size * 4 + st.q.size * 2 + st.Fb.size)
+    gamma = np.array(st.Gamma)
 
     prof = G.profile_steps(prob, 4, flush_l2=True)
     lps = G.launches_per_step(prob)
     nf = prob.nf
     prob.close()
     return dict(cells=cells, nf=nf, g=g, total_ms=total_ms, e2e_s=e2e_s, cd=cd, cl=cl, prof=prof, lps=lps,
-                clocks=clocks, state_bytes=state_bytes, bodies=1)
+                clocks=clocks, state_bytes=state_bytes, bodies=1, gamma=gamma)
 
 
 # The adjoint workload: a cylinder at Re = 100 on 256x256 cells x 4 levels
@@ -536,7 +537,8 @@ def batch_specs(G, seed=BATCH["seed"]):
 def batch_block(args, d):
     """Batch throughput: Σ_members nx·ny·mg per step over the device time of
     one batch step (graph launch, L2 flushed between steps), with the tuned
-    lane count and with one lane (the members one after another)."""
+    lane count and transform plan, and with one lane (the members one after
+    another, same plan)."""
     import ibpm_gpu as G
     specs = batch_specs(G)
     t0 = time.perf_counter()
@@ -546,6 +548,7 @@ def batch_block(args, d):
     K = BATCH["steps"]
     b.advance(3)
     tuned = b.lanes
+    plan = b.plan
     ms = b.bench_steps(K, flush_l2=True)
     t_tuned = float(np.sum(ms)) / 1e3
     b.set_lanes(1)
@@ -559,6 +562,7 @@ def batch_block(args, d):
     b.close()
     return {"workload": BATCH_WORKLOAD, "metric": METRIC, "value": cells * K / t_tuned, "unit": METRIC,
             "steps": K, "lanes": tuned, "ms_per_batch_step": 1e3 * t_tuned / K,
+            "transform_plan": {0: "latency (radix 4)", 1: "throughput (radix 8)"}.get(plan, plan),
             "one_lane": {"value": cells * K / t_seq, "ms_per_batch_step": 1e3 * t_seq / K},
             "speedup_over_one_lane": t_seq / t_tuned,
             "e2e": {"value": cells * K / e2e_s, "unit": METRIC, "h2d_bytes_per_step": 0,
@@ -700,6 +704,94 @@ def fp64_history(args, d, scale):
     return cd[:, 0], cl[:, 0]
 
 
+# Shedding: the same workload continued until the wake sheds periodically,
+# in chunks of 5000 steps (t = 10 each), at most 100 000 steps (t = 200).
+SHED = dict(chunk=5000, max_steps=100000, cycles=6, amp_tol=5e-3)
+
+
+def shedding_cycles(cl, dt, cycles):
+    """Period and amplitude of the last ``cycles`` full CL cycles: upward
+    crossings of the mean of the last third, located by linear interpolation;
+    the amplitude of a cycle is half its peak-to-peak.  None while fewer
+    cycles exist."""
+    x = cl - np.mean(cl[2 * len(cl) // 3:])
+    i = np.nonzero((x[:-1] < 0) & (x[1:] >= 0))[0]
+    if i.size < cycles + 1:
+        return None
+    tc = (i + x[i] / (x[i] - x[i + 1])) * dt
+    amps = np.array([0.5 * (np.max(cl[a:b + 1]) - np.min(cl[a:b + 1])) for a, b in zip(i[:-1], i[1:])])
+    per = np.diff(tc[-cycles - 1:])
+    return {"period": float(np.mean(per)), "period_spread": float(np.ptp(per) / np.mean(per)),
+            "cl_amplitude": float(np.mean(amps[-cycles:])), "amplitudes": amps,
+            "window": [float(tc[-cycles - 1]), float(tc[-1])], "crossings": i}
+
+
+def strouhal_block(args, d):
+    """Vortex shedding of the workload: the FP64 path is continued until the
+    CL amplitude of the last three cycles agrees to 0.5% (the limit cycle),
+    then the FP32-refined path runs the same steps from the same start.  St =
+    f D / U (D = 1, U = 1) from the mean period of the last cycles of each;
+    the mean CD is taken over the same cycles."""
+    import ibpm_gpu as G
+    g = G.make_grid(H, BOUNDARY, MG)
+
+    def run(precision, nmax, stop):
+        prob = G.IBProblem(g, [G.make_cylinder(0.5, g.h, 0.0, 0.0, n=NB)], DT, RE, freestream=(1.0, 0.0, 0.0),
+                           device=d.local, sync_fields=False, precision=precision, refine_sweeps=1)
+        st = G.IBState(prob)
+        st.Gamma[...] = vortex_gamma(g.nx, g.ny, g.mg, g.h, g.offx, g.offy)
+        G.push_state(st, prob, fields=("Gamma",))
+        G.vort2flux(st, prob)
+        cds, cls = [], []
+        n = 0
+        t0 = time.perf_counter()
+        while n < nmax:
+            m = min(SHED["chunk"], nmax - n)
+            cd, cl = G.advance(st, prob, n * DT, nsteps=m)
+            cds.append(cd[:, 0])
+            cls.append(cl[:, 0])
+            n += m
+            if stop and stop(np.concatenate(cls)):
+                break
+        wall = time.perf_counter() - t0
+        prob.close()
+        return np.concatenate(cds), np.concatenate(cls), wall
+
+    def settled(cl):
+        c = shedding_cycles(cl, DT, SHED["cycles"])
+        if c is None or c["cl_amplitude"] < 1e-2:
+            return False
+        a = c["amplitudes"][-3:]
+        return bool(np.ptp(a) / np.mean(a) < SHED["amp_tol"])
+
+    cd64, cl64, wall64 = run("fp64", SHED["max_steps"], settled)
+    n = cd64.size
+    cd32, cl32, wall32 = run("fp32_refined", n, None)
+    out = {"workload": WORKLOAD + ", continued to the periodic wake", "steps": n, "t_end": n * DT,
+           "limit_cycle": settled(cl64), "seconds": {"fp64": wall64, "fp32_refined": wall32},
+           "reference": "the FP64 GPU path (it matches the FP64 oracle to 1e-10 per step)"}
+    res = {}
+    for name, cd, cl in (("fp64", cd64, cl64), ("fp32_refined", cd32, cl32)):
+        c = shedding_cycles(cl, DT, SHED["cycles"])
+        if c is None:
+            res[name] = None
+            continue
+        a, b = c["crossings"][-SHED["cycles"] - 1], c["crossings"][-1]
+        res[name] = {"strouhal": 1.0 / c["period"], "period_spread": c["period_spread"],
+                     "cl_amplitude": c["cl_amplitude"], "cd_mean": float(np.mean(cd[a:b])),
+                     "window_t": c["window"]}
+    out.update(res)
+    if res.get("fp64") and res.get("fp32_refined"):
+        r, f = res["fp32_refined"], res["fp64"]
+        out["strouhal_rel_err"] = abs(r["strouhal"] - f["strouhal"]) / f["strouhal"]
+        out["cl_amplitude_rel_err"] = abs(r["cl_amplitude"] - f["cl_amplitude"]) / f["cl_amplitude"]
+        out["cd_mean_rel_err"] = abs(r["cd_mean"] - f["cd_mean"]) / f["cd_mean"]
+    out["note"] = ("St from the mean period of the last %d CL cycles (upward crossings of the mean, linear "
+                   "interpolation); the phase of the two runs drifts apart, the limit cycle does not"
+                   % SHED["cycles"])
+    return out
+
+
 def run_ours(args, d):
     K = args.steps
     sampler = ClockSampler(d.local)
@@ -744,6 +836,9 @@ def run_ours(args, d):
         "cl_err_after_10_steps_rel_to_cd_after_10": float(np.max(np.abs(cl32[10:] - cl64[10:])) /
                                                           np.max(np.abs(cd64[10:]))) if K > 10 else None,
         "max_abs_cl": float(np.max(np.abs(cl64))), "max_abs_cd": float(np.max(np.abs(cd64))),
+        "vorticity_rel_l2": float(np.linalg.norm(r32["gamma"] - r64["gamma"]) / np.linalg.norm(r64["gamma"])),
+        "vorticity_rel_l2_finest": float(np.linalg.norm(r32["gamma"][:, 0] - r64["gamma"][:, 0]) /
+                                         np.linalg.norm(r64["gamma"][:, 0])),
         "note": "the lift of this start is 1e-6..1e-4 (CD 1.4..1640): CL errors are stated absolute and on the "
                 "force scale (max |CD| over the same steps); the first 10 steps are the impulsive start",
     }
@@ -799,6 +894,11 @@ def run_ours(args, d):
             out["eldredge"] = eldredge_block(args, d)
         except Exception as e:  # reported, not fatal
             out["eldredge"] = {"workload": ELDREDGE_WORKLOAD, "error": str(e)[:300]}
+    if d.world == 1 and not args.no_strouhal:
+        try:
+            out["strouhal"] = strouhal_block(args, d)
+        except Exception as e:  # reported, not fatal
+            out["strouhal"] = {"error": str(e)[:300]}
     if not args.no_batch:
         try:
             out["batch"] = batch_block(args, d)
@@ -829,6 +929,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-eldredge", action="store_true")
+    ap.add_argument("--no-strouhal", action="store_true")
     args = ap.parse_args()
     d = Dist()
     try:

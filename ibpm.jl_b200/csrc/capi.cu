@@ -1181,6 +1181,36 @@ extern "C" int ibpm_get_binv(ibpm_handle* h, double* Binv) {
     return IBPM_OK;
 }
 
+// Transform plan of the handle's sine transforms: the latency plan (radix 4,
+// the default for single-slab launches) or the throughput plan (radix 8).
+// The step graphs are captured again on the next advance.
+static void set_plans(ibpm_handle* h, int single_slab, int multi_slab) {
+    for (DstPlan* p : {&h->px, &h->py}) {
+        p->plan1 = single_slab;
+        p->planN = multi_slab;
+    }
+    h->graphs_ready = false;
+    for (int p = 0; p < 2; ++p) if (h->gadj[p]) { cudaGraphExecDestroy(h->gadj[p]); h->gadj[p] = nullptr; }
+}
+
+extern "C" int ibpm_set_transform_plan(ibpm_handle* h, int32_t single_slab, int32_t multi_slab) {
+    if (!h) return IBPM_ERR_INVALID;
+    for (int v : {single_slab, multi_slab})
+        if (v != IBPM_PLAN_LATENCY && v != IBPM_PLAN_THROUGHPUT)
+            return fail(h, IBPM_ERR_INVALID, "transform plan must be IBPM_PLAN_LATENCY or IBPM_PLAN_THROUGHPUT");
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->st));
+    set_plans(h, single_slab, multi_slab);
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_get_transform_plan(const ibpm_handle* h, int32_t* single_slab, int32_t* multi_slab) {
+    if (!h || !single_slab || !multi_slab) return IBPM_ERR_INVALID;
+    *single_slab = h->px.plan1;
+    *multi_slab = h->px.planN;
+    return IBPM_OK;
+}
+
 extern "C" int ibpm_sync(ibpm_handle* h) {
     if (!h) return IBPM_ERR_INVALID;
     CK(cudaSetDevice(h->device));
@@ -1658,6 +1688,7 @@ struct ibpm_batch {
     std::vector<cudaStream_t> lane_st;
     std::vector<cudaEvent_t> ev;               // fork + one join event per lane
     int lanes = 0;
+    int plan = IBPM_PLAN_LATENCY;              // transform plan of the members' single-slab launches
     int cur = 0;                               // parity shared by the members
     int cold = kColdSteps;
     cudaGraphExec_t g[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cold][parity]
@@ -1768,19 +1799,24 @@ static void batch_destroy_impl(ibpm_batch* b) {
 }
 
 // Time `steps` batch steps for each candidate lane count (powers of two up to
-// the member count); keep the fastest.  The members are reset afterwards.
+// the member count) and each transform plan of the members' single-slab
+// launches (latency or throughput); keep the fastest pair.  The members are
+// reset afterwards.
 static int batch_tune(ibpm_batch* b, int steps) {
     const int n = (int)b->m.size();
-    std::vector<int> cand;
-    for (int l = 1; l < n; l *= 2) cand.push_back(l);
-    cand.push_back(n);
+    std::vector<std::pair<int, int>> cand;   // (plan, lanes)
+    for (int pl : {IBPM_PLAN_LATENCY, IBPM_PLAN_THROUGHPUT}) {
+        for (int l = 1; l < n; l *= 2) cand.push_back({pl, l});
+        cand.push_back({pl, n});
+    }
     double best = 1e300;
-    int best_l = n;
+    int best_l = n, best_p = IBPM_PLAN_LATENCY;
     cudaEvent_t e0, e1;
     BCK(cudaEventCreate(&e0));
     BCK(cudaEventCreate(&e1));
     int rc = IBPM_OK;
-    for (int l : cand) {
+    for (auto [pl, l] : cand) {
+        for (auto* h : b->m) set_plans(h, pl, h->px.planN);
         if ((rc = batch_graphs(b, l))) break;
         for (int s = 0; s < 2 && rc == IBPM_OK; ++s)
             if (batch_step(b) != cudaSuccess) rc = bfail(b, IBPM_ERR_CUDA, "batch tuning step failed");
@@ -1792,15 +1828,19 @@ static int batch_tune(ibpm_batch* b, int steps) {
         if (cudaEventSynchronize(e1) != cudaSuccess) { rc = bfail(b, IBPM_ERR_CUDA, "batch tuning sync failed"); break; }
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) { best = ms; best_l = l; }
+        if (ms < best) { best = ms; best_l = l; best_p = pl; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
-    for (auto* h : b->m)
+    for (auto* h : b->m) {
         if ((rc = reset_state(h))) return bfail(b, rc, h->err);
+        set_plans(h, best_p, h->px.planN);
+        if ((rc = ensure_graphs(h, b->hist_cap))) return bfail(b, rc, h->err);  // the members' own graphs
+    }
     b->cur = 0;
     b->cold = 2;
+    b->plan = best_p;
     return batch_graphs(b, best_l);
 }
 
@@ -1863,6 +1903,21 @@ extern "C" ibpm_handle* ibpm_batch_member(ibpm_batch* b, int32_t i) {
 }
 
 extern "C" int ibpm_batch_lanes(const ibpm_batch* b) { return b ? b->lanes : IBPM_ERR_INVALID; }
+
+extern "C" int ibpm_batch_plan(const ibpm_batch* b) { return b ? b->plan : IBPM_ERR_INVALID; }
+
+extern "C" int ibpm_batch_set_plan(ibpm_batch* b, int32_t plan) {
+    if (!b || (plan != IBPM_PLAN_LATENCY && plan != IBPM_PLAN_THROUGHPUT)) return IBPM_ERR_INVALID;
+    BCK(cudaSetDevice(b->device));
+    BCK(cudaStreamSynchronize(b->st));
+    for (auto* h : b->m) {
+        set_plans(h, plan, h->px.planN);
+        const int rc = ensure_graphs(h, b->hist_cap);   // the members' own graphs
+        if (rc) return bfail(b, rc, h->err);
+    }
+    b->plan = plan;
+    return batch_graphs(b, b->lanes);
+}
 
 extern "C" int ibpm_batch_set_lanes(ibpm_batch* b, int32_t lanes) {
     if (!b || lanes < 1 || lanes > (int)b->m.size()) return IBPM_ERR_INVALID;

@@ -87,13 +87,13 @@ struct StageDesc {
     int ns[8], r[8], off[8];
 };
 
-static StageDesc stage_desc(int N) {
+static StageDesc stage_desc(int N, int PL) {
     StageDesc d{};
-    const int S = dstk::ct_nstages(N);
+    const int S = dstk::ct_nstages(N, PL);
     for (int s = 0; s < S; ++s) {
-        d.ns[d.n] = dstk::ct_stage_ns(N, s);
-        d.r[d.n] = dstk::ct_radix(N, s);
-        d.off[d.n] = dstk::ct_tw_off(N, s);
+        d.ns[d.n] = dstk::ct_stage_ns(N, s, PL);
+        d.r[d.n] = dstk::ct_radix(N, s, PL);
+        d.off[d.n] = dstk::ct_tw_off(N, s, PL);
         if (d.ns[d.n] > 1) ++d.n;
     }
     return d;
@@ -104,23 +104,10 @@ static StageDesc stage_desc(int N) {
 //         exp(+2πi k r/(Ns R)) (complex) from 2N on (≤ N of them);
 //   FP32 (from double 4N on, as floats): 4 sin²(π(t+1)/(2N)) at [0, N),
 //         sin(πt/N) at [N, 2N), the twiddles (complex) from 2N on;
-// each FP32 entry is the FP64 value rounded once.
-__global__ void dst_tables_kernel(int N, double* base, StageDesc d, int ntw) {
-    double* c = base;
-    double* s = base + N;
-    double2* W = reinterpret_cast<double2*>(base + 2 * N);
-    float* a32 = reinterpret_cast<float*>(base + 4 * N);
-    float* s32 = a32 + N;
-    float2* W32 = reinterpret_cast<float2*>(a32 + 2 * N);
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
-        s[t] = sinpi((double)t / (double)N);
-        s32[t] = (float)s[t];
-        // evaluated as the reference forms the Laplacian eigenvalues:
-        // cos.(π*(1:(n-1))/n) (laplacian.jl:173)
-        c[t] = (t < N - 1) ? cos(M_PI * (double)(t + 1) / (double)N) : 0.0;
-        const double h = sinpi((double)(t + 1) / (2.0 * (double)N));
-        a32[t] = (t < N - 1) ? (float)(4.0 * h * h) : 0.0f;
-    }
+// each FP32 entry is the FP64 value rounded once.  The throughput plan's
+// twiddles (when built) follow from double 6N on: FP64 (≤ N complex), then
+// FP32 (≤ N complex).
+__global__ void dst_twiddles_kernel(StageDesc d, int ntw, double2* W, float2* W32) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntw; i += gridDim.x * blockDim.x) {
         int st = 0;
         while (st + 1 < d.n && i >= d.off[st + 1]) ++st;
@@ -133,11 +120,35 @@ __global__ void dst_tables_kernel(int N, double* base, StageDesc d, int ntw) {
     }
 }
 
-cudaError_t dst_tables_build(int N, double* base, cudaStream_t st) {
-    const StageDesc d = stage_desc(N);
-    const int ntw = dstk::ct_tw_count(N);
-    dst_tables_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, base, d, ntw);
+__global__ void dst_tables_kernel(int N, double* base) {
+    double* c = base;
+    double* s = base + N;
+    float* a32 = reinterpret_cast<float*>(base + 4 * N);
+    float* s32 = a32 + N;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
+        s[t] = sinpi((double)t / (double)N);
+        s32[t] = (float)s[t];
+        // evaluated as the reference forms the Laplacian eigenvalues:
+        // cos.(π*(1:(n-1))/n) (laplacian.jl:173)
+        c[t] = (t < N - 1) ? cos(M_PI * (double)(t + 1) / (double)N) : 0.0;
+        const double h = sinpi((double)(t + 1) / (2.0 * (double)N));
+        a32[t] = (t < N - 1) ? (float)(4.0 * h * h) : 0.0f;
+    }
+}
+
+static cudaError_t twiddles_build(int N, int PL, double2* W, float2* W32, cudaStream_t st) {
+    const int ntw = dstk::ct_tw_count(N, PL);
+    if (ntw > N) return cudaErrorInvalidValue;  // the block holds at most N per plan
+    if (ntw > 0) dst_twiddles_kernel<<<(ntw + 255) / 256, 256, 0, st>>>(stage_desc(N, PL), ntw, W, W32);
     return cudaGetLastError();
+}
+
+cudaError_t dst_tables_build(int N, double* base, cudaStream_t st) {
+    dst_tables_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, base);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return twiddles_build(N, 0, reinterpret_cast<double2*>(base + 2 * N),
+                          reinterpret_cast<float2*>(reinterpret_cast<float*>(base + 4 * N) + 2 * N), st);
 }
 
 DstPlan dst_plan_at(double* base, int N) {
@@ -149,6 +160,9 @@ DstPlan dst_plan_at(double* base, int N) {
     p.a32 = reinterpret_cast<float*>(base + 4 * N);
     p.s32 = p.a32 + N;
     p.W32 = reinterpret_cast<float2*>(p.a32 + 2 * N);
+    p.Wt = nullptr;
+    p.Wt32 = nullptr;
+    p.plan1 = p.planN = DST_PLAN_LATENCY;
     return p;
 }
 
@@ -157,9 +171,12 @@ int dst_plan_create(DstPlan* p, int N, cudaStream_t st) {
     p->W = nullptr; p->s = nullptr; p->c = nullptr;
     if (!dst_supported(N)) return -1;
     double* base = nullptr;
-    if (cudaMalloc(&base, sizeof(double) * dst_table_doubles(N)) != cudaSuccess) return -2;
+    if (cudaMalloc(&base, sizeof(double) * dst_table_doubles_all(N)) != cudaSuccess) return -2;
     *p = dst_plan_at(base, N);
     if (dst_tables_build(N, base, st) != cudaSuccess) return -2;
+    p->Wt = reinterpret_cast<double2*>(base + 6 * N);
+    p->Wt32 = reinterpret_cast<float2*>(base + 8 * N);
+    if (twiddles_build(N, dstk::ct_plan(N, 1), p->Wt, p->Wt32, st) != cudaSuccess) return -2;
     if (dst_init_attributes(N) != cudaSuccess) return -2;
     return 0;
 }
@@ -168,6 +185,7 @@ void dst_plan_destroy(DstPlan* p) {
     if (p->c) cudaFree(p->c);  // the block starts at c
     p->W = nullptr; p->s = nullptr; p->c = nullptr;
     p->W32 = nullptr; p->s32 = nullptr; p->a32 = nullptr;
+    p->Wt = nullptr; p->Wt32 = nullptr;
 }
 
 // Opt the kernels of length N into large dynamic shared memory (before any

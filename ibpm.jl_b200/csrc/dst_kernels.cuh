@@ -21,7 +21,10 @@
 // little work to fill the GPU, and the time of a launch is the length of each
 // thread's dependent chain, which the wider group halves against radix 8.
 // From N = 1024 on (enough line pairs to fill the GPU) the plan is radices
-// (8, 5, 4, 3, 2) with TP = N/8.  N is a template parameter, so every stride,
+// (8, 5, 4, 3, 2) with TP = N/8.  That throughput plan (PL = 1) is also
+// instantiated below N = 1024: it spends about two thirds of the latency plan's
+// instructions per line pair, which pays when many launches share the GPU
+// (batched simulations, multi-slab launches).  N is a template parameter, so every stride,
 // radix and loop bound is a compile-time constant.  Shared-memory indices are padded by one element
 // every eight (pad(i) = i + i/8) so the stride-8 writes of the first stage are
 // free of bank conflicts.
@@ -34,10 +37,14 @@
 namespace ibpm {
 namespace dstk {
 
-__host__ __device__ constexpr bool ct_fine(int N) { return N < 1024; }
-__host__ __device__ constexpr int ct_radix(int N, int s) {
+// Transform plans: 0 = latency (radix 4 below N = 1024), 1 = throughput
+// (radix 8).  From N = 1024 on both are the radix-8 plan.
+__host__ __device__ constexpr bool ct_fine(int N, int PL = 0) { return N < 1024 && PL == 0; }
+__host__ __device__ constexpr int ct_plan(int N, int PL) { return N < 1024 ? PL : 0; }
+__host__ __device__ constexpr int ct_radix(int N, int s, int PL = 0) {
     int n = N, idx = 0;
-    const int rs[5] = {ct_fine(N) ? 4 : 8, 5, ct_fine(N) ? 3 : 4, ct_fine(N) ? 2 : 3, ct_fine(N) ? 8 : 2};
+    const bool f = ct_fine(N, PL);
+    const int rs[5] = {f ? 4 : 8, 5, f ? 3 : 4, f ? 2 : 3, f ? 8 : 2};
     for (int i = 0; i < 5; ++i) {
         while (n % rs[i] == 0) {
             if (idx == s) return rs[i];
@@ -47,15 +54,16 @@ __host__ __device__ constexpr int ct_radix(int N, int s) {
     }
     return 1;
 }
-__host__ __device__ constexpr int ct_nstages(int N) {
+__host__ __device__ constexpr int ct_nstages(int N, int PL = 0) {
     int n = N, s = 0;
-    const int rs[5] = {ct_fine(N) ? 4 : 8, 5, ct_fine(N) ? 3 : 4, ct_fine(N) ? 2 : 3, ct_fine(N) ? 8 : 2};
+    const bool f = ct_fine(N, PL);
+    const int rs[5] = {f ? 4 : 8, 5, f ? 3 : 4, f ? 2 : 3, f ? 8 : 2};
     for (int i = 0; i < 5; ++i)
         while (n % rs[i] == 0) { n /= rs[i]; ++s; }
     return n == 1 ? s : -1;
 }
-__host__ __device__ constexpr int ct_tp(int N) {
-    int t = (((ct_fine(N) ? N / 4 : N / 8) + 31) / 32) * 32;
+__host__ __device__ constexpr int ct_tp(int N, int PL = 0) {
+    int t = (((ct_fine(N, PL) ? N / 4 : N / 8) + 31) / 32) * 32;
     return t < 32 ? 32 : t;
 }
 __host__ __device__ constexpr int ct_pad(int i) { return i + (i >> 3); }
@@ -64,22 +72,24 @@ __host__ __device__ constexpr int ct_buf(int N) { return ct_pad(N) + 8; }  // + 
 // Twiddles of stage S (sub-transform length Ns before it, radix R) are stored
 // contiguously as T[(r-1)·Ns + k] = exp(+2πi k r/(Ns R)), r = 1…R-1, k < Ns, so
 // the threads of a stage (consecutive k) read consecutive entries.
-__host__ __device__ constexpr int ct_stage_ns(int N, int S) {
+__host__ __device__ constexpr int ct_stage_ns(int N, int S, int PL = 0) {
     int ns = 1;
-    for (int s = 0; s < S; ++s) ns *= ct_radix(N, s);
+    for (int s = 0; s < S; ++s) ns *= ct_radix(N, s, PL);
     return ns;
 }
-__host__ __device__ constexpr int ct_tw_off(int N, int S) {
+__host__ __device__ constexpr int ct_tw_off(int N, int S, int PL = 0) {
     int off = 0;
     for (int s = 0; s < S; ++s) {
-        const int ns = ct_stage_ns(N, s);
-        if (ns > 1) off += (ct_radix(N, s) - 1) * ns;
+        const int ns = ct_stage_ns(N, s, PL);
+        if (ns > 1) off += (ct_radix(N, s, PL) - 1) * ns;
     }
     return off;
 }
-__host__ __device__ constexpr int ct_tw_count(int N) { return ct_tw_off(N, ct_nstages(N)); }
+__host__ __device__ constexpr int ct_tw_count(int N, int PL = 0) { return ct_tw_off(N, ct_nstages(N, PL), PL); }
 // Groups (line pairs) per CTA of the x-pass: up to 128 threads, or one group.
-__host__ __device__ constexpr int ct_groups(int N) { return ct_tp(N) >= 128 ? 1 : 128 / ct_tp(N); }
+__host__ __device__ constexpr int ct_groups(int N, int PL = 0) {
+    return ct_tp(N, PL) >= 128 ? 1 : 128 / ct_tp(N, PL);
+}
 
 // Complex arithmetic for both precisions (V = double2 or float2).
 template <class T> struct cplx_of;
@@ -236,12 +246,12 @@ __device__ __forceinline__ void fft_stage(cplx_t<T>* buf, const cplx_t<T>* W, in
     gsync<TP, G>(gid);
 }
 
-template <int N, int TP, int G, int S, int Ns, class T>
+template <int N, int TP, int G, int S, int Ns, class T, int PL>
 __device__ __forceinline__ void fft_stages(cplx_t<T>* buf, const cplx_t<T>* W, int tid, int gid) {
-    if constexpr (S < ct_nstages(N)) {
-        constexpr int R = ct_radix(N, S);
-        fft_stage<N, TP, G, R, Ns, ct_tw_off(N, S), T>(buf, W, tid, gid);
-        fft_stages<N, TP, G, S + 1, Ns * R, T>(buf, W, tid, gid);
+    if constexpr (S < ct_nstages(N, PL)) {
+        constexpr int R = ct_radix(N, S, PL);
+        fft_stage<N, TP, G, R, Ns, ct_tw_off(N, S, PL), T>(buf, W, tid, gid);
+        fft_stages<N, TP, G, S + 1, Ns * R, T, PL>(buf, W, tid, gid);
     }
 }
 
@@ -349,13 +359,13 @@ __device__ __forceinline__ void dst_post(cplx_t<T>* buf, int tid, int gid, cplx_
     }
 }
 
-// One DST-I of a line pair: load → pre → FFT → post → emit.
-template <int N, int TP, int G, class T, class Load, class Emit>
+// One DST-I of a line pair: load → pre → FFT (plan PL) → post → emit.
+template <int N, int TP, int G, class T, int PL = 0, class Load, class Emit>
 __device__ __forceinline__ void dst_pair(cplx_t<T>* buf, const cplx_t<T>* W, const T* s, int tid, int gid,
                                          Load load, Emit emit) {
     dst_pre<N, TP, T>(buf, s, tid, load);
     gsync<TP, G>(gid);
-    fft_stages<N, TP, G, 0, 1, T>(buf, W, tid, gid);
+    fft_stages<N, TP, G, 0, 1, T, PL>(buf, W, tid, gid);
     dst_post<N, TP, G, T>(buf, tid, gid, buf + ct_pad(N), emit);
 }
 
@@ -366,20 +376,26 @@ template <class T> struct Tabs {
     const T* s;
     const T* c;
 };
-template <class T> __host__ __device__ Tabs<T> tabs_of(const DstPlan& p);
-template <> __host__ __device__ inline Tabs<double> tabs_of<double>(const DstPlan& p) { return {p.W, p.s, p.c}; }
-template <> __host__ __device__ inline Tabs<float> tabs_of<float>(const DstPlan& p) { return {p.W32, p.s32, p.a32}; }
+// The stage twiddles are those of plan PL (W / W32: latency plan, Wt / Wt32:
+// throughput plan).
+template <class T> __host__ __device__ Tabs<T> tabs_of(const DstPlan& p, int PL = 0);
+template <> __host__ __device__ inline Tabs<double> tabs_of<double>(const DstPlan& p, int PL) {
+    return {PL ? p.Wt : p.W, p.s, p.c};
+}
+template <> __host__ __device__ inline Tabs<float> tabs_of<float>(const DstPlan& p, int PL) {
+    return {PL ? p.Wt32 : p.W32, p.s32, p.a32};
+}
 
 // Copy the transform tables into shared memory: stage twiddles (complex),
 // then sin(πm/N) for m ≤ N/2.
-template <int N, class T>
+template <int N, class T, int PL = 0>
 __device__ __forceinline__ void stage_tables(cplx_t<T>* tw, T* sn, const Tabs<T>& p) {
-    for (int i = threadIdx.x; i < ct_tw_count(N); i += blockDim.x) cp_async<sizeof(cplx_t<T>)>(tw + i, p.W + i);
+    for (int i = threadIdx.x; i < ct_tw_count(N, PL); i += blockDim.x) cp_async<sizeof(cplx_t<T>)>(tw + i, p.W + i);
     for (int i = threadIdx.x; i <= N / 2; i += blockDim.x) cp_async<sizeof(T)>(sn + i, p.s + i);
 }
-template <int N, class T>
+template <int N, class T, int PL = 0>
 __host__ __device__ constexpr size_t tables_bytes() {
-    return (size_t)ct_tw_count(N) * sizeof(cplx_t<T>) + (size_t)((N / 2 + 4) & ~3) * sizeof(T);
+    return (size_t)ct_tw_count(N, PL) * sizeof(cplx_t<T>) + (size_t)((N / 2 + 4) & ~3) * sizeof(T);
 }
 
 // ---------------------------------------------------------------------------
@@ -391,27 +407,27 @@ template <int LOAD>
 __host__ __device__ constexpr bool x_res() { return LOAD == XLOAD_RES_LAP || LOAD == XLOAD_RES_A; }
 // Shared memory of the x-pass: tables, one FFT buffer per group, and for the
 // residual loads six staged rows of N doubles per group (16-byte aligned).
-template <int N, int LOAD>
+template <int N, int LOAD, int PL>
 __host__ __device__ constexpr size_t x_res_off() {
-    return ((tables_bytes<N, x_real_t<LOAD>>() + (size_t)ct_groups(N) * ct_buf(N) * sizeof(cplx_t<x_real_t<LOAD>>) +
-             15) / 16) * 16;
+    return ((tables_bytes<N, x_real_t<LOAD>, PL>() +
+             (size_t)ct_groups(N, PL) * ct_buf(N) * sizeof(cplx_t<x_real_t<LOAD>>) + 15) / 16) * 16;
 }
-template <int N, int LOAD>
+template <int N, int LOAD, int PL>
 __host__ __device__ constexpr size_t x_smem_bytes() {
-    return x_res_off<N, LOAD>() + (x_res<LOAD>() ? (size_t)ct_groups(N) * 6 * N * sizeof(double) : 0);
+    return x_res_off<N, LOAD, PL>() + (x_res<LOAD>() ? (size_t)ct_groups(N, PL) * 6 * N * sizeof(double) : 0);
 }
 
-template <int N, int LOAD, int EMIT>
-__global__ void __launch_bounds__(ct_groups(N) * ct_tp(N)) dst_x_kernel(XPassArgs a, Geom g, DstPlan p) {
+template <int N, int LOAD, int EMIT, int PL>
+__global__ void __launch_bounds__(ct_groups(N, PL) * ct_tp(N, PL)) dst_x_kernel(XPassArgs a, Geom g, DstPlan p) {
     using T = x_real_t<LOAD>;
     using V = cplx_t<T>;
-    constexpr int TP = ct_tp(N);
-    constexpr int G = ct_groups(N);
+    constexpr int TP = ct_tp(N, PL);
+    constexpr int G = ct_groups(N, PL);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* tw = reinterpret_cast<V*>(smem_raw);
-    T* sn = reinterpret_cast<T*>(tw + ct_tw_count(N));
-    V* bufs = reinterpret_cast<V*>(smem_raw + tables_bytes<N, T>());
-    stage_tables<N, T>(tw, sn, tabs_of<T>(p));  // constant tables: before the dependency wait
+    T* sn = reinterpret_cast<T*>(tw + ct_tw_count(N, PL));
+    V* bufs = reinterpret_cast<V*>(smem_raw + tables_bytes<N, T, PL>());
+    stage_tables<N, T, PL>(tw, sn, tabs_of<T>(p, PL));  // constant tables: before the dependency wait
     cp_async_wait();
     __syncthreads();
     pdl_wait();
@@ -442,7 +458,7 @@ __global__ void __launch_bounds__(ct_groups(N) * ct_tp(N)) dst_x_kernel(XPassArg
     };
     // Residual loads: the group stages x̃ rows la-1 … la+2 (zero outside the
     // slab) and b rows la, la+1 in shared memory, rows of stride N doubles.
-    double* rs = RES ? reinterpret_cast<double*>(smem_raw + x_res_off<N, LOAD>()) + (size_t)gid * 6 * N : nullptr;
+    double* rs = RES ? reinterpret_cast<double*>(smem_raw + x_res_off<N, LOAD, PL>()) + (size_t)gid * 6 * N : nullptr;
     if constexpr (RES) {
         const double* bin = static_cast<const double*>(a.in) + a.in_map.off(y);
 #pragma unroll 1
@@ -532,7 +548,7 @@ __global__ void __launch_bounds__(ct_groups(N) * ct_tp(N)) dst_x_kernel(XPassArg
             }
         }
     }
-    dst_pair<N, TP, G, T>(buf, tw, sn, tid, gid, load, [&](int o, V v) { buf[ct_pad(o)] = v; });
+    dst_pair<N, TP, G, T, PL>(buf, tw, sn, tid, gid, load, [&](int o, V v) { buf[ct_pad(o)] = v; });
     gsync<TP, G>(gid);
 #pragma unroll
     for (int k = 0; k < EO; ++k) {
@@ -588,38 +604,39 @@ __global__ void __launch_bounds__(ct_groups(N) * ct_tp(N)) dst_x_kernel(XPassArg
 // (more CTAs for a single slab: the refined step's y-passes are single-slab
 // and latency-bound); FP64 passes keep at least two with the fine plan, so a
 // CTA reads tiles of four 8-byte columns.
-template <int N, class T>
+template <int N, class T, int PL>
 __host__ __device__ constexpr int y_groups() {
-    return (std::is_same<T, double>::value && ct_fine(N) && ct_groups(N) < 2) ? 2 : ct_groups(N);
+    return (std::is_same<T, double>::value && ct_fine(N, PL) && ct_groups(N, PL) < 2) ? 2 : ct_groups(N, PL);
 }
-template <int N, class T>
-__host__ __device__ constexpr int y_threads() { return y_groups<N, T>() * ct_tp(N); }
-template <int N, class T>
-__host__ __device__ constexpr int y_tile_w() { return 2 * y_groups<N, T>(); }
+template <int N, class T, int PL>
+__host__ __device__ constexpr int y_threads() { return y_groups<N, T, PL>() * ct_tp(N, PL); }
+template <int N, class T, int PL>
+__host__ __device__ constexpr int y_tile_w() { return 2 * y_groups<N, T, PL>(); }
 __host__ __device__ constexpr int round4(int n) { return ((n + 3) / 4) * 4; }
-template <int N, class T>
+template <int N, class T, int PL>
 __host__ __device__ constexpr size_t y_smem_bytes(int n2) {
-    return tables_bytes<N, T>() + (size_t)round4(n2) * sizeof(T) +  // spectral table of y
-           (size_t)round4(n2 * (y_tile_w<N, T>() + 1)) * sizeof(T) +
-           (size_t)y_groups<N, T>() * ct_buf(N) * sizeof(cplx_t<T>);
+    return tables_bytes<N, T, PL>() + (size_t)round4(n2) * sizeof(T) +  // spectral table of y
+           (size_t)round4(n2 * (y_tile_w<N, T, PL>() + 1)) * sizeof(T) +
+           (size_t)y_groups<N, T, PL>() * ct_buf(N) * sizeof(cplx_t<T>);
 }
 
-template <int N, class T>
+template <int N, class T, int PL>
 // (3 resident 256-thread CTAs per SM keep the FP64 pass at 80 registers without
 // spills: the five-slab trial solve's y-pass then needs 1.4 waves instead of 2.2)
-__global__ void __launch_bounds__(y_threads<N, T>(), (!ct_fine(N) || N > 512) ? 1 : (y_threads<N, T>() <= 128 ? 5 : 3))
+__global__ void __launch_bounds__(y_threads<N, T, PL>(),
+                                  (!ct_fine(N, PL) || N > 512) ? 1 : (y_threads<N, T, PL>() <= 128 ? 5 : 3))
     dst_y_kernel(T* data, SlabMap map, Geom g, DstPlan p, const T* __restrict__ cx, SpecParams sp) {
     using V = cplx_t<T>;
-    constexpr int TP = ct_tp(N);
-    constexpr int G = y_groups<N, T>();
-    constexpr int TW = y_tile_w<N, T>();
+    constexpr int TP = ct_tp(N, PL);
+    constexpr int G = y_groups<N, T, PL>();
+    constexpr int TW = y_tile_w<N, T, PL>();
     constexpr int TWp = TW + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P = g.P, n1 = g.n1, n2 = g.n2;
-    const Tabs<T> tb = tabs_of<T>(p);
+    const Tabs<T> tb = tabs_of<T>(p, PL);
     V* tw = reinterpret_cast<V*>(smem_raw);
-    T* sn = reinterpret_cast<T*>(tw + ct_tw_count(N));
-    T* cyv = reinterpret_cast<T*>(smem_raw + tables_bytes<N, T>());
+    T* sn = reinterpret_cast<T*>(tw + ct_tw_count(N, PL));
+    T* cyv = reinterpret_cast<T*>(smem_raw + tables_bytes<N, T, PL>());
     T* tile = cyv + round4(n2);
     const int tile_d = round4(n2 * TWp);
     const int gid = threadIdx.x / TP, tid = threadIdx.x % TP;
@@ -628,7 +645,7 @@ __global__ void __launch_bounds__(y_threads<N, T>(), (!ct_fine(N) || N > 512) ? 
     T* base = data + map.off(blockIdx.y);
     const int lev = map.level(blockIdx.y);
 
-    stage_tables<N, T>(tw, sn, tb);  // constant tables: before the dependency wait
+    stage_tables<N, T, PL>(tw, sn, tb);  // constant tables: before the dependency wait
     for (int j = threadIdx.x; j < n2; j += blockDim.x) cp_async<sizeof(T)>(cyv + j, tb.c + j);
     pdl_wait();
     pdl_trigger();
@@ -689,11 +706,11 @@ __global__ void __launch_bounds__(y_threads<N, T>(), (!ct_fine(N) || N > 512) ? 
                 }
             }
         };
-        dst_pair<N, TP, G, T>(buf, tw, sn, tid, gid, load, emit);
+        dst_pair<N, TP, G, T, PL>(buf, tw, sn, tid, gid, load, emit);
         gsync<TP, G>(gid);
         divide();
         gsync<TP, G>(gid);
-        dst_pair<N, TP, G, T>(buf, tw, sn, tid, gid, load, emit);
+        dst_pair<N, TP, G, T, PL>(buf, tw, sn, tid, gid, load, emit);
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
@@ -706,16 +723,23 @@ __global__ void __launch_bounds__(y_threads<N, T>(), (!ct_fine(N) || N > 512) ? 
 // ---------------------------------------------------------------------------
 // Launchers for one compile-time length.
 // ---------------------------------------------------------------------------
-template <int N, int LOAD, int EMIT>
+template <int N, int LOAD, int EMIT, int PL>
 cudaError_t launch_x_n(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {
-    constexpr int TP = ct_tp(N);
-    constexpr int G = ct_groups(N);
+    constexpr int TP = ct_tp(N, PL);
+    constexpr int G = ct_groups(N, PL);
     const int lines = a.line1 - a.line0;
     if (lines <= 0 || a.nslabs <= 0) return cudaSuccess;
     const int pairs = (lines + 1) / 2;
     dim3 grid((pairs + G - 1) / G, a.nslabs);
-    const size_t smem = x_smem_bytes<N, LOAD>();
-    return launch_k(dst_x_kernel<N, LOAD, EMIT>, grid, dim3(G * TP), smem, st, a, g, px);
+    const size_t smem = x_smem_bytes<N, LOAD, PL>();
+    return launch_k(dst_x_kernel<N, LOAD, EMIT, PL>, grid, dim3(G * TP), smem, st, a, g, px);
+}
+
+// The plan of a launch: the plan's single-slab or multi-slab choice; the
+// throughput plan needs its twiddle table.
+inline int launch_plan(int N, const DstPlan& p, int nslabs) {
+    const int pl = ct_plan(N, nslabs > 1 ? p.planN : p.plan1);
+    return (pl == 1 && p.Wt) ? 1 : 0;
 }
 
 // The (load, emit) pairs the library uses: FP64 solves, and the three passes
@@ -728,30 +752,36 @@ cudaError_t launch_x_n(const Geom& g, const DstPlan& px, const XPassArgs& a, cud
 
 template <int N>
 cudaError_t launch_x_t(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {
-#define IBPM_X_DISPATCH(L, E) \
-    if (a.load == L && a.emit == E) return launch_x_n<N, L, E>(g, px, a, st);
+    const bool wide = launch_plan(N, px, a.nslabs) == 1;
+#define IBPM_X_DISPATCH(L, E)                                                               \
+    if (a.load == L && a.emit == E)                                                         \
+        return wide ? launch_x_n<N, L, E, ct_plan(N, 1)>(g, px, a, st) : launch_x_n<N, L, E, 0>(g, px, a, st);
     IBPM_X_COMBOS(IBPM_X_DISPATCH)
 #undef IBPM_X_DISPATCH
     return cudaErrorInvalidValue;
 }
 
-template <int N, class T>
+template <int N, class T, int PL>
 cudaError_t launch_y_n(const Geom& g, const DstPlan& py, const DstPlan& px, void* data, SlabMap map, int nslabs,
                        const SpecParams& sp, cudaStream_t st) {
-    constexpr int TW = y_tile_w<N, T>();
-    const size_t smem = y_smem_bytes<N, T>(g.n2);
+    constexpr int TW = y_tile_w<N, T, PL>();
+    const size_t smem = y_smem_bytes<N, T, PL>(g.n2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     dim3 grid((g.n1 + TW - 1) / TW, nslabs);
-    const int threads = y_threads<N, T>();
-    return launch_k(dst_y_kernel<N, T>, grid, dim3(threads), smem, st, static_cast<T*>(data), map, g, py,
+    const int threads = y_threads<N, T, PL>();
+    return launch_k(dst_y_kernel<N, T, PL>, grid, dim3(threads), smem, st, static_cast<T*>(data), map, g, py,
                     static_cast<const T*>(tabs_of<T>(px).c), sp);
 }
 
 template <int N>
 cudaError_t launch_y_t(const Geom& g, const DstPlan& py, const DstPlan& px, void* data, SlabMap map, int nslabs,
                        const SpecParams& sp, cudaStream_t st) {
-    return sp.f32 ? launch_y_n<N, float>(g, py, px, data, map, nslabs, sp, st)
-                  : launch_y_n<N, double>(g, py, px, data, map, nslabs, sp, st);
+    constexpr int W = ct_plan(N, 1);
+    if (launch_plan(N, py, nslabs) == 1)
+        return sp.f32 ? launch_y_n<N, float, W>(g, py, px, data, map, nslabs, sp, st)
+                      : launch_y_n<N, double, W>(g, py, px, data, map, nslabs, sp, st);
+    return sp.f32 ? launch_y_n<N, float, 0>(g, py, px, data, map, nslabs, sp, st)
+                  : launch_y_n<N, double, 0>(g, py, px, data, map, nslabs, sp, st);
 }
 
 template <class K>
@@ -762,15 +792,22 @@ cudaError_t smem_attrs(K kernel) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
-template <int N>
-cudaError_t attr_t() {
+template <int N, int PL>
+cudaError_t attr_plan() {
     cudaError_t e;
 #define IBPM_X_ATTR(L, E) \
-    if ((e = smem_attrs(dst_x_kernel<N, L, E>))) return e;
+    if ((e = smem_attrs(dst_x_kernel<N, L, E, PL>))) return e;
     IBPM_X_COMBOS(IBPM_X_ATTR)
 #undef IBPM_X_ATTR
-    if ((e = smem_attrs(dst_y_kernel<N, double>))) return e;
-    return smem_attrs(dst_y_kernel<N, float>);
+    if ((e = smem_attrs(dst_y_kernel<N, double, PL>))) return e;
+    return smem_attrs(dst_y_kernel<N, float, PL>);
+}
+
+template <int N>
+cudaError_t attr_t() {
+    cudaError_t e = attr_plan<N, 0>();
+    if (e != cudaSuccess || ct_plan(N, 1) == 0) return e;
+    return attr_plan<N, ct_plan(N, 1)>();
 }
 
 }  // namespace dstk

@@ -169,9 +169,18 @@ struct DstPlan {
     float2* W32;
     float* s32;
     float* a32;          // 2 (1 − cos(π (k+1)/N)) = 4 sin²(π (k+1)/(2N)), free of cancellation
+    // stage twiddles of the throughput plan (radix 8), FP64 and FP32; null
+    // when the block holds only the latency plan's tables
+    double2* Wt;
+    float2* Wt32;
+    // plan of single-slab and of multi-slab launches (DST_PLAN_*)
+    int plan1, planN;
 };
-// Doubles in the table block of one length (FP64 tables, then FP32 tables).
+enum DstPlanKind { DST_PLAN_LATENCY = 0, DST_PLAN_THROUGHPUT = 1 };
+// Doubles in the table block of one length (FP64 tables, then FP32 tables),
+// and with the throughput plan's twiddles after them.
 inline long long dst_table_doubles(int N) { return 6LL * N; }
+inline long long dst_table_doubles_all(int N) { return 9LL * N; }
 
 bool dst_supported(int N);
 int dst_plan_create(DstPlan* p, int N, cudaStream_t st);  // 0 on success

@@ -13,7 +13,7 @@ module IBPMGPU
 using ..ibpm: ibpm, IBState, AbstractIBProblem, MultiGrid, RigidBody, Static, MovingGrid, MotionFunction,
               MotionType, get_body_info
 
-export IBProblemGPU, sync!, push!, adjoint_run, set_vorticity!
+export IBProblemGPU, sync!, push!, adjoint_run, set_vorticity!, set_transform_plan!
 
 const LIB = get(ENV, "IBPM_GPU_LIB", joinpath(@__DIR__, "..", "lib", "libibpm_gpu.so"))
 
@@ -178,6 +178,22 @@ function set_vorticity!(prob::IBProblemGPU, ω::AbstractMatrix{Float64})
                prob.handle, Γ, zeros(g.nq, g.mg), C_NULL, z, z, z, C_NULL)
     check(rc, prob.handle)
     check(ccall((:ibpm_vort2flux, LIB), Cint, (Ptr{Cvoid},), prob.handle), prob.handle)
+end
+
+"""
+    set_transform_plan!(prob; single=:latency, multi=:latency)
+
+Plans of the device sine transforms for launches over one level (`single`)
+and over several (`multi`): `:latency` (radix 4, N/4 threads per line pair,
+the shortest chain per launch) or `:throughput` (radix 8, N/8 threads, fewer
+instructions).  No counterpart in the reference, whose FFTW plans are fixed
+(src/fluid-operators/laplacian.jl:30-39).
+"""
+function set_transform_plan!(prob::IBProblemGPU; single::Symbol=:latency, multi::Symbol=:latency)
+    code(s) = s === :latency ? Int32(0) : s === :throughput ? Int32(1) :
+              throw(ArgumentError("plan must be :latency or :throughput"))
+    check(ccall((:ibpm_set_transform_plan, LIB), Cint, (Ptr{Cvoid}, Int32, Int32), prob.handle,
+                code(single), code(multi)), prob.handle)
 end
 
 """

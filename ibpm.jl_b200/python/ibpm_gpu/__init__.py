@@ -41,6 +41,10 @@ IBPM_ERR_UNSUPPORTED = -4
 IBPM_ERR_NOMEM = -5
 IBPM_PREC_FP64 = 0
 IBPM_PREC_FP32_REFINED = 1
+# transform plans (ibpm_set_transform_plan): radix 4 / N/4 threads per line
+# pair (shortest chain per launch), radix 8 / N/8 threads (fewer instructions)
+IBPM_PLAN_LATENCY = 0
+IBPM_PLAN_THROUGHPUT = 1
 PRECISIONS = {"fp64": IBPM_PREC_FP64, "fp32_refined": IBPM_PREC_FP32_REFINED}
 KERNEL_COUNT = 12
 
@@ -142,6 +146,14 @@ def load_library(path=None):
     lib.ibpm_batch_member.argtypes = [H, C.c_int32]
     lib.ibpm_batch_lanes.restype = C.c_int
     lib.ibpm_batch_lanes.argtypes = [H]
+    lib.ibpm_batch_plan.restype = C.c_int
+    lib.ibpm_batch_plan.argtypes = [H]
+    lib.ibpm_batch_set_plan.restype = C.c_int
+    lib.ibpm_batch_set_plan.argtypes = [H, C.c_int32]
+    lib.ibpm_set_transform_plan.restype = C.c_int
+    lib.ibpm_set_transform_plan.argtypes = [H, C.c_int32, C.c_int32]
+    lib.ibpm_get_transform_plan.restype = C.c_int
+    lib.ibpm_get_transform_plan.argtypes = [H, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     lib.ibpm_batch_set_lanes.restype = C.c_int
     lib.ibpm_batch_set_lanes.argtypes = [H, C.c_int32]
     lib.ibpm_batch_last_error.restype = C.c_char_p
@@ -560,6 +572,19 @@ def launches_per_step(prob):
     return n
 
 
+def set_transform_plan(prob, single_slab=IBPM_PLAN_LATENCY, multi_slab=IBPM_PLAN_LATENCY):
+    """Plans of the problem's sine transforms, for launches over one level
+    and over several (IBPM_PLAN_LATENCY or IBPM_PLAN_THROUGHPUT)."""
+    prob._check(prob.lib.ibpm_set_transform_plan(prob.handle, int(single_slab), int(multi_slab)))
+
+
+def transform_plan(prob):
+    """(single-slab plan, multi-slab plan) of the problem."""
+    a, b = C.c_int32(), C.c_int32()
+    prob._check(prob.lib.ibpm_get_transform_plan(prob.handle, C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
 def pull_state(state, prob):
     """Copy the device state into ``state``."""
     prob._check(prob.lib.ibpm_get_state(prob.handle, _ptr(state.Gamma), _ptr(state.q), _ptr(state.q0),
@@ -743,6 +768,14 @@ class Batch:
 
     def set_lanes(self, lanes):
         self._check(self.lib.ibpm_batch_set_lanes(self.handle, int(lanes)))
+
+    @property
+    def plan(self):
+        """Transform plan of the members' single-level launches."""
+        return self.lib.ibpm_batch_plan(self.handle)
+
+    def set_plan(self, plan):
+        self._check(self.lib.ibpm_batch_set_plan(self.handle, int(plan)))
 
     def advance(self, nsteps=1):
         """Advance every member; returns per-member (CD, CL) histories (nsteps, nbodies)."""

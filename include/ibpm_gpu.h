@@ -302,6 +302,12 @@ int ibpm_batch_get_forces(const ibpm_batch* b, int32_t i, double* CD, double* CL
 /* Device time of each of nsteps batch steps (CUDA events; L2 flushed between steps if flush_l2). */
 int ibpm_batch_bench(ibpm_batch* b, int32_t nsteps, int32_t flush_l2, double* step_ms);
 
+/* Transform plan of the members' single-slab launches (IBPM_PLAN_*): the one
+ * lanes = 0 chose with the lane count, or the one set; setting it captures the
+ * batch step again (the state is kept). */
+int ibpm_batch_plan(const ibpm_batch* b);
+int ibpm_batch_set_plan(ibpm_batch* b, int32_t plan);
+
 /* Page-locked host memory for state mirrors (faster get/set_state); NULL on
  * failure.  No counterpart in the reference (Julia arrays are pageable). */
 void* ibpm_host_alloc(int64_t bytes);
@@ -317,6 +323,24 @@ int ibpm_host_free(void* p);
 
 /* Name of kernel class k (0 <= k < IBPM_KERNEL_COUNT). */
 const char* ibpm_kernel_name(int32_t k);
+
+/* Plans of the 2-D sine transforms (no counterpart in the reference, which
+ * calls FFTW's r2r plans, src/fluid-operators/laplacian.jl:30-39).  A plan
+ * fixes the FFT factorisation and the threads per line pair:
+ *   IBPM_PLAN_LATENCY     radix 4, N/4 threads per line pair: the shortest
+ *                         chain per launch, for launches too small to fill
+ *                         the GPU (a single level of one simulation);
+ *   IBPM_PLAN_THROUGHPUT  radix 8, N/8 threads: about two thirds of the
+ *                         instructions, for launches that fill the GPU.
+ * From N = 1024 on both are the radix-8 plan.  A handle starts with the
+ * latency plan for both kinds of launch; ibpm_batch_create with lanes = 0
+ * chooses its members' single-slab plan by timing.  Results agree to
+ * rounding (the factorisations differ).
+ * Setting a plan captures the step graphs again on the next advance. */
+#define IBPM_PLAN_LATENCY    0
+#define IBPM_PLAN_THROUGHPUT 1
+int ibpm_set_transform_plan(ibpm_handle* h, int32_t single_slab, int32_t multi_slab);
+int ibpm_get_transform_plan(const ibpm_handle* h, int32_t* single_slab, int32_t* multi_slab);
 
 /* Number of kernel launches in one step (one replay of the step graph). */
 int ibpm_launches_per_step(ibpm_handle* h);
