@@ -555,6 +555,8 @@ def batch_block(args, d):
     b.advance(2)
     ms1 = b.bench_steps(K, flush_l2=True)
     t_seq = float(np.sum(ms1)) / 1e3
+    b.set_lanes(tuned)            # end to end with the tuned lanes
+    b.advance(2)
     t0 = time.perf_counter()
     forces = b.advance(K)
     e2e_s = time.perf_counter() - t0
