@@ -1937,8 +1937,10 @@ static int batch_sync_members(ibpm_batch* b) {
         if (h->cur != b->cur)
             return bfail(b, IBPM_ERR_INVALID, "member " + std::to_string(i) +
                                                   " was advanced on its own: batch members must step together");
-        if (!h->graphs_ready)  // a changed base flux
-            return bfail(b, IBPM_ERR_UNSUPPORTED, "member " + std::to_string(i) + " changed its base flux");
+        if (!h->graphs_ready)  // a changed base flux or transform plan
+            return bfail(b, IBPM_ERR_UNSUPPORTED, "member " + std::to_string(i) +
+                                                      " changed its base flux or transform plan on its own "
+                                                      "(a batch's plan is set by ibpm_batch_set_plan)");
         b->cold = std::max(b->cold, h->cold);      // set_state on a member re-arms its first steps
     }
     return IBPM_OK;

@@ -80,7 +80,106 @@ __global__ void gj_extract_kernel(const double* aug, double* A, int n) {
     A[t] = aug[(long long)r * 2 * n + n + col];
 }
 
+// The same elimination in ONE block with [B | I] in shared memory, for n up
+// to kGjSmemMax: the pivot search, row swap, normalisation and elimination of
+// each column are separated by block barriers instead of kernel boundaries
+// (2n + 2 launches become one).  Every element sees the same operations in
+// the same order as above (largest |pivot|, first index on ties; row c
+// divided by the pivot; aug[r][col] -= f·aug[c][col] with f saved before the
+// column is eliminated), so the result is the multi-launch one.
+constexpr int kGjThreads = 1024;
+constexpr int kGjSmemMax = 112;   // 2·112²·8 B + 112·8 B = 201 KB of shared memory
+static size_t gj_smem_bytes(int n) { return ((size_t)2 * n * n + n) * sizeof(double); }
+
+__global__ void __launch_bounds__(kGjThreads, 1) gj_inverse_smem_kernel(double* A, int n, int* info) {
+    extern __shared__ __align__(16) double gsm[];
+    __shared__ double wv[kGjThreads / 32];
+    __shared__ int wi[kGjThreads / 32];
+    __shared__ int s_piv;
+    const int n2 = 2 * n;
+    double* aug = gsm;
+    double* fcol = gsm + (size_t)n * n2;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int t = tid; t < n * n2; t += kGjThreads) {
+        const int r = t / n2, col = t - r * n2;
+        aug[t] = (col < n) ? A[(long long)r * n + col] : (col - n == r ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    int bad = 0;
+    for (int c = 0; c < n; ++c) {
+        // pivot: the largest |aug[r][c]|, r >= c, the smallest r among equals
+        double best = -1.0;
+        int bidx = n;
+        for (int r = c + tid; r < n; r += kGjThreads) {
+            const double v = fabs(aug[r * n2 + c]);
+            if (v > best) { best = v; bidx = r; }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double o = __shfl_down_sync(0xffffffffu, best, off);
+            const int oi = __shfl_down_sync(0xffffffffu, bidx, off);
+            if (o > best || (o == best && oi < bidx)) { best = o; bidx = oi; }
+        }
+        if (lane == 0) { wv[warp] = best; wi[warp] = bidx; }
+        __syncthreads();
+        if (warp == 0) {
+            best = wv[lane];
+            bidx = wi[lane];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double o = __shfl_down_sync(0xffffffffu, best, off);
+                const int oi = __shfl_down_sync(0xffffffffu, bidx, off);
+                if (o > best || (o == best && oi < bidx)) { best = o; bidx = oi; }
+            }
+            if (lane == 0) s_piv = (bidx >= n || best == 0.0) ? -1 : bidx;
+        }
+        __syncthreads();
+        const int p = s_piv;
+        if (p < 0) { bad = c + 1; break; }     // every thread reads the same p
+        if (p != c) {
+            for (int col = tid; col < n2; col += kGjThreads) {
+                const double t = aug[c * n2 + col];
+                aug[c * n2 + col] = aug[p * n2 + col];
+                aug[p * n2 + col] = t;
+            }
+        }
+        __syncthreads();
+        const double piv = aug[c * n2 + c];
+        __syncthreads();
+        for (int col = tid; col < n2; col += kGjThreads) aug[c * n2 + col] /= piv;
+        for (int r = tid; r < n; r += kGjThreads) fcol[r] = (r == c) ? 0.0 : aug[r * n2 + c];
+        __syncthreads();
+        for (int t = tid; t < n * n2; t += kGjThreads) {
+            const int r = t / n2, col = t - r * n2;
+            if (r == c) continue;
+            const double f = fcol[r];
+            if (f == 0.0) continue;
+            aug[r * n2 + col] -= f * aug[c * n2 + col];
+        }
+        __syncthreads();
+    }
+    for (int t = tid; t < n * n; t += kGjThreads) {
+        const int r = t / n, col = t - r * n;
+        A[t] = aug[r * n2 + n + col];
+    }
+    if (tid == 0) *info = bad;
+}
+
 cudaError_t launch_gj_inverse(double* A, int n, double* work, int* info, cudaStream_t st) {
+    if (n >= 1 && n <= kGjSmemMax) {
+        // the shared-memory opt-in is a function attribute: set outside stream
+        // capture (the handle's setup inverts B before any capture)
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaError_t e = cudaStreamIsCapturing(st, &cs);
+        if (e != cudaSuccess) return e;
+        if (cs == cudaStreamCaptureStatusNone) {
+            e = cudaFuncSetAttribute(gj_inverse_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)gj_smem_bytes(kGjSmemMax));
+            if (e != cudaSuccess) return e;
+        }
+        gj_inverse_smem_kernel<<<1, kGjThreads, gj_smem_bytes(n), st>>>(A, n, info);
+        return cudaGetLastError();
+    }
     double* aug = work;
     double* fcol = work + (size_t)2 * n * n;
     cudaMemsetAsync(info, 0, sizeof(int), st);

@@ -165,3 +165,15 @@ def test_batch_plan_is_the_members_plan(plan):
         assert np.array_equal(forces[i][0], cd) and np.array_equal(forces[i][1], cl), (name, prec, plan)
         solo.close()
     batch.close()
+
+
+def test_batch_member_plan_change_is_refused():
+    """A member's plan belongs to its batch: changed on the member's own
+    handle, the next batch step is refused instead of running stale graphs."""
+    import ibpm_gpu as G
+    batch = G.Batch([_spec("sq64_mg3", "fp64"), _spec("sq64_mg1_plate", "fp64")], lanes=2)
+    batch.advance(1)
+    G.set_transform_plan(batch.members[0], THR, LAT)
+    with pytest.raises(G.IBPMError):
+        batch.advance(1)
+    batch.close()
