@@ -913,6 +913,12 @@ def run_ours(args, d):
                                    "sample": "%d steps of the same workload in oracle/ibpm_ref.py (%.1f s), "
                                              "scipy.fft on all host threads; B^-1 replaced by a seeded dense "
                                              "matrix of the same size" % (args.cpu_steps, secs)}
+            # the reference's own FFTW plans run on one thread
+            n1 = max(1, args.cpu_steps // 4)
+            rate1, secs1 = cpu_step_rate(n1, 1)
+            out["cpu_baseline"]["single_thread"] = {"value": rate1, "cores": 1,
+                                                    "sample": "%d steps, scipy.fft on one thread (%.1f s)"
+                                                              % (n1, secs1)}
         except Exception as e:  # the CPU leg is a reported baseline only
             out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
     if d.rank == 0:
