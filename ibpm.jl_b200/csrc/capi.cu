@@ -652,7 +652,17 @@ static int build_binv(ibpm_handle* h) {
         cudaFree(GB); cudaFree(PB); cudaFree(QB); cudaFree(work); cudaFree(info);
         return rc;
     }
-    auto cleanup = [&]() { cudaFree(GB); cudaFree(PB); cudaFree(QB); cudaFree(work); cudaFree(info); };
+    // B at create is built with the single-level (latency) plan on every
+    // launch, so B⁻¹, and every step it feeds, does not depend on the
+    // multi-level plan chosen for the steps
+    const int planN[2] = {h->px.planN, h->py.planN};
+    h->px.planN = h->px.plan1;
+    h->py.planN = h->py.plan1;
+    auto cleanup = [&]() {
+        h->px.planN = planN[0];
+        h->py.planN = planN[1];
+        cudaFree(GB); cudaFree(PB); cudaFree(QB); cudaFree(work); cudaFree(info);
+    };
     for (int c0 = 0; c0 < nf && rc == IBPM_OK; c0 += chunk) {
         const int R = std::min(chunk, nf - c0);
         if (cudaMemsetAsync(GB, 0, sizeof(double) * bstride * R, h->st) != cudaSuccess) { rc = IBPM_ERR_CUDA; break; }
@@ -1195,9 +1205,11 @@ static void set_plans(ibpm_handle* h, int single_slab, int multi_slab) {
 
 extern "C" int ibpm_set_transform_plan(ibpm_handle* h, int32_t single_slab, int32_t multi_slab) {
     if (!h) return IBPM_ERR_INVALID;
-    for (int v : {single_slab, multi_slab})
-        if (v != IBPM_PLAN_LATENCY && v != IBPM_PLAN_THROUGHPUT)
-            return fail(h, IBPM_ERR_INVALID, "transform plan must be IBPM_PLAN_LATENCY or IBPM_PLAN_THROUGHPUT");
+    if (single_slab != IBPM_PLAN_LATENCY && single_slab != IBPM_PLAN_THROUGHPUT)
+        return fail(h, IBPM_ERR_INVALID, "single-slab plan must be IBPM_PLAN_LATENCY or IBPM_PLAN_THROUGHPUT");
+    if (multi_slab != IBPM_PLAN_LATENCY && multi_slab != IBPM_PLAN_THROUGHPUT && multi_slab != IBPM_PLAN_AUTO)
+        return fail(h, IBPM_ERR_INVALID,
+                    "multi-slab plan must be IBPM_PLAN_LATENCY, IBPM_PLAN_THROUGHPUT or IBPM_PLAN_AUTO");
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->st));
     set_plans(h, single_slab, multi_slab);

@@ -177,6 +177,7 @@ int dst_plan_create(DstPlan* p, int N, cudaStream_t st) {
     p->Wt = reinterpret_cast<double2*>(base + 6 * N);
     p->Wt32 = reinterpret_cast<float2*>(base + 8 * N);
     if (twiddles_build(N, dstk::ct_plan(N, 1), p->Wt, p->Wt32, st) != cudaSuccess) return -2;
+    p->planN = DST_PLAN_AUTO;
     if (dst_init_attributes(N) != cudaSuccess) return -2;
     return 0;
 }

@@ -738,7 +738,9 @@ cudaError_t launch_x_n(const Geom& g, const DstPlan& px, const XPassArgs& a, cud
 // The plan of a launch: the plan's single-slab or multi-slab choice; the
 // throughput plan needs its twiddle table.
 inline int launch_plan(int N, const DstPlan& p, int nslabs) {
-    const int pl = ct_plan(N, nslabs > 1 ? p.planN : p.plan1);
+    int pl = nslabs > 1 ? p.planN : p.plan1;
+    if (pl == DST_PLAN_AUTO) pl = nslabs >= kAutoWideSlabs ? DST_PLAN_THROUGHPUT : p.plan1;
+    pl = ct_plan(N, pl);
     return (pl == 1 && p.Wt) ? 1 : 0;
 }
 

@@ -181,17 +181,18 @@ function set_vorticity!(prob::IBProblemGPU, ω::AbstractMatrix{Float64})
 end
 
 """
-    set_transform_plan!(prob; single=:latency, multi=:latency)
+    set_transform_plan!(prob; single=:latency, multi=:auto)
 
 Plans of the device sine transforms for launches over one level (`single`)
 and over several (`multi`): `:latency` (radix 4, N/4 threads per line pair,
 the shortest chain per launch) or `:throughput` (radix 8, N/8 threads, fewer
-instructions).  No counterpart in the reference, whose FFTW plans are fixed
+instructions); `multi` may also be `:auto` (the throughput plan for launches
+of 16 or more slabs, else `single`).  No counterpart in the reference, whose FFTW plans are fixed
 (src/fluid-operators/laplacian.jl:30-39).
 """
-function set_transform_plan!(prob::IBProblemGPU; single::Symbol=:latency, multi::Symbol=:latency)
-    code(s) = s === :latency ? Int32(0) : s === :throughput ? Int32(1) :
-              throw(ArgumentError("plan must be :latency or :throughput"))
+function set_transform_plan!(prob::IBProblemGPU; single::Symbol=:latency, multi::Symbol=:auto)
+    code(s) = s === :latency ? Int32(0) : s === :throughput ? Int32(1) : s === :auto ? Int32(2) :
+              throw(ArgumentError("plan must be :latency, :throughput or :auto"))
     check(ccall((:ibpm_set_transform_plan, LIB), Cint, (Ptr{Cvoid}, Int32, Int32), prob.handle,
                 code(single), code(multi)), prob.handle)
 end

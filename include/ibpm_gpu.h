@@ -332,13 +332,20 @@ const char* ibpm_kernel_name(int32_t k);
  *                         the GPU (a single level of one simulation);
  *   IBPM_PLAN_THROUGHPUT  radix 8, N/8 threads: about two thirds of the
  *                         instructions, for launches that fill the GPU.
+ *   IBPM_PLAN_AUTO        (multi-slab launches only) the throughput plan for
+ *                         launches of 16 or more slabs (the columns of B,
+ *                         the unit solves of moving bodies), else the
+ *                         single-slab plan (the levels of one step).
  * From N = 1024 on both are the radix-8 plan.  A handle starts with the
- * latency plan for both kinds of launch; ibpm_batch_create with lanes = 0
- * chooses its members' single-slab plan by timing.  Results agree to
- * rounding (the factorisations differ).
- * Setting a plan captures the step graphs again on the next advance. */
+ * latency plan for single-slab launches and IBPM_PLAN_AUTO for multi-slab
+ * ones; ibpm_batch_create with lanes = 0 chooses its members' single-slab
+ * plan by timing.  Results agree to rounding (the factorisations differ).
+ * Setting a plan captures the step graphs again on the next advance.  B⁻¹
+ * of fixed bodies is built at create with the latency plan on every launch,
+ * whatever plans are set later. */
 #define IBPM_PLAN_LATENCY    0
 #define IBPM_PLAN_THROUGHPUT 1
+#define IBPM_PLAN_AUTO       2
 int ibpm_set_transform_plan(ibpm_handle* h, int32_t single_slab, int32_t multi_slab);
 int ibpm_get_transform_plan(const ibpm_handle* h, int32_t* single_slab, int32_t* multi_slab);
 

@@ -68,7 +68,10 @@ def test_moving_bodies_match_oracle(name, mg, amp):
 def test_still_motion_function_is_the_static_problem():
     """Points that stay at their reference configuration step as the static
     body (the per-step B⁻¹ is rebuilt by the setup's own kernels; the
-    projection source is gathered instead of reduced over a sorted list)."""
+    projection source is gathered instead of reduced over a sorted list).
+    The rebuild's many-column transforms take the radix-8 throughput plan,
+    the setup's the radix-4 latency plan, so the two B⁻¹ agree to rounding
+    (amplified by cond(B) ≈ 1e4), not to the bit."""
     import ibpm_gpu as G
     c = CASES["sq64_mg3"]
     g = G.make_grid(c["h"], c["bnd"], c["mg"])
@@ -83,7 +86,7 @@ def test_still_motion_function_is_the_static_problem():
     # the lift of this symmetric case is ~1e-11: compare it on the drag's scale
     assert rel(cdm, cds) < 1e-13 and np.max(np.abs(clm - cls)) < 1e-13 * np.max(np.abs(cds))
     assert rel(sm.Gamma, ss.Gamma) < 1e-13
-    assert np.array_equal(pm.binv(), ps.binv())
+    assert rel(pm.binv(), ps.binv()) < 1e-10
     pm.close()
     ps.close()
 

@@ -11,7 +11,7 @@ from ibpm_cases import CASES, build_bodies, gpu_problem, oracle_problem, random_
 pytestmark = pytest.mark.gpu
 TOL = 1e-10
 SMALL = ["sq64_mg3", "rect64x32_mg2_two", "sq64_mg1_plate"]
-LAT, THR = 0, 1
+LAT, THR, AUTO = 0, 1, 2
 
 
 def _run(gp, op, seed, nsteps):
@@ -118,12 +118,14 @@ def test_plans_agree_at_512(precision, tol):
 def test_plan_arguments_are_checked():
     import ibpm_gpu as G
     gp = gpu_problem("sq64_mg1_plate")
-    assert G.transform_plan(gp) == (LAT, LAT)
+    assert G.transform_plan(gp) == (LAT, AUTO)
     with pytest.raises(G.IBPMError):
-        G.set_transform_plan(gp, 2, LAT)
+        G.set_transform_plan(gp, AUTO, LAT)            # AUTO is for multi-slab launches only
     with pytest.raises(G.IBPMError):
         G.set_transform_plan(gp, LAT, -1)
-    assert G.transform_plan(gp) == (LAT, LAT)
+    assert G.transform_plan(gp) == (LAT, AUTO)
+    G.set_transform_plan(gp, THR, LAT)
+    assert G.transform_plan(gp) == (THR, LAT)
     gp.close()
 
 
@@ -157,7 +159,7 @@ def test_batch_plan_is_the_members_plan(plan):
         sp = specs[i]
         solo = G.IBProblem(sp["grid"], sp["bodies"], sp["dt"], sp["Re"], freestream=sp["freestream"],
                            precision=prec, sync_fields=False)
-        G.set_transform_plan(solo, plan, LAT)
+        G.set_transform_plan(solo, plan, AUTO)
         st = G.IBState(solo)
         to_gpu_state(starts[i], st)
         G.push_state(st, solo)
