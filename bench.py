@@ -866,7 +866,9 @@ def run_ours(args, d):
         "config": {"workload": WORKLOAD, "precision": "fp32_refined (1 FP64-residual sweep per Poisson solve, "
                    "warm start; FP64 trial solve)", "l2": "flushed between steps (512 MiB write outside the "
                    "timed event pairs)", "parallelism": "replicas x%d" % d.world,
-                   "graph": "one CUDA graph replay per step"},
+                   "graph": "one CUDA graph replay per step",
+                   "transform_plans": "radix-4 latency plan on single-level launches; multi-level launches "
+                                      "automatic (radix 8 from 16 slabs on, so the five-level ones stay radix 4)"},
         "e2e": e2e_of(r32),
         "gpu_launches": r32["lps"] * K,
         "fp64_plain": {"value": value64, "ms_per_step": r64["total_ms"] / K, "e2e": e2e_of(r64),
