@@ -1,8 +1,9 @@
 /*
  * ibpm_gpu.h — C ABI of libibpm_gpu.so, a B200 (sm_100a) implementation of the
- * static-body time step of the immersed boundary projection method
- * (NUFgroup/IBPM.jl), meant to be bound from Julia with `ccall`, from Python
- * with ctypes, or from C/C++ directly.
+ * time step of the immersed boundary projection method (NUFgroup/IBPM.jl):
+ * static bodies, a moving grid or moving bodies, its discrete adjoint and
+ * batches of independent problems.  Meant to be bound from Julia with
+ * `ccall`, from Python with ctypes, or from C/C++ directly.
  *
  * Every entry point is `extern "C"`, takes plain pointers and sizes, and
  * returns an int status (IBPM_OK = 0, negative = error).  The text of the last
