@@ -5,7 +5,7 @@
 // deterministic like the forward step.  Index comments use 0-based indices:
 // Γ-like (i, j) with i < nx-1, j < ny-1; fluxes qx[I, J] (I ≤ nx, J < ny) and
 // qy[I, J] (I < nx, J ≤ ny) at I + J(nx+1) and nu + I + J nx; edge vectors with
-// the reference's LEFT/RIGHT/BOT/TOP segment offsets (fluid-domain.jl:205-206).
+// the reference's LEFT/RIGHT/BOT/TOP segment offsets (fluid-domain.jl:68-69).
 #include "ibpm_internal.cuh"
 
 namespace ibpm {
@@ -60,7 +60,7 @@ __device__ double get_bc_T_at(const Geom& g, int i, int j, const BV& b) {
 }
 
 // ---------------------------------------------------------------------------
-// Adjoint level chain of vort2flux! (curl.jl:425-440), one level:
+// Adjoint level chain of vort2flux! (curl.jl:147-162), one level:
 //   ψ̄ = rot(q̄) + get_bc!ᵀ(b̄_prev)      (the interior of curl! is rot!ᵀ)
 //   bc_out = the edge part of curl!ᵀ(q̄), with its bottom row at ψbc[(B-1)+i]
 // Threads [0, nΓ) write ψ̄, threads [nΓ, nΓ + nbc) write bc_out.

@@ -246,7 +246,7 @@ cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double d
 }
 
 // Γsrc = C'(E' F̃b) at the Γ points whose rot! stencil touches a regularised
-// flux point (timestepping.jl:217, curl.jl:300-312): Γ = (qx₁ − qx₂) +
+// flux point (timestepping.jl:217, curl.jl:22-34): Γ = (qx₁ − qx₂) +
 // (qy₁ − qy₂) over the point's four fluxes, each flux the sum over its sorted
 // contributor list (interface-coupling.jl:103-107).  One warp per Γ point:
 // the lanes take the contributors of all four fluxes (about 50 at one point
@@ -302,7 +302,7 @@ cudaError_t launch_stress_src(const BodyDev& b, const double* Fb, double h, doub
     return launch_k(stress_src_kernel, dim3(blocks), dim3(256), 0, st, b, Fb, h, dt, hist, counter, status, Gsrc);
 }
 
-// C'E' e_kk for unit forces kk = col0 + r (B_times!, laplacian.jl:318), written
+// C'E' e_kk for unit forces kk = col0 + r (B_times!, laplacian.jl:162), written
 // into the level-1 slab of batch member r (slab zeroed beforehand).  One thread
 // per point of the 14×14 box of Γ points the 13×13 flux window can reach.
 __global__ void unit_src_kernel(BodyDev b, Geom g, int col0, int ncol, double* G, long long bstride) {

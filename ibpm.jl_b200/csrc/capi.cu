@@ -68,13 +68,11 @@ struct ibpm_handle {
     int cold = kColdSteps;                 // steps left that lack good initial guesses
     float* T32 = nullptr;                  // mg slabs of FP32 transform scratch
     double* Pp = nullptr;                  // A⁻¹C'E'F̃b of the previous step (level 1)
-    bool cluster = false;                  // level solves in one cluster launch (cluster_solve.cuh)
     // linearised problem (ibpm_set_base_state): base Γ, base q, base flux
     bool lin = false;
     double* GB = nullptr;
     double* qB = nullptr;
     double q0Bx[8] = {0}, q0By[8] = {0};
-    float* D32 = nullptr;                  // mg slabs: each level's last FP32 correction
     // moving grid (ibpm_set_moving_grid): per-step (Ω, Ux0, Uy0) rows indexed by `counter`
     bool moving = false;
     double mv_xc = 0, mv_yc = 0;
@@ -210,11 +208,11 @@ static SpecParams spec(const ibpm_handle* h, int mode, int f32 = 0) {
     SpecParams sp;
     sp.mode = mode;
     sp.f32 = f32;
-    sp.scale = 1.0 / (4.0 * h->g.nx * h->g.ny);  // laplacian.jl:194
+    sp.scale = 1.0 / (4.0 * h->g.nx * h->g.ny);  // laplacian.jl:38
     sp.dt = h->dt;
     for (int l = 0; l < 8; ++l) {
         const double hc = h->h * std::ldexp(1.0, l);
-        sp.den[l] = 2.0 * h->Re * (hc * hc);       // laplacian.jl:225
+        sp.den[l] = 2.0 * h->Re * (hc * hc);       // laplacian.jl:69
     }
     return sp;
 }
@@ -244,7 +242,7 @@ static int poisson(ibpm_handle* h, const double* b, SlabMap bmap, double* tmp, S
 
 static double c_lap(const ibpm_handle* h, int lev) {
     const double hc = h->h * std::ldexp(1.0, lev);
-    return h->dt / (2.0 * h->Re * (hc * hc));  // laplacian.jl:225
+    return h->dt / (2.0 * h->Re * (hc * hc));  // laplacian.jl:69
 }
 
 // The moving grid's base flux for the kernels, or none (uniform q0x, q0y).
@@ -304,7 +302,7 @@ static RhsArgs rhs_args(const ibpm_handle* h, int p) {
     return ra;
 }
 
-// vort2flux! (curl.jl:411-443) on `nbatch` independent fields G (slab-major,
+// vort2flux! (curl.jl:133-165) on `nbatch` independent fields G (slab-major,
 // batch stride bstride), level by level as the reference: coarsify chain,
 // Δ⁻¹ solves from the coarsest level inwards with the edge values of the next
 // coarser ψ, then q = curl ψ on levels [qlev0, qlev0 + qnlev) into q (nq per
@@ -415,25 +413,6 @@ static int resid(ibpm_handle* h, int mode, const double* b, const double* x, int
     return IBPM_OK;
 }
 
-// One cluster launch: the FP32 correction of level `lev` from T32, emitted as
-// ψ += d (dstore/dc for the level chain) or P += d; Γ −= P.
-static int level_solve(ibpm_handle* h, int lev, int mode, int emit, double* out, double* aux, bool chain) {
-    const Geom& g = h->g;
-    const int mg = g.mg;
-    const long long bs = g.S * mg;
-    ClusterSolveArgs a{};
-    a.r = h->T32; a.rmap = levmap(g, lev, 1, bs);
-    a.dc = (chain && lev < mg - 1) ? h->D32 : nullptr; a.dcmap = levmap(g, lev + 1, 1, bs);
-    a.out = out; a.out_map = (emit == XEMIT_ACC_SUB || out != h->Pp) ? levmap(g, lev, 1, bs) : levmap(g, 0, 1, g.S);
-    a.aux = aux; a.aux_map = levmap(g, 0, 1, g.S);
-    a.dstore = (chain && lev > 0) ? h->D32 : nullptr; a.dstore_map = levmap(g, lev, 1, bs);
-    a.sp = spec(h, mode, 1);
-    a.emit = emit;
-    LAUNCH(K_LSOLVE, (4.0 + 16.0 + (a.dstore ? 4.0 : 0.0) + (emit == XEMIT_ACC_SUB ? 16.0 : 0.0)) * g.n1 * g.n2,
-           launch_cluster_solve(g, h->px, a, 1, h->st));
-    return IBPM_OK;
-}
-
 // vort2flux! with every level's Δ⁻¹ solve refined from the ψ in h->psi.
 static int vort2flux_refined(ibpm_handle* h, double* G, int nsw, double* q, int qnlev) {
     const Geom& g = h->g;
@@ -443,24 +422,10 @@ static int vort2flux_refined(ibpm_handle* h, double* G, int nsw, double* q, int 
         LAUNCH(K_COARSIFY, 8.0 * 1.25 * g.n1 * g.n2,
                launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), 1, h->st));
     int rc;
-    if (h->cluster && nsw == 1) {
-        // every level's residual against the present ψ at once; each level's
-        // solve then adds the edge terms of the coarser level's correction
-        if ((rc = resid(h, RESID_LAP, G, h->psi, 0, mg, false))) return rc;
-        for (int lev = mg - 1; lev >= 0; --lev)
-            if ((rc = level_solve(h, lev, SPEC_DELTA, XEMIT_ADD, h->psi, nullptr, true))) return rc;
-    } else if (h->cluster) {
-        for (int lev = mg - 1; lev >= 0; --lev)
-            for (int s = 0; s < nsw; ++s) {
-                if ((rc = resid(h, RESID_LAP, G, h->psi, lev, 1, false))) return rc;
-                if ((rc = level_solve(h, lev, SPEC_DELTA, XEMIT_ADD, h->psi, nullptr, false))) return rc;
-            }
-    } else {
-        for (int lev = mg - 1; lev >= 0; --lev) {
-            const double* coarse = (lev < mg - 1) ? h->psi : nullptr;
-            for (int s = 0; s < nsw; ++s) {
-                if ((rc = correction32(h, XLOAD_RES_LAP, G, coarse, h->psi, 0.0, lev, XEMIT_ADD, h->psi))) return rc;
-            }
+    for (int lev = mg - 1; lev >= 0; --lev) {
+        const double* coarse = (lev < mg - 1) ? h->psi : nullptr;
+        for (int s = 0; s < nsw; ++s) {
+            if ((rc = correction32(h, XLOAD_RES_LAP, G, coarse, h->psi, 0.0, lev, XEMIT_ADD, h->psi))) return rc;
         }
     }
     CurlArgs ca{};
@@ -494,13 +459,8 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
     if ((rc = stress_and_src(h))) return rc;
     for (int s = 0; s < nsw; ++s) {
         const bool last = s + 1 == nsw;
-        if (h->cluster) {
-            if ((rc = resid(h, RESID_A, h->Gsrc, h->Pp, 0, 1, true))) return rc;
-            rc = level_solve(h, 0, SPEC_AINV, last ? XEMIT_ACC_SUB : XEMIT_ADD, last ? Gnew : h->Pp, h->Pp, false);
-        } else {
-            rc = correction32(h, XLOAD_RES_A, h->Gsrc, nullptr, h->Pp, c_lap(h, 0), 0,
-                              last ? XEMIT_ACC_SUB : XEMIT_ADD, last ? Gnew : h->Pp);
-        }
+        rc = correction32(h, XLOAD_RES_A, h->Gsrc, nullptr, h->Pp, c_lap(h, 0), 0,
+                          last ? XEMIT_ACC_SUB : XEMIT_ADD, last ? Gnew : h->Pp);
         if (rc) return rc;
     }
     // --- vort2flux!(state.ψ, state.q, state.Γ)
@@ -637,7 +597,7 @@ static int build_coupling(ibpm_handle* h, const ibpm_problem_desc* d) {
 }
 
 // B[:, j] = E · vort2flux(A⁻¹₁ C'E' e_j)[level-1 flux] (B_times!,
-// laplacian.jl:299-325), `chunk` columns per batch, then Binv = B⁻¹.
+// laplacian.jl:143-169), `chunk` columns per batch, then Binv = B⁻¹.
 static int build_binv(ibpm_handle* h) {
     const Geom& g = h->g;
     const int nf = h->nf, mg = g.mg;
@@ -700,7 +660,6 @@ static void free_handle(ibpm_handle* h) {
     }
     if (h->T32) cudaFree(h->T32);
     if (h->Pp) cudaFree(h->Pp);
-    if (h->D32) cudaFree(h->D32);
     if (h->mtab) cudaFree(h->mtab);
     for (void* p : {(void*)h->d_x0, (void*)h->d_ub, (void*)h->d_bbox, (void*)h->btab, (void*)h->bGB, (void*)h->bPB,
                     (void*)h->bQB, (void*)h->bwork, (void*)h->binfo})
@@ -798,15 +757,6 @@ static int create_impl(ibpm_handle* h, const ibpm_problem_desc* d) {
         if ((rc = dalloc(h, &h->T32, slabs)) || (rc = dalloc(h, &h->Pp, g.S))) return rc;
         CK(cudaMemsetAsync(h->T32, 0, sizeof(float) * slabs, h->st));
         CK(cudaMemsetAsync(h->Pp, 0, sizeof(double) * g.S, h->st));
-        // one-launch level solves where the level fits a cluster (IBPM_CLUSTER=1); three passes otherwise
-        const char* nc = getenv("IBPM_CLUSTER");
-        if ((nc && nc[0] == '1') && cluster_solve_supported(g.nx, g.ny) &&
-            cluster_init_attributes(g.nx) == cudaSuccess) {
-            if ((rc = dalloc(h, &h->D32, slabs))) return rc;
-            CK(cudaMemsetAsync(h->D32, 0, sizeof(float) * slabs, h->st));
-            h->cluster = true;
-        }
-        cudaGetLastError();  // a device that cannot place the cluster leaves its error here
     }
     if ((rc = build_coupling(h, d))) return rc;
     if ((rc = build_binv(h))) return rc;
@@ -1347,7 +1297,7 @@ extern "C" int ibpm_profile(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, do
 // recomputation, and the gradient of a time-averaged force objective.
 // ---------------------------------------------------------------------------
 
-// Transpose of the level chain of vort2flux! (curl.jl:425-440), finest level
+// Transpose of the level chain of vort2flux! (curl.jl:147-162), finest level
 // first: ψ̄ = curl!ᵀ(q̄) + get_bc!ᵀ(edge adjoint of the finer level), Γ̄ += Δ⁻¹ψ̄
 // (Δ⁻¹ is symmetric).  q̄ is given on levels [0, qnlev), zero above.
 static int solves_T(ibpm_handle* h, const double* qbar, int qnlev, double* Gacc) {
@@ -1376,7 +1326,7 @@ static int solves_T(ibpm_handle* h, const double* qbar, int qnlev, double* Gacc)
     return IBPM_OK;
 }
 
-// Transpose of the coarsify chain (curl.jl:419-421): coarsest level first.
+// Transpose of the coarsify chain (curl.jl:141-143): coarsest level first.
 static int coarsify_T(ibpm_handle* h, double* Gacc) {
     const Geom& g = h->g;
     const int mg = g.mg;

@@ -6,22 +6,6 @@
 
 namespace ibpm {
 
-cudaError_t cluster_solve_64(const Geom&, const DstPlan&, const ClusterSolveArgs&, int, cudaStream_t);
-cudaError_t cluster_attr_64();
-cudaError_t cluster_solve_128(const Geom&, const DstPlan&, const ClusterSolveArgs&, int, cudaStream_t);
-cudaError_t cluster_attr_128();
-cudaError_t cluster_solve_192(const Geom&, const DstPlan&, const ClusterSolveArgs&, int, cudaStream_t);
-cudaError_t cluster_attr_192();
-cudaError_t cluster_solve_200(const Geom&, const DstPlan&, const ClusterSolveArgs&, int, cudaStream_t);
-cudaError_t cluster_attr_200();
-cudaError_t cluster_solve_256(const Geom&, const DstPlan&, const ClusterSolveArgs&, int, cudaStream_t);
-cudaError_t cluster_attr_256();
-cudaError_t cluster_solve_384(const Geom&, const DstPlan&, const ClusterSolveArgs&, int, cudaStream_t);
-cudaError_t cluster_attr_384();
-cudaError_t cluster_solve_400(const Geom&, const DstPlan&, const ClusterSolveArgs&, int, cudaStream_t);
-cudaError_t cluster_attr_400();
-cudaError_t cluster_solve_512(const Geom&, const DstPlan&, const ClusterSolveArgs&, int, cudaStream_t);
-cudaError_t cluster_attr_512();
 
 cudaError_t dst_x_32(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
 cudaError_t dst_y_32(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
@@ -129,7 +113,7 @@ __global__ void dst_tables_kernel(int N, double* base) {
         s[t] = sinpi((double)t / (double)N);
         s32[t] = (float)s[t];
         // evaluated as the reference forms the Laplacian eigenvalues:
-        // cos.(π*(1:(n-1))/n) (laplacian.jl:173)
+        // cos.(π*(1:(n-1))/n) (laplacian.jl:17)
         c[t] = (t < N - 1) ? cos(M_PI * (double)(t + 1) / (double)N) : 0.0;
         const double h = sinpi((double)(t + 1) / (2.0 * (double)N));
         a32[t] = (t < N - 1) ? (float)(4.0 * h * h) : 0.0f;
@@ -244,54 +228,6 @@ cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px, vo
         case 1024: return dst_y_1024(g, py, px, data, map, nslabs, sp, st);
         case 2048: return dst_y_2048(g, py, px, data, map, nslabs, sp, st);
         default: return cudaErrorInvalidValue;
-    }
-}
-
-// The one-launch FP32 level solve (cluster_solve.cuh): square levels of the
-// lengths below (16 CTAs of at most 1024 threads hold a level).
-bool cluster_solve_supported(int nx, int ny) {
-    if (nx != ny) return false;
-    switch (nx) {
-        case 64:
-        case 128:
-        case 192:
-        case 200:
-        case 256:
-        case 384:
-        case 400:
-        case 512:
-            return true;
-        default:
-            return false;
-    }
-}
-
-cudaError_t cluster_init_attributes(int N) {
-    switch (N) {
-        case 64: return cluster_attr_64();
-        case 128: return cluster_attr_128();
-        case 192: return cluster_attr_192();
-        case 200: return cluster_attr_200();
-        case 256: return cluster_attr_256();
-        case 384: return cluster_attr_384();
-        case 400: return cluster_attr_400();
-        case 512: return cluster_attr_512();
-        default: return cudaErrorNotSupported;
-    }
-}
-
-cudaError_t launch_cluster_solve(const Geom& g, const DstPlan& p, const ClusterSolveArgs& a, int nslabs,
-                                 cudaStream_t st) {
-    switch (p.N) {
-        case 64: return cluster_solve_64(g, p, a, nslabs, st);
-        case 128: return cluster_solve_128(g, p, a, nslabs, st);
-        case 192: return cluster_solve_192(g, p, a, nslabs, st);
-        case 200: return cluster_solve_200(g, p, a, nslabs, st);
-        case 256: return cluster_solve_256(g, p, a, nslabs, st);
-        case 384: return cluster_solve_384(g, p, a, nslabs, st);
-        case 400: return cluster_solve_400(g, p, a, nslabs, st);
-        case 512: return cluster_solve_512(g, p, a, nslabs, st);
-        default: return cudaErrorNotSupported;
     }
 }
 

@@ -1,6 +1,6 @@
 // Batched 2-D DST-I (FFTW RODFT00, unnormalised) for the Poisson-type solves of
 // the IBPM step: x = S((S b) ./ M .* scale), S the 2-D DST-I
-// (src/fluid-operators/dst-inversion.jl:145-156, laplacian.jl:180-232).
+// (src/fluid-operators/dst-inversion.jl:39-50, laplacian.jl:24-76).
 //
 // A 1-D DST-I of length n = N-1,  Y_k = 2 Σ_m f_m sin(π m k / N)  (f_m = X_{m-1}),
 // is computed for TWO real lines at once (f = a + i b) with one complex FFT of
@@ -670,7 +670,7 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
         auto divide = [&]() {
             if constexpr (std::is_same<T, double>::value) {
                 // w ./= M ; w .*= scale  with Λ = -2 (cos(π i/nx) + cos(π j/ny) - 2)
-                // (laplacian.jl:173-197, 217-227)
+                // (laplacian.jl:17-41, 61-71)
                 const double cxa = __ldg(&cx[ia]);
                 const double cxb = hasb ? __ldg(&cx[ia + 1]) : 0.0;
                 const double den = sp.den[lev];

@@ -1,8 +1,6 @@
-// DST kernels for transform length 384 (dst_kernels.cuh) and the one-launch
-// level solve of a square 384-cell level (cluster_solve.cuh).
-#include "cluster_solve.cuh"
+// DST kernels for transform length 384 (see dst_kernels.cuh).
+#include "dst_kernels.cuh"
 
 namespace ibpm {
 IBPM_DST_DEFINE(384)
-IBPM_CLUSTER_DEFINE(384)
 }  // namespace ibpm

@@ -1,8 +1,6 @@
-// DST kernels for transform length 400 (dst_kernels.cuh) and the one-launch
-// level solve of a square 400-cell level (cluster_solve.cuh).
-#include "cluster_solve.cuh"
+// DST kernels for transform length 400 (see dst_kernels.cuh).
+#include "dst_kernels.cuh"
 
 namespace ibpm {
 IBPM_DST_DEFINE(400)
-IBPM_CLUSTER_DEFINE(400)
 }  // namespace ibpm

@@ -5,14 +5,14 @@
 //     "slab" of (ny-1) rows of pitch P = nx doubles; element (i, j) (0-based,
 //     i < nx-1 fastest, j < ny-1) sits at row j, column i.  The reference keeps
 //     the same field as a column-major (nx-1)×(ny-1) matrix
-//     (src/fluid-domain/fluid-domain.jl:192); the pitch pads each row to 32 B.
+//     (src/fluid-domain/fluid-domain.jl:55); the pitch pads each row to 32 B.
 //   * A field with levels (and optionally a batch of right-hand sides) is
 //     slab-major: slab index = batch * mg + level.
 //   * A flux field of one level is the reference's flat vector of nq doubles:
-//     qx (nx+1)×ny column-major, then qy nx×(ny+1) (fluid-domain.jl:201-202).
+//     qx (nx+1)×ny column-major, then qy nx×(ny+1) (fluid-domain.jl:64-65).
 //   * Boundary vectors (Γbc / ψbc) use the reference's segment offsets
 //     LEFT = 0, RIGHT = ny+1, BOT = 2(ny+1), TOP = 2(ny+1)+nx+1
-//     (fluid-domain.jl:205-206); element v of a segment belongs to the edge
+//     (fluid-domain.jl:68-69); element v of a segment belongs to the edge
 //     vertex v (0 … nx or 0 … ny).
 #pragma once
 
@@ -198,8 +198,8 @@ void set_global_error(const char* msg);
 void dst_plan_destroy(DstPlan* p);
 
 // Spectral divisor applied between the two y-transforms of a Poisson solve:
-//   DELTA: w ← (w / Λ) · scale                       (Δ⁻¹, laplacian.jl:180-197)
-//   AINV:  w ← (w / (1 + Λ·dt / den[lev])) · scale    (A⁻¹, laplacian.jl:217-227)
+//   DELTA: w ← (w / Λ) · scale                       (Δ⁻¹, laplacian.jl:24-41)
+//   AINV:  w ← (w / (1 + Λ·dt / den[lev])) · scale    (A⁻¹, laplacian.jl:61-71)
 enum SpecMode { SPEC_DELTA = 0, SPEC_AINV = 1 };
 struct SpecParams {
     int mode;
@@ -239,23 +239,6 @@ struct XPassArgs {
 };
 cudaError_t launch_dst_x(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st);
 
-// One FP32 correction solve of a whole square level in one cluster launch
-// (cluster_solve.cuh): r → x-DST, y-DST, divide, y-DST, x-DST → emit.
-//   XEMIT_ADD      out += d (and dstore = d, FP32, when set)
-//   XEMIT_ACC_SUB  aux += d; out −= aux
-struct ClusterSolveArgs {
-    const float* r; SlabMap rmap;        // FP32 right-hand side (a refinement residual)
-    const float* dc; SlabMap dcmap;      // FP32 correction of the coarser level: its edge terms are added, or null
-    double* out; SlabMap out_map;
-    double* aux; SlabMap aux_map;
-    float* dstore; SlabMap dstore_map;
-    SpecParams sp;
-    int emit;
-};
-bool cluster_solve_supported(int nx, int ny);
-cudaError_t cluster_init_attributes(int N);  // cudaErrorNotSupported when the device cannot place the cluster
-cudaError_t launch_cluster_solve(const Geom& g, const DstPlan& p, const ClusterSolveArgs& a, int nslabs,
-                                 cudaStream_t st);
 
 // FP64 residual of a refinement sweep, stored in FP32 (stencil.cu):
 //   RESID_LAP  r = b + apply_bc!(get_bc!(coarse)) − L x    (vort2flux! levels)

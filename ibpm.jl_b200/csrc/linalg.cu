@@ -1,5 +1,5 @@
 // Dense FP64 inverse of the Schur complement B on the device.  The reference
-// forms inv(B) with LAPACK (src/fluid-operators/laplacian.jl:274); B built
+// forms inv(B) with LAPACK (src/fluid-operators/laplacian.jl:118); B built
 // through the nested-grid vort2flux is not symmetric (its relative asymmetry is
 // 1e-6 … 1e-4 on the configurations tested), so a Cholesky factor would change
 // the solution well above round-off.  This is Gauss–Jordan elimination with

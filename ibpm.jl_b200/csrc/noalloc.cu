@@ -8,7 +8,7 @@
 // side and the result buffer; the one intermediate slab of the solve and the
 // transform tables live in file-scope __device__ arrays of fixed size, which
 // every GPU that loads the library holds until the process exits
-// (2.1 MB + 48 KB).
+// (2.1 MB + 104 KB).
 #include "../../include/ibpm_gpu.h"
 #include "ibpm_internal.cuh"
 
@@ -21,20 +21,30 @@ namespace {
 
 constexpr int kMaxN = 512;                                         // nx, ny <= 512
 constexpr size_t kSlabDoubles = (size_t)(kMaxN - 1) * kMaxN;       // (ny-1) rows of pitch nx
-constexpr size_t kTableDoubles = 6 * (size_t)kMaxN;                // FP64 + FP32 tables of one length
+// The supported lengths, each with a fixed block of 6N doubles (FP64 and
+// FP32 tables of one length) at a fixed offset: 6 * 2168 doubles in all.
+constexpr int kLengths[] = {32, 64, 128, 192, 200, 256, 384, 400, 512};
+constexpr int kNumLengths = sizeof(kLengths) / sizeof(kLengths[0]);
+constexpr size_t table_offset(int k) { return k == 0 ? 0 : table_offset(k - 1) + 6 * (size_t)kLengths[k - 1]; }
+constexpr size_t kTableDoubles = table_offset(kNumLengths);
 
 __device__ __align__(256) double g_noalloc_slab[kSlabDoubles];
-__device__ __align__(256) double g_noalloc_tables[2 * kTableDoubles];  // x tables, then y tables
+__device__ __align__(256) double g_noalloc_tables[kTableDoubles];
 
 struct DeviceScratch {
     bool ready = false;
     double* slab = nullptr;    // device address of g_noalloc_slab on this device
     double* tables = nullptr;  // device address of g_noalloc_tables on this device
-    int nx = 0, ny = 0;        // lengths the tables currently hold
 };
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
 DeviceScratch g_scratch[kMaxDevices];
+
+int length_index(int N) {
+    for (int k = 0; k < kNumLengths; ++k)
+        if (kLengths[k] == N) return k;
+    return -1;
+}
 
 int noalloc_fail(int code, const std::string& msg) {
     set_global_error(msg.c_str());
@@ -48,7 +58,7 @@ extern "C" int ibpm_lap_inv_noalloc(int32_t nx, int32_t ny, const double* rhs, d
     if (nx > kMaxN || ny > kMaxN)
         return noalloc_fail(IBPM_ERR_INVALID, "ibpm_lap_inv_noalloc: nx and ny must be at most 512 (got " +
                                                   std::to_string(nx) + " x " + std::to_string(ny) + ")");
-    if (!dst_supported(nx) || !dst_supported(ny))
+    if (length_index(nx) < 0 || length_index(ny) < 0)
         return noalloc_fail(IBPM_ERR_UNSUPPORTED,
                             "ibpm_lap_inv_noalloc: nx and ny must be one of 32, 64, 128, 192, 200, 256, 384, "
                             "400, 512");
@@ -69,25 +79,18 @@ extern "C" int ibpm_lap_inv_noalloc(int32_t nx, int32_t ny, const double* rhs, d
         e = cudaGetSymbolAddress(reinterpret_cast<void**>(&ds.tables), g_noalloc_tables);
         if (e != cudaSuccess)
             return noalloc_fail(IBPM_ERR_CUDA, std::string("cudaGetSymbolAddress(tables): ") + cudaGetErrorString(e));
-        for (int N : {32, 64, 128, 192, 200, 256, 384, 400, 512}) {
-            e = dst_init_attributes(N);
+        // Every supported length's tables, once: later calls (and a graph
+        // that captured one) find them in place, whatever sizes ran between.
+        for (int k = 0; k < kNumLengths; ++k) {
+            e = dst_init_attributes(kLengths[k]);
+            if (e == cudaSuccess) e = dst_tables_build(kLengths[k], ds.tables + table_offset(k), st);
             if (e != cudaSuccess)
-                return noalloc_fail(IBPM_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(e));
+                return noalloc_fail(IBPM_ERR_CUDA, std::string("set-up: ") + cudaGetErrorString(e));
         }
         ds.ready = true;
     }
-    double* tx = ds.tables;
-    double* ty = ds.tables + kTableDoubles;
-    if (ds.nx != nx) {
-        e = dst_tables_build(nx, tx, st);
-        if (e != cudaSuccess) return noalloc_fail(IBPM_ERR_CUDA, std::string("tables: ") + cudaGetErrorString(e));
-        ds.nx = nx;
-    }
-    if (ds.ny != ny) {
-        e = dst_tables_build(ny, ty, st);
-        if (e != cudaSuccess) return noalloc_fail(IBPM_ERR_CUDA, std::string("tables: ") + cudaGetErrorString(e));
-        ds.ny = ny;
-    }
+    double* tx = ds.tables + table_offset(length_index(nx));
+    double* ty = ds.tables + table_offset(length_index(ny));
     const Geom g = make_geom(nx, ny, 1);
     const DstPlan px = dst_plan_at(tx, nx), py = dst_plan_at(ty, ny);
     // Every slab element that the transforms read (columns < nx-1) is written
@@ -102,7 +105,7 @@ extern "C" int ibpm_lap_inv_noalloc(int32_t nx, int32_t ny, const double* rhs, d
     a.nslabs = 1; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_PLAIN; a.emit = XEMIT_STORE;
     SpecParams sp{};
     sp.mode = SPEC_DELTA;
-    sp.scale = 1.0 / (4.0 * nx * ny);  // laplacian.jl:194
+    sp.scale = 1.0 / (4.0 * nx * ny);  // get_lap_inv, laplacian.jl:38
     if ((e = launch_dst_x(g, px, a, st)) != cudaSuccess ||
         (e = launch_dst_y(g, py, px, ds.slab, m, 1, sp, st)) != cudaSuccess ||
         (e = launch_dst_x(g, px, a, st)) != cudaSuccess)

@@ -14,7 +14,7 @@ namespace ibpm {
 //   rhs  = A Γ + β1 dt N + β2 dt Nprev + rhsbc  (timestepping.jl:111-118)
 // A Γ is evaluated as the 5-point stencil Γ + c (Σ neighbours − 4Γ), c =
 // dt/(2 Re hc²), with zero Dirichlet edges: the operator the reference applies
-// through two DSTs with the eigenvalues 1 − Λ c (laplacian.jl:229-232), whose
+// through two DSTs with the eigenvalues 1 − Λ c (laplacian.jl:73-76), whose
 // eigenvectors are exactly the DST-I basis.
 // ---------------------------------------------------------------------------
 // LIN: the linearised problem's term (nonlinear.jl:45-65, 144-163),
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
     const int i = i0 + 1, j = j0 + 1;  // Julia Γ index
     double N;
     if constexpr (!LIN) {
-        // C' fq (rot!, curl.jl:300-312) scaled by 1/(4 hc²)
+        // C' fq (rot!, curl.jl:22-34) scaled by 1/(4 hc²)
         N = ((fqxJ(i + 1, j) - fqxJ(i + 1, j + 1)) + (fqyJ(i + 1, j + 1) - fqyJ(i, j + 1))) * a.nl_scale[lev];
     } else {
         const double* GB = a.GB + a.Gmap.off(lev);
@@ -166,10 +166,10 @@ cudaError_t launch_coarsify(const Geom& g, double* G, SlabMap fine_map, SlabMap 
 }
 
 // ---------------------------------------------------------------------------
-// Multigrid curl (curl.jl:359-394): q = C ψ with edge streamfunction from
+// Multigrid curl (curl.jl:81-116): q = C ψ with edge streamfunction from
 // ψbc = get_bc!(ψ[lev+1]) (zero on the coarsest level).  Reproduces the
 // reference exactly, including the bottom row of x-fluxes reading ψbc[(B-1)+i]
-// (curl.jl:370), i.e. edge vertex i-2, where the top row reads vertex i-1.
+// (curl.jl:92), i.e. edge vertex i-2, where the top row reads vertex i-1.
 // One thread per flux element; blockIdx.y = batch × levels.
 // ---------------------------------------------------------------------------
 __global__ void curl_kernel(CurlArgs a, Geom g) {
@@ -215,8 +215,8 @@ cudaError_t launch_curl(const Geom& g, const CurlArgs& a, cudaStream_t st) {
 // Residual of one refinement sweep of a Poisson-type solve, in FP64, stored in
 // FP32 (it is small: the change of the solution since its previous solve).
 // L x = 4x − Σ neighbours with zero Dirichlet edges is the operator the DST-I
-// solve with Λ inverts (laplacian.jl:170-197); apply_bc!(get_bc!(coarse)) is
-// the edge term of a vort2flux! level (curl.jl:429-436, mg-utils.jl:7-60).
+// solve with Λ inverts (laplacian.jl:14-41); apply_bc!(get_bc!(coarse)) is
+// the edge term of a vort2flux! level (curl.jl:151-158, mg-utils.jl:7-60).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) resid_kernel(ResidArgs a, Geom g) {
     pdl_wait();

@@ -8,12 +8,21 @@
 # state between calls; `prob.sync_fields = true` copies Γ, ψ, q and the
 # nonlinear terms back after every step (parity runs), otherwise only CD, CL
 # and F̃b come back and `sync!(state, prob)` pulls the fields on demand.
+# What run_sim! reads besides advance! is served from the device too:
+# compute_cfl (src/ibpm.jl:83-88) pulls the fine-level flux first, and
+# save_data! (src/timestepping/save_info.jl:93-106) pulls the whole state
+# before any step whose time it saves, so neither sees stale fields.
+# `prob.scheme` is the reference's AB2(dt) (models.jl:70-72) and `prob.model`
+# carries the grid, bodies, Re, freestream and the q5 work array that
+# compute_cfl's generic method uses, so `ibpm.IBState(prob)` builds a state
+# for a GPU problem as it does for a reference one (state-types.jl:25-47; its
+# base_flux! call takes the device's base flux).
 module IBPMGPU
 
 using ..ibpm: ibpm, IBState, AbstractIBProblem, MultiGrid, RigidBody, Static, MovingGrid, MotionFunction,
-              MotionType, get_body_info
+              MotionType, get_body_info, AB2, AdamsBashforth
 
-export IBProblemGPU, sync!, push!, adjoint_run, set_vorticity!, set_transform_plan!
+export IBProblemGPU, sync!, push_state!, adjoint_run, set_vorticity!, set_transform_plan!
 
 const LIB = get(ENV, "IBPM_GPU_LIB", joinpath(@__DIR__, "..", "lib", "libibpm_gpu.so"))
 
@@ -47,6 +56,10 @@ mutable struct IBProblemGPU <: AbstractIBProblem
     sync_fields::Bool
     motion::Union{Nothing, MovingGrid}
     body_motions::Union{Nothing, Vector{MotionFunction}}
+    # the IBProblem fields that run_sim!'s helpers read (problem-types.jl:23-28):
+    # model.grid, model.bodies, model.Re, model.freestream, model.work.q5; scheme.dt
+    model::NamedTuple
+    scheme::AdamsBashforth
 end
 
 lasterr(h) = unsafe_string(ccall((:ibpm_last_error, LIB), Cstring, (Ptr{Cvoid},), h))
@@ -57,10 +70,12 @@ check(rc, h) = rc == 0 || error("libibpm_gpu error $rc: $(lasterr(h))")
                  precision=:fp64, refine_sweeps=1)
 
 GPU counterpart of `IBProblem(grid, bodies, dt, Re; freestream)`
-(src/pre-processing/problem-types.jl:188-199) for `RigidBody{Static}` bodies,
+(src/pre-processing/problem-types.jl:23-41) for `RigidBody{Static}` bodies,
 or one `RigidBody{MovingGrid}` (its base flux is recomputed from the motion at
-every step's t, timestepping.jl:41-43, 273-318).  The freestream functions are
-evaluated at t = 0, as IBState's base_flux! does for static bodies.
+every step's t, timestepping.jl:41-43, 273-318).  For static bodies the
+freestream functions are evaluated at t = 0 only, as the reference does: its
+base flux is set once when the IBState is built (state-types.jl:45) and
+advance! updates it only for a MovingGrid (timestepping.jl:41-43).
 `precision = :fp32_refined` runs the sine transforms in FP32 with
 FP64-residual refinement of every Poisson solve.
 """
@@ -86,7 +101,8 @@ function IBProblemGPU(grid::MultiGrid, bodies::Vector{<:RigidBody}, dt::Float64,
     body_motions = mt == MotionFunction ? MotionFunction[b.motion for b in bodies] : nothing
     mt in (Static, MovingGrid, MotionFunction) ||
         error("IBProblemGPU: bodies must be Static, one MovingGrid, or all MotionFunction")
-    p = IBProblemGPU(h[], grid, length(bodies), dt, sync_fields, motion, body_motions)
+    model = (grid=grid, bodies=bodies, Re=Re, freestream=freestream, work=(q5=zeros(grid.nq),))
+    p = IBProblemGPU(h[], grid, length(bodies), dt, sync_fields, motion, body_motions, model, AB2(dt))
     finalizer(p) do x
         x.handle == C_NULL || ccall((:ibpm_destroy, LIB), Cint, (Ptr{Cvoid},), x.handle)
         x.handle = C_NULL
@@ -111,8 +127,23 @@ motion_row(m::MovingGrid, t::Float64) = Float64[m.U(t), m.V(t), m.θ(t), m.θ̇(
 motion_row(m::MotionFunction, t::Float64) =
     Float64[m.xc[1](t), m.xc[2](t), m.xc[3](t), m.uc[1](t), m.uc[2](t), m.uc[3](t)]
 
+"""
+    base_flux!(state, prob::IBProblemGPU, t)
+
+The base flux q0 that the device uses (base_flux!, timestepping.jl:228-233,
+252-270): uniform per level for static bodies, that of the last step's motion
+for a MovingGrid.  `ibpm.IBState(prob)` calls it at construction.
+"""
+function ibpm.base_flux!(state::IBState, prob::IBProblemGPU, t::Float64)
+    rc = ccall((:ibpm_get_state, LIB), Cint,
+               (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+                Ptr{Float64}, Ptr{Float64}),
+               prob.handle, C_NULL, C_NULL, state.q0, C_NULL, C_NULL, C_NULL, C_NULL)
+    check(rc, prob.handle)
+end
+
 "Copy every IBState field to the device (the reference's column-major layouts)."
-function push!(state::IBState, prob::IBProblemGPU)
+function push_state!(state::IBState, prob::IBProblemGPU)
     rc = ccall((:ibpm_set_state, LIB), Cint,
                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
                 Ptr{Float64}, Ptr{Float64}),
@@ -129,6 +160,38 @@ function sync!(state::IBState, prob::IBProblemGPU)
                prob.handle, state.Γ, state.q, state.q0, state.ψ, state.nonlin[1], state.nonlin[2],
                state.F̃b)
     check(rc, prob.handle)
+end
+
+"""
+    compute_cfl(state, prob::IBProblemGPU)
+
+The reference's CFL number max|q₁|·Δt/Δx (src/ibpm.jl:83-88) from the device's
+fine-level flux, which is copied into `state.q[:, 1]` first.
+"""
+function ibpm.compute_cfl(state::IBState, prob::IBProblemGPU)
+    g = prob.model_grid
+    qall = zeros(g.nq, g.mg)
+    rc = ccall((:ibpm_get_state, LIB), Cint,
+               (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+                Ptr{Float64}, Ptr{Float64}),
+               prob.handle, C_NULL, qall, C_NULL, C_NULL, C_NULL, C_NULL, C_NULL)
+    check(rc, prob.handle)
+    state.q .= qall
+    return maximum(abs, @view state.q[:, 1]) * prob.scheme.dt / g.h
+end
+
+"""
+    save_data!(tnow, t, prob::IBProblemGPU, state, data)
+
+The reference's save_data! (src/timestepping/save_info.jl:93-106), after
+copying the device state into `state` whenever one of `data`'s save times
+is `tnow` (the same test the reference applies), so a saved state — the
+restart state by default — is never stale.
+"""
+function ibpm.save_data!(tnow, t, prob::IBProblemGPU, state, data)
+    saves = any(j -> sum(@. (abs(data[j].t - tnow) + 1.0) ≈ 1.0) > 0, 1:length(data))
+    saves && !prob.sync_fields && sync!(state, prob)
+    return invoke(ibpm.save_data!, Tuple{Any, Any, Any, Any, Any}, tnow, t, prob, state, data)
 end
 
 """
@@ -163,7 +226,7 @@ end
     set_vorticity!(prob, ω)
 
 Start state from a finest-level vorticity field ω ((nx-1)×(ny-1)): Γ = h²ω on
-level 1, zero elsewhere and zero history, then vort2flux! (curl.jl:411-443)
+level 1, zero elsewhere and zero history, then vort2flux! (curl.jl:133-165)
 makes ψ and q consistent.  This is the start state whose gradient
 `adjoint_run` returns as `grad_omega0`.
 """
@@ -188,7 +251,7 @@ and over several (`multi`): `:latency` (radix 4, N/4 threads per line pair,
 the shortest chain per launch) or `:throughput` (radix 8, N/8 threads, fewer
 instructions); `multi` may also be `:auto` (the throughput plan for launches
 of 16 or more slabs, else `single`).  No counterpart in the reference, whose FFTW plans are fixed
-(src/fluid-operators/laplacian.jl:30-39).
+(src/fluid-operators/dst-inversion.jl:10-20).
 """
 function set_transform_plan!(prob::IBProblemGPU; single::Symbol=:latency, multi::Symbol=:auto)
     code(s) = s === :latency ? Int32(0) : s === :throughput ? Int32(1) : s === :auto ? Int32(2) :

@@ -3,16 +3,16 @@
 The reference's user-facing pieces for the static-body time step are kept,
 with the same names and argument meanings:
 
-* ``make_grid(h, boundary, mg)``       src/fluid-domain/fluid-domain.jl:181-210
+* ``make_grid(h, boundary, mg)``       src/fluid-domain/fluid-domain.jl:44-73
 * ``make_cylinder``, ``make_plate``, ``make_naca``
                                        src/structure-domain/sample-bodies.jl:17-134
 * ``IBProblem(grid, bodies, dt, Re, freestream=...)``
-                                       src/pre-processing/problem-types.jl:188-199
+                                       src/pre-processing/problem-types.jl:23-41
 * ``MovingGrid(U, V, theta, theta_dot)`` src/structure-domain/motion-types.jl:40-48
 * ``MotionFunction(xc, uc)``            src/structure-domain/motion-types.jl:13-17
-* ``IBState(prob)``                    src/pre-processing/state-types.jl:271-293
+* ``IBState(prob)``                    src/pre-processing/state-types.jl:25-47
 * ``advance(state, prob, t)``          advance!(state, prob, t), src/timestepping/timestepping.jl:35-67
-* ``vort2flux(state, prob)``           vort2flux!(ψ, q, Γ, model, mg), src/fluid-operators/curl.jl:411-443
+* ``vort2flux(state, prob)``           vort2flux!(ψ, q, Γ, model, mg), src/fluid-operators/curl.jl:133-165
 
 All arrays use the reference's shapes and column-major layouts (``order='F'``
 views are not needed: ``state.Gamma`` is the (nΓ, mg) matrix flattened by
@@ -191,7 +191,7 @@ def _ptr(a):
 # --------------------------------------------------------------------------
 @dataclass
 class MultiGrid:
-    """fluid-domain.jl:147-162."""
+    """fluid-domain.jl:10-25."""
     nx: int
     ny: int
     mg: int
@@ -214,7 +214,7 @@ class MultiGrid:
 
 
 def make_grid(h, boundary, mg=1):
-    """fluid-domain.jl:181-210: nx = round(len/h), ny = round(ylen nx/len), h = len/nx."""
+    """fluid-domain.jl:44-73: nx = round(len/h), ny = round(ylen nx/len), h = len/nx."""
     offx = -boundary[0]
     offy = -boundary[2]
     ln = boundary[1] - boundary[0]
@@ -330,7 +330,7 @@ class IBProblem:
 
     ``freestream`` = (Ux, Uy, inclination): constants or callables of t,
     evaluated at t = 0 as the reference's IBState does for static bodies
-    (state-types.jl:291, timestepping.jl:252-270).  The handle owns the device
+    (state-types.jl:45, timestepping.jl:252-270).  The handle owns the device
     state; ``IBState`` objects are host mirrors of it.
 
     ``precision``: "fp64" (the reference's arithmetic) or "fp32_refined"
@@ -431,7 +431,7 @@ class IBProblem:
         self._check(self.lib.ibpm_set_base_state(self.handle, _ptr(G), _ptr(q)))
 
     def binv(self):
-        """prob.Binv (laplacian.jl:274) as an (nf, nf) array."""
+        """prob.Binv (laplacian.jl:118) as an (nf, nf) array."""
         out = np.empty((self.nf, self.nf), order="F")
         self._check(self.lib.ibpm_get_binv(self.handle, out.ctypes.data_as(_DP)))
         return out
@@ -441,7 +441,7 @@ class IBProblem:
 
 
 class IBState:
-    """Host mirror of IBState (state-types.jl:253-268): q, q0 (nq, mg); Γ, ψ,
+    """Host mirror of IBState (state-types.jl:7-22): q, q0 (nq, mg); Γ, ψ,
     nonlin[k] (nΓ, mg); F̃b (nf, 1); CD, CL per body — all column-major."""
 
     def __init__(self, prob):
@@ -587,11 +587,34 @@ def transform_plan(prob):
     return a.value, b.value
 
 
+def _field_shapes(prob):
+    g = prob.grid
+    return {"Gamma": (g.nGamma, g.mg), "q": (g.nq, g.mg), "q0": (g.nq, g.mg), "psi": (g.nGamma, g.mg),
+            "nonlin": (g.nGamma, g.mg), "Fb": (prob.nf, 1)}
+
+
+def _checked(prob, name, a, writable=False):
+    """``a`` as the library reads or writes it: float64, column-major, of the
+    field's shape.  A wrong shape raises (the C ABI takes bare pointers and
+    cannot tell)."""
+    shape = _field_shapes(prob)[name]
+    a = np.asarray(a)
+    if a.ndim == 1 and shape[1] == 1:
+        a = a.reshape(shape, order="F")
+    if a.shape != shape:
+        raise IBPMError(IBPM_ERR_INVALID, "state.%s must have shape %s, not %s" % (name, shape, a.shape))
+    if writable and not (a.dtype == np.float64 and a.flags.f_contiguous and a.flags.writeable):
+        raise IBPMError(IBPM_ERR_INVALID, "state.%s must be a writable column-major float64 array" % name)
+    return a if writable else np.asfortranarray(a, dtype=np.float64)
+
+
 def pull_state(state, prob):
     """Copy the device state into ``state``."""
-    prob._check(prob.lib.ibpm_get_state(prob.handle, _ptr(state.Gamma), _ptr(state.q), _ptr(state.q0),
-                                        _ptr(state.psi), _ptr(state.nonlin[0]), _ptr(state.nonlin[1]),
-                                        _ptr(state.Fb)))
+    dst = [_checked(prob, "Gamma", state.Gamma, True), _checked(prob, "q", state.q, True),
+           _checked(prob, "q0", state.q0, True), _checked(prob, "psi", state.psi, True),
+           _checked(prob, "nonlin", state.nonlin[0], True), _checked(prob, "nonlin", state.nonlin[1], True),
+           _checked(prob, "Fb", state.Fb, True)]
+    prob._check(prob.lib.ibpm_get_state(prob.handle, *[_ptr(a) for a in dst]))
 
 
 def push_state(state, prob, fields=("Gamma", "q", "q0", "psi", "nonlin", "Fb")):
@@ -599,7 +622,7 @@ def push_state(state, prob, fields=("Gamma", "q", "q0", "psi", "nonlin", "Fb")):
     f = set(fields)
 
     def arr(name, a):
-        return np.asfortranarray(a, dtype=np.float64) if name in f else None
+        return _checked(prob, name, a) if name in f else None
 
     keep = [arr("Gamma", state.Gamma), arr("q", state.q), arr("q0", state.q0), arr("psi", state.psi),
             arr("nonlin", state.nonlin[0]), arr("nonlin", state.nonlin[1]), arr("Fb", state.Fb)]
@@ -638,7 +661,10 @@ def advance(state, prob, t=0.0, nsteps=1):
         state.CL[:] = cl[-1]
     if prob.sync_fields:
         pull_state(state, prob)
-    prob._check(rc)
+    if rc != IBPM_OK:
+        err = IBPMError(rc, prob.lib.ibpm_last_error(prob.handle).decode())
+        err.CD, err.CL = cd, cl     # the histories up to the failure (non-finite rows included)
+        raise err
     return cd, cl
 
 
@@ -659,9 +685,17 @@ def vort2flux(state, prob):
 
 def run_sim(t, state, prob):
     """run_sim! of src/ibpm.jl:90-106 without logging: one step per entry of
-    ``t``; stops (like the reference) on a non-finite lift coefficient."""
-    cd, cl = advance(state, prob, np.asarray(t, dtype=np.float64), nsteps=len(t))
-    return cd, cl
+    ``t``.  Like the reference (src/ibpm.jl:95-97) it stops quietly at the
+    first step whose lift coefficient is not finite: the histories returned
+    end with that step's row."""
+    try:
+        return advance(state, prob, np.asarray(t, dtype=np.float64), nsteps=len(t))
+    except IBPMError as e:
+        if e.code != IBPM_ERR_NONFINITE:
+            raise
+        bad = np.flatnonzero(~np.all(np.isfinite(e.CL), axis=1))
+        last = int(bad[0]) + 1 if bad.size else len(e.CL)
+        return e.CD[:last], e.CL[:last]
 
 
 # --------------------------------------------------------------------------

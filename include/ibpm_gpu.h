@@ -47,8 +47,8 @@ typedef struct ibpm_handle ibpm_handle;
 
 /*
  * Problem description: the data of IBProblem(grid, bodies, dt, Re; freestream)
- * (src/pre-processing/problem-types.jl:188-199) for RigidBody{Static} bodies.
- * Grid fields are those of make_grid (src/fluid-domain/fluid-domain.jl:181-210)
+ * (src/pre-processing/problem-types.jl:23-41) for RigidBody{Static} bodies.
+ * Grid fields are those of make_grid (src/fluid-domain/fluid-domain.jl:44-73)
  * after its rounding: h = len/nx.  nx and ny must be multiples of 4
  * (get_bc!/coarsify! of src/fluid-operators/mg-utils.jl need nx/4, ny/4).
  */
@@ -76,9 +76,9 @@ const char* ibpm_version(void);
 /*
  * Build a problem on the device: grid tables, the regularisation weights of E
  * (interface-coupling.jl:72-137), the Schur complement B column by column with
- * B_times! (laplacian.jl:254-275, 299-325) and its inverse.  Replaces
- * IBProblem(...) (problem-types.jl:188-199).  The state starts as IBState(prob)
- * (state-types.jl:271-293): zeros, with the uniform base flux q0.
+ * B_times! (laplacian.jl:98-119, 143-169) and its inverse.  Replaces
+ * IBProblem(...) (problem-types.jl:23-41).  The state starts as IBState(prob)
+ * (state-types.jl:25-47): zeros, with the uniform base flux q0.
  */
 int ibpm_create(const ibpm_problem_desc* desc, ibpm_handle** out);
 
@@ -94,7 +94,7 @@ int ibpm_sizes(const ibpm_handle* h, int64_t* nGamma, int64_t* nq, int32_t* mg,
 
 /*
  * Copy a state in.  Any pointer may be NULL (field left unchanged).  The
- * layouts are IBState's (state-types.jl:253-268).  q0 must be uniform per
+ * layouts are IBState's (state-types.jl:7-22).  q0 must be uniform per
  * level and component, as base_flux! makes it for static bodies
  * (timestepping.jl:252-270); anything else returns IBPM_ERR_UNSUPPORTED.
  * On a moving grid q0 is ignored: every step recomputes it.
@@ -198,13 +198,13 @@ int ibpm_advance_bodies(ibpm_handle* h, int32_t nsteps, const double* motion,
 int ibpm_get_body_points(ibpm_handle* h, double* xb, double* ub);
 
 /*
- * vort2flux!(state.ψ, state.q, state.Γ, model, mg) (curl.jl:411-443): make ψ
+ * vort2flux!(state.ψ, state.q, state.Γ, model, mg) (curl.jl:133-165): make ψ
  * and q consistent with Γ (coarsifies Γ into the coarse-level centres first).
  */
 int ibpm_vort2flux(ibpm_handle* h);
 
 /* Copy out the precomputed inverse Schur complement (nf×nf, column-major),
- * the reference's prob.Binv (laplacian.jl:274). */
+ * the reference's prob.Binv (laplacian.jl:118). */
 int ibpm_get_binv(ibpm_handle* h, double* Binv);
 
 /* Block until all work queued on the handle's stream is done. */
@@ -213,7 +213,7 @@ int ibpm_sync(ibpm_handle* h);
 /*
  * x = Δ⁻¹ rhs on one (nx-1)×(ny-1) field with zero Dirichlet edges — the
  * operator the reference applies on every level of vort2flux!
- * (src/fluid-operators/laplacian.jl:180-197) — without allocating any device
+ * (src/fluid-operators/laplacian.jl:24-41) — without allocating any device
  * memory.  No counterpart in the reference: it is for callers that cannot call
  * cudaMalloc (a host runtime that owns the device memory through its own pool,
  * an application with a fixed memory budget).  rhs and x are device pointers
@@ -221,11 +221,12 @@ int ibpm_sync(ibpm_handle* h);
  * `stream` (a cudaStream_t, or NULL for the legacy default stream) and the call
  * returns without waiting for it.  Limit: nx, ny <= 512 and in the supported
  * transform lengths; larger sizes return IBPM_ERR_INVALID.  The intermediate
- * slab and transform tables are file-scope device arrays (2.1 MB + 48 KB on
+ * slab and transform tables are file-scope device arrays (2.1 MB + 104 KB on
  * every GPU that loads the library, held until exit), shared by all calls:
  * calls that overlap on the GPU (other streams, other threads) race on them.
- * The first call on a device looks up their device addresses and sets kernel
- * attributes; make that first call before any stream capture.  Errors are
+ * The first call on a device looks up their device addresses, sets kernel
+ * attributes and fills the tables of every supported length (later calls
+ * only read them); make that first call before any stream capture.  Errors are
  * reported by ibpm_last_error(NULL).
  */
 int ibpm_lap_inv_noalloc(int32_t nx, int32_t ny, const double* rhs, double* x, void* stream);
@@ -326,7 +327,7 @@ int ibpm_host_free(void* p);
 const char* ibpm_kernel_name(int32_t k);
 
 /* Plans of the 2-D sine transforms (no counterpart in the reference, which
- * calls FFTW's r2r plans, src/fluid-operators/laplacian.jl:30-39).  A plan
+ * calls FFTW's r2r plans, src/fluid-operators/dst-inversion.jl:10-20).  A plan
  * fixes the FFT factorisation and the threads per line pair:
  *   IBPM_PLAN_LATENCY     radix 4, N/4 threads per line pair: the shortest
  *                         chain per launch, for launches too small to fill

@@ -92,7 +92,7 @@ def apply_bc_T(rbar, fac, g):
 
 
 def coarsify_T(Gbar, g, mg=None):
-    """Transpose of the coarsify chain of vort2flux! (curl.jl:419-421,
+    """Transpose of the coarsify chain of vort2flux! (curl.jl:141-143,
     mg-utils.jl:71-106), in place on Gbar (..., mg, nx-1, ny-1): the centre of
     level l was overwritten by the restriction of level l-1, so its adjoint
     moves to level l-1 and the centre's own adjoint is cleared (coarsest
@@ -116,7 +116,7 @@ def coarsify_T(Gbar, g, mg=None):
 
 
 def rot_T(Gbar, g):
-    """Transpose of rot (C', curl.jl:300-312): Γ̄ → (q̄x, q̄y)."""
+    """Transpose of rot (C', curl.jl:22-34): Γ̄ → (q̄x, q̄y)."""
     nx, ny = g.nx, g.ny
     lead = Gbar.shape[:-2]
     qx = np.zeros(lead + (nx + 1, ny))
@@ -129,7 +129,7 @@ def rot_T(Gbar, g):
 
 
 def curl_mg_T(qxb, qyb, g):
-    """Transpose of curl_mg (curl.jl:359-394, with its bottom-row reading of
+    """Transpose of curl_mg (curl.jl:81-116, with its bottom-row reading of
     ψbc[(B-1)+i]): (q̄x, q̄y) → (ψ̄, ψ̄bc)."""
     nx, ny = g.nx, g.ny
     B, T, L, Rt = g.BOT, g.TOP, g.LEFT, g.RIGHT
@@ -171,7 +171,7 @@ def curl_mg_T(qxb, qyb, g):
 
 def solves_T(qxb, qyb, Lam, g, mg=None):
     """Transpose of the level chain of vort2flux! after its coarsify chain
-    (curl.jl:425-440): flux adjoints of every level (..., mg, ·, ·) → adjoint
+    (curl.jl:147-162): flux adjoints of every level (..., mg, ·, ·) → adjoint
     of the (coarsified) Γ.  Finest level first, the reverse of the forward."""
     mg = g.mg if mg is None else mg
     lead = qxb.shape[:-3]

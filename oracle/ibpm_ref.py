@@ -8,11 +8,11 @@ path (``ibpm.jl_b200``) never calls it and has no CPU fallback.
 It restates, in numpy/scipy, the algorithm of these reference files (paths are
 relative to the IBPM.jl project root):
 
-* ``src/fluid-domain/fluid-domain.jl:181-210``   ``make_grid``
-* ``src/fluid-operators/laplacian.jl:170-245``   eigenvalues, Δ⁻¹, A, A⁻¹, B⁻¹
-* ``src/fluid-operators/dst-inversion.jl:145-156`` ``dst_inv!``
+* ``src/fluid-domain/fluid-domain.jl:44-73``   ``make_grid``
+* ``src/fluid-operators/laplacian.jl:14-89``   eigenvalues, Δ⁻¹, A, A⁻¹, B⁻¹
+* ``src/fluid-operators/dst-inversion.jl:39-50`` ``dst_inv!``
 * ``src/fluid-operators/mg-utils.jl:7-106``      ``get_bc!``, ``apply_bc!``, ``coarsify!``
-* ``src/fluid-operators/curl.jl:300-443``        ``rot!``, ``curl!`` (multigrid), ``vort2flux!``
+* ``src/fluid-operators/curl.jl:22-165``        ``rot!``, ``curl!`` (multigrid), ``vort2flux!``
 * ``src/fluid-operators/nonlinear.jl:17-201``    ``avg_flux``, ``direct_product!``, ``nonlinear!``
 * ``src/interface-coupling/interface-coupling.jl:6-137`` ``δh``, ``setup_reg`` (E, E')
 * ``src/timestepping/timestepping.jl:35-354``    ``advance!`` and its helpers
@@ -33,7 +33,7 @@ column-major ``(nΓ, mg)`` / ``(nq, mg)`` matrices.
 
 The 2-D DST-I is ``scipy.fft.dstn(type=1)``: unnormalised
 ``Y_k = 2 Σ_j X_j sin(π (j+1)(k+1)/(n+1))``, the definition of FFTW's RODFT00
-that the reference plans in ``dst-inversion.jl:116-126``.
+that the reference plans in ``dst-inversion.jl:10-20``.
 """
 from __future__ import annotations
 
@@ -48,7 +48,7 @@ WORKERS = 1  # scipy.fft worker threads; the timed CPU baseline may raise it
 
 
 # --------------------------------------------------------------------------
-# Grid  (fluid-domain.jl:147-210)
+# Grid  (fluid-domain.jl:10-73)
 # --------------------------------------------------------------------------
 @dataclass
 class MultiGrid:
@@ -76,7 +76,7 @@ class MultiGrid:
     def nq(self):
         return self.nu + self.nv
 
-    # BC vector offsets, 0-based starts of each segment (fluid-domain.jl:205-206)
+    # BC vector offsets, 0-based starts of each segment (fluid-domain.jl:68-69)
     @property
     def LEFT(self):
         return 0
@@ -103,7 +103,7 @@ class MultiGrid:
 
 
 def make_grid(h, boundary, mg=1):
-    """fluid-domain.jl:181-210. ``boundary`` = (xmin, xmax, ymin, ymax)."""
+    """fluid-domain.jl:44-73. ``boundary`` = (xmin, xmax, ymin, ymax)."""
     offx = -boundary[0]
     offy = -boundary[2]
     ln = boundary[1] - boundary[0]
@@ -146,22 +146,22 @@ def flux_from_ref(qr, g):
 
 
 # --------------------------------------------------------------------------
-# Spectral solves  (laplacian.jl:170-245, dst-inversion.jl:145-156)
+# Spectral solves  (laplacian.jl:14-89, dst-inversion.jl:39-50)
 # --------------------------------------------------------------------------
 def lap_eigs(g):
-    """laplacian.jl:170-175: Λ[i,j] = -2(cos(πi/nx) + cos(πj/ny) - 2)."""
+    """laplacian.jl:14-19: Λ[i,j] = -2(cos(πi/nx) + cos(πj/ny) - 2)."""
     ci = np.cos(np.pi * np.arange(1, g.nx) / g.nx)
     cj = np.cos(np.pi * np.arange(1, g.ny) / g.ny)
     return -2.0 * (ci[:, None] + cj[None, :] - 2.0)
 
 
 def dst2(x):
-    """2-D RODFT00 over the last two axes (dst-inversion.jl:111-114)."""
+    """2-D RODFT00 over the last two axes (dst-inversion.jl:5-8)."""
     return sfft.dstn(x, type=1, axes=(-2, -1), workers=WORKERS)
 
 
 def dst_inv(b, M, scale):
-    """dst-inversion.jl:145-156: x = S((S b) ./ M .* scale)."""
+    """dst-inversion.jl:39-50: x = S((S b) ./ M .* scale)."""
     w = dst2(b)
     w /= M
     w *= scale
@@ -169,17 +169,17 @@ def dst_inv(b, M, scale):
 
 
 def lap_inv_scale(g):
-    """The scale 1/(4 nx ny) of get_lap_inv (laplacian.jl:194)."""
+    """The scale 1/(4 nx ny) of get_lap_inv (laplacian.jl:38)."""
     return 1.0 / (4 * g.nx * g.ny)
 
 
 def ainv_eigs(Lam, dt, Re, hc):
-    """get_Ainv (laplacian.jl:217-227): Λ̃ = 1 + Λ dt / (2 Re hc²)."""
+    """get_Ainv (laplacian.jl:61-71): Λ̃ = 1 + Λ dt / (2 Re hc²)."""
     return 1.0 + Lam * dt / (2 * Re * hc ** 2)
 
 
 def a_eigs(Lam, dt, Re, hc):
-    """get_A (laplacian.jl:229-232): the divisor 1 ./ (1 - Λ dt / (2 Re hc²))."""
+    """get_A (laplacian.jl:73-76): the divisor 1 ./ (1 - Λ dt / (2 Re hc²))."""
     return 1.0 / (1.0 - Lam * dt / (2 * Re * hc ** 2))
 
 
@@ -236,17 +236,17 @@ def coarsify(Gc, G, g):
 # Curl, rot, vort2flux  (curl.jl)
 # --------------------------------------------------------------------------
 def rot(qx, qy, g):
-    """curl.jl:300-312: Γ = C'q."""
+    """curl.jl:22-34: Γ = C'q."""
     nx, ny = g.nx, g.ny
     return ((qx[..., 1:nx, 0:ny - 1] - qx[..., 1:nx, 1:ny])
             + (qy[..., 1:nx, 1:ny] - qy[..., 0:nx - 1, 1:ny]))
 
 
 def curl_mg(psi, psibc, g):
-    """curl.jl:359-394: q = Cψ with edge values from ``psibc``.
+    """curl.jl:81-116: q = Cψ with edge values from ``psibc``.
 
     Reproduces the reference exactly, including that the bottom row of x-fluxes
-    reads ψbc[(B-1)+i] (curl.jl:370) while the top row reads ψbc[T+i] (:371).
+    reads ψbc[(B-1)+i] (curl.jl:92) while the top row reads ψbc[T+i] (:371).
     """
     nx, ny = g.nx, g.ny
     B, T, L, R = g.BOT, g.TOP, g.LEFT, g.RIGHT
@@ -267,7 +267,7 @@ def curl_mg(psi, psibc, g):
 
 
 def vort2flux(G, Lam, g, mg=None):
-    """curl.jl:411-443: multiscale ψ, q from Γ.  Mutates the coarse-level
+    """curl.jl:133-165: multiscale ψ, q from Γ.  Mutates the coarse-level
     centres of ``G`` (coarsify, :419-421) and returns (ψ, qx, qy).
 
     ``G`` has shape (..., mg, nx-1, ny-1).
@@ -679,7 +679,7 @@ def moving_grid_rates(prob, t):
 
 @dataclass
 class IBProblem:
-    """problem-types.jl:182-200 + models.jl:27-159 for Static bodies."""
+    """problem-types.jl:23-41 + models.jl:27-159 for Static bodies."""
     grid: MultiGrid
     bodies: list
     dt: float
@@ -716,7 +716,7 @@ class IBProblem:
         self.ET = self.E.T.tocsr()
         if self.build_binv:
             self.B = build_B(self)
-            self.Binv = np.linalg.inv(self.B)     # laplacian.jl:274 (LAPACK getrf/getri)
+            self.Binv = np.linalg.inv(self.B)     # laplacian.jl:118 (LAPACK getrf/getri)
         if isinstance(self.motion, MovingGrid):
             assert len(self.bodies) == 1          # models.jl:137, timestepping.jl:277
             self.XX, self.YY = moving_grid_coords(g, self.xc, self.yc)
@@ -795,7 +795,7 @@ def E_apply(qx1, qy1, prob):
 
 
 def build_B(prob, chunk=64):
-    """get_Binv / B_times! (laplacian.jl:254-275, 299-325): column j of B is
+    """get_Binv / B_times! (laplacian.jl:98-119, 143-169): column j of B is
     E · vort2flux(A⁻¹_1 · C'E' e_j)[level-1 flux].  Computed ``chunk`` columns at
     a time (the columns are independent)."""
     g = prob.grid
@@ -815,7 +815,7 @@ def build_B(prob, chunk=64):
 
 @dataclass
 class IBState:
-    """state-types.jl:253-293 (the fields the static step uses)."""
+    """state-types.jl:7-47 (the fields the static step uses)."""
     Gamma: np.ndarray          # (mg, nx-1, ny-1)
     psi: np.ndarray
     qx: np.ndarray             # (mg, nx+1, ny)
@@ -873,7 +873,7 @@ def base_flux(prob, t=0.0):
 
 
 def make_state(prob):
-    """IBState(prob), state-types.jl:271-293."""
+    """IBState(prob), state-types.jl:25-47."""
     g = prob.grid
     sh = (g.mg, g.nx - 1, g.ny - 1)
     q0x, q0y = base_flux(prob, 0.0)

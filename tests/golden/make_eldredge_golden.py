@@ -11,8 +11,8 @@ contiguously.  h5py is not available, so the vectors are read at their data
 offset and identified by content: t is 0:1e-3:10, CD starts at the steady
 flat-plate drag (≈ 0.394) and CL near zero.  Every 10th entry is kept.
 
-Run from the repository root with the reference tree present:
-    python tests/golden/make_eldredge_golden.py
+Run from the repository root with the path of the reference tree:
+    python tests/golden/make_eldredge_golden.py <IBPM.jl checkout>
 """
 import json
 import os
@@ -20,7 +20,6 @@ import sys
 
 import numpy as np
 
-RESULTS = "/root/reference/benchmarks/eldredge/results"
 HERE = os.path.dirname(os.path.abspath(__file__))
 FILES = (("force_jl2.mat", "eldredge_pitch.json", "pitch_maneuver.jl, MovingGrid", 10001),
          ("force_jl1.mat", "eldredge_pitch_motion.json", "pitch_maneuver_motion.jl, MotionFunction", 10000))
@@ -65,10 +64,13 @@ def extract(src, out, what, nkeep):
     print("wrote %s (%d samples)" % (out, sel.size))
 
 
-def main():
+def main(ref_root):
+    results = os.path.join(ref_root, "benchmarks", "eldredge", "results")
     for name, out, what, nkeep in FILES:
-        extract(os.path.join(RESULTS, name), os.path.join(HERE, out), what, nkeep)
+        extract(os.path.join(results, name), os.path.join(HERE, out), what, nkeep)
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_eldredge_golden.py <IBPM.jl checkout>")
+    main(sys.argv[1])

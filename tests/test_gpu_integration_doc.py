@@ -1,23 +1,17 @@
-"""The Python example of INTEGRATION.md, run as written (from the repository
-root): the documented calls stay the library's calls."""
+"""The Python example that the integration guide quotes (tests/integration_example.py),
+run as written: the documented calls stay the library's calls."""
+import runpy
 import os
-import re
 
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def test_python_example_runs(monkeypatch):
-    with open(os.path.join(ROOT, "INTEGRATION.md")) as f:
-        text = f.read()
-    section = text[text.index("## Python"):]
-    code = re.search(r"```python\n(.*?)```", section, re.S).group(1)
-    monkeypatch.chdir(ROOT)
-    ns = {}
-    exec(compile(code, "INTEGRATION.md", "exec"), ns)
+def test_python_example_runs():
+    ns = runpy.run_path(os.path.join(HERE, "integration_example.py"))
     G = ns["G"]
     assert ns["cd"].shape == (1000, 1) and np.all(np.isfinite(ns["cd"]))
     assert np.isfinite(ns["res"].J) and ns["res"].grad_xb.shape == (314, 2)

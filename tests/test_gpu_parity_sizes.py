@@ -1,0 +1,172 @@
+"""GPU against the FP64 oracle at the benchmark workloads' own sizes, through
+the C ABI (the small-grid parity cases are in test_gpu_parity.py):
+
+* vort2flux! (src/fluid-operators/curl.jl:133-165) at every supported
+  transform length from 128 to 2048, two levels, both transform plans;
+* the headline workload, a cylinder at Re = 100 on 512x512 cells x 5 levels
+  from the seeded vortex start, stepped with advance!
+  (src/timestepping/timestepping.jl:35-67): FP64 to 1e-10 on every field and
+  on CD/CL, the FP32-refined form to 1e-6;
+* the adjoint workload's grid (256x256 x 4 levels) against the oracle's
+  discrete adjoint;
+* a NACA member of the batch workload as the batch builds it.
+
+The oracle builds B once per problem (tens of seconds at 512²); the module
+fixtures share it between the tests."""
+import numpy as np
+import pytest
+
+import bench
+from ibpm_cases import rel
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+TOL32 = 1e-6
+LENGTHS = [128, 192, 256, 384, 512, 768, 1024, 2048]
+
+
+def _plans(N):
+    return ["latency", "throughput"] if N < 1024 else ["latency"]
+
+
+@pytest.mark.parametrize("N,plan", [(N, p) for N in LENGTHS for p in _plans(N)])
+def test_vort2flux_every_length(N, plan):
+    import ibpm_gpu as G
+    from oracle import ibpm_ref as R
+    h = 4.0 / N
+    bnd = (-2.0, 2.0, -2.0, 2.0)
+    gg = G.make_grid(h, bnd, 2)
+    gp = G.IBProblem(gg, [G.make_cylinder(0.25, gg.h, 0.1, 0.0, n=8)], 0.01, 100.0)
+    code = G.IBPM_PLAN_LATENCY if plan == "latency" else G.IBPM_PLAN_THROUGHPUT
+    G.set_transform_plan(gp, code, code)
+    og = R.make_grid(h, bnd, 2)
+    rng = np.random.default_rng(N)
+    Gam = rng.standard_normal((2, og.nx - 1, og.ny - 1))
+    st = G.IBState(gp)
+    st.Gamma[:] = R.gamma_to_ref(Gam)
+    G.push_state(st, gp, fields=("Gamma",))
+    G.vort2flux(st, gp)
+    gp.close()
+    psi, qx, qy = R.vort2flux(Gam, R.lap_eigs(og), og)
+    assert rel(st.Gamma, R.gamma_to_ref(Gam)) < 1e-14
+    assert rel(st.psi, R.gamma_to_ref(psi)) < TOL, (N, plan)
+    assert rel(st.q, R.flux_to_ref(qx, qy)) < TOL, (N, plan)
+
+
+# --------------------------------------------------------------------------
+# The headline workload: 512x512 x 5 levels, 314 points, Re = 100, dt = 0.002
+# --------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def headline_oracle():
+    from oracle import ibpm_ref as R
+    g = R.make_grid(bench.H, bench.BOUNDARY, bench.MG)
+    p = R.IBProblem(grid=g, bodies=[R.make_cylinder(0.5, g.h, 0.0, 0.0, n=bench.NB)], dt=bench.DT, Re=bench.RE)
+    st = R.make_state(p)
+    st.Gamma = R.gamma_from_ref(bench.vortex_gamma(g.nx, g.ny, g.mg, g.h, g.offx, g.offy), g)
+    R.refresh_flux(st, p)
+    start = st.copy()
+    nsteps = 10
+    cd, cl = R.run(p, st, nsteps)
+    return dict(prob=p, start=start, end=st, cd=np.asarray(cd), cl=np.asarray(cl), nsteps=nsteps)
+
+
+def _headline_gpu(precision, start, nsteps):
+    import ibpm_gpu as G
+    from ibpm_cases import to_gpu_state
+    g = G.make_grid(bench.H, bench.BOUNDARY, bench.MG)
+    p = G.IBProblem(g, [G.make_cylinder(0.5, g.h, 0.0, 0.0, n=bench.NB)], bench.DT, bench.RE,
+                    freestream=(1.0, 0.0, 0.0), precision=precision)
+    st = G.IBState(p)
+    to_gpu_state(start, st)
+    G.push_state(st, p)
+    cd, cl = G.advance(st, p, 0.0, nsteps=nsteps)
+    G.pull_state(st, p)
+    p.close()
+    return st, cd, cl
+
+
+def _field_errors(st, ost):
+    from oracle import ibpm_ref as R
+    return {"Gamma": rel(st.Gamma, R.gamma_to_ref(ost.Gamma)), "psi": rel(st.psi, R.gamma_to_ref(ost.psi)),
+            "q": rel(st.q, R.flux_to_ref(ost.qx, ost.qy)),
+            "nonlin1": rel(st.nonlin[0], R.gamma_to_ref(ost.nonlin[0])),
+            "nonlin2": rel(st.nonlin[1], R.gamma_to_ref(ost.nonlin[1])),
+            "Fb": rel(st.Fb[:, 0], ost.Fb)}
+
+
+def test_headline_fp64_matches_oracle(headline_oracle):
+    o = headline_oracle
+    st, cd, cl = _headline_gpu("fp64", o["start"], o["nsteps"])
+    errs = _field_errors(st, o["end"])
+    assert all(v < TOL for v in errs.values()), errs
+    assert rel(cd, o["cd"]) < TOL
+    assert rel(cl, o["cl"]) < TOL          # relative to max |CL| of the run
+
+
+def test_headline_fp32_refined_matches_oracle(headline_oracle):
+    o = headline_oracle
+    st, cd, cl = _headline_gpu("fp32_refined", o["start"], o["nsteps"])
+    errs = _field_errors(st, o["end"])
+    assert all(v < TOL32 for v in errs.values()), errs
+    assert rel(cd, o["cd"]) < TOL32
+    assert rel(cl, o["cl"]) < TOL32        # relative to max |CL| of the run
+
+
+# --------------------------------------------------------------------------
+# The adjoint workload's grid: 256x256 x 4 levels, 157 points
+# --------------------------------------------------------------------------
+def test_adjoint_workload_grid_matches_oracle_adjoint():
+    import ibpm_gpu as G
+    from ibpm_cases import to_gpu_state
+    from oracle import ibpm_adjoint as A
+    from oracle import ibpm_ref as R
+    c = bench.ADJ
+    og = R.make_grid(c["h"], bench.BOUNDARY, c["mg"])
+    op = R.IBProblem(grid=og, bodies=[R.make_cylinder(0.5, og.h, 0.0, 0.0, n=c["nb"])], dt=c["dt"], Re=100.0)
+    rng = np.random.default_rng(c["seed"])
+    ost = R.make_state(op)
+    ost.Gamma[0] = og.h ** 2 * c["sigma"] * rng.standard_normal(ost.Gamma[0].shape)
+    R.refresh_flux(ost, op)
+    nsteps, window, k = 6, 3, 3
+    J, Gb, *_ = A.mean_force_gradient(op, ost.copy(), nsteps, window, k=k)
+    gg = G.make_grid(c["h"], bench.BOUNDARY, c["mg"])
+    gp = G.IBProblem(gg, [G.make_cylinder(0.5, gg.h, 0.0, 0.0, n=c["nb"])], c["dt"], 100.0)
+    st = G.IBState(gp)
+    to_gpu_state(ost, st)
+    G.push_state(st, gp)
+    res = G.adjoint_run(gp, nsteps, k, window)
+    gp.close()
+    assert abs(res.J - J) <= 1e-10 * abs(J)
+    assert rel(res.grad_Gamma0, R.gamma_to_ref(Gb)) < 1e-9
+
+
+# --------------------------------------------------------------------------
+# A NACA member of the batch workload (as bench.batch_specs builds it)
+# --------------------------------------------------------------------------
+def test_batch_naca_member_matches_oracle():
+    import ibpm_gpu as G
+    from ibpm_cases import random_state, to_gpu_state
+    from oracle import ibpm_ref as R
+    specs = bench.batch_specs(G)
+    i = next(k for k, s in enumerate(specs) if s["grid"].nx == 128 and len(s["bodies"][0].xb) > 0
+             and not np.allclose(np.hypot(*s["bodies"][0].xb.T), 0.5))
+    s = specs[i]
+    g = s["grid"]
+    body = s["bodies"][0]
+    og = R.make_grid(g.h, (-1.0, 3.0, -2.0, 2.0), g.mg)
+    assert (og.nx, og.ny) == (g.nx, g.ny)
+    op = R.IBProblem(grid=og, bodies=[R.Body(xb=np.array(body.xb), ds=np.array(body.ds))], dt=s["dt"], Re=s["Re"])
+    ost = random_state(op, seed=9)
+    for precision, tol in (("fp64", TOL), ("fp32_refined", TOL32)):
+        gp = G.IBProblem(g, [G.RigidBody(xb=np.array(body.xb), ds=np.array(body.ds))], s["dt"], s["Re"],
+                         precision=precision)
+        st = G.IBState(gp)
+        to_gpu_state(ost, st)
+        G.push_state(st, gp)
+        cd, cl = G.advance(st, gp, 0.0, nsteps=10)
+        G.pull_state(st, gp)
+        gp.close()
+        oref = ost.copy()
+        ocd, ocl = R.run(op, oref, 10)
+        assert rel(cd, ocd) < tol and rel(cl, ocl) < tol, precision
+        assert rel(st.Gamma, R.gamma_to_ref(oref.Gamma)) < tol, precision

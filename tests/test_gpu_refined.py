@@ -60,29 +60,3 @@ def test_refined_rejects_bad_sweeps():
     import ibpm_gpu as G
     with pytest.raises(G.IBPMError):
         gpu_problem("sq64_mg3", precision="fp32_refined", refine_sweeps=99)
-
-
-@pytest.mark.parametrize("name", ["sq64_mg3", "sq64_mg1_plate", "cyl200_mg3"])
-def test_one_launch_level_solve_matches_three_passes(name, monkeypatch):
-    """Square levels can solve each FP32 correction in one cluster launch
-    (IBPM_CLUSTER=1); the three-pass path computes the same refined step.  With
-    two sweeps both reach the FP64 result, so they agree to 1e-10; with one
-    sweep they agree to the FP32 error of one correction."""
-    import ibpm_gpu as G
-    from oracle import ibpm_ref as R
-    op = oracle_problem(name)
-    for sweeps, tol in ((2, 1e-10), (1, 1e-6)):
-        out = []
-        for env in ("1", "0"):
-            monkeypatch.setenv("IBPM_CLUSTER", env)
-            gp = gpu_problem(name, precision="fp32_refined", refine_sweeps=sweeps)
-            ost = random_state(op, seed=21)
-            st = G.IBState(gp)
-            to_gpu_state(ost, st)
-            G.push_state(st, gp)
-            cd, cl = G.advance(st, gp, 0.0, nsteps=15)
-            G.pull_state(st, gp)
-            out.append((cd, st.Gamma.copy(), st.psi.copy()))
-            gp.close()
-        assert rel(out[0][0], out[1][0]) < tol, (name, sweeps)
-        assert rel(out[0][1], out[1][1]) < tol and rel(out[0][2], out[1][2]) < tol, (name, sweeps)

@@ -12,7 +12,7 @@ def grid():
 
 
 def test_make_grid_rounding():
-    # fluid-domain.jl:189-198: nx = round(len/h), ny = round(ylen nx/len), h = len/nx
+    # fluid-domain.jl:52-61: nx = round(len/h), ny = round(ylen nx/len), h = len/nx
     g = R.make_grid(0.02, (-1.5, 6.5, -2.0, 2.0), mg=5)
     assert (g.nx, g.ny) == (400, 200) and g.h == 8.0 / 400
     g = R.make_grid(0.01, (-1.0, 4.12, -2.56, 2.56), mg=5)
@@ -44,7 +44,7 @@ def test_dst_involution(grid):
 
 
 def test_A_spectral_equals_stencil(grid):
-    """A = I - (dt/2Re hc²) C'C applied through DSTs (laplacian.jl:229-232)
+    """A = I - (dt/2Re hc²) C'C applied through DSTs (laplacian.jl:73-76)
     equals the 5-point stencil with zero Dirichlet edges."""
     rng = np.random.default_rng(3)
     G = rng.standard_normal((grid.nx - 1, grid.ny - 1))
