@@ -68,6 +68,14 @@ struct ibpm_handle {
     int cold = kColdSteps;                 // steps left that lack good initial guesses
     float* T32 = nullptr;                  // mg slabs of FP32 transform scratch
     double* Pp = nullptr;                  // A⁻¹C'E'F̃b of the previous step (level 1)
+    // boundary-transfer vort2flux! (bt.cu; mg >= 2): R = get_bc!∘Δ⁻¹∘apply_bc!
+    // (nE × pitch), the edge vectors, the line samples and the edge part of the
+    // x-spectrum of every level, in FP64 and, for FP32_REFINED, in FP32
+    bool bt = false;
+    int bt_k = 0, bt_kp = 0;               // rank of R's basis and its pitch
+    double *btW = nullptr, *btU = nullptr, *btP = nullptr, *btE = nullptr, *btS = nullptr, *btY = nullptr;
+    float *btW32 = nullptr, *btU32 = nullptr, *btP32 = nullptr, *btE32 = nullptr, *btS32 = nullptr,
+          *btY32 = nullptr;
     // linearised problem (ibpm_set_base_state): base Γ, base q, base flux
     bool lin = false;
     double* GB = nullptr;
@@ -154,8 +162,8 @@ void ibpm::set_global_error(const char* msg) { g_create_err = msg ? msg : ""; }
 // Kernel classes reported by ibpm_profile (order of IBPM_KERNEL_* in the header).
 static const char* kKernelNames[] = {"trial_rhs", "dst_x", "dst_y", "coarsify", "curl",
                                      "E_gather", "binv_gemv", "stress", "proj_src", "adjoint",
-                                     "resid", "level_solve"};
-enum { K_RHS = 0, K_DSTX, K_DSTY, K_COARSIFY, K_CURL, K_E, K_GEMV, K_STRESS, K_SRC, K_ADJ, K_RESID, K_LSOLVE,
+                                     "resid", "bt_chain"};
+enum { K_RHS = 0, K_DSTX, K_DSTY, K_COARSIFY, K_CURL, K_E, K_GEMV, K_STRESS, K_SRC, K_ADJ, K_RESID, K_BTCHAIN,
        K_COUNT };
 
 static int prof_pre(ibpm_handle* h, int label, double bytes) {
@@ -330,6 +338,181 @@ static int vort2flux(ibpm_handle* h, double* G, double* psi, long long bstride, 
     return IBPM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Boundary-transfer vort2flux! (ibpm_internal.cuh, bt.cu).  The reference
+// solves the levels one after another, each with the edge values of the next
+// coarser ψ (curl.jl:147-162).  Here every level's interior part Δ⁻¹Γ_ℓ is
+// one multi-level solve; the edge vectors follow from its line samples by the
+// chain e_ℓ = get_bc!(Δ⁻¹Γ_{ℓ+1}) + R e_{ℓ+1} (mg−1 small launches); one
+// y-pass builds every level's edge part from e_ℓ, and one x-pass transforms
+// the sum of both parts.  The result is the reference's ψ and q up to
+// rounding (both parts are the same linear operators applied in another
+// order).
+// ---------------------------------------------------------------------------
+
+// R at create: the get_bc! samples of Δ⁻¹ of a unit source at every edge entry
+// (FP64 solves, `chunk` columns per batch), then its rank-k basis on the host
+// (bt_lowrank); FP32 copies of the basis for FP32_REFINED.  A rank that does
+// not settle (never seen) leaves the handle on the level-by-level chain.
+static int build_bt(ibpm_handle* h) {
+    const Geom& g = h->g;
+    if (g.mg < 2) return IBPM_OK;
+    const int nE = bt_edge_len(g), ep = bt_edge_pitch(g);
+    const int mg = g.mg;
+    const bool f32 = h->prec == IBPM_PREC_FP32_REFINED;
+    int rc;
+    double *R = nullptr, *GB = nullptr;
+    const int chunk = std::min(nE, kBChunk);
+    if ((rc = dalloc(h, &R, (size_t)nE * ep)) || (rc = dalloc(h, &GB, (size_t)g.S * chunk))) {
+        cudaFree(R);
+        return rc;
+    }
+    SlabMap one = levmap(g, 0, 1, g.S);
+    cudaError_t e = cudaMemsetAsync(R, 0, sizeof(double) * nE * ep, h->st);
+    for (int c0 = 0; c0 < nE && rc == IBPM_OK && e == cudaSuccess; c0 += chunk) {
+        const int ncol = std::min(chunk, nE - c0);
+        e = cudaMemsetAsync(GB, 0, sizeof(double) * g.S * ncol, h->st);
+        if (e == cudaSuccess) e = launch_bt_unit_src(g, c0, ncol, GB, g.S, h->st);
+        if (e == cudaSuccess) rc = poisson(h, GB, one, GB, one, GB, one, ncol, SPEC_DELTA, XEMIT_STORE);
+        if (e == cudaSuccess && rc == IBPM_OK) e = launch_bt_gather(g, c0, ncol, GB, g.S, R, h->st);
+    }
+    std::vector<double> Rh((size_t)nE * ep);
+    if (e == cudaSuccess && rc == IBPM_OK)
+        e = cudaMemcpyAsync(Rh.data(), R, sizeof(double) * Rh.size(), cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    cudaFree(GB);
+    cudaFree(R);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(h, IBPM_ERR_CUDA, std::string("R setup: ") + cudaGetErrorString(e));
+    BtLowRank lr;
+    if (bt_lowrank(Rh, nE, ep, std::max(0, mg - 2), 1e-14, std::min(nE, 1024), lr)) return IBPM_OK;
+    h->bt_k = lr.k;
+    h->bt_kp = lr.kp;
+    const size_t nw = (size_t)lr.k * ep, nu = std::max<size_t>(1, lr.U.size()), np = (size_t)(mg - 1) * lr.kp;
+    const size_t slabs = (size_t)g.S * mg, ns = (size_t)bt_sample_len(g) * mg, ne = (size_t)ep * mg;
+    if ((rc = dalloc(h, &h->btW, nw)) || (rc = dalloc(h, &h->btU, nu)) || (rc = dalloc(h, &h->btP, np)) ||
+        (rc = dalloc(h, &h->btE, ne)) || (rc = dalloc(h, &h->btS, ns)) || (rc = dalloc(h, &h->btY, slabs)))
+        return rc;
+    CK(cudaMemcpyAsync(h->btW, lr.W.data(), sizeof(double) * nw, cudaMemcpyHostToDevice, h->st));
+    if (!lr.U.empty())
+        CK(cudaMemcpyAsync(h->btU, lr.U.data(), sizeof(double) * lr.U.size(), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemsetAsync(h->btP, 0, sizeof(double) * np, h->st));
+    CK(cudaMemsetAsync(h->btE, 0, sizeof(double) * ne, h->st));
+    CK(cudaMemsetAsync(h->btS, 0, sizeof(double) * ns, h->st));
+    CK(cudaMemsetAsync(h->btY, 0, sizeof(double) * slabs, h->st));  // the coarsest slab stays zero
+    if (f32) {
+        if ((rc = dalloc(h, &h->btW32, nw)) || (rc = dalloc(h, &h->btU32, nu)) || (rc = dalloc(h, &h->btP32, np)) ||
+            (rc = dalloc(h, &h->btE32, ne)) || (rc = dalloc(h, &h->btS32, ns)) || (rc = dalloc(h, &h->btY32, slabs)))
+            return rc;
+        CK(launch_to_f32(h->btW, h->btW32, (long long)nw, h->st));
+        CK(launch_to_f32(h->btU, h->btU32, (long long)nu, h->st));
+        CK(cudaMemsetAsync(h->btP32, 0, sizeof(float) * np, h->st));
+        CK(cudaMemsetAsync(h->btE32, 0, sizeof(float) * ne, h->st));
+        CK(cudaMemsetAsync(h->btS32, 0, sizeof(float) * ns, h->st));
+        CK(cudaMemsetAsync(h->btY32, 0, sizeof(float) * slabs, h->st));
+    }
+    h->bt = true;
+    return IBPM_OK;
+}
+
+// From the y-pass output Y of every level (x-spectral; FP64 or FP32): the line
+// samples of levels 1 … mg−1, the edge chain down to level 0, and the edge
+// part of every level but the coarsest, by one y-pass, into btY / btY32.
+static int bt_edges(ibpm_handle* h, const void* Y, bool f32) {
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    const long long bs = g.S * mg;
+    const int nE = bt_edge_len(g);
+    const double es = f32 ? 4.0 : 8.0;
+    void* S = f32 ? (void*)h->btS32 : (void*)h->btS;
+    void* E = f32 ? (void*)h->btE32 : (void*)h->btE;
+    LAUNCH(K_BTCHAIN, es * ((double)g.n1 * (g.ny / 2 + 3) + 2.0 * g.n1) * (mg - 1),
+           launch_dst_lines(g, h->px, Y, levmap(g, 1, mg - 1, bs), mg - 1, S, f32 ? 1 : 0, h->st));
+    BtChainArgs a{};
+    a.W = f32 ? (const void*)h->btW32 : (const void*)h->btW;
+    a.U = f32 ? (const void*)h->btU32 : (const void*)h->btU;
+    a.samples = S; a.e = E; a.p = f32 ? (void*)h->btP32 : (void*)h->btP;
+    a.k = h->bt_k; a.kp = h->bt_kp; a.f32 = f32 ? 1 : 0;
+    if (mg > 2) LAUNCH(K_BTCHAIN, es * ((double)h->bt_k * (nE + 2.0 * nE) + (mg - 1.0) * h->bt_kp),
+                       launch_bt_project(g, a, h->st));
+    LAUNCH(K_BTCHAIN, es * ((mg - 2.0) * nE * h->bt_kp + 3.0 * nE * (mg - 1)), launch_bt_expand(g, a, h->st));
+    BtSynth bsy{};
+    bsy.e = E; bsy.sx = f32 ? (const void*)h->px.s32 : (const void*)h->px.s; bsy.nx = g.nx;
+    LAUNCH(K_DSTY, es * g.n1 * g.n2 * (mg - 1),
+           launch_dst_ybc(g, h->py, h->px, f32 ? (void*)h->btY32 : (void*)h->btY, levmap(g, 0, mg - 1, bs), mg - 1,
+                          spec(h, SPEC_DELTA, f32 ? 1 : 0), bsy, h->st));
+    return IBPM_OK;
+}
+
+static int curl_levels(ibpm_handle* h, double* q, int qnlev) {
+    const Geom& g = h->g;
+    CurlArgs ca{};
+    ca.psi = h->psi; ca.psi_map = levmap(g, 0, qnlev);
+    ca.coarse = h->psi; ca.coarse_map = levmap(g, 1, qnlev);
+    ca.q = q; ca.q_bstride = 0; ca.q_lstride = g.nq; ca.q_lev0 = 0;
+    ca.nlev = qnlev; ca.nbatch = 1; ca.mg = g.mg;
+    LAUNCH(K_CURL, 8.0 * ((double)g.n1 * g.n2 + g.nq) * qnlev, launch_curl(g, ca, h->st));
+    return IBPM_OK;
+}
+
+// vort2flux! (FP64) of the handle's field G into h->psi and q (levels < qnlev).
+static int vort2flux_bt(ibpm_handle* h, double* G, double* q, int qnlev) {
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    const long long bs = g.S * mg;
+    const double slab = (double)g.n1 * g.n2;
+    for (int lev = 1; lev < mg; ++lev)
+        LAUNCH(K_COARSIFY, 8.0 * 1.25 * slab,
+               launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), 1, h->st));
+    SlabMap all = levmap(g, 0, mg, bs);
+    XPassArgs a{};
+    a.in = G; a.out = h->rhs; a.in_map = all; a.out_map = all;
+    a.nslabs = mg; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_PLAIN; a.emit = XEMIT_STORE;
+    LAUNCH(K_DSTX, 16.0 * slab * mg, launch_dst_x(g, h->px, a, h->st));
+    LAUNCH(K_DSTY, 16.0 * slab * mg, launch_dst_y(g, h->py, h->px, h->rhs, all, mg, spec(h, SPEC_DELTA), h->st));
+    int rc = bt_edges(h, h->rhs, false);
+    if (rc) return rc;
+    XPassArgs c{};
+    c.in = h->rhs; c.in2 = h->btY; c.in_map = all; c.in2_map = all; c.out = h->psi; c.out_map = all;
+    c.nslabs = mg; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_SUM; c.emit = XEMIT_STORE;
+    LAUNCH(K_DSTX, 24.0 * slab * mg, launch_dst_x(g, h->px, c, h->st));
+    return curl_levels(h, q, qnlev);
+}
+
+// vort2flux! of FP32_REFINED: `nsw` sweeps ψ ← ψ + d, the corrections d of
+// every level from FP64 residuals against the present ψ (all levels read the
+// ψ of before the sweep), r_ℓ = Γ_ℓ + apply_bc!(get_bc!(ψ_{ℓ+1})) − L ψ_ℓ.
+// The corrections satisfy the level chain of vort2flux! themselves,
+// L d_ℓ = r_ℓ + apply_bc!(get_bc!(d_{ℓ+1})), so the boundary transfer solves
+// them in FP32 as above.
+static int vort2flux_refined_bt(ibpm_handle* h, double* G, int nsw, double* q, int qnlev) {
+    const Geom& g = h->g;
+    const int mg = g.mg;
+    const long long bs = g.S * mg;
+    const double slab = (double)g.n1 * g.n2;
+    for (int lev = 1; lev < mg; ++lev)
+        LAUNCH(K_COARSIFY, 8.0 * 1.25 * slab,
+               launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), 1, h->st));
+    SlabMap all = levmap(g, 0, mg, bs);
+    for (int s = 0; s < nsw; ++s) {
+        XPassArgs a{};
+        a.in = G; a.out = h->T32; a.in_map = all; a.out_map = all;
+        a.coarse = h->psi; a.coarse_map = levmap(g, 1, mg, bs);
+        a.aux = h->psi; a.aux_map = all;
+        a.nslabs = mg; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_RES_LAP; a.emit = XEMIT_F32;
+        LAUNCH(K_DSTX, (8.0 + 8.0 + 4.0) * slab * mg, launch_dst_x(g, h->px, a, h->st));
+        LAUNCH(K_DSTY, 8.0 * slab * mg,
+               launch_dst_y(g, h->py, h->px, h->T32, all, mg, spec(h, SPEC_DELTA, 1), h->st));
+        int rc = bt_edges(h, h->T32, true);
+        if (rc) return rc;
+        XPassArgs c{};
+        c.in = h->T32; c.in2 = h->btY32; c.in_map = all; c.in2_map = all; c.out = h->psi; c.out_map = all;
+        c.nslabs = mg; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_F32_SUM; c.emit = XEMIT_ADD;
+        LAUNCH(K_DSTX, (4.0 + 4.0 + 16.0) * slab * mg, launch_dst_x(g, h->px, c, h->st));
+    }
+    return curl_levels(h, q, qnlev);
+}
+
 // One step, reading the state from parity p and leaving it in parity p^1.
 static int enqueue_step_fp64(ibpm_handle* h, int p) {
     const Geom& g = h->g;
@@ -342,7 +525,8 @@ static int enqueue_step_fp64(ibpm_handle* h, int p) {
     SlabMap all = levmap(g, 0, mg);
     int rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg, SPEC_AINV, XEMIT_STORE);
     if (rc) return rc;
-    rc = vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->qs, 0, 0, 1);  // only the level-1 trial flux is read
+    rc = h->bt ? vort2flux_bt(h, Gnew, h->qs, 1)  // only the level-1 trial flux is read
+               : vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->qs, 0, 0, 1);
     if (rc) return rc;
     // --- boundary_forces! (timestepping.jl:154-163) and update_stress! (:330-354)
     LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h),
@@ -354,7 +538,7 @@ static int enqueue_step_fp64(ibpm_handle* h, int p) {
     rc = poisson(h, h->Gsrc, one, h->rhs, one, Gnew, one, 1, SPEC_AINV, XEMIT_SUB);
     if (rc) return rc;
     // --- vort2flux!(state.ψ, state.q, state.Γ) (timestepping.jl:64)
-    return vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->q, 0, 0, mg);
+    return h->bt ? vort2flux_bt(h, Gnew, h->q, mg) : vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->q, 0, 0, mg);
 }
 
 // ---------------------------------------------------------------------------
@@ -395,24 +579,6 @@ static int correction32(ibpm_handle* h, int load, const double* b, const double*
     return IBPM_OK;
 }
 
-// FP64 residual of the levels [lev0, lev0 + nlev) into T32: RESID_LAP with the
-// coarser ψ's edge terms, or RESID_A with c of each level.
-static int resid(ibpm_handle* h, int mode, const double* b, const double* x, int lev0, int nlev, bool one_slab_src) {
-    const Geom& g = h->g;
-    const long long bs = g.S * g.mg;
-    ResidArgs a{};
-    a.b = b; a.bmap = one_slab_src ? levmap(g, 0, 1, g.S) : levmap(g, lev0, nlev, bs);
-    a.x = x; a.xmap = one_slab_src ? levmap(g, 0, 1, g.S) : levmap(g, lev0, nlev, bs);
-    a.coarse = mode == RESID_LAP ? h->psi : nullptr; a.cmap = levmap(g, lev0 + 1, nlev, bs);
-    a.r = h->T32; a.rmap = levmap(g, lev0, nlev, bs);
-    for (int l = 0; l < 8; ++l) a.cA[l] = c_lap(h, l);
-    a.mode = mode; a.mg = g.mg;
-    // the source slab of RESID_A is level 1's: its level index must read as lev0
-    if (one_slab_src) { a.bmap.lev0 = 0; a.bmap.lstride = 0; a.xmap.lstride = 0; }
-    LAUNCH(K_RESID, (8.0 * 2 + 4.0) * g.n1 * g.n2 * nlev, launch_resid(g, a, nlev, h->st));
-    return IBPM_OK;
-}
-
 // vort2flux! with every level's Δ⁻¹ solve refined from the ψ in h->psi.
 static int vort2flux_refined(ibpm_handle* h, double* G, int nsw, double* q, int qnlev) {
     const Geom& g = h->g;
@@ -449,7 +615,8 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
     SlabMap all = levmap(g, 0, mg, bs);
     int rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg, SPEC_AINV, XEMIT_STORE);
     if (rc) return rc;
-    rc = vort2flux_refined(h, Gnew, nsw, h->qs, 1);  // only the level-1 trial flux is read
+    rc = h->bt ? vort2flux_refined_bt(h, Gnew, nsw, h->qs, 1)  // only the level-1 trial flux is read
+               : vort2flux_refined(h, Gnew, nsw, h->qs, 1);
     if (rc) return rc;
     // --- boundary_forces! and update_stress! (FP64)
     LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h),
@@ -464,7 +631,7 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
         if (rc) return rc;
     }
     // --- vort2flux!(state.ψ, state.q, state.Γ)
-    return vort2flux_refined(h, Gnew, nsw, h->q, mg);
+    return h->bt ? vort2flux_refined_bt(h, Gnew, nsw, h->q, mg) : vort2flux_refined(h, Gnew, nsw, h->q, mg);
 }
 
 // update_bodies! for MotionFunction bodies (timestepping.jl:386-398): move the
@@ -660,6 +827,10 @@ static void free_handle(ibpm_handle* h) {
     }
     if (h->T32) cudaFree(h->T32);
     if (h->Pp) cudaFree(h->Pp);
+    for (void* p : {(void*)h->btW, (void*)h->btU, (void*)h->btP, (void*)h->btE, (void*)h->btS, (void*)h->btY,
+                    (void*)h->btW32, (void*)h->btU32, (void*)h->btP32, (void*)h->btE32, (void*)h->btS32,
+                    (void*)h->btY32})
+        if (p) cudaFree(p);
     if (h->mtab) cudaFree(h->mtab);
     for (void* p : {(void*)h->d_x0, (void*)h->d_ub, (void*)h->d_bbox, (void*)h->btab, (void*)h->bGB, (void*)h->bPB,
                     (void*)h->bQB, (void*)h->bwork, (void*)h->binfo})
@@ -760,6 +931,11 @@ static int create_impl(ibpm_handle* h, const ibpm_problem_desc* d) {
     }
     if ((rc = build_coupling(h, d))) return rc;
     if ((rc = build_binv(h))) return rc;
+    {
+        // the boundary-transfer level chain (IBPM_BT=0: the reference's sequential one)
+        const char* bt = getenv("IBPM_BT");
+        if (!(bt && bt[0] == '0') && (rc = build_bt(h))) return rc;
+    }
     CK(cudaStreamSynchronize(h->st));
     return IBPM_OK;
 }
@@ -1123,7 +1299,8 @@ extern "C" int ibpm_advance_moving(ibpm_handle* h, int32_t nsteps, const double*
 extern "C" int ibpm_vort2flux(ibpm_handle* h) {
     if (!h) return IBPM_ERR_INVALID;
     CK(cudaSetDevice(h->device));
-    int rc = vort2flux(h, h->G[h->cur], h->psi, h->g.S * h->g.mg, 1, h->q, 0, 0, h->g.mg);
+    int rc = h->bt ? vort2flux_bt(h, h->G[h->cur], h->q, h->g.mg)
+                   : vort2flux(h, h->G[h->cur], h->psi, h->g.S * h->g.mg, 1, h->q, 0, 0, h->g.mg);
     if (rc) return rc;
     CK(cudaStreamSynchronize(h->st));
     return IBPM_OK;

@@ -7,58 +7,26 @@
 namespace ibpm {
 
 
-cudaError_t dst_x_32(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_32(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_32();
-cudaError_t dst_x_64(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_64(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_64();
-cudaError_t dst_x_128(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_128(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_128();
-cudaError_t dst_x_192(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_192(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_192();
-cudaError_t dst_x_200(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_200(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_200();
-cudaError_t dst_x_256(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_256(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_256();
-cudaError_t dst_x_384(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_384(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_384();
-cudaError_t dst_x_400(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_400(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_400();
-cudaError_t dst_x_512(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_512(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_512();
-cudaError_t dst_x_768(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_768(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_768();
-cudaError_t dst_x_1024(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_1024(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_1024();
-cudaError_t dst_x_2048(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);
-cudaError_t dst_y_2048(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, cudaStream_t);
-cudaError_t dst_attr_2048();
+// Every supported transform length N = nx or ny.
+#define IBPM_DST_LENGTHS(X) X(32) X(64) X(128) X(192) X(200) X(256) X(384) X(400) X(512) X(768) X(1024) X(2048)
+
+#define IBPM_DST_DECLARE(N)                                                                                   \
+    cudaError_t dst_x_##N(const Geom&, const DstPlan&, const XPassArgs&, cudaStream_t);                      \
+    cudaError_t dst_y_##N(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, \
+                          cudaStream_t);                                                                     \
+    cudaError_t dst_attr_##N();                                                                              \
+    cudaError_t dst_ybc_##N(const Geom&, const DstPlan&, const DstPlan&, void*, SlabMap, int, const SpecParams&, \
+                            const BtSynth&, cudaStream_t);                                                   \
+    cudaError_t dst_lines_##N(const Geom&, const DstPlan&, const void*, SlabMap, int, void*, int, cudaStream_t);
+IBPM_DST_LENGTHS(IBPM_DST_DECLARE)
+#undef IBPM_DST_DECLARE
 
 // Supported transform lengths N = nx or ny: 32, 64, 128, 192, 200, 256, 384, 400, 512, 768, 1024, 2048.
 bool dst_supported(int N) {
     switch (N) {
-        case 32:
-        case 64:
-        case 128:
-        case 192:
-        case 200:
-        case 256:
-        case 384:
-        case 400:
-        case 512:
-        case 768:
-        case 1024:
-        case 2048:
+#define IBPM_CASE(L) case L:
+        IBPM_DST_LENGTHS(IBPM_CASE)
+#undef IBPM_CASE
             return true;
         default:
             return false;
@@ -177,36 +145,18 @@ void dst_plan_destroy(DstPlan* p) {
 // launch or graph capture).
 cudaError_t dst_init_attributes(int N) {
     switch (N) {
-        case 32: return dst_attr_32();
-        case 64: return dst_attr_64();
-        case 128: return dst_attr_128();
-        case 192: return dst_attr_192();
-        case 200: return dst_attr_200();
-        case 256: return dst_attr_256();
-        case 384: return dst_attr_384();
-        case 400: return dst_attr_400();
-        case 512: return dst_attr_512();
-        case 768: return dst_attr_768();
-        case 1024: return dst_attr_1024();
-        case 2048: return dst_attr_2048();
+#define IBPM_CASE(L) case L: return dst_attr_##L();
+        IBPM_DST_LENGTHS(IBPM_CASE)
+#undef IBPM_CASE
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_dst_x(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {
     switch (px.N) {
-        case 32: return dst_x_32(g, px, a, st);
-        case 64: return dst_x_64(g, px, a, st);
-        case 128: return dst_x_128(g, px, a, st);
-        case 192: return dst_x_192(g, px, a, st);
-        case 200: return dst_x_200(g, px, a, st);
-        case 256: return dst_x_256(g, px, a, st);
-        case 384: return dst_x_384(g, px, a, st);
-        case 400: return dst_x_400(g, px, a, st);
-        case 512: return dst_x_512(g, px, a, st);
-        case 768: return dst_x_768(g, px, a, st);
-        case 1024: return dst_x_1024(g, px, a, st);
-        case 2048: return dst_x_2048(g, px, a, st);
+#define IBPM_CASE(L) case L: return dst_x_##L(g, px, a, st);
+        IBPM_DST_LENGTHS(IBPM_CASE)
+#undef IBPM_CASE
         default: return cudaErrorInvalidValue;
     }
 }
@@ -215,18 +165,31 @@ cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px, vo
                          const SpecParams& sp, cudaStream_t st) {
     if (nslabs <= 0) return cudaSuccess;
     switch (py.N) {
-        case 32: return dst_y_32(g, py, px, data, map, nslabs, sp, st);
-        case 64: return dst_y_64(g, py, px, data, map, nslabs, sp, st);
-        case 128: return dst_y_128(g, py, px, data, map, nslabs, sp, st);
-        case 192: return dst_y_192(g, py, px, data, map, nslabs, sp, st);
-        case 200: return dst_y_200(g, py, px, data, map, nslabs, sp, st);
-        case 256: return dst_y_256(g, py, px, data, map, nslabs, sp, st);
-        case 384: return dst_y_384(g, py, px, data, map, nslabs, sp, st);
-        case 400: return dst_y_400(g, py, px, data, map, nslabs, sp, st);
-        case 512: return dst_y_512(g, py, px, data, map, nslabs, sp, st);
-        case 768: return dst_y_768(g, py, px, data, map, nslabs, sp, st);
-        case 1024: return dst_y_1024(g, py, px, data, map, nslabs, sp, st);
-        case 2048: return dst_y_2048(g, py, px, data, map, nslabs, sp, st);
+#define IBPM_CASE(L) case L: return dst_y_##L(g, py, px, data, map, nslabs, sp, st);
+        IBPM_DST_LENGTHS(IBPM_CASE)
+#undef IBPM_CASE
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_dst_ybc(const Geom& g, const DstPlan& py, const DstPlan& px, void* out, SlabMap map, int nslabs,
+                           const SpecParams& sp, const BtSynth& bs, cudaStream_t st) {
+    if (nslabs <= 0) return cudaSuccess;
+    switch (py.N) {
+#define IBPM_CASE(L) case L: return dst_ybc_##L(g, py, px, out, map, nslabs, sp, bs, st);
+        IBPM_DST_LENGTHS(IBPM_CASE)
+#undef IBPM_CASE
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_dst_lines(const Geom& g, const DstPlan& px, const void* Y, SlabMap map, int nslabs,
+                             void* samples, int f32, cudaStream_t st) {
+    if (nslabs <= 0) return cudaSuccess;
+    switch (px.N) {
+#define IBPM_CASE(L) case L: return dst_lines_##L(g, px, Y, map, nslabs, samples, f32, st);
+        IBPM_DST_LENGTHS(IBPM_CASE)
+#undef IBPM_CASE
         default: return cudaErrorInvalidValue;
     }
 }

@@ -402,7 +402,7 @@ __host__ __device__ constexpr size_t tables_bytes() {
 // x-pass: lines are rows of a slab (contiguous).  One group per line pair.
 // ---------------------------------------------------------------------------
 template <int LOAD>
-using x_real_t = std::conditional_t<(LOAD == XLOAD_PLAIN || LOAD == XLOAD_BC), double, float>;
+using x_real_t = std::conditional_t<(LOAD == XLOAD_PLAIN || LOAD == XLOAD_BC || LOAD == XLOAD_SUM), double, float>;
 template <int LOAD>
 __host__ __device__ constexpr bool x_res() { return LOAD == XLOAD_RES_LAP || LOAD == XLOAD_RES_A; }
 // Shared memory of the x-pass: tables, one FFT buffer per group, and for the
@@ -444,7 +444,8 @@ __global__ void __launch_bounds__(ct_groups(N, PL) * ct_tp(N, PL)) dst_x_kernel(
 
     CoarseBC cb;
     cb.rc = nullptr; cb.P = P; cb.nx = g.nx; cb.ny = g.ny;
-    if ((LOAD == XLOAD_BC || LOAD == XLOAD_RES_LAP) && a.coarse) cb.rc = a.coarse + a.coarse_map.off(y);
+    if ((LOAD == XLOAD_BC || LOAD == XLOAD_RES_LAP) && a.coarse && a.in_map.level(y) + 1 < g.mg)
+        cb.rc = a.coarse + a.coarse_map.off(y);
     const double* xg = (LOAD == XLOAD_RES_LAP || LOAD == XLOAD_RES_A) ? a.aux + a.aux_map.off(y) : nullptr;
 
     // apply_bc!(r, get_bc!(coarse), 1.0) (mg-utils.jl:43-60) in the reference's
@@ -512,6 +513,10 @@ __global__ void __launch_bounds__(ct_groups(N, PL) * ct_tp(N, PL)) dst_x_kernel(
         if constexpr (LOAD == XLOAD_F32) {
             const float* ra = static_cast<const float*>(a.in) + ioff;
             return V{ra[i], hasb ? ra[i + P] : 0.0f};
+        } else if constexpr (LOAD == XLOAD_SUM || LOAD == XLOAD_F32_SUM) {
+            const T* ra = static_cast<const T*>(a.in) + ioff;
+            const T* rb = static_cast<const T*>(a.in2) + a.in2_map.off(y) + (long long)la * P;
+            return V{ra[i] + rb[i], hasb ? ra[i + P] + rb[i + P] : T(0)};
         } else if constexpr (RES) {
             return V{(T)res_val(i, 0), hasb ? (T)res_val(i, 1) : T(0)};
         } else {
@@ -613,19 +618,33 @@ __host__ __device__ constexpr int y_threads() { return y_groups<N, T, PL>() * ct
 template <int N, class T, int PL>
 __host__ __device__ constexpr int y_tile_w() { return 2 * y_groups<N, T, PL>(); }
 __host__ __device__ constexpr int round4(int n) { return ((n + 3) / 4) * 4; }
+// Scratch of the edge-source synthesis (SYNTH): per-warp partial sums of the
+// bottom and top rows' sine transforms, then the sums themselves.
 template <int N, class T, int PL>
+__host__ __device__ constexpr int y_synth_slots() {
+    return (y_threads<N, T, PL>() / 32 + 1) * 2 * y_tile_w<N, T, PL>();
+}
+template <int N, class T, int PL, bool SYNTH = false>
 __host__ __device__ constexpr size_t y_smem_bytes(int n2) {
     return tables_bytes<N, T, PL>() + (size_t)round4(n2) * sizeof(T) +  // spectral table of y
            (size_t)round4(n2 * (y_tile_w<N, T, PL>() + 1)) * sizeof(T) +
-           (size_t)y_groups<N, T, PL>() * ct_buf(N) * sizeof(cplx_t<T>);
+           (size_t)y_groups<N, T, PL>() * ct_buf(N) * sizeof(cplx_t<T>) +
+           (SYNTH ? (size_t)y_synth_slots<N, T, PL>() * sizeof(T) : 0);
 }
 
-template <int N, class T, int PL>
+// SYNTH: the input is not read but built, the x-spectrum of apply_bc!(e_ℓ)
+// for the edge vector of the slab's level (BtSynth): with S(i, k) =
+// 2 sin(π i k / nx) the x-pass's sine transform,
+//     X(k, j) = S(1, k) e_L(j) + S(nx−1, k) e_R(j)
+//             + [j = 1] Σ_i S(i, k) e_B(i) + [j = ny−1] Σ_i S(i, k) e_T(i),
+// and the result goes to `out` (same slab map) instead of back into `data`.
+template <int N, class T, int PL, bool SYNTH = false>
 // (3 resident 256-thread CTAs per SM keep the FP64 pass at 80 registers without
 // spills: the five-slab trial solve's y-pass then needs 1.4 waves instead of 2.2)
 __global__ void __launch_bounds__(y_threads<N, T, PL>(),
                                   (!ct_fine(N, PL) || N > 512) ? 1 : (y_threads<N, T, PL>() <= 128 ? 5 : 3))
-    dst_y_kernel(T* data, SlabMap map, Geom g, DstPlan p, const T* __restrict__ cx, SpecParams sp) {
+    dst_y_kernel(T* data, SlabMap map, Geom g, DstPlan p, const T* __restrict__ cx, SpecParams sp,
+                 T* out = nullptr, BtSynth bs = BtSynth{}) {
     using V = cplx_t<T>;
     constexpr int TP = ct_tp(N, PL);
     constexpr int G = y_groups<N, T, PL>();
@@ -649,14 +668,76 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
     for (int j = threadIdx.x; j < n2; j += blockDim.x) cp_async<sizeof(T)>(cyv + j, tb.c + j);
     pdl_wait();
     pdl_trigger();
-    for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
-        const int j = idx / TW, c = idx - j * TW;
-        const int i = i0 + c;
-        if (i < n1) cp_async<sizeof(T)>(tile + j * TWp + c, base + (long long)j * P + i);
-        else tile[j * TWp + c] = T(0);
+    if constexpr (SYNTH) {
+        const long long ep = ((2LL * n1 + 2LL * n2) + 3) & ~3LL;
+        const T* e = static_cast<const T*>(bs.e) + (long long)lev * ep;
+        const T* sxt = static_cast<const T*>(bs.sx);
+        const int nx = bs.nx;
+        auto sinpix = [&](long long t) -> T {  // sin(π t / nx), t ≥ 0
+            t %= 2LL * nx;
+            return t < nx ? __ldg(&sxt[t]) : -__ldg(&sxt[t - nx]);
+        };
+        T* red = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(tile + tile_d) +
+                                      (size_t)G * ct_buf(N) * sizeof(V));
+        // bottom and top rows: Σ_i S(i, k) e(i) for the CTA's columns k
+        T accB[TW], accT[TW];
+#pragma unroll
+        for (int c = 0; c < TW; ++c) accB[c] = accT[c] = T(0);
+        for (int i = threadIdx.x; i < n1; i += blockDim.x) {
+            const T eb = e[i], et = e[n1 + i];
+#pragma unroll
+            for (int c = 0; c < TW; ++c) {
+                const T sv = T(2) * sinpix((long long)(i + 1) * (i0 + c + 1));
+                accB[c] += sv * eb;
+                accT[c] += sv * et;
+            }
+        }
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+        for (int c = 0; c < TW; ++c) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                accB[c] += __shfl_xor_sync(0xffffffffu, accB[c], off);
+                accT[c] += __shfl_xor_sync(0xffffffffu, accT[c], off);
+            }
+            if (lane == 0) {
+                red[w * 2 * TW + c] = accB[c];
+                red[w * 2 * TW + TW + c] = accT[c];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 2 * TW) {
+            T acc = T(0);
+            for (int u = 0; u < nw; ++u) acc += red[u * 2 * TW + threadIdx.x];
+            red[nw * 2 * TW + threadIdx.x] = acc;
+        }
+        __syncthreads();
+        const T* bh = red + nw * 2 * TW;  // [0, TW): bottom, [TW, 2TW): top
+        const T* eL = e + 2 * n1;
+        const T* eR = eL + n2;
+        for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
+            const int j = idx / TW, c = idx - j * TW;
+            const int i = i0 + c;
+            T v = T(0);
+            if (i < n1) {
+                const long long k = i + 1;
+                v = T(2) * sinpix(k) * eL[j] + T(2) * sinpix(k * (nx - 1)) * eR[j];
+                if (j == 0) v += bh[c];
+                if (j == n2 - 1) v += bh[TW + c];
+            }
+            tile[j * TWp + c] = v;
+        }
+        __syncthreads();
+    } else {
+        for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
+            const int j = idx / TW, c = idx - j * TW;
+            const int i = i0 + c;
+            if (i < n1) cp_async<sizeof(T)>(tile + j * TWp + c, base + (long long)j * P + i);
+            else tile[j * TWp + c] = T(0);
+        }
+        cp_async_wait();
+        __syncthreads();
     }
-    cp_async_wait();
-    __syncthreads();
 
     const int ca = 2 * gid;
     const int ia = i0 + ca;
@@ -713,10 +794,84 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
         dst_pair<N, TP, G, T, PL>(buf, tw, sn, tid, gid, load, emit);
     }
     __syncthreads();
+    T* dst = SYNTH ? out + map.off(blockIdx.y) : base;
     for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
         const int j = idx / TW, c = idx - j * TW;
         const int i = i0 + c;
-        if (i < n1) base[(long long)j * P + i] = tile[j * TWp + c];
+        if (i < n1) dst[(long long)j * P + i] = tile[j * TWp + c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Line samples of a boundary-transfer vort2flux! (ibpm_internal.cuh, BtSynth)
+// from the y-pass output Y (x-spectral, y-physical) of the levels of `map`:
+// block 0 of a slab transforms the rows at ny/4 and at 3ny/4 back along x (one
+// line pair) and keeps x = nx/4 … 3nx/4; the other blocks form the columns at
+// nx/4 and 3nx/4, ψ(i0, j) = Σ_k S(i0, k) Y(k, j), one warp per row j.  There
+// S(nx/4, k) = 2 sin(πk/4) and S(3nx/4, k) = 2 sin(3πk/4) repeat with period
+// 8 in k.
+// ---------------------------------------------------------------------------
+template <int N, class T, int PL>
+__host__ __device__ constexpr size_t lines_smem_bytes() {
+    return tables_bytes<N, T, PL>() + (size_t)ct_buf(N) * sizeof(cplx_t<T>);
+}
+
+template <int N, class T, int PL>
+__global__ void __launch_bounds__(ct_tp(N, PL)) dst_lines_kernel(const T* Y, SlabMap map, Geom g, DstPlan p,
+                                                                 T* samples) {
+    using V = cplx_t<T>;
+    constexpr int TP = ct_tp(N, PL);
+    const int P = g.P, nx = g.nx, ny = g.ny, n1 = g.n1;
+    const T* base = Y + map.off(blockIdx.y);
+    T* smp = samples + (long long)map.level(blockIdx.y) * (nx + ny + 4);
+    if (blockIdx.x == 0) {
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        V* tw = reinterpret_cast<V*>(smem_raw);
+        T* sn = reinterpret_cast<T*>(tw + ct_tw_count(N, PL));
+        V* buf = reinterpret_cast<V*>(smem_raw + tables_bytes<N, T, PL>());
+        stage_tables<N, T, PL>(tw, sn, tabs_of<T>(p, PL));
+        cp_async_wait();
+        __syncthreads();
+        pdl_wait();
+        pdl_trigger();
+        const T* ra = base + (long long)(ny / 4 - 1) * P;
+        const T* rb = base + (long long)(3 * ny / 4 - 1) * P;
+        const int o0 = nx / 4 - 1, o1 = 3 * nx / 4 - 1;
+        T* rowB = smp;
+        T* rowT = smp + nx / 2 + 1;
+        dst_pair<N, TP, 1, T, PL>(buf, tw, sn, threadIdx.x, 0, [&](int i) -> V { return V{ra[i], rb[i]}; },
+                                  [&](int o, V v) {
+                                      if (o >= o0 && o <= o1) {
+                                          rowB[o - o0] = v.x;
+                                          rowT[o - o0] = v.y;
+                                      }
+                                  });
+        return;
+    }
+    pdl_wait();
+    pdl_trigger();
+    const int lane = threadIdx.x & 31;
+    const int r = (blockIdx.x - 1) * (TP / 32) + (threadIdx.x >> 5);
+    if (r > ny / 2) return;
+    const T* row = base + (long long)(ny / 4 - 1 + r) * P;
+    const T s2 = T(1.41421356237309504880);  // 2 sin(π/4)
+    const T wl[8] = {T(0), s2, T(2), s2, T(0), -s2, T(-2), -s2};
+    const T wr[8] = {T(0), s2, T(-2), s2, T(0), -s2, T(2), -s2};
+    T aL = T(0), aR = T(0);
+    for (int m = lane; m < n1; m += 32) {
+        const T v = row[m];
+        const int k = (m + 1) & 7;
+        aL += wl[k] * v;
+        aR += wr[k] * v;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        aL += __shfl_xor_sync(0xffffffffu, aL, off);
+        aR += __shfl_xor_sync(0xffffffffu, aR, off);
+    }
+    if (lane == 0) {
+        smp[nx + 2 + r] = aL;
+        smp[nx + 2 + ny / 2 + 1 + r] = aR;
     }
 }
 
@@ -750,7 +905,8 @@ inline int launch_plan(int N, const DstPlan& p, int nslabs) {
     X(XLOAD_PLAIN, XEMIT_STORE) X(XLOAD_PLAIN, XEMIT_SUB) X(XLOAD_BC, XEMIT_STORE)       \
     X(XLOAD_BC, XEMIT_SUB) X(XLOAD_F32, XEMIT_F32) X(XLOAD_RES_LAP, XEMIT_F32)           \
     X(XLOAD_RES_A, XEMIT_F32) X(XLOAD_F32, XEMIT_ADD) X(XLOAD_F32, XEMIT_ADD_FROM)       \
-    X(XLOAD_F32, XEMIT_ACC_SUB) X(XLOAD_PLAIN, XEMIT_ADD_STORE)
+    X(XLOAD_F32, XEMIT_ACC_SUB) X(XLOAD_PLAIN, XEMIT_ADD_STORE) X(XLOAD_SUM, XEMIT_STORE)                  \
+    X(XLOAD_F32_SUM, XEMIT_ADD)
 
 template <int N>
 cudaError_t launch_x_t(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {
@@ -772,7 +928,7 @@ cudaError_t launch_y_n(const Geom& g, const DstPlan& py, const DstPlan& px, void
     dim3 grid((g.n1 + TW - 1) / TW, nslabs);
     const int threads = y_threads<N, T, PL>();
     return launch_k(dst_y_kernel<N, T, PL>, grid, dim3(threads), smem, st, static_cast<T*>(data), map, g, py,
-                    static_cast<const T*>(tabs_of<T>(px).c), sp);
+                    static_cast<const T*>(tabs_of<T>(px).c), sp, static_cast<T*>(nullptr), BtSynth{});
 }
 
 template <int N>
@@ -784,6 +940,49 @@ cudaError_t launch_y_t(const Geom& g, const DstPlan& py, const DstPlan& px, void
                       : launch_y_n<N, double, W>(g, py, px, data, map, nslabs, sp, st);
     return sp.f32 ? launch_y_n<N, float, 0>(g, py, px, data, map, nslabs, sp, st)
                   : launch_y_n<N, double, 0>(g, py, px, data, map, nslabs, sp, st);
+}
+
+template <int N, class T, int PL>
+cudaError_t launch_ybc_n(const Geom& g, const DstPlan& py, const DstPlan& px, void* out, SlabMap map, int nslabs,
+                         const SpecParams& sp, const BtSynth& bs, cudaStream_t st) {
+    constexpr int TW = y_tile_w<N, T, PL>();
+    const size_t smem = y_smem_bytes<N, T, PL, true>(g.n2);
+    if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+    dim3 grid((g.n1 + TW - 1) / TW, nslabs);
+    return launch_k(dst_y_kernel<N, T, PL, true>, grid, dim3(y_threads<N, T, PL>()), smem, st,
+                    static_cast<T*>(nullptr), map, g, py, static_cast<const T*>(tabs_of<T>(px).c), sp,
+                    static_cast<T*>(out), bs);
+}
+
+template <int N>
+cudaError_t launch_ybc_t(const Geom& g, const DstPlan& py, const DstPlan& px, void* out, SlabMap map, int nslabs,
+                         const SpecParams& sp, const BtSynth& bs, cudaStream_t st) {
+    constexpr int W = ct_plan(N, 1);
+    if (launch_plan(N, py, nslabs) == 1)
+        return sp.f32 ? launch_ybc_n<N, float, W>(g, py, px, out, map, nslabs, sp, bs, st)
+                      : launch_ybc_n<N, double, W>(g, py, px, out, map, nslabs, sp, bs, st);
+    return sp.f32 ? launch_ybc_n<N, float, 0>(g, py, px, out, map, nslabs, sp, bs, st)
+                  : launch_ybc_n<N, double, 0>(g, py, px, out, map, nslabs, sp, bs, st);
+}
+
+template <int N, class T, int PL>
+cudaError_t launch_lines_n(const Geom& g, const DstPlan& px, const void* Y, SlabMap map, int nslabs, void* smp,
+                           cudaStream_t st) {
+    constexpr int TP = ct_tp(N, PL);
+    dim3 grid(1 + (g.ny / 2 + 1 + TP / 32 - 1) / (TP / 32), nslabs);
+    return launch_k(dst_lines_kernel<N, T, PL>, grid, dim3(TP), lines_smem_bytes<N, T, PL>(), st,
+                    static_cast<const T*>(Y), map, g, px, static_cast<T*>(smp));
+}
+
+template <int N>
+cudaError_t launch_lines_t(const Geom& g, const DstPlan& px, const void* Y, SlabMap map, int nslabs, void* smp,
+                           int f32, cudaStream_t st) {
+    constexpr int W = ct_plan(N, 1);
+    if (launch_plan(N, px, 1) == 1)
+        return f32 ? launch_lines_n<N, float, W>(g, px, Y, map, nslabs, smp, st)
+                   : launch_lines_n<N, double, W>(g, px, Y, map, nslabs, smp, st);
+    return f32 ? launch_lines_n<N, float, 0>(g, px, Y, map, nslabs, smp, st)
+               : launch_lines_n<N, double, 0>(g, px, Y, map, nslabs, smp, st);
 }
 
 template <class K>
@@ -802,6 +1001,10 @@ cudaError_t attr_plan() {
     IBPM_X_COMBOS(IBPM_X_ATTR)
 #undef IBPM_X_ATTR
     if ((e = smem_attrs(dst_y_kernel<N, double, PL>))) return e;
+    if ((e = smem_attrs(dst_y_kernel<N, double, PL, true>))) return e;
+    if ((e = smem_attrs(dst_y_kernel<N, float, PL, true>))) return e;
+    if ((e = smem_attrs(dst_lines_kernel<N, double, PL>))) return e;
+    if ((e = smem_attrs(dst_lines_kernel<N, float, PL>))) return e;
     return smem_attrs(dst_y_kernel<N, float, PL>);
 }
 
@@ -824,6 +1027,14 @@ cudaError_t attr_t() {
                           const SpecParams& sp, cudaStream_t st) {                                         \
         return dstk::launch_y_t<N>(g, py, px, d, m, n, sp, st);                                            \
     }                                                                                                      \
-    cudaError_t dst_attr_##N() { return dstk::attr_t<N>(); }
+    cudaError_t dst_attr_##N() { return dstk::attr_t<N>(); }                                               \
+    cudaError_t dst_ybc_##N(const Geom& g, const DstPlan& py, const DstPlan& px, void* o, SlabMap m, int n,  \
+                            const SpecParams& sp, const BtSynth& bs, cudaStream_t st) {                     \
+        return dstk::launch_ybc_t<N>(g, py, px, o, m, n, sp, bs, st);                                      \
+    }                                                                                                      \
+    cudaError_t dst_lines_##N(const Geom& g, const DstPlan& px, const void* Y, SlabMap m, int n, void* smp, \
+                              int f32, cudaStream_t st) {                                                  \
+        return dstk::launch_lines_t<N>(g, px, Y, m, n, smp, f32, st);                                      \
+    }
 
 }  // namespace ibpm

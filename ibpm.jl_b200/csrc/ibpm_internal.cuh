@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace ibpm {
 
 struct Geom {
@@ -224,13 +226,20 @@ struct SpecParams {
 //     XEMIT_STORE    out = v (double)       XEMIT_SUB      out −= v (double)
 //     XEMIT_F32      out = v (float)        XEMIT_ADD      out += v (double)
 //     XEMIT_ADD_FROM out = aux + v          XEMIT_ACC_SUB  aux += v; out −= aux
-enum XLoad { XLOAD_PLAIN = 0, XLOAD_BC = 1, XLOAD_F32 = 2, XLOAD_RES_LAP = 3, XLOAD_RES_A = 4 };
+//   and the last pass of a boundary-transfer vort2flux! (bt.cu), which
+//   transforms the sum of the interior and edge parts of the x-spectrum:
+//     XLOAD_SUM      in + in2 (double)     XLOAD_F32_SUM  in + in2 (float)
+// The coarser-level field of XLOAD_BC / RES_LAP is read only for slabs whose
+// level is below the coarsest (a multi-level launch includes the coarsest).
+enum XLoad { XLOAD_PLAIN = 0, XLOAD_BC = 1, XLOAD_F32 = 2, XLOAD_RES_LAP = 3, XLOAD_RES_A = 4, XLOAD_SUM = 5,
+             XLOAD_F32_SUM = 6 };
 //     XEMIT_ADD_STORE out += v; aux = v (double; the adjoint level chain)
 enum XEmit { XEMIT_STORE = 0, XEMIT_SUB = 1, XEMIT_F32 = 2, XEMIT_ADD = 3, XEMIT_ADD_FROM = 4, XEMIT_ACC_SUB = 5,
              XEMIT_ADD_STORE = 6 };
 struct XPassArgs {
     const void* in; void* out;
     SlabMap in_map, out_map;
+    const void* in2; SlabMap in2_map;            // XLOAD_SUM / F32_SUM: second addend
     const double* coarse;  SlabMap coarse_map;   // XLOAD_BC / RES_LAP: coarser-level field
     double* aux; SlabMap aux_map;                // RES_*: current solution; ADD_FROM / ACC_SUB (see above)
     double cA;                                   // XLOAD_RES_A: c = dt / (2 Re hc²)
@@ -240,24 +249,72 @@ struct XPassArgs {
 cudaError_t launch_dst_x(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st);
 
 
-// FP64 residual of a refinement sweep, stored in FP32 (stencil.cu):
-//   RESID_LAP  r = b + apply_bc!(get_bc!(coarse)) − L x    (vort2flux! levels)
-//   RESID_A    r = b − (x + c L x)                         (A⁻¹ solves)
-enum ResidMode { RESID_LAP = 0, RESID_A = 1 };
-struct ResidArgs {
-    const double* b; SlabMap bmap;
-    const double* x; SlabMap xmap;
-    const double* coarse; SlabMap cmap;  // RESID_LAP: coarser-level ψ, or null
-    float* r; SlabMap rmap;
-    double cA[8];                         // RESID_A: dt / (2 Re hc²) per level
-    int mode, mg;
-};
-cudaError_t launch_resid(const Geom& g, const ResidArgs& a, int nslabs, cudaStream_t st);
 
 // y-direction pass of a Poisson-type solve, in place on every slab selected by
 // `map`: DST-I, spectral divide (SpecParams), DST-I.
 cudaError_t launch_dst_y(const Geom& g, const DstPlan& py, const DstPlan& px_cos, void* data, SlabMap map,
                          int nslabs, const SpecParams& sp, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Boundary-transfer form of vort2flux! (bt.cu).  Δ⁻¹ is linear, so each
+// level's streamfunction splits into an interior and an edge part,
+//     ψ_ℓ = Δ⁻¹ Γ_ℓ + Δ⁻¹ apply_bc!(e_ℓ),   e_ℓ = get_bc!(ψ_{ℓ+1})
+// (curl.jl:147-158, mg-utils.jl:7-60), and the edge vectors chain as
+//     e_ℓ = get_bc!(Δ⁻¹ Γ_{ℓ+1}) + R e_{ℓ+1},   R = get_bc! ∘ Δ⁻¹ ∘ apply_bc!,
+// R one nE×nE matrix for every level (the reference's Δ⁻¹ carries no h,
+// models.jl:46).  An edge vector holds the nE = 2(nx−1) + 2(ny−1) entries that
+// apply_bc! adds: bottom i = 1…nx−1, top, left j = 1…ny−1, right.
+// The x-spectrum of apply_bc!(e) is known in closed form (one sine transform
+// of the bottom and top rows, two sines for the left and right columns), so
+// the edge part is one y-pass from e and the last x-pass adds both parts.
+// Line samples of a level (what get_bc! reads from it): the row at ny/4 and
+// at 3ny/4 (x = nx/4 … 3nx/4, nx/2+1 values each), then the column at nx/4 and
+// at 3nx/4 (y = ny/4 … 3ny/4), each taken from the y-pass output (x-spectral).
+// ---------------------------------------------------------------------------
+inline int bt_edge_len(const Geom& g) { return 2 * g.n1 + 2 * g.n2; }
+inline int bt_edge_pitch(const Geom& g) { return (bt_edge_len(g) + 3) & ~3; }  // R row pitch
+inline int bt_sample_len(const Geom& g) { return g.nx + g.ny + 4; }
+struct BtSynth {
+    const void* e;        // edge vectors, level-major (bt_edge_pitch apart), T
+    const void* sx;       // sin(π t/nx), t < nx, of the x-length (T)
+    int nx;
+};
+cudaError_t launch_dst_ybc(const Geom& g, const DstPlan& py, const DstPlan& px, void* out, SlabMap map, int nslabs,
+                           const SpecParams& sp, const BtSynth& bs, cudaStream_t st);
+cudaError_t launch_dst_lines(const Geom& g, const DstPlan& px, const void* Y, SlabMap map, int nslabs,
+                             void* samples, int f32, cudaStream_t st);
+// The chain in a rank-k basis of R (R ≈ Q W, Q orthonormal columns,
+// W = Qᵀ R, k ≈ 135 for FP64 accuracy whatever the grid size: R is the
+// Green's function between well-separated point sets, smooth, with fast
+// decaying singular values):
+//     p_ℓ = W g_ℓ (g_ℓ = get_bc!(samples of ℓ+1)),  ℓ = 0 … mg−2
+//     e_ℓ = g_ℓ + Σ_{m=0}^{mg−3−ℓ} U_m p_{ℓ+1+m},   U_m = Q (W Q)^m
+// which is e_ℓ = g_ℓ + R e_{ℓ+1} unrolled (two launches, none serial).
+struct BtChainArgs {
+    const void* W;        // k × pitch (bt_edge_pitch), row-major (T)
+    const void* U;        // mg−2 matrices nE × kp, row-major (T)
+    const void* samples;  // bt_sample_len per level (T), level-major
+    void* p;              // (mg−1) × kp projections (T)
+    void* e;              // edge vectors (T), level-major, bt_edge_pitch apart
+    int k, kp;            // rank and its pitch (multiple of 4)
+    int f32;
+};
+cudaError_t launch_bt_project(const Geom& g, const BtChainArgs& a, cudaStream_t st);
+cudaError_t launch_bt_expand(const Geom& g, const BtChainArgs& a, cudaStream_t st);
+// Setup of R: unit sources of edge entries [c0, c0 + ncol) into ncol slabs
+// (bstride apart, zeroed first), and the gather of their solves' get_bc!
+// entries into R's columns (FP64), then the FP32 copy.
+cudaError_t launch_bt_unit_src(const Geom& g, int c0, int ncol, double* G, long long bstride, cudaStream_t st);
+cudaError_t launch_bt_gather(const Geom& g, int c0, int ncol, const double* psi, long long bstride, double* R,
+                             cudaStream_t st);
+cudaError_t launch_to_f32(const double* a, float* b, long long n, cudaStream_t st);
+// Host: the rank-k basis of R (bt.cu) — W = Qᵀ R (k × pitch) and
+// U_m = Q (W Q)^m (nE × kp each, m < nmat); -1 if the rank reaches kmax.
+struct BtLowRank {
+    int k = 0, kp = 0;
+    std::vector<double> W, U;
+};
+int bt_lowrank(const std::vector<double>& R, int nE, int ep, int nmat, double tol, int kmax, BtLowRank& out);
 
 // Base flux of a moving grid (base_flux!, timestepping.jl:273-318): on level
 // spacing hc, q0x = YY·(−hc Ω) + hc Ux0 at every x-flux of row J and

@@ -211,52 +211,4 @@ cudaError_t launch_curl(const Geom& g, const CurlArgs& a, cudaStream_t st) {
     return launch_k(curl_kernel, grid, dim3(256), 0, st, a, g);
 }
 
-// ---------------------------------------------------------------------------
-// Residual of one refinement sweep of a Poisson-type solve, in FP64, stored in
-// FP32 (it is small: the change of the solution since its previous solve).
-// L x = 4x − Σ neighbours with zero Dirichlet edges is the operator the DST-I
-// solve with Λ inverts (laplacian.jl:14-41); apply_bc!(get_bc!(coarse)) is
-// the edge term of a vort2flux! level (curl.jl:151-158, mg-utils.jl:7-60).
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) resid_kernel(ResidArgs a, Geom g) {
-    pdl_wait();
-    pdl_trigger();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int y = blockIdx.z;
-    const int n1 = g.n1, n2 = g.n2, P = g.P;
-    if (i >= n1 || j >= n2) return;
-    const int lev = a.bmap.level(y);
-    const double* x = a.x + a.xmap.off(y);
-    const long long o = (long long)j * P + i;
-    const double xc = x[o];
-    double nb = 0.0;
-    if (i > 0) nb += x[o - 1];
-    if (i + 1 < n1) nb += x[o + 1];
-    if (j > 0) nb += x[o - P];
-    if (j + 1 < n2) nb += x[o + P];
-    const double Lx = 4.0 * xc - nb;
-    double v = a.b[a.bmap.off(y) + o];
-    if (a.mode == RESID_LAP) {
-        if (a.coarse && lev < a.mg - 1) {
-            CoarseBC cb;
-            cb.rc = a.coarse + a.cmap.off(y); cb.P = P; cb.nx = g.nx; cb.ny = g.ny;
-            if (j == 0) v += cb.bot(i + 1);
-            if (j == n2 - 1) v += cb.top(i + 1);
-            if (i == 0) v += cb.left(j + 1);
-            if (i == n1 - 1) v += cb.right(j + 1);
-        }
-        v -= Lx;
-    } else {
-        v -= xc + a.cA[lev] * Lx;
-    }
-    a.r[a.rmap.off(y) + o] = (float)v;
-}
-
-cudaError_t launch_resid(const Geom& g, const ResidArgs& a, int nslabs, cudaStream_t st) {
-    dim3 blk(32, 8);
-    dim3 grid((g.n1 + 31) / 32, (g.n2 + 7) / 8, nslabs);
-    return launch_k(resid_kernel, grid, blk, 0, st, a, g);
-}
-
 }  // namespace ibpm

@@ -321,7 +321,8 @@ int ibpm_host_free(void* p);
 /* Kernel classes reported by ibpm_profile. */
 #define IBPM_KERNEL_COUNT 12 /* trial_rhs, dst_x, dst_y, coarsify, curl, E_gather,
                                 binv_gemv, stress, proj_src, adjoint, resid,
-                                level_solve */
+                                bt_chain (the line samples and edge chain of
+                                the boundary-transfer vort2flux!) */
 
 /* Name of kernel class k (0 <= k < IBPM_KERNEL_COUNT). */
 const char* ibpm_kernel_name(int32_t k);
