@@ -381,7 +381,72 @@ XB_WORKLOAD = ("position gradient of mean total lift (last 100 of 400 steps), tw
                "8 seeded finite-difference directions")
 
 
-def position_gradient_block(args, d):
+# The large two-body workload: two cylinders D = 1 (628 points each) at
+# (0, ±0.75), Re = 150, 1024x1024 cells x 5 levels, h = 0.005, dt = 0.001
+# (nf = 2512), FP32-refined.  The block times `steps` steps of both paths from
+# rest and their CD/CL differences, and the position gradient of the mean
+# total lift (last 100 of `adj_steps` steps, checkpoint every 100) against
+# finite differences along 8 seeded directions.
+C5 = dict(h=0.005, mg=5, dt=0.001, nb=628, Re=150.0, steps=1000, adj_steps=400, window=100, k=100, seed=7, ndir=8,
+          off=(0.003085, -0.0017775))   # the gradient check moves the bodies off the grid lines (as XB, in h)
+C5_WORKLOAD = ("two cylinders D=1 (628 pts each) at (0,+-0.75) Re=150, 1024x1024 cells x 5 levels, h=0.005, "
+               "dt=0.001, nf=2512, from rest")
+
+
+def c5_bodies(G, g, off=(0.0, 0.0), xb=None):
+    ox, oy = off
+    n = C5["nb"]
+    bs = [G.make_cylinder(0.5, g.h, ox, 0.75 + oy, n=n), G.make_cylinder(0.5, g.h, ox, -0.75 + oy, n=n)]
+    if xb is not None:
+        bs[0].xb, bs[1].xb = xb[:n].copy(), xb[n:].copy()
+    return bs
+
+
+def config5_block(args, d):
+    import ibpm_gpu as G
+    g = G.make_grid(C5["h"], BOUNDARY, C5["mg"])
+    cells = g.nx * g.ny * g.mg
+    n = C5["steps"]
+    out = {"workload": C5_WORKLOAD, "metric": METRIC, "unit": METRIC}
+    hist = {}
+    for prec in ("fp32_refined", "fp64"):
+        t0 = time.perf_counter()
+        p = G.IBProblem(g, c5_bodies(G, g), C5["dt"], C5["Re"], device=d.local, sync_fields=False, precision=prec)
+        setup_s = time.perf_counter() - t0
+        st = G.IBState(p)
+        G.bench_steps(p, 3, flush_l2=True)
+        ms = G.bench_steps(p, n, flush_l2=True)
+        for a in (st.Gamma, st.q, st.psi, st.nonlin[0], st.nonlin[1], st.Fb):
+            a[...] = 0.0
+        G.push_state(st, p)
+        p.sync()
+        t0 = time.perf_counter()
+        cd, cl = G.advance(st, p, 0.0, nsteps=n)
+        e2e_s = time.perf_counter() - t0
+        hist[prec] = (cd, cl)
+        out[prec] = {"value": cells * n / (float(np.sum(ms)) / 1e3), "ms_per_step": float(np.mean(ms)),
+                     "setup_s": setup_s, "e2e": {"value": cells * n / e2e_s, "unit": METRIC,
+                                                 "note": "advance! of %d steps from rest, CD/CL returned" % n},
+                     "launches_per_step": G.launches_per_step(p), "nf": p.nf,
+                     "cd_final": cd[-1].tolist(), "cl_final": cl[-1].tolist()}
+        p.close()
+    (cd32, cl32), (cd64, cl64) = hist["fp32_refined"], hist["fp64"]
+    out["refined_vs_fp64"] = out["fp32_refined"]["value"] / out["fp64"]["value"]
+    out["accuracy"] = {"steps": n,
+                       "cd_max_rel_err": float(np.max(np.abs(cd32 - cd64) / np.abs(cd64))),
+                       "cl_err_rel_to_max_cl": float(np.max(np.abs(cl32 - cl64)) / np.max(np.abs(cl64))),
+                       "cl_err_rel_to_max_cd": float(np.max(np.abs(cl32 - cl64)) / np.max(np.abs(cd64))),
+                       "max_abs_cl": float(np.max(np.abs(cl64))), "max_abs_cd": float(np.max(np.abs(cd64)))}
+    try:
+        out["position_gradient"] = position_gradient_block(args, d, C5, "the same geometry: mean total lift "
+                                                           "(last 100 of 400 steps), checkpoint every 100 steps, "
+                                                           "8 seeded finite-difference directions (FP64)")
+    except Exception as e:  # reported, not fatal
+        out["position_gradient"] = {"error": str(e)[:300]}
+    return out
+
+
+def position_gradient_block(args, d, XB=XB, workload=XB_WORKLOAD):
     import ibpm_gpu as G
     g = G.make_grid(XB["h"], BOUNDARY, XB["mg"])
     ox, oy = XB["off"]
@@ -405,7 +470,7 @@ def position_gradient_block(args, d):
         G.push_state(st, p)
         G.vort2flux(st, p)
         return st
-    n, win = XB["steps"], XB["window"]
+    n, win = XB.get("adj_steps", XB["steps"]), XB["window"]
 
     def J_of(xb):
         p = problem(xb)
@@ -439,7 +504,7 @@ def position_gradient_block(args, d):
         ad = float(np.sum(res.grad_xb * dv))
         checks.append({"fd": fd, "adjoint": ad, "err_over_norm": abs(fd - ad) / (gn * float(np.linalg.norm(dv))),
                        "rel_err": abs(fd - ad) / abs(fd)})
-    return {"workload": XB_WORKLOAD, "precision": "fp64", "J": res.J, "grad_xb_norm": gn,
+    return {"workload": workload, "precision": "fp64", "J": res.J, "grad_xb_norm": gn,
             "forward_s": t_fwd, "adjoint_run_s": t_adj, "adjoint_over_forward": t_adj / t_fwd,
             "reverse_over_forward": (t_adj - t_fwd) / t_fwd,
             "fd_eps": eps, "fd_checks": checks,
@@ -688,22 +753,62 @@ def eldredge_block(args, d):
     return out
 
 
-def fp64_history(args, d, scale):
-    """CD/CL of K FP64 steps (one advance call) from the vortex start with its
-    amplitude scaled by ``scale``: the flow's own sensitivity to a change of
-    the start state, the yardstick for the FP32-refined path's differences
-    after many steps (the Re = 100 wake amplifies any difference)."""
+CONFIG_STEPS = 4000   # the workload's stated run length (t = 8)
+
+
+def history(d, precision="fp64", scale=1.0, nsteps=CONFIG_STEPS):
+    """CD/CL of nsteps steps (one advance call) from the vortex start with its
+    amplitude scaled by ``scale``, and the final Γ.  With scale ≠ 1 on the
+    FP64 path: the flow's own sensitivity to a change of the start state, the
+    yardstick for the FP32-refined path's differences after many steps (the
+    Re = 100 wake amplifies any difference)."""
     import ibpm_gpu as G
     g = G.make_grid(H, BOUNDARY, MG)
     prob = G.IBProblem(g, [G.make_cylinder(0.5, g.h, 0.0, 0.0, n=NB)], DT, RE, freestream=(1.0, 0.0, 0.0),
-                       device=d.local, sync_fields=False)
+                       device=d.local, sync_fields=False, precision=precision)
     st = G.IBState(prob)
     st.Gamma[...] = scale * vortex_gamma(g.nx, g.ny, g.mg, g.h, g.offx, g.offy)
     G.push_state(st, prob, fields=("Gamma",))
     G.vort2flux(st, prob)
-    cd, cl = G.advance(st, prob, 0.0, nsteps=args.steps)
+    cd, cl = G.advance(st, prob, 0.0, nsteps=nsteps)
+    G.pull_state(st, prob)
+    gamma = np.array(st.Gamma)
     prob.close()
-    return cd[:, 0], cl[:, 0]
+    return cd[:, 0], cl[:, 0], gamma
+
+
+def accuracy_block(d):
+    """The FP32-refined path against the FP64 path over the workload's full
+    4000 steps from the vortex start: CD relative to itself, CL relative to
+    its own largest magnitude and on the force scale (max |CD|), by step
+    range, beside the FP64 path's own divergence from a perturbed start."""
+    cd32, cl32, g32 = history(d, "fp32_refined")
+    cd64, cl64, g64 = history(d, "fp64")
+    pcd, pcl, _ = history(d, "fp64", 1.0 + 1e-9)
+    K = CONFIG_STEPS
+
+    def errs(a, b, c, dd, m0, m1):
+        return {"cd_max_rel_err": float(np.max(np.abs(a[m0:m1] - b[m0:m1]) / np.abs(b[m0:m1]))),
+                "cl_max_abs_err": float(np.max(np.abs(c[m0:m1] - dd[m0:m1]))),
+                "cl_err_rel_to_max_cl": float(np.max(np.abs(c[m0:m1] - dd[m0:m1])) / np.max(np.abs(dd[m0:m1]))),
+                "cl_err_rel_to_max_cd": float(np.max(np.abs(c[m0:m1] - dd[m0:m1])) / np.max(np.abs(b[m0:m1])))}
+    acc = {"reference": "the FP64 GPU path on the same start state (it matches the FP64 oracle to 1e-10)",
+           "steps": K}
+    acc.update(errs(cd32, cd64, cl32, cl64, 0, K))
+    acc.update({
+        "cl_err_argmax_step": int(np.argmax(np.abs(cl32 - cl64))),
+        "cd_err_argmax_step": int(np.argmax(np.abs(cd32 - cd64) / np.abs(cd64))),
+        "max_abs_cl": float(np.max(np.abs(cl64))), "max_abs_cd": float(np.max(np.abs(cd64))),
+        "vorticity_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+        "vorticity_rel_l2_finest": float(np.linalg.norm(g32[:, 0] - g64[:, 0]) / np.linalg.norm(g64[:, 0])),
+        "by_range": {"%d-%d" % (m0, m1): {"refined": errs(cd32, cd64, cl32, cl64, m0, m1),
+                                          "fp64_perturbed": errs(pcd, cd64, pcl, cl64, m0, m1)}
+                     for m0, m1 in ((0, 10), (10, 100), (100, 1000), (1000, K))},
+        "note": "by_range: max differences over steps [m0, m1); fp64_perturbed = the FP64 path started from "
+                "the vortex amplitude x (1 + 1e-9); the first 10 steps are the impulsive start, during which "
+                "the lift is 1e-6..1e-4 against CD up to 1640",
+    })
+    return acc
 
 
 # Shedding: the same workload continued until the wake sheds periodically,
@@ -820,44 +925,10 @@ def run_ours(args, d):
     launch_bytes = sum(v[1] for v in prof.values()) / 4.0
     launch_bytes64 = sum(v[1] for v in r64["prof"].values()) / 4.0
     bstep64 = step_bytes_model(g.nx, g.ny, g.mg, r64["nf"])
-    cd32, cd64, cl32, cl64 = r32["cd"], r64["cd"], r32["cl"], r64["cl"]
-    accuracy = {
-        "reference": "the FP64 GPU path on the same start state (it matches the FP64 oracle to 1e-10)",
-        "steps": K,
-        "cd_max_rel_err": float(np.max(np.abs(cd32 - cd64) / np.abs(cd64))),
-        "cd_max_rel_err_after_10_steps": float(np.max(np.abs(cd32[10:] - cd64[10:]) / np.abs(cd64[10:])))
-        if K > 10 else None,
-        "cl_max_abs_err": float(np.max(np.abs(cl32 - cl64))),
-        "cl_err_rel_to_max_cl": float(np.max(np.abs(cl32 - cl64)) / np.max(np.abs(cl64))),
-        "cl_err_rel_to_max_cd": float(np.max(np.abs(cl32 - cl64)) / np.max(np.abs(cd64))),
-        "cl_err_argmax_step": int(np.argmax(np.abs(cl32 - cl64))),
-        "cd_err_argmax_step": int(np.argmax(np.abs(cd32 - cd64) / np.abs(cd64))),
-        "cl_max_abs_err_after_10_steps": float(np.max(np.abs(cl32[10:] - cl64[10:]))) if K > 10 else None,
-        "cl_err_after_10_steps_rel_to_max_cl": float(np.max(np.abs(cl32[10:] - cl64[10:])) / np.max(np.abs(cl64[10:])))
-        if K > 10 else None,
-        "cl_err_after_10_steps_rel_to_cd_after_10": float(np.max(np.abs(cl32[10:] - cl64[10:])) /
-                                                          np.max(np.abs(cd64[10:]))) if K > 10 else None,
-        "max_abs_cl": float(np.max(np.abs(cl64))), "max_abs_cd": float(np.max(np.abs(cd64))),
-        "vorticity_rel_l2": float(np.linalg.norm(r32["gamma"] - r64["gamma"]) / np.linalg.norm(r64["gamma"])),
-        "vorticity_rel_l2_finest": float(np.linalg.norm(r32["gamma"][:, 0] - r64["gamma"][:, 0]) /
-                                         np.linalg.norm(r64["gamma"][:, 0])),
-        "note": "the lift of this start is 1e-6..1e-4 (CD 1.4..1640): CL errors are stated absolute and on the "
-                "force scale (max |CD| over the same steps); the first 10 steps are the impulsive start",
-    }
-    # how the differences grow with the step count, beside the FP64 path's own
-    # divergence from a start vorticity scaled by 1 + 1e-9
     try:
-        pcd, pcl = fp64_history(args, d, 1.0 + 1e-9)
-        marks = [m for m in (10, 100, 1000, K) if m <= K]
-        accuracy["by_step"] = {
-            str(m): {"refined_cd_rel": float(np.max(np.abs(cd32[:m] - cd64[:m]) / np.abs(cd64[:m]))),
-                     "refined_cl_abs": float(np.max(np.abs(cl32[:m] - cl64[:m]))),
-                     "fp64_perturbed_cd_rel": float(np.max(np.abs(pcd[:m] - cd64[:m]) / np.abs(cd64[:m]))),
-                     "fp64_perturbed_cl_abs": float(np.max(np.abs(pcl[:m] - cl64[:m])))} for m in marks}
-        accuracy["by_step_note"] = ("max differences over the first m steps; fp64_perturbed = the FP64 path "
-                                    "started from the vortex amplitude x (1 + 1e-9)")
+        accuracy = accuracy_block(d)
     except Exception as e:  # reported, not fatal
-        accuracy["by_step"] = {"error": str(e)[:200]}
+        accuracy = {"error": str(e)[:300]}
     out = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": d.world, "steps": K,
         "warmup": args.warmup, "ms_per_step": r32["total_ms"] / K, "higher_is_better": True,
@@ -893,6 +964,11 @@ def run_ours(args, d):
     }
     if not args.no_adjoint:
         out["adjoint"] = adjoint_block(args, d)
+    if not args.no_large:
+        try:
+            out["two_cylinders_1024"] = config5_block(args, d)
+        except Exception as e:  # reported, not fatal
+            out["two_cylinders_1024"] = {"workload": C5_WORKLOAD, "error": str(e)[:300]}
     if not args.no_eldredge:
         try:
             out["eldredge"] = eldredge_block(args, d)
@@ -940,6 +1016,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-eldredge", action="store_true")
     ap.add_argument("--no-strouhal", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
     args = ap.parse_args()
     d = Dist()
     try:

@@ -10,6 +10,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -354,13 +356,32 @@ static int vort2flux(ibpm_handle* h, double* G, double* psi, long long bstride, 
 // (FP64 solves, `chunk` columns per batch), then its rank-k basis on the host
 // (bt_lowrank); FP32 copies of the basis for FP32_REFINED.  A rank that does
 // not settle (never seen) leaves the handle on the level-by-level chain.
+static int upload_bt(ibpm_handle* h, const BtLowRank& lr);
+
+// R depends only on (nx, ny) and each mg needs its own U_m: handles of one
+// size (finite-difference runs, batch members) share the host factors.
+struct BtCacheKey {
+    int nx, ny, mg;
+    bool operator<(const BtCacheKey& o) const {
+        return nx != o.nx ? nx < o.nx : ny != o.ny ? ny < o.ny : mg < o.mg;
+    }
+};
+static std::mutex g_bt_mutex;
+static std::map<BtCacheKey, std::shared_ptr<const BtLowRank>> g_bt_cache;
+
 static int build_bt(ibpm_handle* h) {
     const Geom& g = h->g;
     if (g.mg < 2) return IBPM_OK;
     const int nE = bt_edge_len(g), ep = bt_edge_pitch(g);
     const int mg = g.mg;
-    const bool f32 = h->prec == IBPM_PREC_FP32_REFINED;
     int rc;
+    std::shared_ptr<const BtLowRank> cached;
+    {
+        std::lock_guard<std::mutex> lock(g_bt_mutex);
+        auto it = g_bt_cache.find(BtCacheKey{g.nx, g.ny, mg});
+        if (it != g_bt_cache.end()) cached = it->second;
+    }
+    if (cached) return upload_bt(h, *cached);
     double *R = nullptr, *GB = nullptr;
     const int chunk = std::min(nE, kBChunk);
     if ((rc = dalloc(h, &R, (size_t)nE * ep)) || (rc = dalloc(h, &GB, (size_t)g.S * chunk))) {
@@ -384,8 +405,20 @@ static int build_bt(ibpm_handle* h) {
     cudaFree(R);
     if (rc) return rc;
     if (e != cudaSuccess) return fail(h, IBPM_ERR_CUDA, std::string("R setup: ") + cudaGetErrorString(e));
-    BtLowRank lr;
-    if (bt_lowrank(Rh, nE, ep, std::max(0, mg - 2), 1e-14, std::min(nE, 1024), lr)) return IBPM_OK;
+    auto lr = std::make_shared<BtLowRank>();
+    if (bt_lowrank(Rh, nE, ep, std::max(0, mg - 2), 1e-14, std::min(nE, 1024), *lr)) return IBPM_OK;
+    {
+        std::lock_guard<std::mutex> lock(g_bt_mutex);
+        g_bt_cache[BtCacheKey{g.nx, g.ny, mg}] = lr;
+    }
+    return upload_bt(h, *lr);
+}
+
+static int upload_bt(ibpm_handle* h, const BtLowRank& lr) {
+    const Geom& g = h->g;
+    const int mg = g.mg, ep = bt_edge_pitch(g);
+    const bool f32 = h->prec == IBPM_PREC_FP32_REFINED;
+    int rc;
     h->bt_k = lr.k;
     h->bt_kp = lr.kp;
     const size_t nw = (size_t)lr.k * ep, nu = std::max<size_t>(1, lr.U.size()), np = (size_t)(mg - 1) * lr.kp;
@@ -774,7 +807,7 @@ static int build_binv(ibpm_handle* h) {
     int rc;
     const long long bstride = g.S * mg;
     if ((rc = dalloc(h, &GB, (size_t)bstride * chunk)) || (rc = dalloc(h, &PB, (size_t)bstride * chunk)) ||
-        (rc = dalloc(h, &QB, (size_t)g.nq * chunk)) || (rc = dalloc(h, &work, (size_t)2 * nf * nf + 2 * nf)) ||
+        (rc = dalloc(h, &QB, (size_t)g.nq * chunk)) || (rc = dalloc(h, &work, gj_work_doubles(nf))) ||
         (rc = dalloc(h, &info, 1))) {
         cudaFree(GB); cudaFree(PB); cudaFree(QB); cudaFree(work); cudaFree(info);
         return rc;
@@ -1254,7 +1287,7 @@ extern "C" int ibpm_set_motion_function(ibpm_handle* h) {
     if ((rc = dalloc(h, &h->d_x0, 2 * h->nb)) || (rc = dalloc(h, &h->d_ub, 2 * h->nb)) ||
         (rc = dalloc(h, &h->d_bbox, 4)) || (rc = dalloc(h, &h->bGB, (size_t)bstride * chunk)) ||
         (rc = dalloc(h, &h->bPB, (size_t)bstride * chunk)) || (rc = dalloc(h, &h->bQB, (size_t)g.nq * chunk)) ||
-        (rc = dalloc(h, &h->bwork, (size_t)2 * nf * nf + 2 * nf)) || (rc = dalloc(h, &h->binfo, 1)))
+        (rc = dalloc(h, &h->bwork, gj_work_doubles(nf))) || (rc = dalloc(h, &h->binfo, 1)))
         return rc;
     // the reference configuration x0 is the body as created (RigidBody.x0)
     CK(cudaMemcpyAsync(h->d_x0, h->d_xb, sizeof(double) * 2 * h->nb, cudaMemcpyDeviceToDevice, h->st));

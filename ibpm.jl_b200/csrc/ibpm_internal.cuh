@@ -419,9 +419,13 @@ cudaError_t launch_unit_src(const Geom& g, const BodyDev& b, int col0, int ncol,
                             long long bstride, cudaStream_t st);
 
 // Dense linear algebra (linalg.cu): in-place inverse by Gauss–Jordan with
-// partial pivoting of the row-major n×n matrix A; `work` holds 2 n² + 2 n
-// doubles and `info` one int (set to the failing column + 1 on a zero pivot).
+// partial pivoting of the row-major n×n matrix A; `work` holds
+// gj_work_doubles(n) doubles and `info` one int (set to the failing column + 1
+// on a zero pivot).
+// From n = 513 on the elimination runs panel by panel (64 columns), each
+// panel as one rank-64 update of the augmented matrix.
 cudaError_t launch_gj_inverse(double* A, int n, double* work, int* info, cudaStream_t st);
+size_t gj_work_doubles(int n);   // doubles of `work` for launch_gj_inverse
 
 // ---------------------------------------------------------------------------
 // Discrete adjoint of the step (adjoint.cu)

@@ -794,22 +794,27 @@ def E_apply(qx1, qy1, prob):
     return (prob.E @ np.concatenate([qxf, qyf], axis=1).T).T.reshape(lead + (-1,))
 
 
-def build_B(prob, chunk=64):
-    """get_Binv / B_times! (laplacian.jl:98-119, 143-169): column j of B is
-    E · vort2flux(A⁻¹_1 · C'E' e_j)[level-1 flux].  Computed ``chunk`` columns at
-    a time (the columns are independent)."""
+def B_times(prob, Z):
+    """B_times! (laplacian.jl:143-169) of the columns of Z (nf, R):
+    E · vort2flux(A⁻¹_1 · C'E' z)[level-1 flux] for each column z."""
     g = prob.grid
+    R = Z.shape[1]
+    G = np.zeros((R, g.mg, g.nx - 1, g.ny - 1))
+    G[:, 0] = ainv_level(ECt(Z, prob), prob, 0)
+    _, qx, qy = vort2flux(G, prob.Lam, g)
+    return E_apply(qx[:, 0], qy[:, 0], prob).T
+
+
+def build_B(prob, chunk=64):
+    """get_Binv (laplacian.jl:98-119): column j of B is B_times!(e_j), computed
+    ``chunk`` columns at a time (the columns are independent)."""
     nf = prob.nf
     B = np.zeros((nf, nf))
     for c0 in range(0, nf, chunk):
         c1 = min(nf, c0 + chunk)
-        R = c1 - c0
-        Z = np.zeros((nf, R))
-        Z[np.arange(c0, c1), np.arange(R)] = 1.0
-        G = np.zeros((R, g.mg, g.nx - 1, g.ny - 1))
-        G[:, 0] = ainv_level(ECt(Z, prob), prob, 0)
-        _, qx, qy = vort2flux(G, prob.Lam, g)
-        B[:, c0:c1] = E_apply(qx[:, 0], qy[:, 0], prob).T
+        Z = np.zeros((nf, c1 - c0))
+        Z[np.arange(c0, c1), np.arange(c1 - c0)] = 1.0
+        B[:, c0:c1] = B_times(prob, Z)
     return B
 
 

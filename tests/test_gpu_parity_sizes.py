@@ -94,6 +94,16 @@ def _field_errors(st, ost):
             "Fb": rel(st.Fb[:, 0], ost.Fb)}
 
 
+def test_headline_binv_matches_oracle(headline_oracle):
+    """nf = 628: B⁻¹ by the blocked (panel) Gauss–Jordan elimination."""
+    import ibpm_gpu as G
+    g = G.make_grid(bench.H, bench.BOUNDARY, bench.MG)
+    p = G.IBProblem(g, [G.make_cylinder(0.5, g.h, 0.0, 0.0, n=bench.NB)], bench.DT, bench.RE)
+    Binv = p.binv()
+    p.close()
+    assert rel(Binv, headline_oracle["prob"].Binv) < 1e-8
+
+
 def test_headline_fp64_matches_oracle(headline_oracle):
     o = headline_oracle
     st, cd, cl = _headline_gpu("fp64", o["start"], o["nsteps"])
