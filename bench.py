@@ -943,7 +943,7 @@ def run_ours(args, d):
                    "graph": "one CUDA graph replay per step",
                    "warmup_replays": "max(W, 10): the FP32-refined path's 8 two-sweep start-up steps are not timed",
                    "transform_plans": "radix-4 latency plan on single-level launches; multi-level launches "
-                                      "automatic (radix 8 from 16 slabs on, so the five-level ones stay radix 4)"},
+                                      "automatic: radix 8 from 4 slabs on (the all-level launches)"},
         "e2e": e2e_of(r32),
         "gpu_launches": r32["lps"] * K,
         "fp64_plain": {"value": value64, "ms_per_step": r64["total_ms"] / K, "e2e": e2e_of(r64),

@@ -37,26 +37,30 @@ __device__ __forceinline__ T g_entry(const T* smp, const Geom& g, int m) {
 
 constexpr int kMaxLev = 8;
 
-// p_ℓ[r] = Σ_i W[r, i] g_ℓ[i] for every level ℓ = 0 … mg−2: one warp per row r
-// of W (read once for all levels), lanes over i in a fixed order.
+// p_ℓ[r] = Σ_s Ws[r, s] smp_{ℓ+1}[s] for every level ℓ = 0 … mg−2, with
+// Ws = W A_s the projection folded with get_bc!'s averaging of the samples
+// (A_s: g = A_s · samples).  One warp per row r of Ws (read once for all
+// levels), lanes over s in a fixed order; the loads of four consecutive
+// lane steps are issued together.
 template <class T>
-__global__ void __launch_bounds__(256) bt_project_kernel(const T* __restrict__ W, const T* __restrict__ samples,
+__global__ void __launch_bounds__(128) bt_project_kernel(const T* __restrict__ Ws, const T* __restrict__ samples,
                                                          T* p, int k, int kp, Geom g) {
     pdl_wait();
     pdl_trigger();
-    const int nE = 2 * g.n1 + 2 * g.n2, ep = (nE + 3) & ~3, L = g.mg - 1;
-    const int sl = g.nx + g.ny + 4;
-    const int r = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    const int L = g.mg - 1;
+    const int sl = g.nx + g.ny + 4, sp = (sl + 3) & ~3;
+    const int r = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (r >= k) return;
     T acc[kMaxLev];
 #pragma unroll
     for (int l = 0; l < kMaxLev; ++l) acc[l] = T(0);
-    const T* row = W + (long long)r * ep;
-    for (int i = lane; i < nE; i += 32) {
-        const T w = __ldg(&row[i]);
+    const T* row = Ws + (long long)r * sp;
+#pragma unroll 4
+    for (int s = lane; s < sl; s += 32) {
+        const T wv = __ldg(&row[s]);
 #pragma unroll
         for (int l = 0; l < kMaxLev; ++l)
-            if (l < L) acc[l] += w * g_entry(samples + (long long)(l + 1) * sl, g, i);
+            if (l < L) acc[l] += wv * __ldg(&samples[(long long)(l + 1) * sl + s]);
     }
 #pragma unroll
     for (int l = 0; l < kMaxLev; ++l) {
@@ -90,6 +94,7 @@ __global__ void __launch_bounds__(256) bt_expand_kernel(const T* __restrict__ U,
     for (int l = 0; l < kMaxLev; ++l) acc[l] = T(0);
     for (int m = 0; m + 2 < g.mg; ++m) {
         const T* row = U + ((long long)m * nE + i) * kp;
+#pragma unroll 4
         for (int r = lane; r < k; r += 32) {
             const T u = __ldg(&row[r]);
 #pragma unroll
@@ -167,7 +172,8 @@ void parallel_for(int n, F f) {
 // below tol × R's largest column norm.  Then W = Qᵀ R, M = W Q and
 // U_m = Q M^m for m < nmat.  Every step has a fixed order, so the factors
 // do not depend on the thread count.
-int bt_lowrank(const std::vector<double>& R, int nE, int ep, int nmat, double tol, int kmax, BtLowRank& out) {
+int bt_lowrank(const std::vector<double>& R, int nx_, int ny_, int nmat, double tol, int kmax, BtLowRank& out) {
+    const int nE = 2 * (nx_ - 1) + 2 * (ny_ - 1), ep = (nE + 3) & ~3;
     std::vector<double> A((size_t)nE * nE);  // column-major residual columns
     parallel_for(nE, [&](int j0, int j1) {
         for (int j = j0; j < j1; ++j)
@@ -235,6 +241,33 @@ int bt_lowrank(const std::vector<double>& R, int nE, int ep, int nmat, double to
             }
         }
     });
+    // Ws = W A_s: edge entry m (get_bc! vertex v = m' + 1 of its edge) is
+    // sample v/2 of the edge's line (v even) or the mean of samples (v±1)/2
+    const int sl = nx_ + ny_ + 4, sp = (sl + 3) & ~3;
+    out.Ws.assign((size_t)k * sp, 0.0);
+    auto add_edge = [&](double* ws, const double* w, int off, int n1e, int seg) {
+        for (int mm = 0; mm < n1e; ++mm) {
+            const int v = mm + 1;
+            const double wv = w[off + mm];
+            if ((v & 1) == 0) ws[seg + v / 2] += wv;
+            else {
+                ws[seg + (v + 1) / 2] += 0.5 * wv;
+                ws[seg + (v - 1) / 2] += 0.5 * wv;
+            }
+        }
+    };
+    parallel_for(k, [&](int r0, int r1) {
+        for (int r = r0; r < r1; ++r) {
+            double* ws = &out.Ws[(size_t)r * sp];
+            const double* w = &out.W[(size_t)r * ep];
+            const int n1 = nx_ - 1, n2 = ny_ - 1;
+            add_edge(ws, w, 0, n1, 0);                                  // bottom: row samples at 0
+            add_edge(ws, w, n1, n1, nx_ / 2 + 1);                       // top
+            add_edge(ws, w, 2 * n1, n2, nx_ + 2);                       // left: column samples
+            add_edge(ws, w, 2 * n1 + n2, n2, nx_ + 2 + ny_ / 2 + 1);    // right
+        }
+    });
+    out.sp = sp;
     std::vector<double> M((size_t)k * k);
     parallel_for(k, [&](int a0, int a1) {
         for (int a = a0; a < a1; ++a)
@@ -266,11 +299,11 @@ int bt_lowrank(const std::vector<double>& R, int nE, int ep, int nmat, double to
 }
 
 cudaError_t launch_bt_project(const Geom& g, const BtChainArgs& a, cudaStream_t st) {
-    dim3 grid((a.k + 7) / 8);
+    dim3 grid((a.k + 3) / 4);
     if (a.f32)
-        return launch_k(bt_project_kernel<float>, grid, dim3(256), 0, st, static_cast<const float*>(a.W),
+        return launch_k(bt_project_kernel<float>, grid, dim3(128), 0, st, static_cast<const float*>(a.W),
                         static_cast<const float*>(a.samples), static_cast<float*>(a.p), a.k, a.kp, g);
-    return launch_k(bt_project_kernel<double>, grid, dim3(256), 0, st, static_cast<const double*>(a.W),
+    return launch_k(bt_project_kernel<double>, grid, dim3(128), 0, st, static_cast<const double*>(a.W),
                     static_cast<const double*>(a.samples), static_cast<double*>(a.p), a.k, a.kp, g);
 }
 

@@ -406,7 +406,7 @@ static int build_bt(ibpm_handle* h) {
     if (rc) return rc;
     if (e != cudaSuccess) return fail(h, IBPM_ERR_CUDA, std::string("R setup: ") + cudaGetErrorString(e));
     auto lr = std::make_shared<BtLowRank>();
-    if (bt_lowrank(Rh, nE, ep, std::max(0, mg - 2), 1e-14, std::min(nE, 1024), *lr)) return IBPM_OK;
+    if (bt_lowrank(Rh, g.nx, g.ny, std::max(0, mg - 2), 1e-14, std::min(nE, 1024), *lr)) return IBPM_OK;
     {
         std::lock_guard<std::mutex> lock(g_bt_mutex);
         g_bt_cache[BtCacheKey{g.nx, g.ny, mg}] = lr;
@@ -421,12 +421,12 @@ static int upload_bt(ibpm_handle* h, const BtLowRank& lr) {
     int rc;
     h->bt_k = lr.k;
     h->bt_kp = lr.kp;
-    const size_t nw = (size_t)lr.k * ep, nu = std::max<size_t>(1, lr.U.size()), np = (size_t)(mg - 1) * lr.kp;
+    const size_t nw = lr.Ws.size(), nu = std::max<size_t>(1, lr.U.size()), np = (size_t)(mg - 1) * lr.kp;
     const size_t slabs = (size_t)g.S * mg, ns = (size_t)bt_sample_len(g) * mg, ne = (size_t)ep * mg;
     if ((rc = dalloc(h, &h->btW, nw)) || (rc = dalloc(h, &h->btU, nu)) || (rc = dalloc(h, &h->btP, np)) ||
         (rc = dalloc(h, &h->btE, ne)) || (rc = dalloc(h, &h->btS, ns)) || (rc = dalloc(h, &h->btY, slabs)))
         return rc;
-    CK(cudaMemcpyAsync(h->btW, lr.W.data(), sizeof(double) * nw, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->btW, lr.Ws.data(), sizeof(double) * nw, cudaMemcpyHostToDevice, h->st));
     if (!lr.U.empty())
         CK(cudaMemcpyAsync(h->btU, lr.U.data(), sizeof(double) * lr.U.size(), cudaMemcpyHostToDevice, h->st));
     CK(cudaMemsetAsync(h->btP, 0, sizeof(double) * np, h->st));

@@ -622,7 +622,7 @@ __host__ __device__ constexpr int round4(int n) { return ((n + 3) / 4) * 4; }
 // bottom and top rows' sine transforms, then the sums themselves.
 template <int N, class T, int PL>
 __host__ __device__ constexpr int y_synth_slots() {
-    return (y_threads<N, T, PL>() / 32 + 1) * 2 * y_tile_w<N, T, PL>();
+    return (y_threads<N, T, PL>() / 32 + 2) * 2 * y_tile_w<N, T, PL>();
 }
 template <int N, class T, int PL, bool SYNTH = false>
 __host__ __device__ constexpr size_t y_smem_bytes(int n2) {
@@ -669,27 +669,35 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
     pdl_wait();
     pdl_trigger();
     if constexpr (SYNTH) {
-        const long long ep = ((2LL * n1 + 2LL * n2) + 3) & ~3LL;
+        const int ep = ((2 * n1 + 2 * n2) + 3) & ~3;
         const T* e = static_cast<const T*>(bs.e) + (long long)lev * ep;
         const T* sxt = static_cast<const T*>(bs.sx);
-        const int nx = bs.nx;
-        auto sinpix = [&](long long t) -> T {  // sin(π t / nx), t ≥ 0
-            t %= 2LL * nx;
+        const int nx = bs.nx, nx2 = 2 * bs.nx;
+        auto sinpix = [&](int t) -> T {  // sin(π t / nx), 0 ≤ t < 2 nx
             return t < nx ? __ldg(&sxt[t]) : -__ldg(&sxt[t - nx]);
         };
         T* red = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(tile + tile_d) +
                                       (size_t)G * ct_buf(N) * sizeof(V));
-        // bottom and top rows: Σ_i S(i, k) e(i) for the CTA's columns k
+        // bottom and top rows: Σ_i S(i, k) e(i) for the CTA's columns k, the
+        // sine argument (i + 1) k mod 2nx advanced by a fixed step per thread
         T accB[TW], accT[TW];
+        int tk[TW], dk[TW];
 #pragma unroll
-        for (int c = 0; c < TW; ++c) accB[c] = accT[c] = T(0);
+        for (int c = 0; c < TW; ++c) {
+            accB[c] = accT[c] = T(0);
+            const int k = i0 + c + 1;
+            tk[c] = (int)(((long long)(threadIdx.x + 1) * k) % nx2);
+            dk[c] = (int)(((long long)blockDim.x * k) % nx2);
+        }
         for (int i = threadIdx.x; i < n1; i += blockDim.x) {
             const T eb = e[i], et = e[n1 + i];
 #pragma unroll
             for (int c = 0; c < TW; ++c) {
-                const T sv = T(2) * sinpix((long long)(i + 1) * (i0 + c + 1));
+                const T sv = T(2) * sinpix(tk[c]);
                 accB[c] += sv * eb;
                 accT[c] += sv * et;
+                tk[c] += dk[c];
+                if (tk[c] >= nx2) tk[c] -= nx2;
             }
         }
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -710,9 +718,16 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
             T acc = T(0);
             for (int u = 0; u < nw; ++u) acc += red[u * 2 * TW + threadIdx.x];
             red[nw * 2 * TW + threadIdx.x] = acc;
+        } else if (threadIdx.x < 4 * TW) {
+            // S(1, k) and S(nx − 1, k) of the column c
+            const int c = (threadIdx.x - 2 * TW) >> 1;
+            const long long k = i0 + c + 1;
+            const int t = (int)(((threadIdx.x & 1) ? k * (nx - 1) : k) % nx2);
+            red[(nw + 1) * 2 * TW + (threadIdx.x - 2 * TW)] = T(2) * sinpix(t);
         }
         __syncthreads();
-        const T* bh = red + nw * 2 * TW;  // [0, TW): bottom, [TW, 2TW): top
+        const T* bh = red + nw * 2 * TW;         // [0, TW): bottom, [TW, 2TW): top
+        const T* sLR = red + (nw + 1) * 2 * TW;  // [2c]: S(1, k_c), [2c + 1]: S(nx−1, k_c)
         const T* eL = e + 2 * n1;
         const T* eR = eL + n2;
         for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
@@ -720,8 +735,7 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
             const int i = i0 + c;
             T v = T(0);
             if (i < n1) {
-                const long long k = i + 1;
-                v = T(2) * sinpix(k) * eL[j] + T(2) * sinpix(k * (nx - 1)) * eR[j];
+                v = sLR[2 * c] * eL[j] + sLR[2 * c + 1] * eR[j];
                 if (j == 0) v += bh[c];
                 if (j == n2 - 1) v += bh[TW + c];
             }

@@ -182,7 +182,7 @@ struct DstPlan {
 // of at least kAutoWideSlabs slabs (the columns of B, the moving bodies'
 // unit solves), else the single-slab plan (the levels of one step).
 enum DstPlanKind { DST_PLAN_LATENCY = 0, DST_PLAN_THROUGHPUT = 1, DST_PLAN_AUTO = 2 };
-constexpr int kAutoWideSlabs = 16;
+constexpr int kAutoWideSlabs = 4;
 // Doubles in the table block of one length (FP64 tables, then FP32 tables),
 // and with the throughput plan's twiddles after them.
 inline long long dst_table_doubles(int N) { return 6LL * N; }
@@ -288,10 +288,11 @@ cudaError_t launch_dst_lines(const Geom& g, const DstPlan& px, const void* Y, Sl
 // Green's function between well-separated point sets, smooth, with fast
 // decaying singular values):
 //     p_ℓ = W g_ℓ (g_ℓ = get_bc!(samples of ℓ+1)),  ℓ = 0 … mg−2
+//         (as Ws · samples, Ws = W with get_bc!'s averaging folded in)
 //     e_ℓ = g_ℓ + Σ_{m=0}^{mg−3−ℓ} U_m p_{ℓ+1+m},   U_m = Q (W Q)^m
 // which is e_ℓ = g_ℓ + R e_{ℓ+1} unrolled (two launches, none serial).
 struct BtChainArgs {
-    const void* W;        // k × pitch (bt_edge_pitch), row-major (T)
+    const void* W;        // Ws: k × sample pitch (bt_sample_len rounded to 4), row-major (T)
     const void* U;        // mg−2 matrices nE × kp, row-major (T)
     const void* samples;  // bt_sample_len per level (T), level-major
     void* p;              // (mg−1) × kp projections (T)
@@ -311,10 +312,11 @@ cudaError_t launch_to_f32(const double* a, float* b, long long n, cudaStream_t s
 // Host: the rank-k basis of R (bt.cu) — W = Qᵀ R (k × pitch) and
 // U_m = Q (W Q)^m (nE × kp each, m < nmat); -1 if the rank reaches kmax.
 struct BtLowRank {
-    int k = 0, kp = 0;
+    int k = 0, kp = 0, sp = 0;
     std::vector<double> W, U;
+    std::vector<double> Ws;   // W folded with get_bc!'s averaging of the line samples (k × sp)
 };
-int bt_lowrank(const std::vector<double>& R, int nE, int ep, int nmat, double tol, int kmax, BtLowRank& out);
+int bt_lowrank(const std::vector<double>& R, int nx, int ny, int nmat, double tol, int kmax, BtLowRank& out);
 
 // Base flux of a moving grid (base_flux!, timestepping.jl:273-318): on level
 // spacing hc, q0x = YY·(−hc Ω) + hc Ux0 at every x-flux of row J and

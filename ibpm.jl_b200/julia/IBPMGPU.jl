@@ -250,7 +250,7 @@ Plans of the device sine transforms for launches over one level (`single`)
 and over several (`multi`): `:latency` (radix 4, N/4 threads per line pair,
 the shortest chain per launch) or `:throughput` (radix 8, N/8 threads, fewer
 instructions); `multi` may also be `:auto` (the throughput plan for launches
-of 16 or more slabs, else `single`).  No counterpart in the reference, whose FFTW plans are fixed
+of 4 or more slabs, else `single`).  No counterpart in the reference, whose FFTW plans are fixed
 (src/fluid-operators/dst-inversion.jl:10-20).
 """
 function set_transform_plan!(prob::IBProblemGPU; single::Symbol=:latency, multi::Symbol=:auto)

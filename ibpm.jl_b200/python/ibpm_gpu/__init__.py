@@ -45,7 +45,7 @@ IBPM_PREC_FP32_REFINED = 1
 # pair (shortest chain per launch), radix 8 / N/8 threads (fewer instructions)
 IBPM_PLAN_LATENCY = 0
 IBPM_PLAN_THROUGHPUT = 1
-IBPM_PLAN_AUTO = 2      # multi-slab launches: throughput plan from 16 slabs on
+IBPM_PLAN_AUTO = 2      # multi-slab launches: throughput plan from 4 slabs on
 PRECISIONS = {"fp64": IBPM_PREC_FP64, "fp32_refined": IBPM_PREC_FP32_REFINED}
 KERNEL_COUNT = 12
 
@@ -576,7 +576,7 @@ def launches_per_step(prob):
 def set_transform_plan(prob, single_slab=IBPM_PLAN_LATENCY, multi_slab=IBPM_PLAN_AUTO):
     """Plans of the problem's sine transforms, for launches over one level
     (IBPM_PLAN_LATENCY or IBPM_PLAN_THROUGHPUT) and over several (either, or
-    IBPM_PLAN_AUTO: the throughput plan from 16 slabs on)."""
+    IBPM_PLAN_AUTO: the throughput plan from 4 slabs on)."""
     prob._check(prob.lib.ibpm_set_transform_plan(prob.handle, int(single_slab), int(multi_slab)))
 
 

@@ -336,7 +336,8 @@ const char* ibpm_kernel_name(int32_t k);
  *   IBPM_PLAN_THROUGHPUT  radix 8, N/8 threads: about two thirds of the
  *                         instructions, for launches that fill the GPU.
  *   IBPM_PLAN_AUTO        (multi-slab launches only) the throughput plan for
- *                         launches of 16 or more slabs (the columns of B,
+ *                         launches of 4 or more slabs (the all-level
+ *                         launches of a step, the columns of B,
  *                         the unit solves of moving bodies), else the
  *                         single-slab plan (the levels of one step).
  * From N = 1024 on both are the radix-8 plan.  A handle starts with the

@@ -77,3 +77,18 @@ def rel(a, b):
     d = np.max(np.abs(np.asarray(a) - b))
     s = np.max(np.abs(b))
     return d / s if s > 0 else d
+
+
+def rounding_perturbed_inverse(B, seed=0):
+    """inv(B') with B' = B perturbed entry by entry at the FP64 rounding level
+    (relative 2^-52 N(0, 1)): another equally valid B⁻¹.  Runs with it show
+    how far rounding alone moves the oracle's results through the Schur
+    complement, whose condition number grows with the body-point count."""
+    rng = np.random.default_rng(seed)
+    return np.linalg.inv(B * (1.0 + 2.0 ** -52 * rng.standard_normal(B.shape)))
+
+
+def force_scale_err(cl, ocl, ocd):
+    """max |CL − CL_oracle| over max |CD_oracle|: the lift error on the force
+    scale (the lift of a symmetric start is many orders below the drag)."""
+    return float(np.max(np.abs(np.asarray(cl) - np.asarray(ocl))) / np.max(np.abs(np.asarray(ocd))))
