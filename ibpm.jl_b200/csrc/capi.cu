@@ -1365,11 +1365,13 @@ static void set_plans(ibpm_handle* h, int single_slab, int multi_slab) {
 
 extern "C" int ibpm_set_transform_plan(ibpm_handle* h, int32_t single_slab, int32_t multi_slab) {
     if (!h) return IBPM_ERR_INVALID;
-    if (single_slab != IBPM_PLAN_LATENCY && single_slab != IBPM_PLAN_THROUGHPUT)
-        return fail(h, IBPM_ERR_INVALID, "single-slab plan must be IBPM_PLAN_LATENCY or IBPM_PLAN_THROUGHPUT");
-    if (multi_slab != IBPM_PLAN_LATENCY && multi_slab != IBPM_PLAN_THROUGHPUT && multi_slab != IBPM_PLAN_AUTO)
+    if (single_slab != IBPM_PLAN_LATENCY && single_slab != IBPM_PLAN_THROUGHPUT && single_slab != IBPM_PLAN_WARP)
         return fail(h, IBPM_ERR_INVALID,
-                    "multi-slab plan must be IBPM_PLAN_LATENCY, IBPM_PLAN_THROUGHPUT or IBPM_PLAN_AUTO");
+                    "single-slab plan must be IBPM_PLAN_LATENCY, IBPM_PLAN_THROUGHPUT or IBPM_PLAN_WARP");
+    if (multi_slab != IBPM_PLAN_LATENCY && multi_slab != IBPM_PLAN_THROUGHPUT && multi_slab != IBPM_PLAN_AUTO &&
+        multi_slab != IBPM_PLAN_WARP)
+        return fail(h, IBPM_ERR_INVALID,
+                    "multi-slab plan must be IBPM_PLAN_LATENCY, IBPM_PLAN_THROUGHPUT, IBPM_PLAN_AUTO or IBPM_PLAN_WARP");
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->st));
     set_plans(h, single_slab, multi_slab);

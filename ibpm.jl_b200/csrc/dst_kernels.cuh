@@ -63,6 +63,7 @@ __host__ __device__ constexpr int ct_nstages(int N, int PL = 0) {
     return n == 1 ? s : -1;
 }
 __host__ __device__ constexpr int ct_tp(int N, int PL = 0) {
+    if (PL == 2) return 32;   // the warp plan: the throughput plan's radices, one warp per line pair
     int t = (((ct_fine(N, PL) ? N / 4 : N / 8) + 31) / 32) * 32;
     return t < 32 ? 32 : t;
 }
@@ -909,9 +910,16 @@ cudaError_t launch_x_n(const Geom& g, const DstPlan& px, const XPassArgs& a, cud
 inline int launch_plan(int N, const DstPlan& p, int nslabs) {
     int pl = nslabs > 1 ? p.planN : p.plan1;
     if (pl == DST_PLAN_AUTO) pl = nslabs >= kAutoWideSlabs ? DST_PLAN_THROUGHPUT : p.plan1;
-    pl = ct_plan(N, pl);
-    return (pl == 1 && p.Wt) ? 1 : 0;
+    const int t = pl == DST_PLAN_WARP ? 2 : (pl == DST_PLAN_THROUGHPUT ? 1 : 0);
+    return (p.Wt && N < 1024) ? t : 0;
 }
+// Run f with the plan as a compile-time constant (0 latency, 1 throughput, 2 warp).
+#define IBPM_PLAN_SWITCH(N, pl, ...)                                  \
+    switch (pl) {                                                     \
+        case 1: { constexpr int PLN = ct_plan(N, 1); __VA_ARGS__; }   \
+        case 2: { constexpr int PLN = ct_plan(N, 2); __VA_ARGS__; }   \
+        default: { constexpr int PLN = 0; __VA_ARGS__; }              \
+    }
 
 // The (load, emit) pairs the library uses: FP64 solves, and the three passes
 // of an FP32 refinement correction.
@@ -922,15 +930,18 @@ inline int launch_plan(int N, const DstPlan& p, int nslabs) {
     X(XLOAD_F32, XEMIT_ACC_SUB) X(XLOAD_PLAIN, XEMIT_ADD_STORE) X(XLOAD_SUM, XEMIT_STORE)                  \
     X(XLOAD_F32_SUM, XEMIT_ADD)
 
-template <int N>
-cudaError_t launch_x_t(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {
-    const bool wide = launch_plan(N, px, a.nslabs) == 1;
-#define IBPM_X_DISPATCH(L, E)                                                               \
-    if (a.load == L && a.emit == E)                                                         \
-        return wide ? launch_x_n<N, L, E, ct_plan(N, 1)>(g, px, a, st) : launch_x_n<N, L, E, 0>(g, px, a, st);
+template <int N, int PL>
+cudaError_t launch_x_p(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {
+#define IBPM_X_DISPATCH(L, E) \
+    if (a.load == L && a.emit == E) return launch_x_n<N, L, E, PL>(g, px, a, st);
     IBPM_X_COMBOS(IBPM_X_DISPATCH)
 #undef IBPM_X_DISPATCH
     return cudaErrorInvalidValue;
+}
+
+template <int N>
+cudaError_t launch_x_t(const Geom& g, const DstPlan& px, const XPassArgs& a, cudaStream_t st) {
+    IBPM_PLAN_SWITCH(N, launch_plan(N, px, a.nslabs), return (launch_x_p<N, PLN>(g, px, a, st)))
 }
 
 template <int N, class T, int PL>
@@ -948,12 +959,9 @@ cudaError_t launch_y_n(const Geom& g, const DstPlan& py, const DstPlan& px, void
 template <int N>
 cudaError_t launch_y_t(const Geom& g, const DstPlan& py, const DstPlan& px, void* data, SlabMap map, int nslabs,
                        const SpecParams& sp, cudaStream_t st) {
-    constexpr int W = ct_plan(N, 1);
-    if (launch_plan(N, py, nslabs) == 1)
-        return sp.f32 ? launch_y_n<N, float, W>(g, py, px, data, map, nslabs, sp, st)
-                      : launch_y_n<N, double, W>(g, py, px, data, map, nslabs, sp, st);
-    return sp.f32 ? launch_y_n<N, float, 0>(g, py, px, data, map, nslabs, sp, st)
-                  : launch_y_n<N, double, 0>(g, py, px, data, map, nslabs, sp, st);
+    IBPM_PLAN_SWITCH(N, launch_plan(N, py, nslabs),
+                     return sp.f32 ? launch_y_n<N, float, PLN>(g, py, px, data, map, nslabs, sp, st)
+                                   : launch_y_n<N, double, PLN>(g, py, px, data, map, nslabs, sp, st))
 }
 
 template <int N, class T, int PL>
@@ -971,12 +979,9 @@ cudaError_t launch_ybc_n(const Geom& g, const DstPlan& py, const DstPlan& px, vo
 template <int N>
 cudaError_t launch_ybc_t(const Geom& g, const DstPlan& py, const DstPlan& px, void* out, SlabMap map, int nslabs,
                          const SpecParams& sp, const BtSynth& bs, cudaStream_t st) {
-    constexpr int W = ct_plan(N, 1);
-    if (launch_plan(N, py, nslabs) == 1)
-        return sp.f32 ? launch_ybc_n<N, float, W>(g, py, px, out, map, nslabs, sp, bs, st)
-                      : launch_ybc_n<N, double, W>(g, py, px, out, map, nslabs, sp, bs, st);
-    return sp.f32 ? launch_ybc_n<N, float, 0>(g, py, px, out, map, nslabs, sp, bs, st)
-                  : launch_ybc_n<N, double, 0>(g, py, px, out, map, nslabs, sp, bs, st);
+    IBPM_PLAN_SWITCH(N, launch_plan(N, py, nslabs),
+                     return sp.f32 ? launch_ybc_n<N, float, PLN>(g, py, px, out, map, nslabs, sp, bs, st)
+                                   : launch_ybc_n<N, double, PLN>(g, py, px, out, map, nslabs, sp, bs, st))
 }
 
 template <int N, class T, int PL>
@@ -991,12 +996,9 @@ cudaError_t launch_lines_n(const Geom& g, const DstPlan& px, const void* Y, Slab
 template <int N>
 cudaError_t launch_lines_t(const Geom& g, const DstPlan& px, const void* Y, SlabMap map, int nslabs, void* smp,
                            int f32, cudaStream_t st) {
-    constexpr int W = ct_plan(N, 1);
-    if (launch_plan(N, px, 1) == 1)
-        return f32 ? launch_lines_n<N, float, W>(g, px, Y, map, nslabs, smp, st)
-                   : launch_lines_n<N, double, W>(g, px, Y, map, nslabs, smp, st);
-    return f32 ? launch_lines_n<N, float, 0>(g, px, Y, map, nslabs, smp, st)
-               : launch_lines_n<N, double, 0>(g, px, Y, map, nslabs, smp, st);
+    IBPM_PLAN_SWITCH(N, launch_plan(N, px, 1),
+                     return f32 ? launch_lines_n<N, float, PLN>(g, px, Y, map, nslabs, smp, st)
+                                : launch_lines_n<N, double, PLN>(g, px, Y, map, nslabs, smp, st))
 }
 
 template <class K>
@@ -1026,7 +1028,8 @@ template <int N>
 cudaError_t attr_t() {
     cudaError_t e = attr_plan<N, 0>();
     if (e != cudaSuccess || ct_plan(N, 1) == 0) return e;
-    return attr_plan<N, ct_plan(N, 1)>();
+    if ((e = attr_plan<N, ct_plan(N, 1)>())) return e;
+    return attr_plan<N, ct_plan(N, 2)>();
 }
 
 }  // namespace dstk

@@ -181,7 +181,7 @@ struct DstPlan {
 // DST_PLAN_AUTO (multi-slab launches only): the throughput plan for launches
 // of at least kAutoWideSlabs slabs (the columns of B, the moving bodies'
 // unit solves), else the single-slab plan (the levels of one step).
-enum DstPlanKind { DST_PLAN_LATENCY = 0, DST_PLAN_THROUGHPUT = 1, DST_PLAN_AUTO = 2 };
+enum DstPlanKind { DST_PLAN_LATENCY = 0, DST_PLAN_THROUGHPUT = 1, DST_PLAN_AUTO = 2, DST_PLAN_WARP = 3 };
 constexpr int kAutoWideSlabs = 4;
 // Doubles in the table block of one length (FP64 tables, then FP32 tables),
 // and with the throughput plan's twiddles after them.

@@ -79,13 +79,21 @@ def rel(a, b):
     return d / s if s > 0 else d
 
 
-def rounding_perturbed_inverse(B, seed=0):
-    """inv(B') with B' = B perturbed entry by entry at the FP64 rounding level
-    (relative 2^-52 N(0, 1)): another equally valid B⁻¹.  Runs with it show
-    how far rounding alone moves the oracle's results through the Schur
-    complement, whose condition number grows with the body-point count."""
+def rounding_perturbed_state(st, seed=0):
+    """A copy of the oracle state ``st`` with every field perturbed entry by
+    entry at the FP64 rounding level (relative 2^-52 N(0, 1)): the start a
+    second, equally valid, implementation might hold after one rounding.
+    Runs from it show how far rounding alone moves the oracle's results.
+    The step amplifies it: the force E(qs + q0) is a cancelling difference
+    (|q0| / |F| of several hundred near the wall) and goes through B⁻¹,
+    whose condition number grows with the body-point count."""
     rng = np.random.default_rng(seed)
-    return np.linalg.inv(B * (1.0 + 2.0 ** -52 * rng.standard_normal(B.shape)))
+    out = st.copy()
+    for name in ("Gamma", "psi", "qx", "qy"):
+        a = getattr(out, name)
+        setattr(out, name, a * (1.0 + 2.0 ** -52 * rng.standard_normal(a.shape)))
+    out.nonlin = [n * (1.0 + 2.0 ** -52 * rng.standard_normal(n.shape)) for n in out.nonlin]
+    return out
 
 
 def force_scale_err(cl, ocl, ocd):
