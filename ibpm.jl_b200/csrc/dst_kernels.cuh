@@ -34,6 +34,12 @@
 
 #include "ibpm_internal.cuh"
 
+// Resident CTAs per SM that the throughput plan's kernels are compiled for
+// (the register budget per thread follows from it).
+#ifndef IBPM_WIDE_MIN_BLOCKS
+#define IBPM_WIDE_MIN_BLOCKS 1
+#endif
+
 namespace ibpm {
 namespace dstk {
 
@@ -63,7 +69,6 @@ __host__ __device__ constexpr int ct_nstages(int N, int PL = 0) {
     return n == 1 ? s : -1;
 }
 __host__ __device__ constexpr int ct_tp(int N, int PL = 0) {
-    if (PL == 2) return 32;   // the warp plan: the throughput plan's radices, one warp per line pair
     int t = (((ct_fine(N, PL) ? N / 4 : N / 8) + 31) / 32) * 32;
     return t < 32 ? 32 : t;
 }
@@ -419,7 +424,8 @@ __host__ __device__ constexpr size_t x_smem_bytes() {
 }
 
 template <int N, int LOAD, int EMIT, int PL>
-__global__ void __launch_bounds__(ct_groups(N, PL) * ct_tp(N, PL)) dst_x_kernel(XPassArgs a, Geom g, DstPlan p) {
+__global__ void __launch_bounds__(ct_groups(N, PL) * ct_tp(N, PL), ct_fine(N, PL) ? 1 : IBPM_WIDE_MIN_BLOCKS)
+    dst_x_kernel(XPassArgs a, Geom g, DstPlan p) {
     using T = x_real_t<LOAD>;
     using V = cplx_t<T>;
     constexpr int TP = ct_tp(N, PL);
@@ -643,7 +649,8 @@ template <int N, class T, int PL, bool SYNTH = false>
 // (3 resident 256-thread CTAs per SM keep the FP64 pass at 80 registers without
 // spills: the five-slab trial solve's y-pass then needs 1.4 waves instead of 2.2)
 __global__ void __launch_bounds__(y_threads<N, T, PL>(),
-                                  (!ct_fine(N, PL) || N > 512) ? 1 : (y_threads<N, T, PL>() <= 128 ? 5 : 3))
+                                  N > 512 ? 1 : (!ct_fine(N, PL) ? IBPM_WIDE_MIN_BLOCKS
+                                                                 : (y_threads<N, T, PL>() <= 128 ? 5 : 3)))
     dst_y_kernel(T* data, SlabMap map, Geom g, DstPlan p, const T* __restrict__ cx, SpecParams sp,
                  T* out = nullptr, BtSynth bs = BtSynth{}) {
     using V = cplx_t<T>;
@@ -910,14 +917,12 @@ cudaError_t launch_x_n(const Geom& g, const DstPlan& px, const XPassArgs& a, cud
 inline int launch_plan(int N, const DstPlan& p, int nslabs) {
     int pl = nslabs > 1 ? p.planN : p.plan1;
     if (pl == DST_PLAN_AUTO) pl = nslabs >= kAutoWideSlabs ? DST_PLAN_THROUGHPUT : p.plan1;
-    const int t = pl == DST_PLAN_WARP ? 2 : (pl == DST_PLAN_THROUGHPUT ? 1 : 0);
-    return (p.Wt && N < 1024) ? t : 0;
+    return (pl == DST_PLAN_THROUGHPUT && p.Wt && N < 1024) ? 1 : 0;
 }
-// Run f with the plan as a compile-time constant (0 latency, 1 throughput, 2 warp).
+// Run the call with the plan as a compile-time constant PLN (0 latency, 1 throughput).
 #define IBPM_PLAN_SWITCH(N, pl, ...)                                  \
     switch (pl) {                                                     \
         case 1: { constexpr int PLN = ct_plan(N, 1); __VA_ARGS__; }   \
-        case 2: { constexpr int PLN = ct_plan(N, 2); __VA_ARGS__; }   \
         default: { constexpr int PLN = 0; __VA_ARGS__; }              \
     }
 
@@ -1028,8 +1033,7 @@ template <int N>
 cudaError_t attr_t() {
     cudaError_t e = attr_plan<N, 0>();
     if (e != cudaSuccess || ct_plan(N, 1) == 0) return e;
-    if ((e = attr_plan<N, ct_plan(N, 1)>())) return e;
-    return attr_plan<N, ct_plan(N, 2)>();
+    return attr_plan<N, ct_plan(N, 1)>();
 }
 
 }  // namespace dstk

@@ -181,7 +181,7 @@ struct DstPlan {
 // DST_PLAN_AUTO (multi-slab launches only): the throughput plan for launches
 // of at least kAutoWideSlabs slabs (the columns of B, the moving bodies'
 // unit solves), else the single-slab plan (the levels of one step).
-enum DstPlanKind { DST_PLAN_LATENCY = 0, DST_PLAN_THROUGHPUT = 1, DST_PLAN_AUTO = 2, DST_PLAN_WARP = 3 };
+enum DstPlanKind { DST_PLAN_LATENCY = 0, DST_PLAN_THROUGHPUT = 1, DST_PLAN_AUTO = 2 };
 constexpr int kAutoWideSlabs = 4;
 // Doubles in the table block of one length (FP64 tables, then FP32 tables),
 // and with the throughput plan's twiddles after them.
@@ -366,6 +366,9 @@ cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st);
 
 cudaError_t launch_coarsify(const Geom& g, double* G, SlabMap fine_map, SlabMap coarse_map,
                             int nslabs, cudaStream_t st);
+// FP64 residual of vort2flux! on every level (all mg slabs of G and psi, the
+// handle's slab layout), stored in FP32 into r (stencil.cu).
+cudaError_t launch_resid_lap(const Geom& g, const double* G, const double* psi, float* r, cudaStream_t st);
 
 struct CurlArgs {
     const double* psi; SlabMap psi_map;

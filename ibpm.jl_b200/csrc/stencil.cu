@@ -211,4 +211,49 @@ cudaError_t launch_curl(const Geom& g, const CurlArgs& a, cudaStream_t st) {
     return launch_k(curl_kernel, grid, dim3(256), 0, st, a, g);
 }
 
+// ---------------------------------------------------------------------------
+// FP64 residual of one refinement sweep of vort2flux! on every level at once,
+// stored in FP32 (it is small: the change of ψ since its previous solve):
+//     r_ℓ = Γ_ℓ + apply_bc!(get_bc!(ψ_{ℓ+1})) − L ψ_ℓ
+// with L x = 4x − Σ neighbours (zero Dirichlet edges), the operator the
+// DST-I solve with Λ inverts (laplacian.jl:14-41), and the edge term of a
+// level of vort2flux! (curl.jl:151-158, mg-utils.jl:7-60); none at the
+// coarsest level.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) resid_lap_kernel(const double* __restrict__ G, const double* __restrict__ psi,
+                                                        float* r, Geom g) {
+    pdl_wait();
+    pdl_trigger();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int lev = blockIdx.z;
+    const int n1 = g.n1, n2 = g.n2, P = g.P;
+    if (i >= n1 || j >= n2) return;
+    const double* x = psi + (long long)lev * g.S;
+    const long long o = (long long)j * P + i;
+    const double xc = x[o];
+    double nb = 0.0;
+    if (i > 0) nb += x[o - 1];
+    if (i + 1 < n1) nb += x[o + 1];
+    if (j > 0) nb += x[o - P];
+    if (j + 1 < n2) nb += x[o + P];
+    double v = G[(long long)lev * g.S + o];
+    if (lev + 1 < g.mg) {
+        CoarseBC cb;
+        cb.rc = psi + (long long)(lev + 1) * g.S; cb.P = P; cb.nx = g.nx; cb.ny = g.ny;
+        if (j == 0) v += cb.bot(i + 1);
+        if (j == n2 - 1) v += cb.top(i + 1);
+        if (i == 0) v += cb.left(j + 1);
+        if (i == n1 - 1) v += cb.right(j + 1);
+    }
+    v -= 4.0 * xc - nb;
+    r[(long long)lev * g.S + o] = (float)v;
+}
+
+cudaError_t launch_resid_lap(const Geom& g, const double* G, const double* psi, float* r, cudaStream_t st) {
+    dim3 blk(32, 8);
+    dim3 grid((g.n1 + 31) / 32, (g.n2 + 7) / 8, g.mg);
+    return launch_k(resid_lap_kernel, grid, blk, 0, st, G, psi, r, g);
+}
+
 }  // namespace ibpm

@@ -46,7 +46,6 @@ IBPM_PREC_FP32_REFINED = 1
 IBPM_PLAN_LATENCY = 0
 IBPM_PLAN_THROUGHPUT = 1
 IBPM_PLAN_AUTO = 2      # multi-slab launches: throughput plan from 4 slabs on
-IBPM_PLAN_WARP = 3      # the throughput plan's radices with one warp per line pair
 PRECISIONS = {"fp64": IBPM_PREC_FP64, "fp32_refined": IBPM_PREC_FP32_REFINED}
 KERNEL_COUNT = 12
 

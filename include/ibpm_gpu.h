@@ -350,7 +350,6 @@ const char* ibpm_kernel_name(int32_t k);
 #define IBPM_PLAN_LATENCY    0
 #define IBPM_PLAN_THROUGHPUT 1
 #define IBPM_PLAN_AUTO       2
-#define IBPM_PLAN_WARP       3   /* the throughput plan's radices with one warp (32 threads) per line pair */
 int ibpm_set_transform_plan(ibpm_handle* h, int32_t single_slab, int32_t multi_slab);
 int ibpm_get_transform_plan(const ibpm_handle* h, int32_t* single_slab, int32_t* multi_slab);
 

@@ -1,5 +1,7 @@
 """Problem definitions shared by the parity tests and the golden-fixture
 generator.  Each case is built identically for the oracle and for the GPU."""
+import contextlib
+
 import numpy as np
 
 CASES = {
@@ -79,21 +81,30 @@ def rel(a, b):
     return d / s if s > 0 else d
 
 
-def rounding_perturbed_state(st, seed=0):
-    """A copy of the oracle state ``st`` with every field perturbed entry by
-    entry at the FP64 rounding level (relative 2^-52 N(0, 1)): the start a
-    second, equally valid, implementation might hold after one rounding.
-    Runs from it show how far rounding alone moves the oracle's results.
-    The step amplifies it: the force E(qs + q0) is a cancelling difference
-    (|q0| / |F| of several hundred near the wall) and goes through B⁻¹,
-    whose condition number grows with the body-point count."""
+@contextlib.contextmanager
+def rounding_noise(seed=0):
+    """Within the block, every sine-transform solve of the oracle (dst_inv,
+    dst-inversion.jl:39-50) returns its result plus FP64 rounding-sized noise
+    relative to the field's magnitude, 2^-52 · max|x| · N(0, 1) per entry: the
+    size of a fast transform's rounding error, which is relative to the
+    norm of the field, not to each entry.  Runs of the oracle inside show how
+    far rounding alone moves its results; the step amplifies it, because the
+    force E(qs + q0) is a cancelling difference at the wall and goes through
+    B⁻¹, whose condition number grows with the body-point count."""
+    from oracle import ibpm_ref as R
+    orig = R.dst_inv
     rng = np.random.default_rng(seed)
-    out = st.copy()
-    for name in ("Gamma", "psi", "qx", "qy"):
-        a = getattr(out, name)
-        setattr(out, name, a * (1.0 + 2.0 ** -52 * rng.standard_normal(a.shape)))
-    out.nonlin = [n * (1.0 + 2.0 ** -52 * rng.standard_normal(n.shape)) for n in out.nonlin]
-    return out
+
+    def noisy(b, M, scale):
+        x = orig(b, M, scale)
+        amp = 2.0 ** -52 * np.max(np.abs(x), axis=(-2, -1), keepdims=True)
+        return x + amp * rng.standard_normal(x.shape)
+
+    R.dst_inv = noisy
+    try:
+        yield
+    finally:
+        R.dst_inv = orig
 
 
 def force_scale_err(cl, ocl, ocd):

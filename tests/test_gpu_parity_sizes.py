@@ -7,11 +7,12 @@ the C ABI (the small-grid parity cases are in test_gpu_parity.py):
   from the seeded vortex start, stepped with advance!
   (src/timestepping/timestepping.jl:35-67).  Here rounding alone moves the
   fields by ~1e-9 per step: the force E(qs + q0) cancels to a few hundredths
-  of |q0| at the wall and goes through B⁻¹ (cond(B) ≈ 3e5).  Two oracle runs
-  from starts that differ at the rounding level (ibpm_cases.
-  rounding_perturbed_state) measure that spread.  FP64: CD to 1e-10, CL to
-  1e-10 on the force scale, every field within 10× the oracle's spread (and
-  1e-8); FP32-refined: CD and CL (force scale) to 1e-6, the fields to 1e-6;
+  of |q0| at the wall and goes through B⁻¹ (cond(B) ≈ 3e5).  A second oracle
+  (B built and run) with transform-sized rounding noise in every solve
+  (ibpm_cases.rounding_noise) measures that spread.  FP64: CD to 1e-10, CL
+  to 1e-10 on the force scale, every field within 10× the oracle's spread
+  (and 1e-8); FP32-refined: CD and CL (force scale) to 1e-6, the fields to
+  1e-6;
 * the adjoint workload's grid (256x256 x 4 levels) against the oracle's
   discrete adjoint;
 * a NACA member of the batch workload as the batch builds it.
@@ -73,10 +74,13 @@ def headline_oracle():
     start = st.copy()
     nsteps = 10
     cd, cl = R.run(p, st, nsteps)
-    # the same run from a start perturbed at the rounding level
-    from ibpm_cases import rounding_perturbed_state
-    st2 = rounding_perturbed_state(start, seed=1)
-    R.run(p, st2, nsteps)
+    # the same problem and run with transform-sized rounding noise in every solve
+    from ibpm_cases import rounding_noise
+    with rounding_noise(seed=1):
+        p2 = R.IBProblem(grid=g, bodies=[R.make_cylinder(0.5, g.h, 0.0, 0.0, n=bench.NB)], dt=bench.DT,
+                         Re=bench.RE)
+        st2 = start.copy()
+        R.run(p2, st2, nsteps)
     return dict(prob=p, start=start, end=st, cd=np.asarray(cd), cl=np.asarray(cl), nsteps=nsteps,
                 spread=_field_errors(st2, st))
 
@@ -172,10 +176,12 @@ def test_adjoint_workload_grid_matches_oracle_adjoint():
     R.refresh_flux(ost, op)
     nsteps, window, k = 6, 3, 3
     J, Gb, *_ = A.mean_force_gradient(op, ost.copy(), nsteps, window, k=k)
-    # the oracle's own spread from a start perturbed at the rounding level
-    # (the gradient goes through B⁻¹ and B⁻ᵀ every step)
-    from ibpm_cases import rounding_perturbed_state
-    _, Gb2, *_ = A.mean_force_gradient(op, rounding_perturbed_state(ost, seed=2), nsteps, window, k=k)
+    # the oracle's own spread under transform-sized rounding noise (its B
+    # rebuilt too: the gradient goes through B⁻¹ and B⁻ᵀ every step)
+    from ibpm_cases import rounding_noise
+    with rounding_noise(seed=2):
+        op2 = R.IBProblem(grid=og, bodies=[R.make_cylinder(0.5, og.h, 0.0, 0.0, n=c["nb"])], dt=c["dt"], Re=100.0)
+        _, Gb2, *_ = A.mean_force_gradient(op2, ost.copy(), nsteps, window, k=k)
     spread = rel(R.gamma_to_ref(Gb2), R.gamma_to_ref(Gb))
     gg = G.make_grid(c["h"], bench.BOUNDARY, c["mg"])
     gp = G.IBProblem(gg, [G.make_cylinder(0.5, gg.h, 0.0, 0.0, n=c["nb"])], c["dt"], 100.0)
