@@ -527,21 +527,14 @@ static int vort2flux_refined_bt(ibpm_handle* h, double* G, int nsw, double* q, i
         LAUNCH(K_COARSIFY, 8.0 * 1.25 * slab,
                launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), 1, h->st));
     SlabMap all = levmap(g, 0, mg, bs);
-    static const bool split = [] { const char* v = getenv("IBPM_BT_RESID"); return v && v[0] == '1'; }();
     for (int s = 0; s < nsw; ++s) {
+        // the residual of every level in one stencil launch (FP32 out), then
+        // its x-transform in place: a light x-pass that more CTAs share an SM with
+        LAUNCH(K_RESID, (8.0 + 8.0 + 4.0) * slab * mg, launch_resid_lap(g, G, h->psi, h->T32, h->st));
         XPassArgs a{};
-        if (split) {
-            LAUNCH(K_RESID, (8.0 + 8.0 + 4.0) * slab * mg, launch_resid_lap(g, G, h->psi, h->T32, h->st));
-            a.in = h->T32; a.out = h->T32; a.in_map = all; a.out_map = all;
-            a.nslabs = mg; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_F32; a.emit = XEMIT_F32;
-            LAUNCH(K_DSTX, 8.0 * slab * mg, launch_dst_x(g, h->px, a, h->st));
-        } else {
-            a.in = G; a.out = h->T32; a.in_map = all; a.out_map = all;
-            a.coarse = h->psi; a.coarse_map = levmap(g, 1, mg, bs);
-            a.aux = h->psi; a.aux_map = all;
-            a.nslabs = mg; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_RES_LAP; a.emit = XEMIT_F32;
-            LAUNCH(K_DSTX, (8.0 + 8.0 + 4.0) * slab * mg, launch_dst_x(g, h->px, a, h->st));
-        }
+        a.in = h->T32; a.out = h->T32; a.in_map = all; a.out_map = all;
+        a.nslabs = mg; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_F32; a.emit = XEMIT_F32;
+        LAUNCH(K_DSTX, 8.0 * slab * mg, launch_dst_x(g, h->px, a, h->st));
         LAUNCH(K_DSTY, 8.0 * slab * mg,
                launch_dst_y(g, h->py, h->px, h->T32, all, mg, spec(h, SPEC_DELTA, 1), h->st));
         int rc = bt_edges(h, h->T32, true);

@@ -1,7 +1,5 @@
 """Problem definitions shared by the parity tests and the golden-fixture
 generator.  Each case is built identically for the oracle and for the GPU."""
-import contextlib
-
 import numpy as np
 
 CASES = {
@@ -81,30 +79,19 @@ def rel(a, b):
     return d / s if s > 0 else d
 
 
-@contextlib.contextmanager
-def rounding_noise(seed=0):
-    """Within the block, every sine-transform solve of the oracle (dst_inv,
-    dst-inversion.jl:39-50) returns its result plus FP64 rounding-sized noise
-    relative to the field's magnitude, 2^-52 · max|x| · N(0, 1) per entry: the
-    size of a fast transform's rounding error, which is relative to the
-    norm of the field, not to each entry.  Runs of the oracle inside show how
-    far rounding alone moves its results; the step amplifies it, because the
-    force E(qs + q0) is a cancelling difference at the wall and goes through
-    B⁻¹, whose condition number grows with the body-point count."""
-    from oracle import ibpm_ref as R
-    orig = R.dst_inv
-    rng = np.random.default_rng(seed)
+# A body point exactly on a grid line puts δh samples exactly at |r| = h, 2h,
+# 3h, where the reference's smoothed delta (rounded 10-digit coefficients,
+# interface-coupling.jl:32-56) jumps by up to 3e-9: which side a sample takes
+# depends on the last bit of r.  Cylinders centred on grid nodes have such
+# points; shifting a body by OFF_GRID (a few 1e-7, not a multiple of h) moves
+# every point off the grid lines.
+OFF_GRID = (1.234e-7, -0.711e-7)
 
-    def noisy(b, M, scale):
-        x = orig(b, M, scale)
-        amp = 2.0 ** -52 * np.max(np.abs(x), axis=(-2, -1), keepdims=True)
-        return x + amp * rng.standard_normal(x.shape)
 
-    R.dst_inv = noisy
-    try:
-        yield
-    finally:
-        R.dst_inv = orig
+def ulp_moved_body(mod, body):
+    """The same body with every point moved by one ulp (towards +inf)."""
+    return mod.Body(xb=np.nextafter(body.xb, np.inf), ds=body.ds.copy()) if hasattr(mod, "Body") else \
+        mod.RigidBody(xb=np.nextafter(body.xb, np.inf), ds=body.ds.copy())
 
 
 def force_scale_err(cl, ocl, ocd):

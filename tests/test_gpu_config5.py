@@ -2,7 +2,10 @@
 (0, ±0.75)) at Re = 150 on 1024x1024 cells x 5 levels, h = 0.005, dt = 0.001
 (src/timestepping/timestepping.jl:35-67 on the geometry of
 examples/double_cyl.jl:19-28).  Its Schur complement (nf = 2512) is inverted by
-the blocked Gauss–Jordan elimination.
+the blocked Gauss–Jordan elimination.  The cylinders are moved off the grid
+lines by ~1e-7 (ibpm_cases.OFF_GRID): points on grid lines sample δh on its
+rounded-coefficient jumps, where a one-ulp move of a point moves the results
+by ~1e-9.
 
 The oracle's own B at this size takes tens of minutes on the host, so B⁻¹ is
 checked column-wise instead: the oracle's B_times! (laplacian.jl:143-169) of a
@@ -10,10 +13,8 @@ few unit vectors, multiplied by the device's B⁻¹, gives the unit vectors to
 the accuracy an inverse has, 10·n·ε·cond₂(B), with ‖B⁻¹‖₂ from the device's
 inverse and ‖B‖₂ by power iteration on the oracle's B.  The steps are then
 checked against the oracle run with the device's B⁻¹ (every other operator
-the oracle's own).  Rounding alone moves the fields through the cancelling
-force E(qs + q0) and B⁻¹: a second oracle run with transform-sized rounding
-noise in every solve measures that spread, and the device must stay within
-10× of it; CD and CL (force scale) to 1e-10."""
+the oracle's own): FP64 to 1e-10, FP32-refined to 1e-6 (CL on the force
+scale)."""
 import numpy as np
 import pytest
 
@@ -24,17 +25,22 @@ pytestmark = pytest.mark.gpu
 C5 = dict(h=0.005, mg=5, Re=150.0, dt=0.001, nb=628, centres=(0.75, -0.75))
 
 
+def _centres():
+    from ibpm_cases import OFF_GRID
+    return [(OFF_GRID[0], y + OFF_GRID[1]) for y in C5["centres"]]
+
+
 def _oracle(build_binv=False):
     from oracle import ibpm_ref as R
     g = R.make_grid(C5["h"], bench.BOUNDARY, C5["mg"])
-    bodies = [R.make_cylinder(0.5, g.h, 0.0, y, n=C5["nb"]) for y in C5["centres"]]
+    bodies = [R.make_cylinder(0.5, g.h, x, y, n=C5["nb"]) for x, y in _centres()]
     return R.IBProblem(grid=g, bodies=bodies, dt=C5["dt"], Re=C5["Re"], build_binv=build_binv)
 
 
 def _gpu(precision="fp64"):
     import ibpm_gpu as G
     g = G.make_grid(C5["h"], bench.BOUNDARY, C5["mg"])
-    bodies = [G.make_cylinder(0.5, g.h, 0.0, y, n=C5["nb"]) for y in C5["centres"]]
+    bodies = [G.make_cylinder(0.5, g.h, x, y, n=C5["nb"]) for x, y in _centres()]
     return G.IBProblem(g, bodies, C5["dt"], C5["Re"], freestream=(1.0, 0.0, 0.0), precision=precision)
 
 
@@ -82,10 +88,6 @@ def test_steps_match_oracle(pair, precision, tol):
     op, gp64 = pair
     gp = gp64 if precision == "fp64" else _gpu(precision)
     ost = random_state(op, seed=17, amp=1e-4)
-    from ibpm_cases import rounding_noise
-    ost2 = ost.copy()
-    with rounding_noise(seed=3):
-        R.run(op, ost2, 3)
     st = G.IBState(gp)
     to_gpu_state(ost, st)
     G.push_state(st, gp)
@@ -95,8 +97,5 @@ def test_steps_match_oracle(pair, precision, tol):
         gp.close()
     ocd, ocl = R.run(op, ost, 3)
     assert rel(cd, ocd) < tol and force_scale_err(cl, ocl, ocd) < tol
-    for name, a, b, b2 in (("Gamma", st.Gamma, R.gamma_to_ref(ost.Gamma), R.gamma_to_ref(ost2.Gamma)),
-                           ("q", st.q, R.flux_to_ref(ost.qx, ost.qy), R.flux_to_ref(ost2.qx, ost2.qy))):
-        spread = rel(b2, b)
-        err = rel(a, b)
-        assert err < max(tol, 10.0 * spread), (name, float(err), float(spread))
+    assert rel(st.Gamma, R.gamma_to_ref(ost.Gamma)) < tol
+    assert rel(st.q, R.flux_to_ref(ost.qx, ost.qy)) < tol
