@@ -145,11 +145,6 @@ __global__ void bt_gather_kernel(Geom g, int c0, int ncol, const double* psi, lo
     R[(long long)m * ep + c0 + b] = v;
 }
 
-__global__ void to_f32_kernel(const double* a, float* b, long long n) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        b[i] = (float)a[i];
-}
-
 // Run f(t0, t1) over [0, n) split across the host's threads.
 template <class F>
 void parallel_for(int n, F f) {
@@ -300,23 +295,14 @@ int bt_lowrank(const std::vector<double>& R, int nx_, int ny_, int nmat, double 
 
 cudaError_t launch_bt_project(const Geom& g, const BtChainArgs& a, cudaStream_t st) {
     dim3 grid((a.k + 3) / 4);
-    if (a.f32)
-        return launch_k(bt_project_kernel<float>, grid, dim3(128), 0, st, static_cast<const float*>(a.W),
-                        static_cast<const float*>(a.samples), static_cast<float*>(a.p), a.k, a.kp, g);
-    return launch_k(bt_project_kernel<double>, grid, dim3(128), 0, st, static_cast<const double*>(a.W),
-                    static_cast<const double*>(a.samples), static_cast<double*>(a.p), a.k, a.kp, g);
+    return launch_k(bt_project_kernel<double>, grid, dim3(128), 0, st, a.W, a.samples, a.p, a.k, a.kp, g);
 }
 
 cudaError_t launch_bt_expand(const Geom& g, const BtChainArgs& a, cudaStream_t st) {
     dim3 grid((bt_edge_len(g) + 7) / 8);
-    const size_t smem = (size_t)(g.mg - 1) * a.kp * (a.f32 ? sizeof(float) : sizeof(double));
-    if (a.f32)
-        return launch_k(bt_expand_kernel<float>, grid, dim3(256), smem, st, static_cast<const float*>(a.U),
-                        static_cast<const float*>(a.samples), static_cast<const float*>(a.p),
-                        static_cast<float*>(a.e), a.k, a.kp, g);
-    return launch_k(bt_expand_kernel<double>, grid, dim3(256), smem, st, static_cast<const double*>(a.U),
-                    static_cast<const double*>(a.samples), static_cast<const double*>(a.p),
-                    static_cast<double*>(a.e), a.k, a.kp, g);
+    const size_t smem = (size_t)(g.mg - 1) * a.kp * sizeof(double);
+    return launch_k(bt_expand_kernel<double>, grid, dim3(256), smem, st, a.U, a.samples,
+                    static_cast<const double*>(a.p), a.e, a.k, a.kp, g);
 }
 
 cudaError_t launch_bt_unit_src(const Geom& g, int c0, int ncol, double* G, long long bstride, cudaStream_t st) {
@@ -328,11 +314,6 @@ cudaError_t launch_bt_gather(const Geom& g, int c0, int ncol, const double* psi,
                              cudaStream_t st) {
     dim3 grid((bt_edge_len(g) + 127) / 128, ncol);
     bt_gather_kernel<<<grid, 128, 0, st>>>(g, c0, ncol, psi, bstride, R);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_to_f32(const double* a, float* b, long long n, cudaStream_t st) {
-    to_f32_kernel<<<1184, 256, 0, st>>>(a, b, n);
     return cudaGetLastError();
 }
 

@@ -71,13 +71,12 @@ struct ibpm_handle {
     float* T32 = nullptr;                  // mg slabs of FP32 transform scratch
     double* Pp = nullptr;                  // A⁻¹C'E'F̃b of the previous step (level 1)
     // boundary-transfer vort2flux! (bt.cu; mg >= 2): R = get_bc!∘Δ⁻¹∘apply_bc!
-    // (nE × pitch), the edge vectors, the line samples and the edge part of the
-    // x-spectrum of every level, in FP64 and, for FP32_REFINED, in FP32
+    // (its rank-k factors), the edge vectors, the line samples (FP64 in both
+    // precisions) and the edge part of the x-spectrum of every level
     bool bt = false;
     int bt_k = 0, bt_kp = 0;               // rank of R's basis and its pitch
     double *btW = nullptr, *btU = nullptr, *btP = nullptr, *btE = nullptr, *btS = nullptr, *btY = nullptr;
-    float *btW32 = nullptr, *btU32 = nullptr, *btP32 = nullptr, *btE32 = nullptr, *btS32 = nullptr,
-          *btY32 = nullptr;
+    float* btY32 = nullptr;                // the FP32 edge part (FP32_REFINED)
     // linearised problem (ibpm_set_base_state): base Γ, base q, base flux
     bool lin = false;
     double* GB = nullptr;
@@ -354,7 +353,7 @@ static int vort2flux(ibpm_handle* h, double* G, double* psi, long long bstride, 
 
 // R at create: the get_bc! samples of Δ⁻¹ of a unit source at every edge entry
 // (FP64 solves, `chunk` columns per batch), then its rank-k basis on the host
-// (bt_lowrank); FP32 copies of the basis for FP32_REFINED.  A rank that does
+// (bt_lowrank), used in FP64 by both precisions.  A rank that does
 // not settle (never seen) leaves the handle on the level-by-level chain.
 static int upload_bt(ibpm_handle* h, const BtLowRank& lr);
 
@@ -434,14 +433,7 @@ static int upload_bt(ibpm_handle* h, const BtLowRank& lr) {
     CK(cudaMemsetAsync(h->btS, 0, sizeof(double) * ns, h->st));
     CK(cudaMemsetAsync(h->btY, 0, sizeof(double) * slabs, h->st));  // the coarsest slab stays zero
     if (f32) {
-        if ((rc = dalloc(h, &h->btW32, nw)) || (rc = dalloc(h, &h->btU32, nu)) || (rc = dalloc(h, &h->btP32, np)) ||
-            (rc = dalloc(h, &h->btE32, ne)) || (rc = dalloc(h, &h->btS32, ns)) || (rc = dalloc(h, &h->btY32, slabs)))
-            return rc;
-        CK(launch_to_f32(h->btW, h->btW32, (long long)nw, h->st));
-        CK(launch_to_f32(h->btU, h->btU32, (long long)nu, h->st));
-        CK(cudaMemsetAsync(h->btP32, 0, sizeof(float) * np, h->st));
-        CK(cudaMemsetAsync(h->btE32, 0, sizeof(float) * ne, h->st));
-        CK(cudaMemsetAsync(h->btS32, 0, sizeof(float) * ns, h->st));
+        if ((rc = dalloc(h, &h->btY32, slabs))) return rc;
         CK(cudaMemsetAsync(h->btY32, 0, sizeof(float) * slabs, h->st));
     }
     h->bt = true;
@@ -457,20 +449,17 @@ static int bt_edges(ibpm_handle* h, const void* Y, bool f32) {
     const long long bs = g.S * mg;
     const int nE = bt_edge_len(g);
     const double es = f32 ? 4.0 : 8.0;
-    void* S = f32 ? (void*)h->btS32 : (void*)h->btS;
-    void* E = f32 ? (void*)h->btE32 : (void*)h->btE;
-    LAUNCH(K_BTCHAIN, es * ((double)g.n1 * (g.ny / 2 + 3) + 2.0 * g.n1) * (mg - 1),
-           launch_dst_lines(g, h->px, Y, levmap(g, 1, mg - 1, bs), mg - 1, S, f32 ? 1 : 0, h->st));
+    // the samples, the chain and the edge vectors are FP64 in both precisions
+    LAUNCH(K_BTCHAIN, (es * (g.ny / 2 + 3.0) * g.n1 + 16.0 * g.n1) * (mg - 1),
+           launch_dst_lines(g, h->px, Y, levmap(g, 1, mg - 1, bs), mg - 1, h->btS, f32 ? 1 : 0, h->st));
     BtChainArgs a{};
-    a.W = f32 ? (const void*)h->btW32 : (const void*)h->btW;
-    a.U = f32 ? (const void*)h->btU32 : (const void*)h->btU;
-    a.samples = S; a.e = E; a.p = f32 ? (void*)h->btP32 : (void*)h->btP;
-    a.k = h->bt_k; a.kp = h->bt_kp; a.f32 = f32 ? 1 : 0;
-    if (mg > 2) LAUNCH(K_BTCHAIN, es * ((double)h->bt_k * (nE + 2.0 * nE) + (mg - 1.0) * h->bt_kp),
+    a.W = h->btW; a.U = h->btU; a.samples = h->btS; a.e = h->btE; a.p = h->btP;
+    a.k = h->bt_k; a.kp = h->bt_kp;
+    if (mg > 2) LAUNCH(K_BTCHAIN, 8.0 * ((double)h->bt_k * (g.nx + g.ny + 4.0) * mg + (mg - 1.0) * h->bt_kp),
                        launch_bt_project(g, a, h->st));
-    LAUNCH(K_BTCHAIN, es * ((mg - 2.0) * nE * h->bt_kp + 3.0 * nE * (mg - 1)), launch_bt_expand(g, a, h->st));
+    LAUNCH(K_BTCHAIN, 8.0 * ((mg - 2.0) * nE * h->bt_kp + 3.0 * nE * (mg - 1)), launch_bt_expand(g, a, h->st));
     BtSynth bsy{};
-    bsy.e = E; bsy.sx = f32 ? (const void*)h->px.s32 : (const void*)h->px.s; bsy.nx = g.nx;
+    bsy.e = h->btE; bsy.sx = h->px.s; bsy.nx = g.nx;
     LAUNCH(K_DSTY, es * g.n1 * g.n2 * (mg - 1),
            launch_dst_ybc(g, h->py, h->px, f32 ? (void*)h->btY32 : (void*)h->btY, levmap(g, 0, mg - 1, bs), mg - 1,
                           spec(h, SPEC_DELTA, f32 ? 1 : 0), bsy, h->st));
@@ -862,7 +851,6 @@ static void free_handle(ibpm_handle* h) {
     if (h->T32) cudaFree(h->T32);
     if (h->Pp) cudaFree(h->Pp);
     for (void* p : {(void*)h->btW, (void*)h->btU, (void*)h->btP, (void*)h->btE, (void*)h->btS, (void*)h->btY,
-                    (void*)h->btW32, (void*)h->btU32, (void*)h->btP32, (void*)h->btE32, (void*)h->btS32,
                     (void*)h->btY32})
         if (p) cudaFree(p);
     if (h->mtab) cudaFree(h->mtab);

@@ -636,7 +636,7 @@ __host__ __device__ constexpr size_t y_smem_bytes(int n2) {
     return tables_bytes<N, T, PL>() + (size_t)round4(n2) * sizeof(T) +  // spectral table of y
            (size_t)round4(n2 * (y_tile_w<N, T, PL>() + 1)) * sizeof(T) +
            (size_t)y_groups<N, T, PL>() * ct_buf(N) * sizeof(cplx_t<T>) +
-           (SYNTH ? (size_t)y_synth_slots<N, T, PL>() * sizeof(T) : 0);
+           (SYNTH ? (size_t)y_synth_slots<N, T, PL>() * sizeof(double) : 0);
 }
 
 // SYNTH: the input is not read but built, the x-spectrum of apply_bc!(e_ℓ)
@@ -677,31 +677,33 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
     pdl_wait();
     pdl_trigger();
     if constexpr (SYNTH) {
+        // the edge vectors and the sums over them are FP64 (they couple the
+        // levels); the tile takes the x-spectrum rounded to T
         const int ep = ((2 * n1 + 2 * n2) + 3) & ~3;
-        const T* e = static_cast<const T*>(bs.e) + (long long)lev * ep;
-        const T* sxt = static_cast<const T*>(bs.sx);
+        const double* e = static_cast<const double*>(bs.e) + (long long)lev * ep;
+        const double* sxt = static_cast<const double*>(bs.sx);
         const int nx = bs.nx, nx2 = 2 * bs.nx;
-        auto sinpix = [&](int t) -> T {  // sin(π t / nx), 0 ≤ t < 2 nx
+        auto sinpix = [&](int t) -> double {  // sin(π t / nx), 0 ≤ t < 2 nx
             return t < nx ? __ldg(&sxt[t]) : -__ldg(&sxt[t - nx]);
         };
-        T* red = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(tile + tile_d) +
-                                      (size_t)G * ct_buf(N) * sizeof(V));
+        double* red = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(tile + tile_d) +
+                                                (size_t)G * ct_buf(N) * sizeof(V));
         // bottom and top rows: Σ_i S(i, k) e(i) for the CTA's columns k, the
         // sine argument (i + 1) k mod 2nx advanced by a fixed step per thread
-        T accB[TW], accT[TW];
+        double accB[TW], accT[TW];
         int tk[TW], dk[TW];
 #pragma unroll
         for (int c = 0; c < TW; ++c) {
-            accB[c] = accT[c] = T(0);
+            accB[c] = accT[c] = 0.0;
             const int k = i0 + c + 1;
             tk[c] = (int)(((long long)(threadIdx.x + 1) * k) % nx2);
             dk[c] = (int)(((long long)blockDim.x * k) % nx2);
         }
         for (int i = threadIdx.x; i < n1; i += blockDim.x) {
-            const T eb = e[i], et = e[n1 + i];
+            const double eb = e[i], et = e[n1 + i];
 #pragma unroll
             for (int c = 0; c < TW; ++c) {
-                const T sv = T(2) * sinpix(tk[c]);
+                const double sv = 2.0 * sinpix(tk[c]);
                 accB[c] += sv * eb;
                 accT[c] += sv * et;
                 tk[c] += dk[c];
@@ -723,7 +725,7 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
         }
         __syncthreads();
         if (threadIdx.x < 2 * TW) {
-            T acc = T(0);
+            double acc = 0.0;
             for (int u = 0; u < nw; ++u) acc += red[u * 2 * TW + threadIdx.x];
             red[nw * 2 * TW + threadIdx.x] = acc;
         } else if (threadIdx.x < 4 * TW) {
@@ -731,23 +733,23 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
             const int c = (threadIdx.x - 2 * TW) >> 1;
             const long long k = i0 + c + 1;
             const int t = (int)(((threadIdx.x & 1) ? k * (nx - 1) : k) % nx2);
-            red[(nw + 1) * 2 * TW + (threadIdx.x - 2 * TW)] = T(2) * sinpix(t);
+            red[(nw + 1) * 2 * TW + (threadIdx.x - 2 * TW)] = 2.0 * sinpix(t);
         }
         __syncthreads();
-        const T* bh = red + nw * 2 * TW;         // [0, TW): bottom, [TW, 2TW): top
-        const T* sLR = red + (nw + 1) * 2 * TW;  // [2c]: S(1, k_c), [2c + 1]: S(nx−1, k_c)
-        const T* eL = e + 2 * n1;
-        const T* eR = eL + n2;
+        const double* bh = red + nw * 2 * TW;         // [0, TW): bottom, [TW, 2TW): top
+        const double* sLR = red + (nw + 1) * 2 * TW;  // [2c]: S(1, k_c), [2c + 1]: S(nx−1, k_c)
+        const double* eL = e + 2 * n1;
+        const double* eR = eL + n2;
         for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
             const int j = idx / TW, c = idx - j * TW;
             const int i = i0 + c;
-            T v = T(0);
+            double v = 0.0;
             if (i < n1) {
                 v = sLR[2 * c] * eL[j] + sLR[2 * c + 1] * eR[j];
                 if (j == 0) v += bh[c];
                 if (j == n2 - 1) v += bh[TW + c];
             }
-            tile[j * TWp + c] = v;
+            tile[j * TWp + c] = (T)v;
         }
         __syncthreads();
     } else {
@@ -833,25 +835,27 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
 // S(nx/4, k) = 2 sin(πk/4) and S(3nx/4, k) = 2 sin(3πk/4) repeat with period
 // 8 in k.
 // ---------------------------------------------------------------------------
-template <int N, class T, int PL>
+template <int N, int PL>
 __host__ __device__ constexpr size_t lines_smem_bytes() {
-    return tables_bytes<N, T, PL>() + (size_t)ct_buf(N) * sizeof(cplx_t<T>);
+    return tables_bytes<N, double, PL>() + (size_t)ct_buf(N) * sizeof(double2);
 }
 
+// T: the type of Y (the FP32 corrections of the refined path or FP64); the
+// samples are formed in FP64 either way (they couple the levels).
 template <int N, class T, int PL>
 __global__ void __launch_bounds__(ct_tp(N, PL)) dst_lines_kernel(const T* Y, SlabMap map, Geom g, DstPlan p,
-                                                                 T* samples) {
-    using V = cplx_t<T>;
+                                                                 double* samples) {
+    using V = double2;
     constexpr int TP = ct_tp(N, PL);
     const int P = g.P, nx = g.nx, ny = g.ny, n1 = g.n1;
     const T* base = Y + map.off(blockIdx.y);
-    T* smp = samples + (long long)map.level(blockIdx.y) * (nx + ny + 4);
+    double* smp = samples + (long long)map.level(blockIdx.y) * (nx + ny + 4);
     if (blockIdx.x == 0) {
         extern __shared__ __align__(16) unsigned char smem_raw[];
         V* tw = reinterpret_cast<V*>(smem_raw);
-        T* sn = reinterpret_cast<T*>(tw + ct_tw_count(N, PL));
-        V* buf = reinterpret_cast<V*>(smem_raw + tables_bytes<N, T, PL>());
-        stage_tables<N, T, PL>(tw, sn, tabs_of<T>(p, PL));
+        double* sn = reinterpret_cast<double*>(tw + ct_tw_count(N, PL));
+        V* buf = reinterpret_cast<V*>(smem_raw + tables_bytes<N, double, PL>());
+        stage_tables<N, double, PL>(tw, sn, tabs_of<double>(p, PL));
         cp_async_wait();
         __syncthreads();
         pdl_wait();
@@ -859,15 +863,16 @@ __global__ void __launch_bounds__(ct_tp(N, PL)) dst_lines_kernel(const T* Y, Sla
         const T* ra = base + (long long)(ny / 4 - 1) * P;
         const T* rb = base + (long long)(3 * ny / 4 - 1) * P;
         const int o0 = nx / 4 - 1, o1 = 3 * nx / 4 - 1;
-        T* rowB = smp;
-        T* rowT = smp + nx / 2 + 1;
-        dst_pair<N, TP, 1, T, PL>(buf, tw, sn, threadIdx.x, 0, [&](int i) -> V { return V{ra[i], rb[i]}; },
-                                  [&](int o, V v) {
-                                      if (o >= o0 && o <= o1) {
-                                          rowB[o - o0] = v.x;
-                                          rowT[o - o0] = v.y;
-                                      }
-                                  });
+        double* rowB = smp;
+        double* rowT = smp + nx / 2 + 1;
+        dst_pair<N, TP, 1, double, PL>(buf, tw, sn, threadIdx.x, 0,
+                                       [&](int i) -> V { return V{(double)ra[i], (double)rb[i]}; },
+                                       [&](int o, V v) {
+                                           if (o >= o0 && o <= o1) {
+                                               rowB[o - o0] = v.x;
+                                               rowT[o - o0] = v.y;
+                                           }
+                                       });
         return;
     }
     pdl_wait();
@@ -876,12 +881,12 @@ __global__ void __launch_bounds__(ct_tp(N, PL)) dst_lines_kernel(const T* Y, Sla
     const int r = (blockIdx.x - 1) * (TP / 32) + (threadIdx.x >> 5);
     if (r > ny / 2) return;
     const T* row = base + (long long)(ny / 4 - 1 + r) * P;
-    const T s2 = T(1.41421356237309504880);  // 2 sin(π/4)
-    const T wl[8] = {T(0), s2, T(2), s2, T(0), -s2, T(-2), -s2};
-    const T wr[8] = {T(0), s2, T(-2), s2, T(0), -s2, T(2), -s2};
-    T aL = T(0), aR = T(0);
+    const double s2 = 1.41421356237309504880;  // 2 sin(π/4)
+    const double wl[8] = {0.0, s2, 2.0, s2, 0.0, -s2, -2.0, -s2};
+    const double wr[8] = {0.0, s2, -2.0, s2, 0.0, -s2, 2.0, -s2};
+    double aL = 0.0, aR = 0.0;
     for (int m = lane; m < n1; m += 32) {
-        const T v = row[m];
+        const double v = (double)row[m];
         const int k = (m + 1) & 7;
         aL += wl[k] * v;
         aR += wr[k] * v;
@@ -994,8 +999,8 @@ cudaError_t launch_lines_n(const Geom& g, const DstPlan& px, const void* Y, Slab
                            cudaStream_t st) {
     constexpr int TP = ct_tp(N, PL);
     dim3 grid(1 + (g.ny / 2 + 1 + TP / 32 - 1) / (TP / 32), nslabs);
-    return launch_k(dst_lines_kernel<N, T, PL>, grid, dim3(TP), lines_smem_bytes<N, T, PL>(), st,
-                    static_cast<const T*>(Y), map, g, px, static_cast<T*>(smp));
+    return launch_k(dst_lines_kernel<N, T, PL>, grid, dim3(TP), lines_smem_bytes<N, PL>(), st,
+                    static_cast<const T*>(Y), map, g, px, static_cast<double*>(smp));
 }
 
 template <int N>

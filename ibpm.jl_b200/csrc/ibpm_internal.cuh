@@ -275,12 +275,13 @@ inline int bt_edge_len(const Geom& g) { return 2 * g.n1 + 2 * g.n2; }
 inline int bt_edge_pitch(const Geom& g) { return (bt_edge_len(g) + 3) & ~3; }  // R row pitch
 inline int bt_sample_len(const Geom& g) { return g.nx + g.ny + 4; }
 struct BtSynth {
-    const void* e;        // edge vectors, level-major (bt_edge_pitch apart), T
-    const void* sx;       // sin(π t/nx), t < nx, of the x-length (T)
+    const double* e;      // edge vectors, level-major (bt_edge_pitch apart), FP64
+    const double* sx;     // sin(π t/nx), t < nx, of the x-length (FP64)
     int nx;
 };
 cudaError_t launch_dst_ybc(const Geom& g, const DstPlan& py, const DstPlan& px, void* out, SlabMap map, int nslabs,
                            const SpecParams& sp, const BtSynth& bs, cudaStream_t st);
+// The line samples (FP64) of the levels of `map` from Y (FP32 when f32).
 cudaError_t launch_dst_lines(const Geom& g, const DstPlan& px, const void* Y, SlabMap map, int nslabs,
                              void* samples, int f32, cudaStream_t st);
 // The chain in a rank-k basis of R (R ≈ Q W, Q orthonormal columns,
@@ -292,23 +293,21 @@ cudaError_t launch_dst_lines(const Geom& g, const DstPlan& px, const void* Y, Sl
 //     e_ℓ = g_ℓ + Σ_{m=0}^{mg−3−ℓ} U_m p_{ℓ+1+m},   U_m = Q (W Q)^m
 // which is e_ℓ = g_ℓ + R e_{ℓ+1} unrolled (two launches, none serial).
 struct BtChainArgs {
-    const void* W;        // Ws: k × sample pitch (bt_sample_len rounded to 4), row-major (T)
-    const void* U;        // mg−2 matrices nE × kp, row-major (T)
-    const void* samples;  // bt_sample_len per level (T), level-major
-    void* p;              // (mg−1) × kp projections (T)
-    void* e;              // edge vectors (T), level-major, bt_edge_pitch apart
-    int k, kp;            // rank and its pitch (multiple of 4)
-    int f32;
+    const double* W;        // Ws: k × sample pitch (bt_sample_len rounded to 4), row-major
+    const double* U;        // mg−2 matrices nE × kp, row-major
+    const double* samples;  // bt_sample_len per level, level-major
+    double* p;              // (mg−1) × kp projections
+    double* e;              // edge vectors, level-major, bt_edge_pitch apart
+    int k, kp;              // rank and its pitch (multiple of 4)
 };
 cudaError_t launch_bt_project(const Geom& g, const BtChainArgs& a, cudaStream_t st);
 cudaError_t launch_bt_expand(const Geom& g, const BtChainArgs& a, cudaStream_t st);
 // Setup of R: unit sources of edge entries [c0, c0 + ncol) into ncol slabs
 // (bstride apart, zeroed first), and the gather of their solves' get_bc!
-// entries into R's columns (FP64), then the FP32 copy.
+// entries into R's columns (FP64).
 cudaError_t launch_bt_unit_src(const Geom& g, int c0, int ncol, double* G, long long bstride, cudaStream_t st);
 cudaError_t launch_bt_gather(const Geom& g, int c0, int ncol, const double* psi, long long bstride, double* R,
                              cudaStream_t st);
-cudaError_t launch_to_f32(const double* a, float* b, long long n, cudaStream_t st);
 // Host: the rank-k basis of R (bt.cu) — W = Qᵀ R (k × pitch) and
 // U_m = Q (W Q)^m (nE × kp each, m < nmat); -1 if the rank reaches kmax.
 struct BtLowRank {
