@@ -39,24 +39,24 @@ constexpr int kMaxLev = 8;
 
 // p_ℓ[r] = Σ_s Ws[r, s] smp_{ℓ+1}[s] for every level ℓ = 0 … mg−2, with
 // Ws = W A_s the projection folded with get_bc!'s averaging of the samples
-// (A_s: g = A_s · samples).  One warp per row r of Ws (read once for all
-// levels), lanes over s in a fixed order; the loads of four consecutive
-// lane steps are issued together.
+// (A_s: g = A_s · samples).  One block per row r of Ws (read once for all
+// levels): its threads take s in a fixed order, the loads of eight steps
+// issued together, then a fixed-order reduction over the block.
 template <class T>
-__global__ void __launch_bounds__(128) bt_project_kernel(const T* __restrict__ Ws, const T* __restrict__ samples,
+__global__ void __launch_bounds__(256) bt_project_kernel(const T* __restrict__ Ws, const T* __restrict__ samples,
                                                          T* p, int k, int kp, Geom g) {
+    __shared__ T red[8 * kMaxLev];
     pdl_wait();
     pdl_trigger();
     const int L = g.mg - 1;
     const int sl = g.nx + g.ny + 4, sp = (sl + 3) & ~3;
-    const int r = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (r >= k) return;
+    const int r = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     T acc[kMaxLev];
 #pragma unroll
     for (int l = 0; l < kMaxLev; ++l) acc[l] = T(0);
     const T* row = Ws + (long long)r * sp;
-#pragma unroll 4
-    for (int s = lane; s < sl; s += 32) {
+#pragma unroll 8
+    for (int s = tid; s < sl; s += 256) {
         const T wv = __ldg(&row[s]);
 #pragma unroll
         for (int l = 0; l < kMaxLev; ++l)
@@ -68,14 +68,22 @@ __global__ void __launch_bounds__(128) bt_project_kernel(const T* __restrict__ W
             T v = acc[l];
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-            if (lane == 0) p[(long long)l * kp + r] = v;
+            if (lane == 0) red[w * kMaxLev + l] = v;
         }
+    }
+    __syncthreads();
+    if (tid < L && r < k) {
+        T v = T(0);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v += red[q * kMaxLev + tid];
+        p[(long long)tid * kp + r] = v;
     }
 }
 
 // e_ℓ[i] = g_ℓ[i] + Σ_{m=0}^{mg−3−ℓ} U_m[i, :] · p_{ℓ+1+m}: one warp per row i,
-// lanes over the rank index in a fixed order; the projections are staged in
-// shared memory.
+// lanes over the rank index in a fixed order.  The (m, rank) steps run as one
+// flat loop, so the loads of eight steps (of all U_m) are issued together; the
+// projections are staged in shared memory.
 template <class T>
 __global__ void __launch_bounds__(256) bt_expand_kernel(const T* __restrict__ U, const T* __restrict__ samples,
                                                         const T* __restrict__ p, T* e, int k, int kp, Geom g) {
@@ -92,15 +100,17 @@ __global__ void __launch_bounds__(256) bt_expand_kernel(const T* __restrict__ U,
     T acc[kMaxLev];
 #pragma unroll
     for (int l = 0; l < kMaxLev; ++l) acc[l] = T(0);
-    for (int m = 0; m + 2 < g.mg; ++m) {
-        const T* row = U + ((long long)m * nE + i) * kp;
-#pragma unroll 4
-        for (int r = lane; r < k; r += 32) {
-            const T u = __ldg(&row[r]);
+    const int nt = (k + 31) >> 5, steps = (g.mg - 2) * nt;
+    int m = 0, t = 0;
+#pragma unroll 8
+    for (int j = 0; j < steps; ++j) {
+        const int r = lane + 32 * t;
+        const T u = r < k ? __ldg(&U[((long long)m * nE + i) * kp + r]) : T(0);
+        const int rr = r < k ? r : 0;
 #pragma unroll
-            for (int l = 0; l < kMaxLev; ++l)
-                if (l + m + 1 < L) acc[l] += u * ps[(l + 1 + m) * kp + r];
-        }
+        for (int l = 0; l < kMaxLev; ++l)
+            if (l + m + 1 < L) acc[l] += u * ps[(l + 1 + m) * kp + rr];
+        if (++t == nt) { t = 0; ++m; }
     }
 #pragma unroll
     for (int l = 0; l < kMaxLev; ++l) {
@@ -294,8 +304,8 @@ int bt_lowrank(const std::vector<double>& R, int nx_, int ny_, int nmat, double 
 }
 
 cudaError_t launch_bt_project(const Geom& g, const BtChainArgs& a, cudaStream_t st) {
-    dim3 grid((a.k + 3) / 4);
-    return launch_k(bt_project_kernel<double>, grid, dim3(128), 0, st, a.W, a.samples, a.p, a.k, a.kp, g);
+    dim3 grid(a.k);
+    return launch_k(bt_project_kernel<double>, grid, dim3(256), 0, st, a.W, a.samples, a.p, a.k, a.kp, g);
 }
 
 cudaError_t launch_bt_expand(const Geom& g, const BtChainArgs& a, cudaStream_t st) {

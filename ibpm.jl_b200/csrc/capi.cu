@@ -73,7 +73,8 @@ struct ibpm_handle {
     // boundary-transfer vort2flux! (bt.cu; mg >= 2): R = get_bc!∘Δ⁻¹∘apply_bc!
     // (its rank-k factors), the edge vectors, the line samples (FP64 in both
     // precisions) and the edge part of the x-spectrum of every level
-    bool bt = false;
+    bool bt = false;                       // the step runs the boundary transfer
+    int chain = IBPM_CHAIN_BOUNDARY_TRANSFER;  // the level chain set (one level: no effect)
     int bt_k = 0, bt_kp = 0;               // rank of R's basis and its pitch
     double *btW = nullptr, *btU = nullptr, *btP = nullptr, *btE = nullptr, *btS = nullptr, *btY = nullptr;
     float* btY32 = nullptr;                // the FP32 edge part (FP32_REFINED)
@@ -442,8 +443,8 @@ static int upload_bt(ibpm_handle* h, const BtLowRank& lr) {
 
 // From the y-pass output Y of every level (x-spectral; FP64 or FP32): the line
 // samples of levels 1 … mg−1, the edge chain down to level 0, and the edge
-// part of every level but the coarsest, by one y-pass, into btY / btY32.
-static int bt_edges(ibpm_handle* h, const void* Y, bool f32) {
+// part of levels 0 … nyb−1 by one y-pass, into btY / btY32.
+static int bt_edges(ibpm_handle* h, const void* Y, bool f32, int nyb) {
     const Geom& g = h->g;
     const int mg = g.mg;
     const long long bs = g.S * mg;
@@ -460,8 +461,8 @@ static int bt_edges(ibpm_handle* h, const void* Y, bool f32) {
     LAUNCH(K_BTCHAIN, 8.0 * ((mg - 2.0) * nE * h->bt_kp + 3.0 * nE * (mg - 1)), launch_bt_expand(g, a, h->st));
     BtSynth bsy{};
     bsy.e = h->btE; bsy.sx = h->px.s; bsy.nx = g.nx;
-    LAUNCH(K_DSTY, es * g.n1 * g.n2 * (mg - 1),
-           launch_dst_ybc(g, h->py, h->px, f32 ? (void*)h->btY32 : (void*)h->btY, levmap(g, 0, mg - 1, bs), mg - 1,
+    LAUNCH(K_DSTY, es * g.n1 * g.n2 * nyb,
+           launch_dst_ybc(g, h->py, h->px, f32 ? (void*)h->btY32 : (void*)h->btY, levmap(g, 0, nyb, bs), nyb,
                           spec(h, SPEC_DELTA, f32 ? 1 : 0), bsy, h->st));
     return IBPM_OK;
 }
@@ -477,8 +478,11 @@ static int curl_levels(ibpm_handle* h, double* q, int qnlev) {
     return IBPM_OK;
 }
 
-// vort2flux! (FP64) of the handle's field G into h->psi and q (levels < qnlev).
-static int vort2flux_bt(ibpm_handle* h, double* G, double* q, int qnlev) {
+// vort2flux! (FP64) of the handle's field G into h->psi (levels < nfull; the
+// coarser ones are left as they were) and q (levels < qnlev < nfull).  The
+// trial vort2flux! of a step needs only the level-1 flux, hence ψ of levels 1
+// and 2; the final one recomputes every level.
+static int vort2flux_bt(ibpm_handle* h, double* G, double* q, int qnlev, int nfull) {
     const Geom& g = h->g;
     const int mg = g.mg;
     const long long bs = g.S * mg;
@@ -492,12 +496,12 @@ static int vort2flux_bt(ibpm_handle* h, double* G, double* q, int qnlev) {
     a.nslabs = mg; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_PLAIN; a.emit = XEMIT_STORE;
     LAUNCH(K_DSTX, 16.0 * slab * mg, launch_dst_x(g, h->px, a, h->st));
     LAUNCH(K_DSTY, 16.0 * slab * mg, launch_dst_y(g, h->py, h->px, h->rhs, all, mg, spec(h, SPEC_DELTA), h->st));
-    int rc = bt_edges(h, h->rhs, false);
+    int rc = bt_edges(h, h->rhs, false, std::min(nfull, mg - 1));
     if (rc) return rc;
     XPassArgs c{};
     c.in = h->rhs; c.in2 = h->btY; c.in_map = all; c.in2_map = all; c.out = h->psi; c.out_map = all;
-    c.nslabs = mg; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_SUM; c.emit = XEMIT_STORE;
-    LAUNCH(K_DSTX, 24.0 * slab * mg, launch_dst_x(g, h->px, c, h->st));
+    c.nslabs = nfull; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_SUM; c.emit = XEMIT_STORE;
+    LAUNCH(K_DSTX, 24.0 * slab * nfull, launch_dst_x(g, h->px, c, h->st));
     return curl_levels(h, q, qnlev);
 }
 
@@ -507,7 +511,7 @@ static int vort2flux_bt(ibpm_handle* h, double* G, double* q, int qnlev) {
 // The corrections satisfy the level chain of vort2flux! themselves,
 // L d_ℓ = r_ℓ + apply_bc!(get_bc!(d_{ℓ+1})), so the boundary transfer solves
 // them in FP32 as above.
-static int vort2flux_refined_bt(ibpm_handle* h, double* G, int nsw, double* q, int qnlev) {
+static int vort2flux_refined_bt(ibpm_handle* h, double* G, int nsw, double* q, int qnlev, int nfull) {
     const Geom& g = h->g;
     const int mg = g.mg;
     const long long bs = g.S * mg;
@@ -526,12 +530,12 @@ static int vort2flux_refined_bt(ibpm_handle* h, double* G, int nsw, double* q, i
         LAUNCH(K_DSTX, 8.0 * slab * mg, launch_dst_x(g, h->px, a, h->st));
         LAUNCH(K_DSTY, 8.0 * slab * mg,
                launch_dst_y(g, h->py, h->px, h->T32, all, mg, spec(h, SPEC_DELTA, 1), h->st));
-        int rc = bt_edges(h, h->T32, true);
+        int rc = bt_edges(h, h->T32, true, std::min(nfull, mg - 1));
         if (rc) return rc;
         XPassArgs c{};
         c.in = h->T32; c.in2 = h->btY32; c.in_map = all; c.in2_map = all; c.out = h->psi; c.out_map = all;
-        c.nslabs = mg; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_F32_SUM; c.emit = XEMIT_ADD;
-        LAUNCH(K_DSTX, (4.0 + 4.0 + 16.0) * slab * mg, launch_dst_x(g, h->px, c, h->st));
+        c.nslabs = nfull; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_F32_SUM; c.emit = XEMIT_ADD;
+        LAUNCH(K_DSTX, (4.0 + 4.0 + 16.0) * slab * nfull, launch_dst_x(g, h->px, c, h->st));
     }
     return curl_levels(h, q, qnlev);
 }
@@ -548,7 +552,7 @@ static int enqueue_step_fp64(ibpm_handle* h, int p) {
     SlabMap all = levmap(g, 0, mg);
     int rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg, SPEC_AINV, XEMIT_STORE);
     if (rc) return rc;
-    rc = h->bt ? vort2flux_bt(h, Gnew, h->qs, 1)  // only the level-1 trial flux is read
+    rc = h->bt ? vort2flux_bt(h, Gnew, h->qs, 1, std::min(2, mg))  // only the level-1 trial flux is read
                : vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->qs, 0, 0, 1);
     if (rc) return rc;
     // --- boundary_forces! (timestepping.jl:154-163) and update_stress! (:330-354)
@@ -561,7 +565,7 @@ static int enqueue_step_fp64(ibpm_handle* h, int p) {
     rc = poisson(h, h->Gsrc, one, h->rhs, one, Gnew, one, 1, SPEC_AINV, XEMIT_SUB);
     if (rc) return rc;
     // --- vort2flux!(state.ψ, state.q, state.Γ) (timestepping.jl:64)
-    return h->bt ? vort2flux_bt(h, Gnew, h->q, mg) : vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->q, 0, 0, mg);
+    return h->bt ? vort2flux_bt(h, Gnew, h->q, mg, mg) : vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->q, 0, 0, mg);
 }
 
 // ---------------------------------------------------------------------------
@@ -638,7 +642,9 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
     SlabMap all = levmap(g, 0, mg, bs);
     int rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg, SPEC_AINV, XEMIT_STORE);
     if (rc) return rc;
-    rc = h->bt ? vort2flux_refined_bt(h, Gnew, nsw, h->qs, 1)  // only the level-1 trial flux is read
+    // every level: a level left at the previous step's ψ would start the final
+    // vort2flux! from a whole step's change, and its FP32 correction error with it
+    rc = h->bt ? vort2flux_refined_bt(h, Gnew, nsw, h->qs, 1, mg)
                : vort2flux_refined(h, Gnew, nsw, h->qs, 1);
     if (rc) return rc;
     // --- boundary_forces! and update_stress! (FP64)
@@ -654,7 +660,7 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
         if (rc) return rc;
     }
     // --- vort2flux!(state.ψ, state.q, state.Γ)
-    return h->bt ? vort2flux_refined_bt(h, Gnew, nsw, h->q, mg) : vort2flux_refined(h, Gnew, nsw, h->q, mg);
+    return h->bt ? vort2flux_refined_bt(h, Gnew, nsw, h->q, mg, mg) : vort2flux_refined(h, Gnew, nsw, h->q, mg);
 }
 
 // update_bodies! for MotionFunction bodies (timestepping.jl:386-398): move the
@@ -953,11 +959,9 @@ static int create_impl(ibpm_handle* h, const ibpm_problem_desc* d) {
     }
     if ((rc = build_coupling(h, d))) return rc;
     if ((rc = build_binv(h))) return rc;
-    {
-        // the boundary-transfer level chain (IBPM_BT=0: the reference's sequential one)
-        const char* bt = getenv("IBPM_BT");
-        if (!(bt && bt[0] == '0') && (rc = build_bt(h))) return rc;
-    }
+    // the boundary-transfer level chain where its factors exist
+    if ((rc = build_bt(h))) return rc;
+    if (g.mg >= 2 && !h->bt) h->chain = IBPM_CHAIN_SEQUENTIAL;
     CK(cudaStreamSynchronize(h->st));
     return IBPM_OK;
 }
@@ -1321,7 +1325,7 @@ extern "C" int ibpm_advance_moving(ibpm_handle* h, int32_t nsteps, const double*
 extern "C" int ibpm_vort2flux(ibpm_handle* h) {
     if (!h) return IBPM_ERR_INVALID;
     CK(cudaSetDevice(h->device));
-    int rc = h->bt ? vort2flux_bt(h, h->G[h->cur], h->q, h->g.mg)
+    int rc = h->bt ? vort2flux_bt(h, h->G[h->cur], h->q, h->g.mg, h->g.mg)
                    : vort2flux(h, h->G[h->cur], h->psi, h->g.S * h->g.mg, 1, h->q, 0, 0, h->g.mg);
     if (rc) return rc;
     CK(cudaStreamSynchronize(h->st));
@@ -1362,6 +1366,41 @@ extern "C" int ibpm_set_transform_plan(ibpm_handle* h, int32_t single_slab, int3
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->st));
     set_plans(h, single_slab, multi_slab);
+    return IBPM_OK;
+}
+
+// The level chain of vort2flux!: the boundary transfer builds its factors on
+// first use; a single level has no chain, and either setting is kept.
+static int set_chain(ibpm_handle* h, int chain) {
+    const bool want = chain == IBPM_CHAIN_BOUNDARY_TRANSFER && h->g.mg >= 2, was = h->bt;
+    if (want && !h->btW) {
+        int rc = build_bt(h);
+        if (rc) return rc;
+        if (!h->btW)
+            return fail(h, IBPM_ERR_UNSUPPORTED, "boundary transfer: the edge operator of this grid has no "
+                                                 "low-rank factors (numerical rank 1024 or more)");
+    }
+    h->chain = chain;
+    h->bt = want;
+    if (want != was) {
+        h->graphs_ready = false;
+        for (int p = 0; p < 2; ++p) if (h->gadj[p]) { cudaGraphExecDestroy(h->gadj[p]); h->gadj[p] = nullptr; }
+    }
+    return IBPM_OK;
+}
+
+extern "C" int ibpm_set_level_chain(ibpm_handle* h, int32_t chain) {
+    if (!h) return IBPM_ERR_INVALID;
+    if (chain != IBPM_CHAIN_SEQUENTIAL && chain != IBPM_CHAIN_BOUNDARY_TRANSFER)
+        return fail(h, IBPM_ERR_INVALID, "level chain must be IBPM_CHAIN_SEQUENTIAL or IBPM_CHAIN_BOUNDARY_TRANSFER");
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->st));
+    return set_chain(h, chain);
+}
+
+extern "C" int ibpm_get_level_chain(const ibpm_handle* h, int32_t* chain) {
+    if (!h || !chain) return IBPM_ERR_INVALID;
+    *chain = h->chain;
     return IBPM_OK;
 }
 
@@ -1850,6 +1889,7 @@ struct ibpm_batch {
     std::vector<cudaEvent_t> ev;               // fork + one join event per lane
     int lanes = 0;
     int plan = IBPM_PLAN_LATENCY;              // transform plan of the members' single-slab launches
+    int chain = IBPM_CHAIN_BOUNDARY_TRANSFER;  // the members' level chain
     int cur = 0;                               // parity shared by the members
     int cold = kColdSteps;
     cudaGraphExec_t g[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cold][parity]
@@ -1959,26 +1999,36 @@ static void batch_destroy_impl(ibpm_batch* b) {
     delete b;
 }
 
-// Time `steps` batch steps for each candidate lane count (powers of two up to
-// the member count) and each transform plan of the members' single-slab
-// launches (latency or throughput); keep the fastest pair.  The members are
-// reset afterwards.
+// Set every member's level chain; false if one of them cannot take it.
+static bool batch_chain_all(ibpm_batch* b, int chain) {
+    for (auto* h : b->m)
+        if (set_chain(h, chain) != IBPM_OK) return false;
+    return true;
+}
+
+// Time `steps` batch steps for each candidate: the members' level chain
+// (sequential or boundary transfer), the transform plan of their single-slab
+// launches (latency or throughput) and the lane count (powers of two up to the
+// member count); keep the fastest.  The members are reset afterwards.
 static int batch_tune(ibpm_batch* b, int steps) {
     const int n = (int)b->m.size();
-    std::vector<std::pair<int, int>> cand;   // (plan, lanes)
-    for (int pl : {IBPM_PLAN_LATENCY, IBPM_PLAN_THROUGHPUT}) {
-        for (int l = 1; l < n; l *= 2) cand.push_back({pl, l});
-        cand.push_back({pl, n});
-    }
+    struct Cand { int chain, plan, lanes; };
+    std::vector<Cand> cand;
+    for (int ch : {IBPM_CHAIN_SEQUENTIAL, IBPM_CHAIN_BOUNDARY_TRANSFER})
+        for (int pl : {IBPM_PLAN_LATENCY, IBPM_PLAN_THROUGHPUT}) {
+            for (int l = 1; l < n; l *= 2) cand.push_back({ch, pl, l});
+            cand.push_back({ch, pl, n});
+        }
     double best = 1e300;
-    int best_l = n, best_p = IBPM_PLAN_LATENCY;
+    Cand win{IBPM_CHAIN_SEQUENTIAL, IBPM_PLAN_LATENCY, n};
     cudaEvent_t e0, e1;
     BCK(cudaEventCreate(&e0));
     BCK(cudaEventCreate(&e1));
     int rc = IBPM_OK;
-    for (auto [pl, l] : cand) {
-        for (auto* h : b->m) set_plans(h, pl, h->px.planN);
-        if ((rc = batch_graphs(b, l))) break;
+    for (const Cand& c : cand) {
+        if (!batch_chain_all(b, c.chain)) continue;   // no boundary-transfer factors for a member
+        for (auto* h : b->m) set_plans(h, c.plan, h->px.planN);
+        if ((rc = batch_graphs(b, c.lanes))) break;
         for (int s = 0; s < 2 && rc == IBPM_OK; ++s)
             if (batch_step(b) != cudaSuccess) rc = bfail(b, IBPM_ERR_CUDA, "batch tuning step failed");
         if (rc) break;
@@ -1989,20 +2039,22 @@ static int batch_tune(ibpm_batch* b, int steps) {
         if (cudaEventSynchronize(e1) != cudaSuccess) { rc = bfail(b, IBPM_ERR_CUDA, "batch tuning sync failed"); break; }
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) { best = ms; best_l = l; best_p = pl; }
+        if (ms < best) { best = ms; win = c; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
+    if (!batch_chain_all(b, win.chain)) return bfail(b, IBPM_ERR_CUDA, "batch tuning: level chain");
     for (auto* h : b->m) {
         if ((rc = reset_state(h))) return bfail(b, rc, h->err);
-        set_plans(h, best_p, h->px.planN);
+        set_plans(h, win.plan, h->px.planN);
         if ((rc = ensure_graphs(h, b->hist_cap))) return bfail(b, rc, h->err);  // the members' own graphs
     }
     b->cur = 0;
     b->cold = 2;
-    b->plan = best_p;
-    return batch_graphs(b, best_l);
+    b->plan = win.plan;
+    b->chain = win.chain;
+    return batch_graphs(b, win.lanes);
 }
 
 extern "C" int ibpm_batch_create(int32_t n, const ibpm_problem_desc* descs, int32_t lanes, ibpm_batch** out) {
@@ -2080,6 +2132,22 @@ extern "C" int ibpm_batch_set_plan(ibpm_batch* b, int32_t plan) {
     return batch_graphs(b, b->lanes);
 }
 
+extern "C" int ibpm_batch_chain(const ibpm_batch* b) { return b ? b->chain : IBPM_ERR_INVALID; }
+
+extern "C" int ibpm_batch_set_chain(ibpm_batch* b, int32_t chain) {
+    if (!b || (chain != IBPM_CHAIN_SEQUENTIAL && chain != IBPM_CHAIN_BOUNDARY_TRANSFER)) return IBPM_ERR_INVALID;
+    BCK(cudaSetDevice(b->device));
+    BCK(cudaStreamSynchronize(b->st));
+    for (size_t i = 0; i < b->m.size(); ++i) {
+        ibpm_handle* h = b->m[i];
+        int rc = set_chain(h, chain);
+        if (rc == IBPM_OK) rc = ensure_graphs(h, b->hist_cap);   // the members' own graphs
+        if (rc) return bfail(b, rc, "member " + std::to_string(i) + ": " + h->err);
+    }
+    b->chain = chain;
+    return batch_graphs(b, b->lanes);
+}
+
 extern "C" int ibpm_batch_set_lanes(ibpm_batch* b, int32_t lanes) {
     if (!b || lanes < 1 || lanes > (int)b->m.size()) return IBPM_ERR_INVALID;
     BCK(cudaSetDevice(b->device));
@@ -2100,8 +2168,9 @@ static int batch_sync_members(ibpm_batch* b) {
                                                   " was advanced on its own: batch members must step together");
         if (!h->graphs_ready)  // a changed base flux or transform plan
             return bfail(b, IBPM_ERR_UNSUPPORTED, "member " + std::to_string(i) +
-                                                      " changed its base flux or transform plan on its own "
-                                                      "(a batch's plan is set by ibpm_batch_set_plan)");
+                                                      " changed its base flux, transform plan or level chain "
+                                                      "on its own (a batch's are set by ibpm_batch_set_plan "
+                                                      "and ibpm_batch_set_chain)");
         b->cold = std::max(b->cold, h->cold);      // set_state on a member re-arms its first steps
     }
     return IBPM_OK;

@@ -22,7 +22,7 @@ module IBPMGPU
 using ..ibpm: ibpm, IBState, AbstractIBProblem, MultiGrid, RigidBody, Static, MovingGrid, MotionFunction,
               MotionType, get_body_info, AB2, AdamsBashforth
 
-export IBProblemGPU, sync!, push_state!, adjoint_run, set_vorticity!, set_transform_plan!
+export IBProblemGPU, sync!, push_state!, adjoint_run, set_vorticity!, set_transform_plan!, set_level_chain!
 
 const LIB = get(ENV, "IBPM_GPU_LIB", joinpath(@__DIR__, "..", "lib", "libibpm_gpu.so"))
 
@@ -258,6 +258,21 @@ function set_transform_plan!(prob::IBProblemGPU; single::Symbol=:latency, multi:
               throw(ArgumentError("plan must be :latency, :throughput or :auto"))
     check(ccall((:ibpm_set_transform_plan, LIB), Cint, (Ptr{Cvoid}, Int32, Int32), prob.handle,
                 code(single), code(multi)), prob.handle)
+end
+
+"""
+    set_level_chain!(prob, chain::Symbol)
+
+How `vort2flux!` runs its levels on the device: `:sequential` (the
+reference's order, src/fluid-operators/curl.jl:133-165, one level after
+another) or `:boundary_transfer` (the default: every level per launch, the
+edge values from a low-rank factorisation of the level-to-level transfer).
+The results agree to rounding.
+"""
+function set_level_chain!(prob::IBProblemGPU, chain::Symbol)
+    c = chain === :sequential ? Int32(0) : chain === :boundary_transfer ? Int32(1) :
+        throw(ArgumentError("chain must be :sequential or :boundary_transfer"))
+    check(ccall((:ibpm_set_level_chain, LIB), Cint, (Ptr{Cvoid}, Int32), prob.handle, c), prob.handle)
 end
 
 """

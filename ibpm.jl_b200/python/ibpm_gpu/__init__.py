@@ -46,6 +46,10 @@ IBPM_PREC_FP32_REFINED = 1
 IBPM_PLAN_LATENCY = 0
 IBPM_PLAN_THROUGHPUT = 1
 IBPM_PLAN_AUTO = 2      # multi-slab launches: throughput plan from 4 slabs on
+# level chains of vort2flux! (ibpm_set_level_chain): the reference's order, one
+# level after another, or the boundary transfer (all levels per launch)
+IBPM_CHAIN_SEQUENTIAL = 0
+IBPM_CHAIN_BOUNDARY_TRANSFER = 1
 PRECISIONS = {"fp64": IBPM_PREC_FP64, "fp32_refined": IBPM_PREC_FP32_REFINED}
 KERNEL_COUNT = 12
 
@@ -155,6 +159,14 @@ def load_library(path=None):
     lib.ibpm_set_transform_plan.argtypes = [H, C.c_int32, C.c_int32]
     lib.ibpm_get_transform_plan.restype = C.c_int
     lib.ibpm_get_transform_plan.argtypes = [H, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    lib.ibpm_set_level_chain.restype = C.c_int
+    lib.ibpm_set_level_chain.argtypes = [H, C.c_int32]
+    lib.ibpm_get_level_chain.restype = C.c_int
+    lib.ibpm_get_level_chain.argtypes = [H, C.POINTER(C.c_int32)]
+    lib.ibpm_batch_chain.restype = C.c_int
+    lib.ibpm_batch_chain.argtypes = [H]
+    lib.ibpm_batch_set_chain.restype = C.c_int
+    lib.ibpm_batch_set_chain.argtypes = [H, C.c_int32]
     lib.ibpm_batch_set_lanes.restype = C.c_int
     lib.ibpm_batch_set_lanes.argtypes = [H, C.c_int32]
     lib.ibpm_batch_last_error.restype = C.c_char_p
@@ -587,6 +599,20 @@ def transform_plan(prob):
     return a.value, b.value
 
 
+def set_level_chain(prob, chain):
+    """How vort2flux! runs its levels: IBPM_CHAIN_SEQUENTIAL (the reference's
+    order) or IBPM_CHAIN_BOUNDARY_TRANSFER (the default where its factors
+    exist).  The results agree to rounding."""
+    prob._check(prob.lib.ibpm_set_level_chain(prob.handle, int(chain)))
+
+
+def level_chain(prob):
+    """The problem's level chain (IBPM_CHAIN_*)."""
+    c = C.c_int32()
+    prob._check(prob.lib.ibpm_get_level_chain(prob.handle, C.byref(c)))
+    return c.value
+
+
 def _field_shapes(prob):
     g = prob.grid
     return {"Gamma": (g.nGamma, g.mg), "q": (g.nq, g.mg), "q0": (g.nq, g.mg), "psi": (g.nGamma, g.mg),
@@ -812,6 +838,14 @@ class Batch:
 
     def set_plan(self, plan):
         self._check(self.lib.ibpm_batch_set_plan(self.handle, int(plan)))
+
+    @property
+    def chain(self):
+        """Level chain of the members' vort2flux! (IBPM_CHAIN_*)."""
+        return self.lib.ibpm_batch_chain(self.handle)
+
+    def set_chain(self, chain):
+        self._check(self.lib.ibpm_batch_set_chain(self.handle, int(chain)))
 
     def advance(self, nsteps=1):
         """Advance every member; returns per-member (CD, CL) histories (nsteps, nbodies)."""

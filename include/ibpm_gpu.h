@@ -309,6 +309,10 @@ int ibpm_batch_bench(ibpm_batch* b, int32_t nsteps, int32_t flush_l2, double* st
  * batch step again (the state is kept). */
 int ibpm_batch_plan(const ibpm_batch* b);
 int ibpm_batch_set_plan(ibpm_batch* b, int32_t plan);
+/* Level chain of the members (IBPM_CHAIN_*): the one lanes = 0 chose, or the
+ * one set; setting it captures the batch step again (the state is kept). */
+int ibpm_batch_chain(const ibpm_batch* b);
+int ibpm_batch_set_chain(ibpm_batch* b, int32_t chain);
 
 /* Page-locked host memory for state mirrors (faster get/set_state); NULL on
  * failure.  No counterpart in the reference (Julia arrays are pageable). */
@@ -352,6 +356,28 @@ const char* ibpm_kernel_name(int32_t k);
 #define IBPM_PLAN_AUTO       2
 int ibpm_set_transform_plan(ibpm_handle* h, int32_t single_slab, int32_t multi_slab);
 int ibpm_get_transform_plan(const ibpm_handle* h, int32_t* single_slab, int32_t* multi_slab);
+
+/* How vort2flux! (src/fluid-operators/curl.jl:133-165) runs its level chain
+ * (no counterpart in the reference, whose levels are solved one after another):
+ *   IBPM_CHAIN_SEQUENTIAL         the reference's order, level mg first, each
+ *                                 level's Δ⁻¹ after the coarser one: three
+ *                                 transform launches of one level each;
+ *   IBPM_CHAIN_BOUNDARY_TRANSFER  every level's interior part in one launch per
+ *                                 pass and the edge values of all levels from a
+ *                                 rank-k factorisation of get_bc! ∘ Δ⁻¹ ∘
+ *                                 apply_bc!: fewer, wider launches, more
+ *                                 transform work in all.
+ * Results agree to rounding.  A handle with mg >= 2 starts with the boundary
+ * transfer where its factors exist (their numerical rank below 1024), else
+ * sequentially; setting the boundary transfer on a handle without factors
+ * builds them (IBPM_ERR_UNSUPPORTED if they do not exist).  ibpm_batch_create
+ * with lanes = 0 chooses its members' chain by timing (a batch fills the GPU
+ * with its members, where the sequential chain does less work).  Setting a
+ * chain captures the step graphs again on the next advance. */
+#define IBPM_CHAIN_SEQUENTIAL        0
+#define IBPM_CHAIN_BOUNDARY_TRANSFER 1
+int ibpm_set_level_chain(ibpm_handle* h, int32_t chain);
+int ibpm_get_level_chain(const ibpm_handle* h, int32_t* chain);
 
 /* Number of kernel launches in one step (one replay of the step graph). */
 int ibpm_launches_per_step(ibpm_handle* h);

@@ -41,8 +41,10 @@ def test_batch_members_match_single_runs(lanes):
         sp = specs[i]
         solo = G.IBProblem(sp["grid"], sp["bodies"], sp["dt"], sp["Re"], freestream=sp["freestream"],
                            precision=prec, sync_fields=False)
-        # the tuner also chooses the members' transform plan for single-level launches
+        # the tuner also chooses the members' transform plan for single-level
+        # launches and their level chain
         G.set_transform_plan(solo, batch.plan, G.IBPM_PLAN_AUTO)
+        G.set_level_chain(solo, batch.chain)
         _start(solo, name, seed=30 + i)
         st = G.IBState(solo)
         cd, cl = G.advance(st, solo, 0.0, nsteps=NSTEPS)
