@@ -619,6 +619,7 @@ def batch_block(args, d):
     tuned = b.lanes
     plan = b.plan
     chain = b.chain
+    grouped = b.grouped
     ms = b.bench_steps(K, flush_l2=True)
     t_tuned = float(np.sum(ms)) / 1e3
     b.set_lanes(1)
@@ -637,6 +638,7 @@ def batch_block(args, d):
             "steps": K, "lanes": tuned, "ms_per_batch_step": 1e3 * t_tuned / K,
             "transform_plan": {0: "latency (radix 4)", 1: "throughput (radix 8)"}.get(plan, plan),
             "level_chain": {0: "sequential", 1: "boundary transfer"}.get(chain, chain),
+            "shared_launches": grouped,
             "one_lane": {"value": cells * K / t_seq, "ms_per_batch_step": 1e3 * t_seq / K, "steps": K1},
             "speedup_over_one_lane": t_seq / t_tuned,
             "e2e": {"value": cells * K / e2e_s, "unit": METRIC, "h2d_bytes_per_step": 0,

@@ -197,12 +197,15 @@ cudaError_t launch_gemv(const double* A, const double* x, double* y, int n, cuda
 }
 
 // update_stress! (timestepping.jl:330-354): fb = F̃b (h/dt) ./ ds,
-// CD_j = 2 Σ ds fb_x, CL_j = 2 Σ ds fb_y, written to hist[step][2][nbodies].
+// CD_j = 2 Σ ds fb_x, CL_j = 2 Σ ds fb_y, written to hist[step][2][nbodies]
+// for step < hist_cap (a later step writes nothing and sets bit 3 of *status).
 // One block; a non-finite CD/CL sets bit 0 of *status.
 __device__ __forceinline__ void stress_block(const BodyDev& b, const double* __restrict__ Fb, double h, double dt,
-                                             double* hist, int* counter, int* status) {
+                                             double* hist, int hist_cap, int* counter, int* status) {
     __shared__ double red[2][256];
     const int step = *counter;
+    const bool keep = step >= 0 && step < hist_cap;
+    if (!keep && threadIdx.x == 0) atomicOr(status, 8);
     const double hdt = h / dt;
     for (int j = 0; j < b.nbodies; ++j) {
         const int p0 = b.body_start[j], p1 = b.body_start[j + 1];
@@ -224,8 +227,10 @@ __device__ __forceinline__ void stress_block(const BodyDev& b, const double* __r
         }
         if (threadIdx.x == 0) {
             const double cd = 2.0 * red[0][0], cl = 2.0 * red[1][0];
-            hist[((long long)step * 2 + 0) * b.nbodies + j] = cd;
-            hist[((long long)step * 2 + 1) * b.nbodies + j] = cl;
+            if (keep) {
+                hist[((long long)step * 2 + 0) * b.nbodies + j] = cd;
+                hist[((long long)step * 2 + 1) * b.nbodies + j] = cl;
+            }
             if (!isfinite(cd) || !isfinite(cl)) atomicOr(status, 1);
         }
         __syncthreads();
@@ -234,15 +239,15 @@ __device__ __forceinline__ void stress_block(const BodyDev& b, const double* __r
 }
 
 __global__ void stress_kernel(BodyDev b, const double* __restrict__ Fb, double h, double dt, double* hist,
-                              int* counter, int* status) {
+                              int hist_cap, int* counter, int* status) {
     pdl_wait();
     pdl_trigger();
-    stress_block(b, Fb, h, dt, hist, counter, status);
+    stress_block(b, Fb, h, dt, hist, hist_cap, counter, status);
 }
 
-cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double dt, double* hist, int* counter,
-                          int* status, cudaStream_t st) {
-    return launch_k(stress_kernel, dim3(1), dim3(256), 0, st, b, Fb, h, dt, hist, counter, status);
+cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double dt, double* hist, int hist_cap,
+                          int* counter, int* status, cudaStream_t st) {
+    return launch_k(stress_kernel, dim3(1), dim3(256), 0, st, b, Fb, h, dt, hist, hist_cap, counter, status);
 }
 
 // Γsrc = C'(E' F̃b) at the Γ points whose rot! stencil touches a regularised
@@ -285,21 +290,22 @@ cudaError_t launch_proj_src(const Geom& g, const BodyDev& b, const double* Fb, d
 // block 0 reduces CD/CL (and advances the step counter), the other blocks
 // form C'E'F̃b, one warp per Γ point.
 __global__ void stress_src_kernel(BodyDev b, const double* __restrict__ Fb, double h, double dt, double* hist,
-                                  int* counter, int* status, double* Gsrc) {
+                                  int hist_cap, int* counter, int* status, double* Gsrc) {
     pdl_wait();
     pdl_trigger();
     if (blockIdx.x == 0) {
-        stress_block(b, Fb, h, dt, hist, counter, status);
+        stress_block(b, Fb, h, dt, hist, hist_cap, counter, status);
         return;
     }
     proj_src_warp(b, Fb, Gsrc, ((blockIdx.x - 1) * blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31);
 }
 
-cudaError_t launch_stress_src(const BodyDev& b, const double* Fb, double h, double dt, double* hist, int* counter,
-                              int* status, double* Gsrc, cudaStream_t st) {
+cudaError_t launch_stress_src(const BodyDev& b, const double* Fb, double h, double dt, double* hist, int hist_cap,
+                              int* counter, int* status, double* Gsrc, cudaStream_t st) {
     const long long threads = (long long)b.n_src * 32;
     const unsigned blocks = 1 + (unsigned)((threads + 255) / 256);
-    return launch_k(stress_src_kernel, dim3(blocks), dim3(256), 0, st, b, Fb, h, dt, hist, counter, status, Gsrc);
+    return launch_k(stress_src_kernel, dim3(blocks), dim3(256), 0, st, b, Fb, h, dt, hist, hist_cap, counter, status,
+                    Gsrc);
 }
 
 // C'E' e_kk for unit forces kk = col0 + r (B_times!, laplacian.jl:162), written

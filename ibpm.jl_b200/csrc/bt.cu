@@ -51,6 +51,8 @@ __global__ void __launch_bounds__(256) bt_project_kernel(const T* __restrict__ W
     const int L = g.mg - 1;
     const int sl = g.nx + g.ny + 4, sp = (sl + 3) & ~3;
     const int r = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    samples += (long long)blockIdx.y * g.mg * sl;   // simulation blockIdx.y of a batch group
+    p += (long long)blockIdx.y * L * kp;
     T acc[kMaxLev];
 #pragma unroll
     for (int l = 0; l < kMaxLev; ++l) acc[l] = T(0);
@@ -93,6 +95,9 @@ __global__ void __launch_bounds__(256) bt_expand_kernel(const T* __restrict__ U,
     pdl_trigger();
     const int nE = 2 * g.n1 + 2 * g.n2, ep = (nE + 3) & ~3, L = g.mg - 1;
     const int sl = g.nx + g.ny + 4;
+    samples += (long long)blockIdx.y * g.mg * sl;   // simulation blockIdx.y of a batch group
+    p += (long long)blockIdx.y * L * kp;
+    e += (long long)blockIdx.y * g.mg * ep;
     for (int t = threadIdx.x; t < L * kp; t += blockDim.x) ps[t] = p[t];
     __syncthreads();
     const int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
@@ -304,12 +309,12 @@ int bt_lowrank(const std::vector<double>& R, int nx_, int ny_, int nmat, double 
 }
 
 cudaError_t launch_bt_project(const Geom& g, const BtChainArgs& a, cudaStream_t st) {
-    dim3 grid(a.k);
+    dim3 grid(a.k, std::max(1, a.nsim));
     return launch_k(bt_project_kernel<double>, grid, dim3(256), 0, st, a.W, a.samples, a.p, a.k, a.kp, g);
 }
 
 cudaError_t launch_bt_expand(const Geom& g, const BtChainArgs& a, cudaStream_t st) {
-    dim3 grid((bt_edge_len(g) + 7) / 8);
+    dim3 grid((bt_edge_len(g) + 7) / 8, std::max(1, a.nsim));
     const size_t smem = (size_t)(g.mg - 1) * a.kp * sizeof(double);
     return launch_k(bt_expand_kernel<double>, grid, dim3(256), smem, st, a.U, a.samples,
                     static_cast<const double*>(a.p), a.e, a.k, a.kp, g);

@@ -126,6 +126,20 @@ struct ibpm_handle {
     double* tapeq1 = nullptr;              // [k][nq]  level-1 q after each step
     double* gxb = nullptr;                 // (nb, 2) accumulator
     int xb_k = 0;
+    // batch groups (ibpm_batch_create): members of one grid and precision keep
+    // their step fields in group arenas, member after member, so that while a
+    // group's step is captured its first member stands for all `gsim` of them:
+    // every transform and stencil launch covers the slabs of all, and the body
+    // operators (E, B⁻¹, update_stress!) run per member on branch streams
+    bool in_batch = false;                 // released with its batch only
+    bool arena = false;                    // step fields live in a group arena
+    int gsim = 1;
+    ibpm_handle* const* gmem = nullptr;    // the group's members (this one first)
+    const double* g_den = nullptr;         // [gsim][9]: 2 Re hc² per level, then dt
+    const double* g_cA = nullptr;          // [gsim]: dt / (2 Re h²)
+    const RhsArgs* g_rhs[2] = {nullptr, nullptr};  // [gsim] trial right-hand side arguments per parity
+    cudaStream_t* g_br = nullptr;          // [gsim] branch streams
+    cudaEvent_t* g_ev = nullptr;           // [gsim + 1] fork and join events
     // measurement
     int launches = 0;                      // kernel launches enqueued (counted always)
     bool prof_on = false;                  // eager profiling: events around every launch
@@ -224,6 +238,7 @@ static SpecParams spec(const ibpm_handle* h, int mode, int f32 = 0) {
         const double hc = h->h * std::ldexp(1.0, l);
         sp.den[l] = 2.0 * h->Re * (hc * hc);       // laplacian.jl:69
     }
+    sp.mden = h->gsim > 1 ? h->g_den : nullptr;
     return sp;
 }
 
@@ -282,13 +297,47 @@ static void moving_rates(const ibpm_handle* h, const double* m, double* r) {
 static int stress_and_src(ibpm_handle* h) {
     if (h->bodies_moving) {
         LAUNCH(K_STRESS, 8.0 * 3 * h->nb,
-               launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->st));
+               launch_stress(h->body, h->Fb, h->h, h->dt, h->hist, h->hist_cap, h->counter, h->status, h->st));
         LAUNCH(K_SRC, 8.0 * 4 * 169 * h->nf, launch_proj_src_moving(h->g, h->body, h->Fb, h->d_bbox, h->Gsrc, h->st));
         return IBPM_OK;
     }
     LAUNCH(K_SRC, 8.0 * (4 * 169 * h->nf + 3 * h->nb),
-           launch_stress_src(h->body, h->Fb, h->h, h->dt, h->hist, h->counter, h->status, h->Gsrc, h->st));
+           launch_stress_src(h->body, h->Fb, h->h, h->dt, h->hist, h->hist_cap, h->counter, h->status, h->Gsrc, h->st));
     return IBPM_OK;
+}
+
+// Run `fn` for every member of the group being captured (the handle alone
+// outside groups), each member on its own branch stream forked from and
+// joined back into the lead's stream.
+template <class F>
+static int per_member(ibpm_handle* h, F fn) {
+    if (h->gsim <= 1) return fn(h);
+    CK(cudaEventRecord(h->g_ev[0], h->st));
+    for (int i = 0; i < h->gsim; ++i) {
+        ibpm_handle* m = h->gmem[i];
+        cudaStream_t own = m->st;
+        CK(cudaStreamWaitEvent(h->g_br[i], h->g_ev[0], 0));
+        m->st = h->g_br[i];
+        const int rc = fn(m);
+        m->st = own;
+        if (rc) {
+            if (m != h) h->err = m->err;
+            return rc;
+        }
+        CK(cudaEventRecord(h->g_ev[1 + i], h->g_br[i]));
+        CK(cudaStreamWaitEvent(h->st, h->g_ev[1 + i], 0));
+    }
+    return IBPM_OK;
+}
+
+// boundary_forces! (timestepping.jl:154-163) of one simulation: F = E(qs + q0),
+// F̃b = B⁻¹ F, then update_stress! and the projection source.
+static int forces_and_src(ibpm_handle* h) {
+    const Geom& g = h->g;
+    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h),
+                    h->bodies_moving ? h->d_ub : nullptr, h->h));
+    LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
+    return stress_and_src(h);
 }
 
 static RhsArgs rhs_args(const ibpm_handle* h, int p) {
@@ -446,23 +495,24 @@ static int upload_bt(ibpm_handle* h, const BtLowRank& lr) {
 // part of levels 0 … nyb−1 by one y-pass, into btY / btY32.
 static int bt_edges(ibpm_handle* h, const void* Y, bool f32, int nyb) {
     const Geom& g = h->g;
-    const int mg = g.mg;
+    const int mg = g.mg, ns = h->gsim;
     const long long bs = g.S * mg;
     const int nE = bt_edge_len(g);
     const double es = f32 ? 4.0 : 8.0;
     // the samples, the chain and the edge vectors are FP64 in both precisions
-    LAUNCH(K_BTCHAIN, (es * (g.ny / 2 + 3.0) * g.n1 + 16.0 * g.n1) * (mg - 1),
-           launch_dst_lines(g, h->px, Y, levmap(g, 1, mg - 1, bs), mg - 1, h->btS, f32 ? 1 : 0, h->st));
+    LAUNCH(K_BTCHAIN, (es * (g.ny / 2 + 3.0) * g.n1 + 16.0 * g.n1) * (mg - 1) * ns,
+           launch_dst_lines(g, h->px, Y, levmap(g, 1, mg - 1, bs), (mg - 1) * ns, h->btS, f32 ? 1 : 0, h->st));
     BtChainArgs a{};
     a.W = h->btW; a.U = h->btU; a.samples = h->btS; a.e = h->btE; a.p = h->btP;
-    a.k = h->bt_k; a.kp = h->bt_kp;
-    if (mg > 2) LAUNCH(K_BTCHAIN, 8.0 * ((double)h->bt_k * (g.nx + g.ny + 4.0) * mg + (mg - 1.0) * h->bt_kp),
-                       launch_bt_project(g, a, h->st));
-    LAUNCH(K_BTCHAIN, 8.0 * ((mg - 2.0) * nE * h->bt_kp + 3.0 * nE * (mg - 1)), launch_bt_expand(g, a, h->st));
+    a.k = h->bt_k; a.kp = h->bt_kp; a.nsim = ns;
+    if (mg > 2)
+        LAUNCH(K_BTCHAIN, 8.0 * ((double)h->bt_k * (g.nx + g.ny + 4.0) * (1.0 + (mg - 1.0) * ns) + (mg - 1.0) * h->bt_kp * ns),
+               launch_bt_project(g, a, h->st));
+    LAUNCH(K_BTCHAIN, 8.0 * ((mg - 2.0) * nE * h->bt_kp + 3.0 * nE * (mg - 1) * ns), launch_bt_expand(g, a, h->st));
     BtSynth bsy{};
     bsy.e = h->btE; bsy.sx = h->px.s; bsy.nx = g.nx;
-    LAUNCH(K_DSTY, es * g.n1 * g.n2 * nyb,
-           launch_dst_ybc(g, h->py, h->px, f32 ? (void*)h->btY32 : (void*)h->btY, levmap(g, 0, nyb, bs), nyb,
+    LAUNCH(K_DSTY, es * g.n1 * g.n2 * nyb * ns,
+           launch_dst_ybc(g, h->py, h->px, f32 ? (void*)h->btY32 : (void*)h->btY, levmap(g, 0, nyb, bs), nyb * ns,
                           spec(h, SPEC_DELTA, f32 ? 1 : 0), bsy, h->st));
     return IBPM_OK;
 }
@@ -472,9 +522,9 @@ static int curl_levels(ibpm_handle* h, double* q, int qnlev) {
     CurlArgs ca{};
     ca.psi = h->psi; ca.psi_map = levmap(g, 0, qnlev);
     ca.coarse = h->psi; ca.coarse_map = levmap(g, 1, qnlev);
-    ca.q = q; ca.q_bstride = 0; ca.q_lstride = g.nq; ca.q_lev0 = 0;
-    ca.nlev = qnlev; ca.nbatch = 1; ca.mg = g.mg;
-    LAUNCH(K_CURL, 8.0 * ((double)g.n1 * g.n2 + g.nq) * qnlev, launch_curl(g, ca, h->st));
+    ca.q = q; ca.q_bstride = (long long)g.nq * g.mg; ca.q_lstride = g.nq; ca.q_lev0 = 0;
+    ca.nlev = qnlev; ca.nbatch = h->gsim; ca.mg = g.mg;
+    LAUNCH(K_CURL, 8.0 * ((double)g.n1 * g.n2 + g.nq) * qnlev * h->gsim, launch_curl(g, ca, h->st));
     return IBPM_OK;
 }
 
@@ -484,24 +534,26 @@ static int curl_levels(ibpm_handle* h, double* q, int qnlev) {
 // and 2; the final one recomputes every level.
 static int vort2flux_bt(ibpm_handle* h, double* G, double* q, int qnlev, int nfull) {
     const Geom& g = h->g;
-    const int mg = g.mg;
+    const int mg = g.mg, ns = h->gsim;
     const long long bs = g.S * mg;
     const double slab = (double)g.n1 * g.n2;
     for (int lev = 1; lev < mg; ++lev)
-        LAUNCH(K_COARSIFY, 8.0 * 1.25 * slab,
-               launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), 1, h->st));
+        LAUNCH(K_COARSIFY, 8.0 * 1.25 * slab * ns,
+               launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), ns, h->st));
     SlabMap all = levmap(g, 0, mg, bs);
     XPassArgs a{};
     a.in = G; a.out = h->rhs; a.in_map = all; a.out_map = all;
-    a.nslabs = mg; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_PLAIN; a.emit = XEMIT_STORE;
-    LAUNCH(K_DSTX, 16.0 * slab * mg, launch_dst_x(g, h->px, a, h->st));
-    LAUNCH(K_DSTY, 16.0 * slab * mg, launch_dst_y(g, h->py, h->px, h->rhs, all, mg, spec(h, SPEC_DELTA), h->st));
+    a.nslabs = mg * ns; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_PLAIN; a.emit = XEMIT_STORE;
+    LAUNCH(K_DSTX, 16.0 * slab * mg * ns, launch_dst_x(g, h->px, a, h->st));
+    LAUNCH(K_DSTY, 16.0 * slab * mg * ns,
+           launch_dst_y(g, h->py, h->px, h->rhs, all, mg * ns, spec(h, SPEC_DELTA), h->st));
     int rc = bt_edges(h, h->rhs, false, std::min(nfull, mg - 1));
     if (rc) return rc;
+    SlabMap part = levmap(g, 0, nfull, bs);
     XPassArgs c{};
-    c.in = h->rhs; c.in2 = h->btY; c.in_map = all; c.in2_map = all; c.out = h->psi; c.out_map = all;
-    c.nslabs = nfull; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_SUM; c.emit = XEMIT_STORE;
-    LAUNCH(K_DSTX, 24.0 * slab * nfull, launch_dst_x(g, h->px, c, h->st));
+    c.in = h->rhs; c.in2 = h->btY; c.in_map = part; c.in2_map = part; c.out = h->psi; c.out_map = part;
+    c.nslabs = nfull * ns; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_SUM; c.emit = XEMIT_STORE;
+    LAUNCH(K_DSTX, 24.0 * slab * nfull * ns, launch_dst_x(g, h->px, c, h->st));
     return curl_levels(h, q, qnlev);
 }
 
@@ -516,28 +568,41 @@ static int vort2flux_refined_bt(ibpm_handle* h, double* G, int nsw, double* q, i
     const int mg = g.mg;
     const long long bs = g.S * mg;
     const double slab = (double)g.n1 * g.n2;
+    const int ns = h->gsim;
     for (int lev = 1; lev < mg; ++lev)
-        LAUNCH(K_COARSIFY, 8.0 * 1.25 * slab,
-               launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), 1, h->st));
-    SlabMap all = levmap(g, 0, mg, bs);
+        LAUNCH(K_COARSIFY, 8.0 * 1.25 * slab * ns,
+               launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), ns, h->st));
+    SlabMap all = levmap(g, 0, mg, bs), part = levmap(g, 0, nfull, bs);
     for (int s = 0; s < nsw; ++s) {
         // the residual of every level in one stencil launch (FP32 out), then
         // its x-transform in place: a light x-pass that more CTAs share an SM with
-        LAUNCH(K_RESID, (8.0 + 8.0 + 4.0) * slab * mg, launch_resid_lap(g, G, h->psi, h->T32, h->st));
+        LAUNCH(K_RESID, (8.0 + 8.0 + 4.0) * slab * mg * ns, launch_resid_lap(g, G, h->psi, h->T32, ns, h->st));
         XPassArgs a{};
         a.in = h->T32; a.out = h->T32; a.in_map = all; a.out_map = all;
-        a.nslabs = mg; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_F32; a.emit = XEMIT_F32;
-        LAUNCH(K_DSTX, 8.0 * slab * mg, launch_dst_x(g, h->px, a, h->st));
-        LAUNCH(K_DSTY, 8.0 * slab * mg,
-               launch_dst_y(g, h->py, h->px, h->T32, all, mg, spec(h, SPEC_DELTA, 1), h->st));
+        a.nslabs = mg * ns; a.line0 = 0; a.line1 = g.n2; a.load = XLOAD_F32; a.emit = XEMIT_F32;
+        LAUNCH(K_DSTX, 8.0 * slab * mg * ns, launch_dst_x(g, h->px, a, h->st));
+        LAUNCH(K_DSTY, 8.0 * slab * mg * ns,
+               launch_dst_y(g, h->py, h->px, h->T32, all, mg * ns, spec(h, SPEC_DELTA, 1), h->st));
         int rc = bt_edges(h, h->T32, true, std::min(nfull, mg - 1));
         if (rc) return rc;
         XPassArgs c{};
-        c.in = h->T32; c.in2 = h->btY32; c.in_map = all; c.in2_map = all; c.out = h->psi; c.out_map = all;
-        c.nslabs = nfull; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_F32_SUM; c.emit = XEMIT_ADD;
-        LAUNCH(K_DSTX, (4.0 + 4.0 + 16.0) * slab * nfull, launch_dst_x(g, h->px, c, h->st));
+        c.in = h->T32; c.in2 = h->btY32; c.in_map = part; c.in2_map = part; c.out = h->psi; c.out_map = part;
+        c.nslabs = nfull * ns; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_F32_SUM; c.emit = XEMIT_ADD;
+        LAUNCH(K_DSTX, (4.0 + 4.0 + 16.0) * slab * nfull * ns, launch_dst_x(g, h->px, c, h->st));
     }
     return curl_levels(h, q, qnlev);
+}
+
+// get_trial_state!'s right-hand side of every level (of every member of the
+// group being captured).
+static int trial_rhs(ibpm_handle* h, int p) {
+    const Geom& g = h->g;
+    RhsArgs ra = rhs_args(h, p);
+    ra.rhs = h->rhs;
+    const double bytes = 8.0 * (4.0 * g.n1 * g.n2 + g.nq) * g.mg * h->gsim;
+    if (h->gsim > 1) LAUNCH(K_RHS, bytes, launch_trial_rhs_group(g, ra, h->g_rhs[p], h->gsim, h->st));
+    else LAUNCH(K_RHS, bytes, launch_trial_rhs(g, ra, h->st));
+    return IBPM_OK;
 }
 
 // One step, reading the state from parity p and leaving it in parity p^1.
@@ -545,27 +610,25 @@ static int enqueue_step_fp64(ibpm_handle* h, int p) {
     const Geom& g = h->g;
     const int mg = g.mg;
     double* Gnew = h->G[p ^ 1];
+    const int ns = h->gsim;
+    const long long qb = (long long)g.nq * mg;
     // --- get_trial_state! (timestepping.jl:86-129)
-    RhsArgs ra = rhs_args(h, p);
-    ra.rhs = h->rhs;
-    LAUNCH(K_RHS, 8.0 * (4.0 * g.n1 * g.n2 + g.nq) * mg, launch_trial_rhs(g, ra, h->st));
+    int rc = trial_rhs(h, p);
+    if (rc) return rc;
     SlabMap all = levmap(g, 0, mg);
-    int rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg, SPEC_AINV, XEMIT_STORE);
+    rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg * ns, SPEC_AINV, XEMIT_STORE);
     if (rc) return rc;
     rc = h->bt ? vort2flux_bt(h, Gnew, h->qs, 1, std::min(2, mg))  // only the level-1 trial flux is read
-               : vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->qs, 0, 0, 1);
+               : vort2flux(h, Gnew, h->psi, g.S * mg, ns, h->qs, qb, 0, 1);
     if (rc) return rc;
-    // --- boundary_forces! (timestepping.jl:154-163) and update_stress! (:330-354)
-    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h),
-                    h->bodies_moving ? h->d_ub : nullptr, h->h));
-    LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
+    // --- boundary_forces! (timestepping.jl:154-163), update_stress! (:330-354)
+    if ((rc = per_member(h, forces_and_src))) return rc;
     // --- project_circ! (timestepping.jl:204-223): Γ = Γs − A⁻¹ C'E' F̃b on level 1
-    if ((rc = stress_and_src(h))) return rc;
     SlabMap one = levmap(g, 0, 1);
-    rc = poisson(h, h->Gsrc, one, h->rhs, one, Gnew, one, 1, SPEC_AINV, XEMIT_SUB);
+    rc = poisson(h, h->Gsrc, one, h->rhs, one, Gnew, one, ns, SPEC_AINV, XEMIT_SUB);
     if (rc) return rc;
     // --- vort2flux!(state.ψ, state.q, state.Γ) (timestepping.jl:64)
-    return h->bt ? vort2flux_bt(h, Gnew, h->q, mg, mg) : vort2flux(h, Gnew, h->psi, g.S * mg, 1, h->q, 0, 0, mg);
+    return h->bt ? vort2flux_bt(h, Gnew, h->q, mg, mg) : vort2flux(h, Gnew, h->psi, g.S * mg, ns, h->q, qb, 0, mg);
 }
 
 // ---------------------------------------------------------------------------
@@ -587,21 +650,22 @@ static int correction32(ibpm_handle* h, int load, const double* b, const double*
                         int lev, int emit, double* out) {
     const Geom& g = h->g;
     const long long bs = g.S * g.mg;
+    const int ns = h->gsim;
     SlabMap m = levmap(g, lev, 1, bs);
-    const double slab = (double)g.n1 * g.n2;
+    const double slab = (double)g.n1 * g.n2 * ns;
     XPassArgs a{};
     a.in = b; a.out = h->T32; a.in_map = m; a.out_map = m;
     a.coarse = coarse; a.coarse_map = levmap(g, lev + 1, 1, bs);
-    a.aux = xg; a.aux_map = m; a.cA = cA;
-    a.nslabs = 1; a.line0 = 0; a.line1 = g.n2; a.load = load; a.emit = XEMIT_F32;
+    a.aux = xg; a.aux_map = m; a.cA = cA; a.mcA = ns > 1 ? h->g_cA : nullptr;
+    a.nslabs = ns; a.line0 = 0; a.line1 = g.n2; a.load = load; a.emit = XEMIT_F32;
     LAUNCH(K_DSTX, slab * (8.0 + 8.0 + 4.0), launch_dst_x(g, h->px, a, h->st));
     LAUNCH(K_DSTY, slab * 8.0,
-           launch_dst_y(g, h->py, h->px, h->T32, m, 1, spec(h, load == XLOAD_RES_A ? SPEC_AINV : SPEC_DELTA, 1),
+           launch_dst_y(g, h->py, h->px, h->T32, m, ns, spec(h, load == XLOAD_RES_A ? SPEC_AINV : SPEC_DELTA, 1),
                         h->st));
     XPassArgs c{};
     c.in = h->T32; c.out = out; c.in_map = m; c.out_map = m;
     c.aux = xg; c.aux_map = m;
-    c.nslabs = 1; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_F32; c.emit = emit;
+    c.nslabs = ns; c.line0 = 0; c.line1 = g.n2; c.load = XLOAD_F32; c.emit = emit;
     LAUNCH(K_DSTX, slab * (4.0 + 16.0 + (emit == XEMIT_ACC_SUB ? 16.0 : 0.0)), launch_dst_x(g, h->px, c, h->st));
     return IBPM_OK;
 }
@@ -611,9 +675,10 @@ static int vort2flux_refined(ibpm_handle* h, double* G, int nsw, double* q, int 
     const Geom& g = h->g;
     const int mg = g.mg;
     const long long bs = g.S * mg;
+    const int ns = h->gsim;
     for (int lev = 1; lev < mg; ++lev)
-        LAUNCH(K_COARSIFY, 8.0 * 1.25 * g.n1 * g.n2,
-               launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), 1, h->st));
+        LAUNCH(K_COARSIFY, 8.0 * 1.25 * g.n1 * g.n2 * ns,
+               launch_coarsify(g, G, levmap(g, lev - 1, 1, bs), levmap(g, lev, 1, bs), ns, h->st));
     int rc;
     for (int lev = mg - 1; lev >= 0; --lev) {
         const double* coarse = (lev < mg - 1) ? h->psi : nullptr;
@@ -624,9 +689,9 @@ static int vort2flux_refined(ibpm_handle* h, double* G, int nsw, double* q, int 
     CurlArgs ca{};
     ca.psi = h->psi; ca.psi_map = levmap(g, 0, qnlev, bs);
     ca.coarse = h->psi; ca.coarse_map = levmap(g, 1, qnlev, bs);
-    ca.q = q; ca.q_bstride = 0; ca.q_lstride = g.nq; ca.q_lev0 = 0;
-    ca.nlev = qnlev; ca.nbatch = 1; ca.mg = mg;
-    LAUNCH(K_CURL, 8.0 * ((double)g.n1 * g.n2 + g.nq) * qnlev, launch_curl(g, ca, h->st));
+    ca.q = q; ca.q_bstride = (long long)g.nq * mg; ca.q_lstride = g.nq; ca.q_lev0 = 0;
+    ca.nlev = qnlev; ca.nbatch = ns; ca.mg = mg;
+    LAUNCH(K_CURL, 8.0 * ((double)g.n1 * g.n2 + g.nq) * qnlev * ns, launch_curl(g, ca, h->st));
     return IBPM_OK;
 }
 
@@ -635,12 +700,12 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
     const int mg = g.mg;
     double* Gnew = h->G[p ^ 1];
     const long long bs = g.S * mg;
+    const int ns = h->gsim;
     // --- get_trial_state! (FP64 trial solve: see the note above)
-    RhsArgs ra = rhs_args(h, p);
-    ra.rhs = h->rhs;
-    LAUNCH(K_RHS, 8.0 * (4.0 * g.n1 * g.n2 + g.nq) * mg, launch_trial_rhs(g, ra, h->st));
+    int rc = trial_rhs(h, p);
+    if (rc) return rc;
     SlabMap all = levmap(g, 0, mg, bs);
-    int rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg, SPEC_AINV, XEMIT_STORE);
+    rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg * ns, SPEC_AINV, XEMIT_STORE);
     if (rc) return rc;
     // every level: a level left at the previous step's ψ would start the final
     // vort2flux! from a whole step's change, and its FP32 correction error with it
@@ -648,11 +713,8 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
                : vort2flux_refined(h, Gnew, nsw, h->qs, 1);
     if (rc) return rc;
     // --- boundary_forces! and update_stress! (FP64)
-    LAUNCH(K_E, 16.0 * 169 * h->nf, launch_E(g, h->body, h->qs, 0, 1, h->q0x[0], h->q0y[0], h->F, h->nf, h->st, mv_of(h),
-                    h->bodies_moving ? h->d_ub : nullptr, h->h));
-    LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
+    if ((rc = per_member(h, forces_and_src))) return rc;
     // --- project_circ!: P = A⁻¹ C'E' F̃b refined from the previous P; Γ[1] −= P
-    if ((rc = stress_and_src(h))) return rc;
     for (int s = 0; s < nsw; ++s) {
         const bool last = s + 1 == nsw;
         rc = correction32(h, XLOAD_RES_A, h->Gsrc, nullptr, h->Pp, c_lap(h, 0), 0,
@@ -986,6 +1048,7 @@ extern "C" int ibpm_create(const ibpm_problem_desc* desc, ibpm_handle** out) {
 
 extern "C" int ibpm_destroy(ibpm_handle* h) {
     if (!h) return IBPM_ERR_INVALID;
+    if (h->in_batch) return fail(h, IBPM_ERR_INVALID, "a batch member is released with its batch (ibpm_batch_destroy)");
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->st);
     free_handle(h);
@@ -1252,6 +1315,7 @@ static int advance_impl(ibpm_handle* h, int32_t nsteps, const double* motion, do
     int hstatus = 0;
     CK(cudaMemcpyAsync(&hstatus, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
+    if (hstatus & 8) return fail(h, IBPM_ERR_CUDA, "internal: a step ran past the force history");
     if (hstatus & 4) return fail(h, IBPM_ERR_INVALID, "a moving body's regularisation stencil left the finest grid");
     if (hstatus & 2) return fail(h, IBPM_ERR_NONFINITE, "the Schur complement B of the moved bodies is singular");
     if (hstatus) return fail(h, IBPM_ERR_NONFINITE, "CD/CL became non-finite");
@@ -1876,12 +1940,29 @@ extern "C" int ibpm_adjoint_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_
 
 // ---------------------------------------------------------------------------
 // Batches of independent simulations.  Each member is an ordinary handle;
-// one step of the batch is one graph launch whose branches are the members'
-// steps, spread over `lanes` concurrent streams (members of one lane run one
-// after another).  Small grids leave most of the GPU idle when run alone;
-// run side by side they fill it.  The lane count is picked by timing.
+// one step of the batch is one graph launch whose branches are the steps of
+// its units, spread over `lanes` concurrent streams (units of one lane run one
+// after another).  A unit is one member, or (grouped) a group of members of
+// one grid, precision, level chain and plan, whose step fields sit in shared
+// arenas: the group's transforms and stencils are launches over the slabs of
+// all its members, its body operators one short branch per member.  Small
+// grids leave most of the GPU idle when run alone; side by side and in shared
+// launches they fill it.  Lanes, plan, chain and grouping are picked by
+// timing.
 // ---------------------------------------------------------------------------
+struct BatchGroup {
+    std::vector<ibpm_handle*> mem;             // lead first
+    std::vector<void*> arenas;                 // step fields, member after member
+    double* den = nullptr;                     // [n][9] spectral factors (SpecParams::mden)
+    double* cA = nullptr;                      // [n]
+    RhsArgs* rhs[2] = {nullptr, nullptr};      // [n] per parity
+    std::vector<cudaStream_t> br;              // branch streams of the body operators
+    std::vector<cudaEvent_t> ev;               // fork + one join event per member
+};
+
 struct ibpm_batch {
+    std::vector<BatchGroup> groups;
+    bool grouped = true;                       // groups step by shared launches
     int device = 0;
     std::vector<ibpm_handle*> m;
     cudaStream_t st = nullptr;                 // the batch stream (fork/join point)
@@ -1933,26 +2014,208 @@ static void batch_free_graphs(ibpm_batch* b) {
             if (x) { cudaGraphExecDestroy(x); x = nullptr; }
 }
 
+// The step fields of a group's members moved into arenas, member after member
+// with the strides the shared launches assume: mg slabs for every slab field
+// (Gsrc and Pp included, though they use one), nq·mg for q and qs, and the
+// boundary-transfer vectors at their per-simulation sizes.  The content is
+// kept; each member then points into the arenas.
+template <class T, class F>
+static cudaError_t rehome(BatchGroup& gr, F field, size_t per, size_t have, cudaStream_t st) {
+    if (!field(gr.mem[0])) return cudaSuccess;   // a field this precision does not use
+    const size_t n = gr.mem.size();
+    T* a = nullptr;
+    cudaError_t e = cudaMalloc((void**)&a, sizeof(T) * per * n);
+    if (e != cudaSuccess) return e;
+    gr.arenas.push_back(a);
+    if ((e = cudaMemsetAsync(a, 0, sizeof(T) * per * n, st)) != cudaSuccess) return e;
+    for (size_t i = 0; i < n; ++i)
+        if ((e = cudaMemcpyAsync(a + i * per, field(gr.mem[i]), sizeof(T) * have, cudaMemcpyDeviceToDevice, st)) !=
+            cudaSuccess)
+            return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    for (size_t i = 0; i < n; ++i) {
+        cudaFree(field(gr.mem[i]));
+        field(gr.mem[i]) = a + i * per;
+    }
+    return cudaSuccess;
+}
+
+// The arena-held fields of a handle (set to nullptr before its release).
+static void forget_arena_fields(ibpm_handle* h) {
+    h->G[0] = h->G[1] = h->Nl[0] = h->Nl[1] = nullptr;
+    h->psi = h->q = h->qs = h->rhs = h->Gsrc = h->Pp = nullptr;
+    h->T32 = nullptr;
+    h->btY = h->btS = h->btE = h->btP = nullptr;
+    h->btY32 = nullptr;
+}
+
+static int batch_make_group(ibpm_batch* b, const std::vector<ibpm_handle*>& mem) {
+    b->groups.emplace_back();
+    BatchGroup& gr = b->groups.back();
+    gr.mem = mem;
+    ibpm_handle* h0 = mem[0];
+    const Geom& g = h0->g;
+    const int mg = g.mg, n = (int)mem.size();
+    const size_t slabs = (size_t)g.S * mg, nq = (size_t)g.nq * mg;
+    cudaStream_t st = b->st;
+    cudaError_t e = cudaSuccess;
+    using D = double;
+    auto rd = [&](auto field, size_t per, size_t have) {
+        if (e == cudaSuccess) e = rehome<D>(gr, field, per, have, st);
+    };
+    auto rf = [&](auto field, size_t per, size_t have) {
+        if (e == cudaSuccess) e = rehome<float>(gr, field, per, have, st);
+    };
+    rd([](ibpm_handle* h) -> double*& { return h->G[0]; }, slabs, slabs);
+    rd([](ibpm_handle* h) -> double*& { return h->G[1]; }, slabs, slabs);
+    rd([](ibpm_handle* h) -> double*& { return h->Nl[0]; }, slabs, slabs);
+    rd([](ibpm_handle* h) -> double*& { return h->Nl[1]; }, slabs, slabs);
+    rd([](ibpm_handle* h) -> double*& { return h->psi; }, slabs, slabs);
+    rd([](ibpm_handle* h) -> double*& { return h->rhs; }, slabs, slabs);
+    rd([](ibpm_handle* h) -> double*& { return h->Gsrc; }, slabs, (size_t)g.S);
+    rd([](ibpm_handle* h) -> double*& { return h->Pp; }, slabs, (size_t)g.S);
+    rd([](ibpm_handle* h) -> double*& { return h->q; }, nq, nq);
+    rd([](ibpm_handle* h) -> double*& { return h->qs; }, nq, nq);
+    rf([](ibpm_handle* h) -> float*& { return h->T32; }, slabs, slabs);
+    rd([](ibpm_handle* h) -> double*& { return h->btY; }, slabs, slabs);
+    rf([](ibpm_handle* h) -> float*& { return h->btY32; }, slabs, slabs);
+    const size_t nsmp = (size_t)bt_sample_len(g) * mg, ne = (size_t)bt_edge_pitch(g) * mg;
+    const size_t np = (size_t)(mg - 1) * h0->bt_kp;
+    rd([](ibpm_handle* h) -> double*& { return h->btS; }, nsmp, nsmp);
+    rd([](ibpm_handle* h) -> double*& { return h->btE; }, ne, ne);
+    if (np) rd([](ibpm_handle* h) -> double*& { return h->btP; }, np, np);
+    for (auto* h : mem) { h->arena = true; h->graphs_ready = false; }
+    if (e != cudaSuccess) return bfail(b, IBPM_ERR_NOMEM, std::string("batch group arenas: ") + cudaGetErrorString(e));
+    BCK(cudaMalloc((void**)&gr.den, sizeof(double) * 9 * n));
+    BCK(cudaMalloc((void**)&gr.cA, sizeof(double) * n));
+    for (int p = 0; p < 2; ++p) BCK(cudaMalloc((void**)&gr.rhs[p], sizeof(RhsArgs) * n));
+    gr.br.resize(n);
+    gr.ev.resize(n + 1);
+    for (auto& x : gr.br) BCK(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    for (auto& x : gr.ev) BCK(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    return IBPM_OK;
+}
+
+// Members of one grid (nx, ny, mg), precision, sweep count and boundary-
+// transfer rank, with fixed bodies on a fixed grid, form a group (two or more).
+static int batch_make_groups(ibpm_batch* b) {
+    std::map<std::vector<int>, std::vector<ibpm_handle*>> keys;
+    for (auto* h : b->m) {
+        if (h->moving || h->bodies_moving || h->lin) continue;
+        keys[{h->g.nx, h->g.ny, h->g.mg, h->prec, h->sweeps, h->btW ? h->bt_kp : -1}].push_back(h);
+    }
+    for (auto& kv : keys)
+        if (kv.second.size() >= 2) {
+            int rc = batch_make_group(b, kv.second);
+            if (rc) return rc;
+        }
+    return IBPM_OK;
+}
+
+static void batch_free_groups(ibpm_batch* b) {
+    for (auto& gr : b->groups) {
+        for (auto* h : gr.mem) forget_arena_fields(h);
+        for (void* a : gr.arenas) cudaFree(a);
+        if (gr.den) cudaFree(gr.den);
+        if (gr.cA) cudaFree(gr.cA);
+        for (auto* r : gr.rhs) if (r) cudaFree(r);
+        for (auto x : gr.br) if (x) cudaStreamDestroy(x);
+        for (auto x : gr.ev) if (x) cudaEventDestroy(x);
+    }
+    b->groups.clear();
+}
+
+// A group steps by shared launches when its members agree on everything the
+// launches fix (level chain, plans); otherwise its members step one by one.
+static bool group_shared(const BatchGroup& gr) {
+    const ibpm_handle* h0 = gr.mem[0];
+    for (auto* h : gr.mem)
+        if (h->bt != h0->bt || h->px.plan1 != h0->px.plan1 || h->px.planN != h0->px.planN ||
+            h->py.plan1 != h0->py.plan1 || h->py.planN != h0->py.planN || h->lin || h->moving || h->bodies_moving)
+            return false;
+    return true;
+}
+
+// The per-member tables of a group's shared launches, from the members'
+// present problem data (uploaded before each capture).
+static int group_tables(ibpm_batch* b, BatchGroup& gr) {
+    const int n = (int)gr.mem.size();
+    std::vector<double> den(9 * (size_t)n), cA(n);
+    std::vector<RhsArgs> ra[2] = {std::vector<RhsArgs>(n), std::vector<RhsArgs>(n)};
+    for (int i = 0; i < n; ++i) {
+        ibpm_handle* h = gr.mem[i];
+        const SpecParams sp = spec(h, SPEC_AINV);
+        for (int l = 0; l < 8; ++l) den[9 * i + l] = sp.den[l];
+        den[9 * i + 8] = sp.dt;
+        cA[i] = c_lap(h, 0);
+        for (int p = 0; p < 2; ++p) {
+            ra[p][i] = rhs_args(h, p);
+            ra[p][i].rhs = h->rhs;
+        }
+    }
+    BCK(cudaMemcpy(gr.den, den.data(), sizeof(double) * den.size(), cudaMemcpyHostToDevice));
+    BCK(cudaMemcpy(gr.cA, cA.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    for (int p = 0; p < 2; ++p)
+        BCK(cudaMemcpy(gr.rhs[p], ra[p].data(), sizeof(RhsArgs) * n, cudaMemcpyHostToDevice));
+    return IBPM_OK;
+}
+
+// The units of a batch step: shared groups (when grouped), then every member
+// not in one.  Entries >= 0 are member indices, < 0 group -1 - index.
+static std::vector<int> batch_units(ibpm_batch* b) {
+    std::vector<int> units;
+    std::vector<char> done(b->m.size(), 0);
+    if (b->grouped)
+        for (size_t k = 0; k < b->groups.size(); ++k)
+            if (group_shared(b->groups[k])) {
+                units.push_back(-1 - (int)k);
+                for (auto* h : b->groups[k].mem)
+                    for (size_t i = 0; i < b->m.size(); ++i) if (b->m[i] == h) done[i] = 1;
+            }
+    for (size_t i = 0; i < b->m.size(); ++i) if (!done[i]) units.push_back((int)i);
+    return units;
+}
+
+// Enqueue one unit's step on stream `st` (a member, or a group by its lead).
+static int batch_enqueue_unit(ibpm_batch* b, int u, cudaStream_t st, int p, bool cold) {
+    if (u >= 0) {
+        ibpm_handle* h = b->m[u];
+        if (h->moving || h->bodies_moving) return bfail(b, IBPM_ERR_UNSUPPORTED, "member " + std::to_string(u) + " moves (not batched)");
+        cudaStream_t own = h->st;
+        h->st = st;                            // the member's launches join the lane
+        const int rc = enqueue_step(h, p, cold);
+        h->st = own;
+        if (rc) b->err = "member " + std::to_string(u) + ": " + h->err;
+        return rc;
+    }
+    BatchGroup& gr = b->groups[-1 - u];
+    ibpm_handle* h = gr.mem[0];
+    cudaStream_t own = h->st;
+    h->st = st;
+    h->gsim = (int)gr.mem.size(); h->gmem = gr.mem.data();
+    h->px.sims = h->py.sims = h->gsim;
+    h->g_den = gr.den; h->g_cA = gr.cA; h->g_rhs[0] = gr.rhs[0]; h->g_rhs[1] = gr.rhs[1];
+    h->g_br = gr.br.data(); h->g_ev = gr.ev.data();
+    const int rc = enqueue_step(h, p, cold);
+    h->st = own;
+    h->gsim = 1; h->gmem = nullptr; h->g_den = nullptr; h->g_cA = nullptr;
+    h->px.sims = h->py.sims = 0;
+    h->g_rhs[0] = h->g_rhs[1] = nullptr; h->g_br = nullptr; h->g_ev = nullptr;
+    if (rc) b->err = "group of " + std::to_string(gr.mem.size()) + " members: " + h->err;
+    return rc;
+}
+
 // Capture the batch step of parity p (cold: the refined members' first steps).
 static int batch_capture(ibpm_batch* b, int lanes, int p, bool cold, cudaGraphExec_t* out) {
     cudaGraph_t graph;
     BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaEventRecord(b->ev[0], b->st);
     int rc = IBPM_OK;
+    const std::vector<int> units = batch_units(b);
     for (int l = 0; l < lanes && e == cudaSuccess && rc == IBPM_OK; ++l) {
         e = cudaStreamWaitEvent(b->lane_st[l], b->ev[0], 0);
-        for (size_t i = l; i < b->m.size() && e == cudaSuccess && rc == IBPM_OK; i += lanes) {
-            ibpm_handle* h = b->m[i];
-            if (h->moving || h->bodies_moving) {
-                rc = bfail(b, IBPM_ERR_UNSUPPORTED, "member " + std::to_string(i) + " moves (not batched)");
-                break;
-            }
-            cudaStream_t own = h->st;
-            h->st = b->lane_st[l];                 // the member's launches join lane l
-            rc = enqueue_step(h, p, cold);
-            h->st = own;
-            if (rc) b->err = "member " + std::to_string(i) + ": " + h->err;
-        }
+        for (size_t i = l; i < units.size() && e == cudaSuccess && rc == IBPM_OK; i += lanes)
+            rc = batch_enqueue_unit(b, units[i], b->lane_st[l], p, cold);
         if (e == cudaSuccess) e = cudaEventRecord(b->ev[1 + l], b->lane_st[l]);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, b->ev[1 + l], 0);
     }
@@ -1968,6 +2231,10 @@ static int batch_capture(ibpm_batch* b, int lanes, int p, bool cold, cudaGraphEx
 
 static int batch_graphs(ibpm_batch* b, int lanes) {
     batch_free_graphs(b);
+    for (auto& gr : b->groups) {
+        int rc = group_tables(b, gr);
+        if (rc) return rc;
+    }
     bool any_refined = false;
     for (auto* h : b->m) any_refined |= h->prec == IBPM_PREC_FP32_REFINED;
     for (int c = 0; c < (any_refined ? 2 : 1); ++c)
@@ -1992,6 +2259,7 @@ static void batch_destroy_impl(ibpm_batch* b) {
     if (!b) return;
     if (b->st) cudaStreamSynchronize(b->st);
     batch_free_graphs(b);
+    batch_free_groups(b);
     for (auto* h : b->m) { if (h) { cudaStreamSynchronize(h->st); free_handle(h); } }
     for (auto s : b->lane_st) cudaStreamDestroy(s);
     for (auto e : b->ev) cudaEventDestroy(e);
@@ -1999,55 +2267,100 @@ static void batch_destroy_impl(ibpm_batch* b) {
     delete b;
 }
 
-// Set every member's level chain; false if one of them cannot take it.
-static bool batch_chain_all(ibpm_batch* b, int chain) {
-    for (auto* h : b->m)
+// Device time of `steps` batch steps with `lanes` lanes (after two untimed).
+static int batch_time(ibpm_batch* b, int lanes, int steps, cudaEvent_t e0, cudaEvent_t e1, float* ms) {
+    int rc = batch_graphs(b, lanes);
+    if (rc) return rc;
+    if (steps + 2 > b->hist_cap) return bfail(b, IBPM_ERR_INVALID, "batch tuning: more steps than the force history holds");
+    for (auto* h : b->m) BCK(cudaMemsetAsync(h->counter, 0, sizeof(int), b->st));   // the force history restarts
+    for (int s = 0; s < 2; ++s)
+        if (batch_step(b) != cudaSuccess) return bfail(b, IBPM_ERR_CUDA, "batch tuning step failed");
+    cudaEventRecord(e0, b->st);
+    for (int s = 0; s < steps; ++s)
+        if (batch_step(b) != cudaSuccess) return bfail(b, IBPM_ERR_CUDA, "batch tuning step failed");
+    cudaEventRecord(e1, b->st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) return bfail(b, IBPM_ERR_CUDA, "batch tuning sync failed");
+    cudaEventElapsedTime(ms, e0, e1);
+    return IBPM_OK;
+}
+
+// Level chain and single-slab plan of some members; false if one of them
+// cannot take the chain.
+static bool set_members(const std::vector<ibpm_handle*>& mem, int chain, int plan) {
+    for (auto* h : mem) {
         if (set_chain(h, chain) != IBPM_OK) return false;
+        set_plans(h, plan, h->px.planN);
+    }
     return true;
 }
 
-// Time `steps` batch steps for each candidate: the members' level chain
-// (sequential or boundary transfer), the transform plan of their single-slab
-// launches (latency or throughput) and the lane count (powers of two up to the
-// member count); keep the fastest.  The members are reset afterwards.
+// Time `steps` batch steps for each candidate: shared launches or not, the
+// members' level chain (sequential or boundary transfer), the transform plan
+// of their single-slab launches (latency or throughput) and the lane count
+// (powers of two up to the number of units); keep the fastest.  With shared
+// launches, each group (largest first) then tries the other chains and plans
+// on its own, the batch's other settings fixed, and keeps one that shortens
+// the batch step by more than 1%: groups of different grids want different
+// ones (the step time is the longest group's chain of launches).  The members
+// are reset afterwards.
 static int batch_tune(ibpm_batch* b, int steps) {
-    const int n = (int)b->m.size();
-    struct Cand { int chain, plan, lanes; };
+    struct Cand { int chain, plan, lanes; bool grouped; };
     std::vector<Cand> cand;
-    for (int ch : {IBPM_CHAIN_SEQUENTIAL, IBPM_CHAIN_BOUNDARY_TRANSFER})
-        for (int pl : {IBPM_PLAN_LATENCY, IBPM_PLAN_THROUGHPUT}) {
-            for (int l = 1; l < n; l *= 2) cand.push_back({ch, pl, l});
-            cand.push_back({ch, pl, n});
-        }
+    for (bool grp : {true, false}) {
+        if (grp && b->groups.empty()) continue;
+        b->grouped = grp;
+        const int nu = (int)batch_units(b).size();    // the members' chains and plans do not change the units
+        for (int ch : {IBPM_CHAIN_SEQUENTIAL, IBPM_CHAIN_BOUNDARY_TRANSFER})
+            for (int pl : {IBPM_PLAN_LATENCY, IBPM_PLAN_THROUGHPUT}) {
+                for (int l = 1; l < nu; l *= 2) cand.push_back({ch, pl, l, grp});
+                cand.push_back({ch, pl, nu, grp});
+            }
+    }
     double best = 1e300;
-    Cand win{IBPM_CHAIN_SEQUENTIAL, IBPM_PLAN_LATENCY, n};
+    Cand win{IBPM_CHAIN_SEQUENTIAL, IBPM_PLAN_LATENCY, (int)b->m.size(), false};
     cudaEvent_t e0, e1;
     BCK(cudaEventCreate(&e0));
     BCK(cudaEventCreate(&e1));
     int rc = IBPM_OK;
     for (const Cand& c : cand) {
-        if (!batch_chain_all(b, c.chain)) continue;   // no boundary-transfer factors for a member
-        for (auto* h : b->m) set_plans(h, c.plan, h->px.planN);
-        if ((rc = batch_graphs(b, c.lanes))) break;
-        for (int s = 0; s < 2 && rc == IBPM_OK; ++s)
-            if (batch_step(b) != cudaSuccess) rc = bfail(b, IBPM_ERR_CUDA, "batch tuning step failed");
-        if (rc) break;
-        cudaEventRecord(e0, b->st);
-        for (int s = 0; s < steps && rc == IBPM_OK; ++s)
-            if (batch_step(b) != cudaSuccess) rc = bfail(b, IBPM_ERR_CUDA, "batch tuning step failed");
-        cudaEventRecord(e1, b->st);
-        if (cudaEventSynchronize(e1) != cudaSuccess) { rc = bfail(b, IBPM_ERR_CUDA, "batch tuning sync failed"); break; }
+        if (!set_members(b->m, c.chain, c.plan)) continue;   // no boundary-transfer factors for a member
+        b->grouped = c.grouped;
         float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
+        if ((rc = batch_time(b, c.lanes, steps, e0, e1, &ms))) break;
         if (ms < best) { best = ms; win = c; }
+    }
+    if (rc == IBPM_OK && !set_members(b->m, win.chain, win.plan)) rc = bfail(b, IBPM_ERR_CUDA, "batch tuning: level chain");
+    b->grouped = win.grouped;
+    if (rc == IBPM_OK && win.grouped) {
+        std::vector<int> order(b->groups.size());
+        for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
+        auto cells = [&](int k) {
+            const Geom& g = b->groups[k].mem[0]->g;
+            return (double)g.nx * g.ny * g.mg * b->groups[k].mem.size();
+        };
+        std::sort(order.begin(), order.end(), [&](int x, int y) { return cells(x) > cells(y); });
+        float base = 0;
+        rc = batch_time(b, win.lanes, 2 * steps, e0, e1, &base);
+        for (int k : order) {
+            if (rc) break;
+            const auto& mem = b->groups[k].mem;
+            const int ch0 = mem[0]->chain, pl0 = mem[0]->px.plan1;
+            int keep_ch = ch0, keep_pl = pl0;
+            for (int ch : {IBPM_CHAIN_SEQUENTIAL, IBPM_CHAIN_BOUNDARY_TRANSFER})
+                for (int pl : {IBPM_PLAN_LATENCY, IBPM_PLAN_THROUGHPUT}) {
+                    if (rc || (ch == ch0 && pl == pl0) || !set_members(mem, ch, pl)) continue;
+                    float ms = 0;
+                    if ((rc = batch_time(b, win.lanes, 2 * steps, e0, e1, &ms))) break;
+                    if (ms < 0.99f * base) { base = ms; keep_ch = ch; keep_pl = pl; }
+                }
+            if (rc == IBPM_OK && !set_members(mem, keep_ch, keep_pl)) rc = bfail(b, IBPM_ERR_CUDA, "batch tuning: level chain");
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
-    if (!batch_chain_all(b, win.chain)) return bfail(b, IBPM_ERR_CUDA, "batch tuning: level chain");
     for (auto* h : b->m) {
         if ((rc = reset_state(h))) return bfail(b, rc, h->err);
-        set_plans(h, win.plan, h->px.planN);
         if ((rc = ensure_graphs(h, b->hist_cap))) return bfail(b, rc, h->err);  // the members' own graphs
     }
     b->cur = 0;
@@ -2094,6 +2407,8 @@ extern "C" int ibpm_batch_create(int32_t n, const ibpm_problem_desc* descs, int3
     for (auto& e : b->ev)
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
             return done(bfail(b, IBPM_ERR_CUDA, "batch event"));
+    for (auto* h : b->m) h->in_batch = true;
+    if ((rc = batch_make_groups(b))) return done(rc);
     b->hist_cap = 1024;
     for (auto* h : b->m)
         if ((rc = ensure_graphs(h, b->hist_cap))) return done(bfail(b, rc, h->err));
@@ -2133,6 +2448,16 @@ extern "C" int ibpm_batch_set_plan(ibpm_batch* b, int32_t plan) {
 }
 
 extern "C" int ibpm_batch_chain(const ibpm_batch* b) { return b ? b->chain : IBPM_ERR_INVALID; }
+
+extern "C" int ibpm_batch_grouped(const ibpm_batch* b) { return b ? (b->grouped ? 1 : 0) : IBPM_ERR_INVALID; }
+
+extern "C" int ibpm_batch_set_grouped(ibpm_batch* b, int32_t on) {
+    if (!b || (on != 0 && on != 1)) return IBPM_ERR_INVALID;
+    BCK(cudaSetDevice(b->device));
+    BCK(cudaStreamSynchronize(b->st));
+    b->grouped = on == 1;
+    return batch_graphs(b, std::min(b->lanes, (int)batch_units(b).size()));
+}
 
 extern "C" int ibpm_batch_set_chain(ibpm_batch* b, int32_t chain) {
     if (!b || (chain != IBPM_CHAIN_SEQUENTIAL && chain != IBPM_CHAIN_BOUNDARY_TRANSFER)) return IBPM_ERR_INVALID;
@@ -2210,6 +2535,7 @@ extern "C" int ibpm_batch_advance(ibpm_batch* b, int32_t nsteps) {
     for (size_t i = 0; i < b->m.size(); ++i) {
         int hs = 0;
         BCK(cudaMemcpy(&hs, b->m[i]->status, sizeof(int), cudaMemcpyDeviceToHost));
+        if (hs & 8) return bfail(b, IBPM_ERR_CUDA, "member " + std::to_string(i) + ": internal: a step ran past the force history");
         if (hs) return bfail(b, IBPM_ERR_NONFINITE, "member " + std::to_string(i) + ": CD/CL became non-finite");
     }
     return IBPM_OK;

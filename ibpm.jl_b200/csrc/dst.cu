@@ -115,6 +115,7 @@ DstPlan dst_plan_at(double* base, int N) {
     p.Wt = nullptr;
     p.Wt32 = nullptr;
     p.plan1 = p.planN = DST_PLAN_LATENCY;
+    p.sims = 0;
     return p;
 }
 

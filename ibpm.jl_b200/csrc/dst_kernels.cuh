@@ -454,6 +454,7 @@ __global__ void __launch_bounds__(ct_groups(N, PL) * ct_tp(N, PL), ct_fine(N, PL
     if ((LOAD == XLOAD_BC || LOAD == XLOAD_RES_LAP) && a.coarse && a.in_map.level(y) + 1 < g.mg)
         cb.rc = a.coarse + a.coarse_map.off(y);
     const double* xg = (LOAD == XLOAD_RES_LAP || LOAD == XLOAD_RES_A) ? a.aux + a.aux_map.off(y) : nullptr;
+    const double cA = (LOAD == XLOAD_RES_A && a.mcA) ? a.mcA[a.in_map.batch(y)] : a.cA;
 
     // apply_bc!(r, get_bc!(coarse), 1.0) (mg-utils.jl:43-60) in the reference's
     // order: bottom row, top row, left column, right column.
@@ -512,7 +513,7 @@ __global__ void __launch_bounds__(ct_groups(N, PL) * ct_tp(N, PL), ct_fine(N, PL
             if (cb.rc) v = with_bc(v, i, la + r);
             v -= lap(i, r);
         } else {
-            v -= rs[(1 + r) * N + i] + a.cA * lap(i, r);
+            v -= rs[(1 + r) * N + i] + cA * lap(i, r);
         }
         return v;
     };
@@ -680,7 +681,7 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
         // the edge vectors and the sums over them are FP64 (they couple the
         // levels); the tile takes the x-spectrum rounded to T
         const int ep = ((2 * n1 + 2 * n2) + 3) & ~3;
-        const double* e = static_cast<const double*>(bs.e) + (long long)lev * ep;
+        const double* e = static_cast<const double*>(bs.e) + ((long long)map.batch(blockIdx.y) * g.mg + lev) * ep;
         const double* sxt = static_cast<const double*>(bs.sx);
         const int nx = bs.nx, nx2 = 2 * bs.nx;
         auto sinpix = [&](int t) -> double {  // sin(π t / nx), 0 ≤ t < 2 nx
@@ -778,7 +779,9 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
                 // (laplacian.jl:17-41, 61-71)
                 const double cxa = __ldg(&cx[ia]);
                 const double cxb = hasb ? __ldg(&cx[ia + 1]) : 0.0;
-                const double den = sp.den[lev];
+                const double* md = sp.mden ? sp.mden + (long long)map.batch(blockIdx.y) * 9 : nullptr;
+                const double den = md ? md[lev] : sp.den[lev];
+                const double dt = md ? md[8] : sp.dt;
                 for (int o = tid; o < n2; o += TP) {
                     const double c2 = cyv[o];
                     const double la = -2.0 * ((cxa + c2) - 2.0);
@@ -788,8 +791,8 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
                         Ma = la;
                         Mb = lb;
                     } else {
-                        Ma = 1.0 + la * sp.dt / den;
-                        Mb = 1.0 + lb * sp.dt / den;
+                        Ma = 1.0 + la * dt / den;
+                        Mb = 1.0 + lb * dt / den;
                     }
                     tile[o * TWp + ca] = (tile[o * TWp + ca] * nr_rcp(Ma)) * sp.scale;
                     tile[o * TWp + ca + 1] = hasb ? (tile[o * TWp + ca + 1] * nr_rcp(Mb)) * sp.scale : 0.0;
@@ -799,7 +802,9 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
                 // no cancellation for the smallest eigenvalues in FP32
                 const float axa = __ldg(&cx[ia]);
                 const float axb = hasb ? __ldg(&cx[ia + 1]) : 0.0f;
-                const float kf = (sp.mode == SPEC_DELTA) ? 0.0f : (float)(sp.dt / sp.den[lev]);
+                const double* md = sp.mden ? sp.mden + (long long)map.batch(blockIdx.y) * 9 : nullptr;
+                const float kf = (sp.mode == SPEC_DELTA) ? 0.0f
+                                 : md ? (float)(md[8] / md[lev]) : (float)(sp.dt / sp.den[lev]);
                 const float sc = (float)sp.scale;
                 for (int o = tid; o < n2; o += TP) {
                     const float la = axa + cyv[o];
@@ -849,7 +854,7 @@ __global__ void __launch_bounds__(ct_tp(N, PL)) dst_lines_kernel(const T* Y, Sla
     constexpr int TP = ct_tp(N, PL);
     const int P = g.P, nx = g.nx, ny = g.ny, n1 = g.n1;
     const T* base = Y + map.off(blockIdx.y);
-    double* smp = samples + (long long)map.level(blockIdx.y) * (nx + ny + 4);
+    double* smp = samples + ((long long)map.batch(blockIdx.y) * g.mg + map.level(blockIdx.y)) * (nx + ny + 4);
     if (blockIdx.x == 0) {
         extern __shared__ __align__(16) unsigned char smem_raw[];
         V* tw = reinterpret_cast<V*>(smem_raw);
@@ -920,6 +925,7 @@ cudaError_t launch_x_n(const Geom& g, const DstPlan& px, const XPassArgs& a, cud
 // The plan of a launch: the plan's single-slab or multi-slab choice; the
 // throughput plan needs its twiddle table.
 inline int launch_plan(int N, const DstPlan& p, int nslabs) {
+    if (p.sims > 1) nslabs /= p.sims;
     int pl = nslabs > 1 ? p.planN : p.plan1;
     if (pl == DST_PLAN_AUTO) pl = nslabs >= kAutoWideSlabs ? DST_PLAN_THROUGHPUT : p.plan1;
     return (pl == DST_PLAN_THROUGHPUT && p.Wt && N < 1024) ? 1 : 0;

@@ -177,6 +177,10 @@ struct DstPlan {
     float2* Wt32;
     // plan of single-slab and of multi-slab launches (DST_PLAN_*)
     int plan1, planN;
+    // simulations sharing each launch (batch groups; 0 or 1: one): the plan
+    // follows the slabs of one simulation, so a member computes what it
+    // computes alone
+    int sims;
 };
 // DST_PLAN_AUTO (multi-slab launches only): the throughput plan for launches
 // of at least kAutoWideSlabs slabs (the columns of B, the moving bodies'
@@ -209,6 +213,10 @@ struct SpecParams {
     double scale;        // 1 / (4 nx ny)
     double dt;
     double den[8];       // 2 Re hc² per level
+    // a launch over the slabs of several simulations of one grid (batch
+    // groups): per simulation (the slab map's batch index) den[0..7] then dt,
+    // 9 doubles each, in place of den and dt; nullptr otherwise
+    const double* mden;
 };
 
 // x-direction DST-I of every line of the slabs selected by `map` over lines
@@ -243,6 +251,7 @@ struct XPassArgs {
     const double* coarse;  SlabMap coarse_map;   // XLOAD_BC / RES_LAP: coarser-level field
     double* aux; SlabMap aux_map;                // RES_*: current solution; ADD_FROM / ACC_SUB (see above)
     double cA;                                   // XLOAD_RES_A: c = dt / (2 Re hc²)
+    const double* mcA;                           // per simulation of a batch group (in_map's batch), or nullptr
     int nslabs, line0, line1;
     int load, emit;
 };
@@ -299,6 +308,9 @@ struct BtChainArgs {
     double* p;              // (mg−1) × kp projections
     double* e;              // edge vectors, level-major, bt_edge_pitch apart
     int k, kp;              // rank and its pitch (multiple of 4)
+    int nsim;               // simulations of one grid (batch groups; 0 means 1): samples, p
+                            // and e of simulation s follow those of s−1 (mg·bt_sample_len,
+                            // (mg−1)·kp and mg·bt_edge_pitch doubles apart)
 };
 cudaError_t launch_bt_project(const Geom& g, const BtChainArgs& a, cudaStream_t st);
 cudaError_t launch_bt_expand(const Geom& g, const BtChainArgs& a, cudaStream_t st);
@@ -362,12 +374,16 @@ struct RhsArgs {
     MovingFlux mv;                        // moving grid: per-face q0 replaces q0x/q0y
 };
 cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st);
+// The trial right-hand sides of nsim simulations of one grid in one launch
+// (batch groups): ga[s] holds simulation s's arguments (device memory), a0
+// those of simulation 0 (mg and the launch shape).
+cudaError_t launch_trial_rhs_group(const Geom& g, const RhsArgs& a0, const RhsArgs* ga, int nsim, cudaStream_t st);
 
 cudaError_t launch_coarsify(const Geom& g, double* G, SlabMap fine_map, SlabMap coarse_map,
                             int nslabs, cudaStream_t st);
-// FP64 residual of vort2flux! on every level (all mg slabs of G and psi, the
-// handle's slab layout), stored in FP32 into r (stencil.cu).
-cudaError_t launch_resid_lap(const Geom& g, const double* G, const double* psi, float* r, cudaStream_t st);
+// FP64 residual of vort2flux! on every level of nsim simulations (mg slabs
+// each, consecutive in G, psi and r), stored in FP32 into r (stencil.cu).
+cudaError_t launch_resid_lap(const Geom& g, const double* G, const double* psi, float* r, int nsim, cudaStream_t st);
 
 struct CurlArgs {
     const double* psi; SlabMap psi_map;
@@ -412,13 +428,15 @@ cudaError_t launch_proj_src_moving(const Geom& g, const BodyDev& b, const double
                                    cudaStream_t st);
 cudaError_t launch_info_to_status(const int* info, int* status, cudaStream_t st);
 cudaError_t launch_gemv(const double* A, const double* x, double* y, int n, cudaStream_t st);
+// The force history holds hist_cap steps: a step past it writes nothing and
+// sets bit 3 of *status.
 cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double dt,
-                          double* hist, int* counter, int* status, cudaStream_t st);
+                          double* hist, int hist_cap, int* counter, int* status, cudaStream_t st);
 cudaError_t launch_proj_src(const Geom& g, const BodyDev& b, const double* Fb, double* Gsrc,
                             cudaStream_t st);
 // launch_stress and launch_proj_src in one launch (fixed bodies)
-cudaError_t launch_stress_src(const BodyDev& b, const double* Fb, double h, double dt, double* hist, int* counter,
-                              int* status, double* Gsrc, cudaStream_t st);
+cudaError_t launch_stress_src(const BodyDev& b, const double* Fb, double h, double dt, double* hist, int hist_cap,
+                              int* counter, int* status, double* Gsrc, cudaStream_t st);
 cudaError_t launch_unit_src(const Geom& g, const BodyDev& b, int col0, int ncol, double* G,
                             long long bstride, cudaStream_t st);
 

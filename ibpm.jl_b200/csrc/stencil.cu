@@ -23,13 +23,16 @@ namespace ibpm {
 // base flux, both products using this state's edge values ¼ get_bc!(Γ[l+1])
 // (the reference passes the perturbation's Γbc to the ΓB product too).
 // MOV: a moving grid's per-face base flux (MovingFlux) instead of q0x, q0y.
-template <bool LIN, bool MOV>
-__global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
+// GRP: the simulations of a batch group, blockIdx.z = simulation · mg + level,
+// each with its own arguments in ga[simulation] (its fields, coefficients).
+template <bool LIN, bool MOV, bool GRP = false>
+__global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a0, const RhsArgs* __restrict__ ga, Geom g) {
     pdl_wait();
     pdl_trigger();
+    const RhsArgs& a = GRP ? ga[blockIdx.z / g.mg] : a0;
     const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
     const int j0 = blockIdx.y * blockDim.y + threadIdx.y;
-    const int lev = blockIdx.z;
+    const int lev = GRP ? (int)(blockIdx.z % g.mg) : (int)blockIdx.z;
     const int nx = g.nx, ny = g.ny, n1 = g.n1, n2 = g.n2, P = g.P;
     if (i0 >= n1 || j0 >= n2) return;
     const double* G = a.G + a.Gmap.off(lev);
@@ -129,9 +132,16 @@ __global__ void __launch_bounds__(256) trial_rhs_kernel(RhsArgs a, Geom g) {
 cudaError_t launch_trial_rhs(const Geom& g, const RhsArgs& a, cudaStream_t st) {
     dim3 blk(32, 8);
     dim3 grid((g.n1 + 31) / 32, (g.n2 + 7) / 8, a.mg);
-    if (a.GB) return launch_k(trial_rhs_kernel<true, false>, grid, blk, 0, st, a, g);
-    if (a.mv.tab) return launch_k(trial_rhs_kernel<false, true>, grid, blk, 0, st, a, g);
-    return launch_k(trial_rhs_kernel<false, false>, grid, blk, 0, st, a, g);
+    const RhsArgs* none = nullptr;
+    if (a.GB) return launch_k(trial_rhs_kernel<true, false>, grid, blk, 0, st, a, none, g);
+    if (a.mv.tab) return launch_k(trial_rhs_kernel<false, true>, grid, blk, 0, st, a, none, g);
+    return launch_k(trial_rhs_kernel<false, false>, grid, blk, 0, st, a, none, g);
+}
+
+cudaError_t launch_trial_rhs_group(const Geom& g, const RhsArgs& a0, const RhsArgs* ga, int nsim, cudaStream_t st) {
+    dim3 blk(32, 8);
+    dim3 grid((g.n1 + 31) / 32, (g.n2 + 7) / 8, nsim * g.mg);
+    return launch_k(trial_rhs_kernel<false, false, true>, grid, blk, 0, st, a0, ga, g);
 }
 
 // ---------------------------------------------------------------------------
@@ -226,10 +236,11 @@ __global__ void __launch_bounds__(256) resid_lap_kernel(const double* __restrict
     pdl_trigger();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int lev = blockIdx.z;
+    // slab z = simulation · mg + level (simulations mg slabs apart)
+    const int z = blockIdx.z, lev = z % g.mg;
     const int n1 = g.n1, n2 = g.n2, P = g.P;
     if (i >= n1 || j >= n2) return;
-    const double* x = psi + (long long)lev * g.S;
+    const double* x = psi + (long long)z * g.S;
     const long long o = (long long)j * P + i;
     const double xc = x[o];
     double nb = 0.0;
@@ -237,22 +248,22 @@ __global__ void __launch_bounds__(256) resid_lap_kernel(const double* __restrict
     if (i + 1 < n1) nb += x[o + 1];
     if (j > 0) nb += x[o - P];
     if (j + 1 < n2) nb += x[o + P];
-    double v = G[(long long)lev * g.S + o];
+    double v = G[(long long)z * g.S + o];
     if (lev + 1 < g.mg) {
         CoarseBC cb;
-        cb.rc = psi + (long long)(lev + 1) * g.S; cb.P = P; cb.nx = g.nx; cb.ny = g.ny;
+        cb.rc = psi + (long long)(z + 1) * g.S; cb.P = P; cb.nx = g.nx; cb.ny = g.ny;
         if (j == 0) v += cb.bot(i + 1);
         if (j == n2 - 1) v += cb.top(i + 1);
         if (i == 0) v += cb.left(j + 1);
         if (i == n1 - 1) v += cb.right(j + 1);
     }
     v -= 4.0 * xc - nb;
-    r[(long long)lev * g.S + o] = (float)v;
+    r[(long long)z * g.S + o] = (float)v;
 }
 
-cudaError_t launch_resid_lap(const Geom& g, const double* G, const double* psi, float* r, cudaStream_t st) {
+cudaError_t launch_resid_lap(const Geom& g, const double* G, const double* psi, float* r, int nsim, cudaStream_t st) {
     dim3 blk(32, 8);
-    dim3 grid((g.n1 + 31) / 32, (g.n2 + 7) / 8, g.mg);
+    dim3 grid((g.n1 + 31) / 32, (g.n2 + 7) / 8, g.mg * nsim);
     return launch_k(resid_lap_kernel, grid, blk, 0, st, G, psi, r, g);
 }
 

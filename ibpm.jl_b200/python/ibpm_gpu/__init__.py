@@ -167,6 +167,10 @@ def load_library(path=None):
     lib.ibpm_batch_chain.argtypes = [H]
     lib.ibpm_batch_set_chain.restype = C.c_int
     lib.ibpm_batch_set_chain.argtypes = [H, C.c_int32]
+    lib.ibpm_batch_grouped.restype = C.c_int
+    lib.ibpm_batch_grouped.argtypes = [H]
+    lib.ibpm_batch_set_grouped.restype = C.c_int
+    lib.ibpm_batch_set_grouped.argtypes = [H, C.c_int32]
     lib.ibpm_batch_set_lanes.restype = C.c_int
     lib.ibpm_batch_set_lanes.argtypes = [H, C.c_int32]
     lib.ibpm_batch_last_error.restype = C.c_char_p
@@ -846,6 +850,14 @@ class Batch:
 
     def set_chain(self, chain):
         self._check(self.lib.ibpm_batch_set_chain(self.handle, int(chain)))
+
+    @property
+    def grouped(self):
+        """Whether members of one grid and precision step by shared launches."""
+        return bool(self.lib.ibpm_batch_grouped(self.handle))
+
+    def set_grouped(self, on):
+        self._check(self.lib.ibpm_batch_set_grouped(self.handle, 1 if on else 0))
 
     def advance(self, nsteps=1):
         """Advance every member; returns per-member (CD, CL) histories (nsteps, nbodies)."""

@@ -283,10 +283,14 @@ int ibpm_adjoint_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_l2, double*
  * Reynolds number, time step, bodies and precision; each is an ordinary
  * handle (ibpm_batch_member) whose state is set and read with
  * ibpm_set_state / ibpm_get_state.  One batch step is one CUDA-graph launch
- * whose branches are the members' steps spread over `lanes` concurrent
- * streams; lanes = 0 picks the lane count by timing a few steps of each
- * power of two up to n (the members are reset to their created state
- * afterwards).  Members must be stepped through the batch only.
+ * whose branches are the steps of its units spread over `lanes` concurrent
+ * streams: a unit is a member, or a group of members of one grid and
+ * precision stepped by shared launches (ibpm_batch_grouped).  lanes = 0
+ * picks shared launches or not, the level chain, the single-slab plan and
+ * the lane count (powers of two up to the number of units) by timing a few
+ * steps of each, then lets each group try the other chains and plans on its
+ * own; the members are reset to their created state afterwards.  Members
+ * must be stepped through the batch only.
  */
 typedef struct ibpm_batch ibpm_batch;
 int ibpm_batch_create(int32_t n, const ibpm_problem_desc* descs, int32_t lanes, ibpm_batch** out);
@@ -305,14 +309,25 @@ int ibpm_batch_get_forces(const ibpm_batch* b, int32_t i, double* CD, double* CL
 int ibpm_batch_bench(ibpm_batch* b, int32_t nsteps, int32_t flush_l2, double* step_ms);
 
 /* Transform plan of the members' single-slab launches (IBPM_PLAN_*): the one
- * lanes = 0 chose with the lane count, or the one set; setting it captures the
- * batch step again (the state is kept). */
+ * lanes = 0 chose with the lane count, or the one set; setting it sets every
+ * member's and captures the batch step again (the state is kept).  lanes = 0
+ * may then give a group of members of one grid another plan or level chain
+ * (ibpm_get_transform_plan and ibpm_get_level_chain of a member tell). */
 int ibpm_batch_plan(const ibpm_batch* b);
 int ibpm_batch_set_plan(ibpm_batch* b, int32_t plan);
 /* Level chain of the members (IBPM_CHAIN_*): the one lanes = 0 chose, or the
  * one set; setting it captures the batch step again (the state is kept). */
 int ibpm_batch_chain(const ibpm_batch* b);
 int ibpm_batch_set_chain(ibpm_batch* b, int32_t chain);
+/* Shared launches (1) or not (0): members of one grid (nx, ny, mg), precision
+ * and sweep count, with fixed bodies, form groups whose step fields share
+ * device arenas; a group steps by launches over the slabs of all its members
+ * (the body operators run per member), which computes bit for bit what each
+ * member computes alone.  lanes = 0 times both; setting it captures the batch
+ * step again (the state is kept).  A member is released with its batch
+ * (ibpm_destroy refuses it). */
+int ibpm_batch_grouped(const ibpm_batch* b);
+int ibpm_batch_set_grouped(ibpm_batch* b, int32_t on);
 
 /* Page-locked host memory for state mirrors (faster get/set_state); NULL on
  * failure.  No counterpart in the reference (Julia arrays are pageable). */

@@ -35,6 +35,7 @@ pb = G.IBProblem(g, [G.make_plate(1.0, 0.0, g.h, 0.0, 0.0, n=51, motion=mf)], 1e
 CD, CL = G.advance(G.IBState(pb), pb, np.arange(100) * 1e-3)      # lab-frame CD, CL per step
 xb, ub = G.body_points(pb)                                        # state.xb and the points' velocities
 
-# many independent simulations, one graph launch per step
+# many independent simulations, one graph launch per step (one grid here:
+# every transform and stencil of a step is one launch over all three)
 batch = G.Batch([dict(grid=g, bodies=[cyl()], dt=0.002, Re=Re) for Re in (40.0, 100.0, 200.0)])
 histories = batch.advance(1000)                                   # [(CD, CL)] per member
