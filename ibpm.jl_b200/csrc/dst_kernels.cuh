@@ -700,8 +700,9 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
             tk[c] = (int)(((long long)(threadIdx.x + 1) * k) % nx2);
             dk[c] = (int)(((long long)blockDim.x * k) % nx2);
         }
+#pragma unroll 4
         for (int i = threadIdx.x; i < n1; i += blockDim.x) {
-            const double eb = e[i], et = e[n1 + i];
+            const double eb = __ldg(&e[i]), et = __ldg(&e[n1 + i]);
 #pragma unroll
             for (int c = 0; c < TW; ++c) {
                 const double sv = 2.0 * sinpix(tk[c]);
@@ -741,12 +742,14 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
         const double* sLR = red + (nw + 1) * 2 * TW;  // [2c]: S(1, k_c), [2c + 1]: S(nx−1, k_c)
         const double* eL = e + 2 * n1;
         const double* eR = eL + n2;
+        // (the loads of eight steps in flight: the loop is a chain of L2 reads otherwise)
+#pragma unroll 8
         for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
             const int j = idx / TW, c = idx - j * TW;
             const int i = i0 + c;
             double v = 0.0;
             if (i < n1) {
-                v = sLR[2 * c] * eL[j] + sLR[2 * c + 1] * eR[j];
+                v = sLR[2 * c] * __ldg(&eL[j]) + sLR[2 * c + 1] * __ldg(&eR[j]);
                 if (j == 0) v += bh[c];
                 if (j == n2 - 1) v += bh[TW + c];
             }
