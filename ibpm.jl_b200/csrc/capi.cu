@@ -632,15 +632,17 @@ static int enqueue_step_fp64(ibpm_handle* h, int p) {
 }
 
 // ---------------------------------------------------------------------------
-// FP32-refined step.  Each Poisson-type solve x = M⁻¹ b (M = L for Δ⁻¹,
-// I + cL for A⁻¹, L x = 4x − Σ neighbours) is one or more sweeps of
+// FP32-refined step.  The projection solve and the final vort2flux! are
+// refined: each Poisson-type solve x = M⁻¹ b (M = L for Δ⁻¹, I + cL for A⁻¹,
+// L x = 4x − Σ neighbours) is one or more sweeps of
 //     x ← x + S32(b − M x)
-// with the residual formed in FP64 inside the first x-pass and the correction
-// S32 = the DST-I solve in FP32 (x-pass, y-pass, x-pass), starting from the
-// previous solution of the same system (ψ of the previous vort2flux, the
-// previous projection).  The error left is the FP32 error of the correction
-// alone, i.e. relative to the change of x since its previous solution.
-// The trial solve Γs = A⁻¹ rhs stays FP64: near the wall its change per step
+// with the residual formed in FP64 (in the first x-pass, or by one stencil
+// launch over all levels) and the correction S32 = the DST-I solve in FP32,
+// starting from the previous solution of the same system (ψ of the trial
+// vort2flux!, the previous projection).  The error left is the FP32 error of
+// the correction alone, i.e. relative to the change of x since its previous
+// solution.  The trial solve and the trial vort2flux! run in FP64 (see the
+// step).  The trial solve Γs = A⁻¹ rhs stays FP64: near the wall its change per step
 // is O(Γ), and the force F = E(qs + q0) is a difference that cancels to
 // O(dt)·|q0| there, so an FP32 error in Γs − Γ reaches CD amplified by
 // |q0|/|F| (≈ 500 at dt = 0.002).  A second FP32 sweep would fix it at three
@@ -707,10 +709,15 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
     SlabMap all = levmap(g, 0, mg, bs);
     rc = poisson(h, h->rhs, all, h->rhs, all, Gnew, all, mg * ns, SPEC_AINV, XEMIT_STORE);
     if (rc) return rc;
-    // every level: a level left at the previous step's ψ would start the final
-    // vort2flux! from a whole step's change, and its FP32 correction error with it
-    rc = h->bt ? vort2flux_refined_bt(h, Gnew, nsw, h->qs, 1, mg)
-               : vort2flux_refined(h, Gnew, nsw, h->qs, 1);
+    // The trial vort2flux! in FP64, as the FP64 step runs it (the boundary
+    // transfer completes only the two levels E reads).  It feeds the forces
+    // directly; in FP32 with one sweep its correction error (a whole step's
+    // change of ψ times the sweep's contraction, ~1e-5) moved the shedding
+    // cycle's CL amplitude by 3e-6, against 2.5e-7 this way, and it cost more.
+    // The final vort2flux! refines from it: levels it did not complete keep
+    // the previous step's ψ and take a whole step's correction there.
+    rc = h->bt ? vort2flux_bt(h, Gnew, h->qs, 1, std::min(2, mg))
+               : vort2flux(h, Gnew, h->psi, g.S * mg, ns, h->qs, (long long)g.nq * mg, 0, 1);
     if (rc) return rc;
     // --- boundary_forces! and update_stress! (FP64)
     if ((rc = per_member(h, forces_and_src))) return rc;
