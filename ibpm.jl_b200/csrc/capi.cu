@@ -22,10 +22,11 @@ using namespace ibpm;
 // FP32_REFINED: steps after create or set_state that run one more correction
 // sweep per solve.  The first lacks good initial guesses (ψ and the previous
 // projection may not belong to the state); the next ones follow an impulsive
-// start, whose per-step changes are orders of magnitude above the later ones
-// (on the 512² × 5-level cylinder the largest one-sweep force errors fall in
-// the first six steps).
-static const int kColdSteps = 8;
+// start, whose per-step changes are orders of magnitude above the later ones.
+// With 8 such steps the largest one-sweep CD error of the two-cylinder 1024²
+// start (dt = 0.001) fell at step 11, 1.7e-6; it decays below 1.2e-7 by step
+// 100.  32 steps cover that transient for a few ms per state change.
+static const int kColdSteps = 32;
 
 struct ibpm_handle {
     int device = 0;

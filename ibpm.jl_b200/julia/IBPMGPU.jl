@@ -76,8 +76,9 @@ every step's t, timestepping.jl:41-43, 273-318).  For static bodies the
 freestream functions are evaluated at t = 0 only, as the reference does: its
 base flux is set once when the IBState is built (state-types.jl:45) and
 advance! updates it only for a MovingGrid (timestepping.jl:41-43).
-`precision = :fp32_refined` runs the sine transforms in FP32 with
-FP64-residual refinement of every Poisson solve.
+`precision = :fp32_refined` runs the sine transforms of the projection solve
+and of the final `vort2flux!` in FP32 with FP64-residual refinement (the trial
+solve and the trial `vort2flux!` stay FP64).
 """
 function IBProblemGPU(grid::MultiGrid, bodies::Vector{<:RigidBody}, dt::Float64, Re::Float64;
                       freestream=(Ux=t->1.0, Uy=t->0.0, inclination=t->0.0), device::Integer=0,

@@ -350,9 +350,10 @@ class IBProblem:
     state; ``IBState`` objects are host mirrors of it.
 
     ``precision``: "fp64" (the reference's arithmetic) or "fp32_refined"
-    (FP32 sine transforms, every Poisson-type solve corrected by
-    ``refine_sweeps`` sweeps of FP64-residual iterative refinement started
-    from the previous solution; state, stencils, Schur solve and forces FP64).
+    (FP32 sine transforms in the projection solve and the final vort2flux!,
+    each corrected by ``refine_sweeps`` sweeps of FP64-residual iterative
+    refinement started from the previous solution; state, stencils, the
+    trial solve and trial vort2flux!, Schur solve and forces FP64).
 
     A body whose ``motion`` is a ``MovingGrid`` (one body only, models.jl:137)
     makes every ``advance`` recompute the base flux from the motion at each

@@ -37,10 +37,12 @@ extern "C" {
 
 /* Arithmetic of the step. */
 #define IBPM_PREC_FP64         0  /* plain FP64 everywhere                        */
-#define IBPM_PREC_FP32_REFINED 1  /* FP32 sine transforms; FP64 state, stencils,
-                                     residuals, Schur solve and forces.  Every
-                                     Poisson-type solve is x = x̃ + S32(b − M x̃)
-                                     with the residual in FP64 and x̃ the previous
+#define IBPM_PREC_FP32_REFINED 1  /* FP32 sine transforms in the projection
+                                     solve and the final vort2flux!; FP64 state,
+                                     stencils, residuals, trial solve, trial
+                                     vort2flux!, Schur solve and forces.  A
+                                     refined solve is x = x̃ + S32(b − M x̃) with
+                                     the residual in FP64 and x̃ the previous
                                      solution (iterative refinement, warm start) */
 
 typedef struct ibpm_handle ibpm_handle;
@@ -67,7 +69,9 @@ typedef struct ibpm_problem_desc {
     int32_t precision;         /* IBPM_PREC_*                                   */
     int32_t device;            /* CUDA device ordinal                           */
     int32_t refine_sweeps;     /* FP32_REFINED: FP64-residual correction sweeps
-                                  per solve (0 means 1); ignored for FP64        */
+                                  per refined solve (0 means 1; the first 32
+                                  steps after create or set_state run one
+                                  more); ignored for FP64                       */
 } ibpm_problem_desc;
 
 /* Library version string. */
