@@ -61,6 +61,8 @@ struct ibpm_handle {
     BodyDev body{};
     // per-step outputs
     double* hist = nullptr; int hist_cap = 0;
+    double* pin_hist = nullptr;            // page-locked host mirror of hist (the advance read-back)
+    int* pin_status = nullptr;             // page-locked host copy of *status
     int* counter = nullptr; int* status = nullptr;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     cudaGraphExec_t gcold[2] = {nullptr, nullptr};  // FP32_REFINED: first step after a state change
@@ -946,6 +948,8 @@ static void free_handle(ibpm_handle* h) {
                     h->counter, h->status};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (h->flush_buf) cudaFree(h->flush_buf);
+    if (h->pin_hist) cudaFreeHost(h->pin_hist);
+    if (h->pin_status) cudaFreeHost(h->pin_status);
     for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
     if (h->have_px) dst_plan_destroy(&h->px);
     if (h->have_py) dst_plan_destroy(&h->py);
@@ -1220,7 +1224,17 @@ static int ensure_graphs(ibpm_handle* h, int cap) {
         h->hist = nullptr;
         int rc = dalloc(h, &h->hist, (size_t)cap * 2 * h->nbodies);
         if (rc) return rc;
+        if (h->pin_hist) cudaFreeHost(h->pin_hist);
+        h->pin_hist = nullptr;
+        if (cudaMallocHost((void**)&h->pin_hist, sizeof(double) * cap * 2 * h->nbodies) != cudaSuccess) {
+            h->pin_hist = nullptr;
+            return fail(h, IBPM_ERR_NOMEM, "cudaMallocHost: force history mirror");
+        }
         h->hist_cap = cap;
+    }
+    if (!h->pin_status && cudaMallocHost((void**)&h->pin_status, sizeof(int)) != cudaSuccess) {
+        h->pin_status = nullptr;
+        return fail(h, IBPM_ERR_NOMEM, "cudaMallocHost: status word");
     }
     if (h->bodies_moving && h->btab_cap < h->hist_cap) {
         if (h->btab) cudaFree(h->btab);
@@ -1281,7 +1295,6 @@ static int advance_impl(ibpm_handle* h, int32_t nsteps, const double* motion, do
     int rc = ensure_graphs(h, std::max(cap, h->hist_cap));
     if (rc) return rc;
     CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
-    std::vector<double> hb;
     int done = 0;
     while (done < nsteps) {
         const int n = std::min(h->hist_cap, nsteps - done);
@@ -1308,10 +1321,16 @@ static int advance_impl(ibpm_handle* h, int32_t nsteps, const double* motion, do
         CK(cudaMemsetAsync(h->counter, 0, sizeof(int), h->st));
         for (int s = 0; s < n; ++s) CK(launch_step(h));
         h->nonlin1_valid = false;
+        // the chunk's CD/CL (and after the last chunk the status word) into
+        // page-locked memory, one synchronisation for both
+        const bool last = done + n >= nsteps;
+        if (CD_out || CL_out)
+            CK(cudaMemcpyAsync(h->pin_hist, h->hist, sizeof(double) * n * 2 * h->nbodies, cudaMemcpyDeviceToHost,
+                               h->st));
+        if (last) CK(cudaMemcpyAsync(h->pin_status, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+        if (CD_out || CL_out || last) CK(cudaStreamSynchronize(h->st));
         if (CD_out || CL_out) {
-            hb.resize((size_t)n * 2 * h->nbodies);
-            CK(cudaMemcpyAsync(hb.data(), h->hist, sizeof(double) * hb.size(), cudaMemcpyDeviceToHost, h->st));
-            CK(cudaStreamSynchronize(h->st));
+            const double* hb = h->pin_hist;
             for (int s = 0; s < n; ++s)
                 for (int j = 0; j < h->nbodies; ++j) {
                     if (CD_out) CD_out[(size_t)(done + s) * h->nbodies + j] = hb[((size_t)s * 2 + 0) * h->nbodies + j];
@@ -1320,9 +1339,7 @@ static int advance_impl(ibpm_handle* h, int32_t nsteps, const double* motion, do
         }
         done += n;
     }
-    int hstatus = 0;
-    CK(cudaMemcpyAsync(&hstatus, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
-    CK(cudaStreamSynchronize(h->st));
+    const int hstatus = *h->pin_status;
     if (hstatus & 8) return fail(h, IBPM_ERR_CUDA, "internal: a step ran past the force history");
     if (hstatus & 4) return fail(h, IBPM_ERR_INVALID, "a moving body's regularisation stencil left the finest grid");
     if (hstatus & 2) return fail(h, IBPM_ERR_NONFINITE, "the Schur complement B of the moved bodies is singular");
