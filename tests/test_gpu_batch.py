@@ -73,21 +73,22 @@ GROUPED = [("sq64_mg3", "fp64", 40.0, 0.01), ("sq64_mg3", "fp64", 150.0, 0.008),
            ("rect64x32_mg2_two", "fp64", 100.0, 0.005)]
 
 
-@pytest.mark.parametrize("chain", [0, 1])
-def test_grouped_members_match_single_runs(chain):
+@pytest.mark.parametrize("chain,lanes", [(0, 2), (1, 2), (1, 0)])
+def test_grouped_members_match_single_runs(chain, lanes):
     """The FP64 and the FP32-refined sq64 members each form a group whose
     transforms and stencils are launches over all its members; every member's
     CD/CL and state are those of its own handle bit for bit, and the same
-    batch stepped member by member gives the same bits."""
+    batch stepped member by member gives the same bits.  With lanes = 0 the
+    tuner may give each group its own transform plan: each member is compared
+    with a handle on that member's plan."""
     import ibpm_gpu as G
     specs = []
     for name, prec, re, dt in GROUPED:
         sp = _spec(name, prec)
         sp["Re"], sp["dt"] = re, dt
         specs.append(sp)
-    batch = G.Batch(specs, lanes=2)
+    batch = G.Batch(specs, lanes=lanes)
     batch.set_chain(chain)
-    assert batch.grouped
     runs = {}
     for grouped in (True, False):
         batch.set_grouped(grouped)
@@ -99,7 +100,7 @@ def test_grouped_members_match_single_runs(chain):
         sp = specs[i]
         solo = G.IBProblem(sp["grid"], sp["bodies"], sp["dt"], sp["Re"], freestream=sp["freestream"],
                            precision=prec, sync_fields=False)
-        G.set_transform_plan(solo, batch.plan, G.IBPM_PLAN_AUTO)
+        G.set_transform_plan(solo, *G.transform_plan(batch.members[i]))
         G.set_level_chain(solo, chain)
         _start(solo, name, seed=60 + i)
         st = G.IBState(solo)
