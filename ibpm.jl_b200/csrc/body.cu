@@ -130,28 +130,6 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Row kk of E (k-major: x components, then y) applied to the fluxes qq plus the
-// base flux, summed over the warp (interface-coupling.jl:122-133).
-__device__ __forceinline__ double E_row(const BodyDev& b, const Geom& g, const double* __restrict__ qq, int kk,
-                                        int lane, double q0x, double q0y, const MovingFlux& mv) {
-    const int comp = kk / b.nb, k = kk % b.nb;
-    const int bx = b.bidx[k], by = b.bidx[b.nb + k];
-    const double* w = b.w + (long long)kk * 169;
-    const double* mrow = mv.tab ? moving_row(mv) : nullptr;
-    double acc = 0.0;
-    for (int t = lane; t < 169; t += 32) {
-        const int l = t / 13, m = t % 13;
-        const int I = bx + l - 6, J = by + m - 6;
-        double qv;
-        if (comp == 0)
-            qv = qq[(I - 1) + (long long)(J - 1) * (g.nx + 1)] + (mrow ? moving_q0x(mv, mrow, J, g.ny, mv.h) : q0x);
-        else
-            qv = qq[g.nu + (I - 1) + (long long)(J - 1) * g.nx] + (mrow ? moving_q0y(mv, mrow, I, g.nx, mv.h) : q0y);
-        acc += w[t] * qv;
-    }
-    return warp_sum(acc);
-}
-
 // E (regT!, interface-coupling.jl:122-133) on (q + q0): one warp per force
 // component and batch member.  F[bt*F_bstride + kk*F_kstride].
 // A moving grid's base flux (MovingFlux, level 1) replaces the uniform q0x, q0y.
@@ -166,8 +144,23 @@ __global__ void E_kernel(BodyDev b, Geom g, const double* __restrict__ q, long l
     const int lane = threadIdx.x & 31;
     if (warp >= b.nf * nbatch) return;
     const int bt = warp / b.nf, kk = warp % b.nf;
+    const int comp = kk / b.nb, k = kk % b.nb;
     const double* qq = q + (long long)bt * q_stride;
-    double acc = E_row(b, g, qq, kk, lane, q0x, q0y, mv);
+    const int bx = b.bidx[k], by = b.bidx[b.nb + k];
+    const double* w = b.w + (long long)kk * 169;
+    const double* mrow = mv.tab ? moving_row(mv) : nullptr;
+    double acc = 0.0;
+    for (int t = lane; t < 169; t += 32) {
+        const int l = t / 13, m = t % 13;
+        const int I = bx + l - 6, J = by + m - 6;
+        double qv;
+        if (comp == 0)
+            qv = qq[(I - 1) + (long long)(J - 1) * (g.nx + 1)] + (mrow ? moving_q0x(mv, mrow, J, g.ny, mv.h) : q0x);
+        else
+            qv = qq[g.nu + (I - 1) + (long long)(J - 1) * g.nx] + (mrow ? moving_q0y(mv, mrow, I, g.nx, mv.h) : q0y);
+        acc += w[t] * qv;
+    }
+    acc = warp_sum(acc);
     if (ub) acc = acc - ub[kk] * hub;
     if (lane == 0) F[(long long)bt * F_bstride + (long long)kk * F_kstride] = acc;
 }
@@ -186,22 +179,17 @@ cudaError_t launch_E(const Geom& g, const BodyDev& b, const double* q, long long
 }
 
 // y = A x, A row-major n×n: one warp per row (F̃b .= Binv*F̃b, timestepping.jl:160).
-__device__ __forceinline__ void gemv_row(const double* __restrict__ A, const double* __restrict__ x, double* y, int n,
-                                         int row, int lane) {
-    const double* a = A + (long long)row * n;
-    double acc = 0.0;
-    for (int c = lane; c < n; c += 32) acc += a[c] * x[c];
-    acc = warp_sum(acc);
-    if (lane == 0) y[row] = acc;
-}
-
 __global__ void gemv_kernel(const double* __restrict__ A, const double* __restrict__ x, double* y, int n) {
     pdl_wait();
     pdl_trigger();
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
-    gemv_row(A, x, y, n, row, lane);
+    const double* a = A + (long long)row * n;
+    double acc = 0.0;
+    for (int c = lane; c < n; c += 32) acc += a[c] * x[c];
+    acc = warp_sum(acc);
+    if (lane == 0) y[row] = acc;
 }
 
 cudaError_t launch_gemv(const double* A, const double* x, double* y, int n, cudaStream_t st) {
@@ -318,49 +306,6 @@ cudaError_t launch_stress_src(const BodyDev& b, const double* Fb, double h, doub
     const unsigned blocks = 1 + (unsigned)((threads + 255) / 256);
     return launch_k(stress_src_kernel, dim3(blocks), dim3(256), 0, st, b, Fb, h, dt, hist, hist_cap, counter, status,
                     Gsrc);
-}
-
-// The three body launches of a batch group: simulation blockIdx.y, the same
-// warp-to-row mapping and arithmetic as E_kernel (one field, no batch),
-// gemv_kernel and stress_src_kernel; blocks past a simulation's rows return.
-__global__ void E_group_kernel(const BodyStep* __restrict__ tab, Geom g) {
-    pdl_wait();
-    pdl_trigger();
-    const BodyStep& m = tab[blockIdx.y];
-    const int kk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (kk >= m.b.nf) return;
-    const double acc = E_row(m.b, g, m.qs, kk, lane, m.q0x, m.q0y, MovingFlux{});
-    if (lane == 0) m.F[kk] = acc;
-}
-
-__global__ void gemv_group_kernel(const BodyStep* __restrict__ tab) {
-    pdl_wait();
-    pdl_trigger();
-    const BodyStep& m = tab[blockIdx.y];
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (row >= m.b.nf) return;
-    gemv_row(m.Binv, m.F, m.Fb, m.b.nf, row, threadIdx.x & 31);
-}
-
-__global__ void stress_src_group_kernel(const BodyStep* __restrict__ tab) {
-    pdl_wait();
-    pdl_trigger();
-    const BodyStep& m = tab[blockIdx.y];
-    if (blockIdx.x == 0) {
-        stress_block(m.b, m.Fb, m.h, m.dt, m.hist, m.hist_cap, m.counter, m.status);
-        return;
-    }
-    proj_src_warp(m.b, m.Fb, m.Gsrc, ((blockIdx.x - 1) * blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31);
-}
-
-cudaError_t launch_body_group(const Geom& g, const BodyStep* tab, int nsim, int max_nf, int max_src, int op,
-                              cudaStream_t st) {
-    const unsigned rows = (unsigned)(((long long)max_nf * 32 + 255) / 256);
-    if (op == 0) return launch_k(E_group_kernel, dim3(rows, nsim), dim3(256), 0, st, tab, g);
-    if (op == 1) return launch_k(gemv_group_kernel, dim3(rows, nsim), dim3(256), 0, st, tab);
-    const unsigned blocks = 1 + (unsigned)(((long long)max_src * 32 + 255) / 256);
-    return launch_k(stress_src_group_kernel, dim3(blocks, nsim), dim3(256), 0, st, tab);
 }
 
 // C'E' e_kk for unit forces kk = col0 + r (B_times!, laplacian.jl:162), written

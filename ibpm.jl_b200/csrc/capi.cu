@@ -132,16 +132,17 @@ struct ibpm_handle {
     // batch groups (ibpm_batch_create): members of one grid and precision keep
     // their step fields in group arenas, member after member, so that while a
     // group's step is captured its first member stands for all `gsim` of them:
-    // every transform and stencil launch covers the slabs of all, and each body
-    // operator (E, B⁻¹, update_stress!) is one launch over the members' tables
+    // every transform and stencil launch covers the slabs of all, and the body
+    // operators (E, B⁻¹, update_stress!) run per member on branch streams
     bool in_batch = false;                 // released with its batch only
     bool arena = false;                    // step fields live in a group arena
     int gsim = 1;
+    ibpm_handle* const* gmem = nullptr;    // the group's members (this one first)
     const double* g_den = nullptr;         // [gsim][9]: 2 Re hc² per level, then dt
     const double* g_cA = nullptr;          // [gsim]: dt / (2 Re h²)
     const RhsArgs* g_rhs[2] = {nullptr, nullptr};  // [gsim] trial right-hand side arguments per parity
-    const BodyStep* g_body = nullptr;      // [gsim] body operator arguments (device)
-    int g_max_nf = 0, g_max_src = 0;       // the largest nf and contributor-list count
+    cudaStream_t* g_br = nullptr;          // [gsim] branch streams
+    cudaEvent_t* g_ev = nullptr;           // [gsim + 1] fork and join events
     // measurement
     int launches = 0;                      // kernel launches enqueued (counted always)
     bool prof_on = false;                  // eager profiling: events around every launch
@@ -308,6 +309,30 @@ static int stress_and_src(ibpm_handle* h) {
     return IBPM_OK;
 }
 
+// Run `fn` for every member of the group being captured (the handle alone
+// outside groups), each member on its own branch stream forked from and
+// joined back into the lead's stream.
+template <class F>
+static int per_member(ibpm_handle* h, F fn) {
+    if (h->gsim <= 1) return fn(h);
+    CK(cudaEventRecord(h->g_ev[0], h->st));
+    for (int i = 0; i < h->gsim; ++i) {
+        ibpm_handle* m = h->gmem[i];
+        cudaStream_t own = m->st;
+        CK(cudaStreamWaitEvent(h->g_br[i], h->g_ev[0], 0));
+        m->st = h->g_br[i];
+        const int rc = fn(m);
+        m->st = own;
+        if (rc) {
+            if (m != h) h->err = m->err;
+            return rc;
+        }
+        CK(cudaEventRecord(h->g_ev[1 + i], h->g_br[i]));
+        CK(cudaStreamWaitEvent(h->st, h->g_ev[1 + i], 0));
+    }
+    return IBPM_OK;
+}
+
 // boundary_forces! (timestepping.jl:154-163) of one simulation: F = E(qs + q0),
 // F̃b = B⁻¹ F, then update_stress! and the projection source.
 static int forces_and_src(ibpm_handle* h) {
@@ -316,19 +341,6 @@ static int forces_and_src(ibpm_handle* h) {
                     h->bodies_moving ? h->d_ub : nullptr, h->h));
     LAUNCH(K_GEMV, 8.0 * h->nf * (h->nf + 2.0), launch_gemv(h->Binv, h->F, h->Fb, h->nf, h->st));
     return stress_and_src(h);
-}
-
-// boundary_forces!, update_stress! and the projection source of the handle, or
-// of every member of the group being captured (three launches over all of
-// them, with the per-simulation arithmetic).
-static int body_ops(ibpm_handle* h) {
-    if (h->gsim <= 1) return forces_and_src(h);
-    const int ns = h->gsim, nf = h->g_max_nf;
-    LAUNCH(K_E, 16.0 * 169 * nf * ns, launch_body_group(h->g, h->g_body, ns, nf, h->g_max_src, 0, h->st));
-    LAUNCH(K_GEMV, 8.0 * nf * (nf + 2.0) * ns, launch_body_group(h->g, h->g_body, ns, nf, h->g_max_src, 1, h->st));
-    LAUNCH(K_SRC, 8.0 * (4 * 169 * nf + 1.5 * nf) * ns,
-           launch_body_group(h->g, h->g_body, ns, nf, h->g_max_src, 2, h->st));
-    return IBPM_OK;
 }
 
 static RhsArgs rhs_args(const ibpm_handle* h, int p) {
@@ -613,7 +625,7 @@ static int enqueue_step_fp64(ibpm_handle* h, int p) {
                : vort2flux(h, Gnew, h->psi, g.S * mg, ns, h->qs, qb, 0, 1);
     if (rc) return rc;
     // --- boundary_forces! (timestepping.jl:154-163), update_stress! (:330-354)
-    if ((rc = body_ops(h))) return rc;
+    if ((rc = per_member(h, forces_and_src))) return rc;
     // --- project_circ! (timestepping.jl:204-223): Γ = Γs − A⁻¹ C'E' F̃b on level 1
     SlabMap one = levmap(g, 0, 1);
     rc = poisson(h, h->Gsrc, one, h->rhs, one, Gnew, one, ns, SPEC_AINV, XEMIT_SUB);
@@ -711,7 +723,7 @@ static int enqueue_step_refined(ibpm_handle* h, int p, int nsw) {
                : vort2flux(h, Gnew, h->psi, g.S * mg, ns, h->qs, (long long)g.nq * mg, 0, 1);
     if (rc) return rc;
     // --- boundary_forces! and update_stress! (FP64)
-    if ((rc = body_ops(h))) return rc;
+    if ((rc = per_member(h, forces_and_src))) return rc;
     // --- project_circ!: P = A⁻¹ C'E' F̃b refined from the previous P; Γ[1] −= P
     for (int s = 0; s < nsw; ++s) {
         const bool last = s + 1 == nsw;
@@ -1958,7 +1970,7 @@ extern "C" int ibpm_adjoint_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_
 // after another).  A unit is one member, or (grouped) a group of members of
 // one grid, precision, level chain and plan, whose step fields sit in shared
 // arenas: the group's transforms and stencils are launches over the slabs of
-// all its members, its body operators one launch each over their tables.  Small
+// all its members, its body operators one short branch per member.  Small
 // grids leave most of the GPU idle when run alone; side by side and in shared
 // launches they fill it.  Lanes, plan, chain and grouping are picked by
 // timing.
@@ -1969,8 +1981,8 @@ struct BatchGroup {
     double* den = nullptr;                     // [n][9] spectral factors (SpecParams::mden)
     double* cA = nullptr;                      // [n]
     RhsArgs* rhs[2] = {nullptr, nullptr};      // [n] per parity
-    BodyStep* body = nullptr;                  // [n] body operator arguments
-    int max_nf = 0, max_src = 0;
+    std::vector<cudaStream_t> br;              // branch streams of the body operators
+    std::vector<cudaEvent_t> ev;               // fork + one join event per member
 };
 
 struct ibpm_batch {
@@ -2102,7 +2114,10 @@ static int batch_make_group(ibpm_batch* b, const std::vector<ibpm_handle*>& mem)
     BCK(cudaMalloc((void**)&gr.den, sizeof(double) * 9 * n));
     BCK(cudaMalloc((void**)&gr.cA, sizeof(double) * n));
     for (int p = 0; p < 2; ++p) BCK(cudaMalloc((void**)&gr.rhs[p], sizeof(RhsArgs) * n));
-    BCK(cudaMalloc((void**)&gr.body, sizeof(BodyStep) * n));
+    gr.br.resize(n);
+    gr.ev.resize(n + 1);
+    for (auto& x : gr.br) BCK(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    for (auto& x : gr.ev) BCK(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
     return IBPM_OK;
 }
 
@@ -2129,7 +2144,8 @@ static void batch_free_groups(ibpm_batch* b) {
         if (gr.den) cudaFree(gr.den);
         if (gr.cA) cudaFree(gr.cA);
         for (auto* r : gr.rhs) if (r) cudaFree(r);
-        if (gr.body) cudaFree(gr.body);
+        for (auto x : gr.br) if (x) cudaStreamDestroy(x);
+        for (auto x : gr.ev) if (x) cudaEventDestroy(x);
     }
     b->groups.clear();
 }
@@ -2151,17 +2167,8 @@ static int group_tables(ibpm_batch* b, BatchGroup& gr) {
     const int n = (int)gr.mem.size();
     std::vector<double> den(9 * (size_t)n), cA(n);
     std::vector<RhsArgs> ra[2] = {std::vector<RhsArgs>(n), std::vector<RhsArgs>(n)};
-    std::vector<BodyStep> bs(n);
-    gr.max_nf = gr.max_src = 0;
     for (int i = 0; i < n; ++i) {
         ibpm_handle* h = gr.mem[i];
-        BodyStep& m = bs[i];
-        m.b = h->body; m.qs = h->qs; m.q0x = h->q0x[0]; m.q0y = h->q0y[0];
-        m.F = h->F; m.Binv = h->Binv; m.Fb = h->Fb; m.h = h->h; m.dt = h->dt;
-        m.hist = h->hist; m.hist_cap = h->hist_cap; m.counter = h->counter; m.status = h->status;
-        m.Gsrc = h->Gsrc;
-        gr.max_nf = std::max(gr.max_nf, h->nf);
-        gr.max_src = std::max(gr.max_src, h->body.n_src);
         const SpecParams sp = spec(h, SPEC_AINV);
         for (int l = 0; l < 8; ++l) den[9 * i + l] = sp.den[l];
         den[9 * i + 8] = sp.dt;
@@ -2175,7 +2182,6 @@ static int group_tables(ibpm_batch* b, BatchGroup& gr) {
     BCK(cudaMemcpy(gr.cA, cA.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
     for (int p = 0; p < 2; ++p)
         BCK(cudaMemcpy(gr.rhs[p], ra[p].data(), sizeof(RhsArgs) * n, cudaMemcpyHostToDevice));
-    BCK(cudaMemcpy(gr.body, bs.data(), sizeof(BodyStep) * n, cudaMemcpyHostToDevice));
     return IBPM_OK;
 }
 
@@ -2211,15 +2217,15 @@ static int batch_enqueue_unit(ibpm_batch* b, int u, cudaStream_t st, int p, bool
     ibpm_handle* h = gr.mem[0];
     cudaStream_t own = h->st;
     h->st = st;
-    h->gsim = (int)gr.mem.size();
+    h->gsim = (int)gr.mem.size(); h->gmem = gr.mem.data();
     h->px.sims = h->py.sims = h->gsim;
     h->g_den = gr.den; h->g_cA = gr.cA; h->g_rhs[0] = gr.rhs[0]; h->g_rhs[1] = gr.rhs[1];
-    h->g_body = gr.body; h->g_max_nf = gr.max_nf; h->g_max_src = gr.max_src;
+    h->g_br = gr.br.data(); h->g_ev = gr.ev.data();
     const int rc = enqueue_step(h, p, cold);
     h->st = own;
-    h->gsim = 1; h->g_den = nullptr; h->g_cA = nullptr;
+    h->gsim = 1; h->gmem = nullptr; h->g_den = nullptr; h->g_cA = nullptr;
     h->px.sims = h->py.sims = 0;
-    h->g_rhs[0] = h->g_rhs[1] = nullptr; h->g_body = nullptr; h->g_max_nf = h->g_max_src = 0;
+    h->g_rhs[0] = h->g_rhs[1] = nullptr; h->g_br = nullptr; h->g_ev = nullptr;
     if (rc) b->err = "group of " + std::to_string(gr.mem.size()) + " members: " + h->err;
     return rc;
 }

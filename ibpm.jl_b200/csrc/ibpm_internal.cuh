@@ -428,23 +428,6 @@ cudaError_t launch_proj_src_moving(const Geom& g, const BodyDev& b, const double
                                    cudaStream_t st);
 cudaError_t launch_info_to_status(const int* info, int* status, cudaStream_t st);
 cudaError_t launch_gemv(const double* A, const double* x, double* y, int n, cudaStream_t st);
-
-// The body operators of the simulations of a batch group (fixed bodies, fixed
-// grid), one table entry per simulation: F = E(qs + q0), F̃b = B⁻¹F, then
-// update_stress! and the projection source, each as one launch over all of
-// them (blockIdx.y = simulation), with the per-simulation kernels' arithmetic.
-struct BodyStep {
-    BodyDev b;
-    const double* qs; double q0x, q0y;     // level-1 trial flux, uniform base flux
-    double* F; const double* Binv; double* Fb;
-    double h, dt;
-    double* hist; int hist_cap; int* counter; int* status;
-    double* Gsrc;
-};
-// op 0: E, 1: B⁻¹, 2: update_stress! and the projection source; max_nf,
-// max_src: the largest nf and contributor-list count of the simulations
-cudaError_t launch_body_group(const Geom& g, const BodyStep* tab, int nsim, int max_nf, int max_src, int op,
-                              cudaStream_t st);
 // The force history holds hist_cap steps: a step past it writes nothing and
 // sets bit 3 of *status.
 cudaError_t launch_stress(const BodyDev& b, const double* Fb, double h, double dt,
