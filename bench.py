@@ -953,8 +953,9 @@ def run_ours(args, d):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 transforms / f64 state, residuals, forces",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "precision": "fp32_refined (1 FP64-residual sweep per refined solve: "
-                   "the projection and the final vort2flux!, warm start; FP64 trial solve and trial vort2flux!)", "l2": "flushed between steps (512 MiB write outside the "
-                   "timed event pairs)", "parallelism": "replicas x%d" % d.world,
+                   "the projection and the final vort2flux!, warm start; FP64 trial solve and trial "
+                   "vort2flux!)",
+                   "l2": "flushed between steps (512 MiB write outside the timed event pairs)", "parallelism": "replicas x%d" % d.world,
                    "graph": "one CUDA graph replay per step",
                    "warmup_replays": "max(W, 40): the FP32-refined path's 32 two-sweep start-up steps are not timed",
                    "transform_plans": "radix-4 latency plan on single-level launches; multi-level launches "
