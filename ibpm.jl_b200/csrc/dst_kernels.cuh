@@ -626,6 +626,26 @@ __host__ __device__ constexpr int y_threads() { return y_groups<N, T, PL>() * ct
 template <int N, class T, int PL>
 __host__ __device__ constexpr int y_tile_w() { return 2 * y_groups<N, T, PL>(); }
 __host__ __device__ constexpr int round4(int n) { return ((n + 3) / 4) * 4; }
+// The column tile is column-major, element (row j, column c) at
+// c·CS + j + j/E (E = elements per 128-byte line: one pad every E rows).
+// The transform reads consecutive rows, and its post-processing writes rows 8
+// apart (each thread owns a run of the scan), both free of bank conflicts
+// with that padding; CS ≡ E/TW (mod E) makes the row-major fill and store
+// (TW columns of E/TW rows per access) conflict-free too.
+template <class T>
+__host__ __device__ constexpr int y_line_elems() { return 128 / (int)sizeof(T); }
+template <int N, class T, int PL>
+__host__ __device__ constexpr int y_col_stride(int n2) {
+    constexpr int E = y_line_elems<T>();
+    constexpr int TW = 2 * y_groups<N, T, PL>();
+    constexpr int R = (E / TW) > 0 ? E / TW : 1;
+    const int base = n2 + (n2 - 1) / E + 1;       // one past the last padded row
+    return base + ((R - base % E) % E + E) % E;
+}
+template <int N, class T, int PL>
+__host__ __device__ constexpr int y_tile_elems(int n2) {
+    return round4(2 * y_groups<N, T, PL>() * y_col_stride<N, T, PL>(n2));
+}
 // Scratch of the edge-source synthesis (SYNTH): per-warp partial sums of the
 // bottom and top rows' sine transforms, then the sums themselves.
 template <int N, class T, int PL>
@@ -635,7 +655,7 @@ __host__ __device__ constexpr int y_synth_slots() {
 template <int N, class T, int PL, bool SYNTH = false>
 __host__ __device__ constexpr size_t y_smem_bytes(int n2) {
     return tables_bytes<N, T, PL>() + (size_t)round4(n2) * sizeof(T) +  // spectral table of y
-           (size_t)round4(n2 * (y_tile_w<N, T, PL>() + 1)) * sizeof(T) +
+           (size_t)y_tile_elems<N, T, PL>(n2) * sizeof(T) +
            (size_t)y_groups<N, T, PL>() * ct_buf(N) * sizeof(cplx_t<T>) +
            (SYNTH ? (size_t)y_synth_slots<N, T, PL>() * sizeof(double) : 0);
 }
@@ -658,7 +678,7 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
     constexpr int TP = ct_tp(N, PL);
     constexpr int G = y_groups<N, T, PL>();
     constexpr int TW = y_tile_w<N, T, PL>();
-    constexpr int TWp = TW + 1;
+    constexpr int E = y_line_elems<T>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P = g.P, n1 = g.n1, n2 = g.n2;
     const Tabs<T> tb = tabs_of<T>(p, PL);
@@ -666,7 +686,10 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
     T* sn = reinterpret_cast<T*>(tw + ct_tw_count(N, PL));
     T* cyv = reinterpret_cast<T*>(smem_raw + tables_bytes<N, T, PL>());
     T* tile = cyv + round4(n2);
-    const int tile_d = round4(n2 * TWp);
+    const int tile_d = y_tile_elems<N, T, PL>(n2);
+    constexpr int CS = y_col_stride<N, T, PL>(N - 1);   // n2 = N − 1 in the y-pass
+    auto off = [](int j) -> int { return j + j / E; };   // row j within a column
+    auto at = [&](int j, int c) -> int { return c * CS + off(j); };
     const int gid = threadIdx.x / TP, tid = threadIdx.x % TP;
     V* buf = reinterpret_cast<V*>(tile + tile_d) + gid * ct_buf(N);
     const int i0 = blockIdx.x * TW;
@@ -753,15 +776,15 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
                 if (j == 0) v += bh[c];
                 if (j == n2 - 1) v += bh[TW + c];
             }
-            tile[j * TWp + c] = (T)v;
+            tile[at(j, c)] = (T)v;
         }
         __syncthreads();
     } else {
         for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
             const int j = idx / TW, c = idx - j * TW;
             const int i = i0 + c;
-            if (i < n1) cp_async<sizeof(T)>(tile + j * TWp + c, base + (long long)j * P + i);
-            else tile[j * TWp + c] = T(0);
+            if (i < n1) cp_async<sizeof(T)>(tile + at(j, c), base + (long long)j * P + i);
+            else tile[at(j, c)] = T(0);
         }
         cp_async_wait();
         __syncthreads();
@@ -771,10 +794,12 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
     const int ia = i0 + ca;
     if (ia < n1) {
         const bool hasb = ia + 1 < n1;
-        auto load = [&](int m) -> V { return V{tile[m * TWp + ca], tile[m * TWp + ca + 1]}; };
+        T* const colA = tile + ca * CS;   // the group's two columns
+        T* const colB = colA + CS;
+        auto load = [&](int m) -> V { return V{colA[off(m)], colB[off(m)]}; };
         auto emit = [&](int o, V v) {
-            tile[o * TWp + ca] = v.x;
-            tile[o * TWp + ca + 1] = v.y;
+            colA[off(o)] = v.x;
+            colB[off(o)] = v.y;
         };
         auto divide = [&]() {
             if constexpr (std::is_same<T, double>::value) {
@@ -797,8 +822,9 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
                         Ma = 1.0 + la * dt / den;
                         Mb = 1.0 + lb * dt / den;
                     }
-                    tile[o * TWp + ca] = (tile[o * TWp + ca] * nr_rcp(Ma)) * sp.scale;
-                    tile[o * TWp + ca + 1] = hasb ? (tile[o * TWp + ca + 1] * nr_rcp(Mb)) * sp.scale : 0.0;
+                    const int oo = off(o);
+                    colA[oo] = (colA[oo] * nr_rcp(Ma)) * sp.scale;
+                    colB[oo] = hasb ? (colB[oo] * nr_rcp(Mb)) * sp.scale : 0.0;
                 }
             } else {
                 // the same divisor from Λ = a_x(i) + a_y(j), a(k) = 4 sin²(πk/(2n)):
@@ -814,8 +840,9 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
                     const float lb = axb + cyv[o];
                     const float Ma = (sp.mode == SPEC_DELTA) ? la : fmaf(la, kf, 1.0f);
                     const float Mb = (sp.mode == SPEC_DELTA) ? lb : fmaf(lb, kf, 1.0f);
-                    tile[o * TWp + ca] = tile[o * TWp + ca] * (__frcp_rn(Ma) * sc);
-                    tile[o * TWp + ca + 1] = hasb ? tile[o * TWp + ca + 1] * (__frcp_rn(Mb) * sc) : 0.0f;
+                    const int oo = off(o);
+                    colA[oo] = colA[oo] * (__frcp_rn(Ma) * sc);
+                    colB[oo] = hasb ? colB[oo] * (__frcp_rn(Mb) * sc) : 0.0f;
                 }
             }
         };
@@ -830,7 +857,7 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
     for (int idx = threadIdx.x; idx < n2 * TW; idx += blockDim.x) {
         const int j = idx / TW, c = idx - j * TW;
         const int i = i0 + c;
-        if (i < n1) dst[(long long)j * P + i] = tile[j * TWp + c];
+        if (i < n1) dst[(long long)j * P + i] = tile[at(j, c)];
     }
 }
 
