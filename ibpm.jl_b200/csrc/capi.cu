@@ -1977,7 +1977,7 @@ extern "C" int ibpm_adjoint_bench(ibpm_handle* h, int32_t nsteps, int32_t flush_
 // ---------------------------------------------------------------------------
 struct BatchGroup {
     std::vector<ibpm_handle*> mem;             // lead first
-    std::vector<void*> arenas;                 // step fields, member after member
+    std::vector<std::pair<char*, size_t>> arenas;  // step fields, member after member (base, bytes)
     double* den = nullptr;                     // [n][9] spectral factors (SpecParams::mden)
     double* cA = nullptr;                      // [n]
     RhsArgs* rhs[2] = {nullptr, nullptr};      // [n] per parity
@@ -2051,7 +2051,7 @@ static cudaError_t rehome(BatchGroup& gr, F field, size_t per, size_t have, cuda
     T* a = nullptr;
     cudaError_t e = cudaMalloc((void**)&a, sizeof(T) * per * n);
     if (e != cudaSuccess) return e;
-    gr.arenas.push_back(a);
+    gr.arenas.push_back({reinterpret_cast<char*>(a), sizeof(T) * per * n});
     if ((e = cudaMemsetAsync(a, 0, sizeof(T) * per * n, st)) != cudaSuccess) return e;
     for (size_t i = 0; i < n; ++i)
         if ((e = cudaMemcpyAsync(a + i * per, field(gr.mem[i]), sizeof(T) * have, cudaMemcpyDeviceToDevice, st)) !=
@@ -2065,13 +2065,20 @@ static cudaError_t rehome(BatchGroup& gr, F field, size_t per, size_t have, cuda
     return cudaSuccess;
 }
 
-// The arena-held fields of a handle (set to nullptr before its release).
-static void forget_arena_fields(ibpm_handle* h) {
-    h->G[0] = h->G[1] = h->Nl[0] = h->Nl[1] = nullptr;
-    h->psi = h->q = h->qs = h->rhs = h->Gsrc = h->Pp = nullptr;
-    h->T32 = nullptr;
-    h->btY = h->btS = h->btE = h->btP = nullptr;
-    h->btY32 = nullptr;
+// The fields of a handle that point into the group's arenas, set to nullptr
+// before the arenas are freed.  A field the group did not move (an arena
+// allocation failed part way) stays with the handle, which releases it.
+static void forget_arena_fields(ibpm_handle* h, const BatchGroup& gr) {
+    auto drop = [&](auto*& p) {
+        const char* c = reinterpret_cast<const char*>(p);
+        for (const auto& a : gr.arenas)
+            if (c && c >= a.first && c < a.first + a.second) { p = nullptr; return; }
+    };
+    drop(h->G[0]); drop(h->G[1]); drop(h->Nl[0]); drop(h->Nl[1]);
+    drop(h->psi); drop(h->q); drop(h->qs); drop(h->rhs); drop(h->Gsrc); drop(h->Pp);
+    drop(h->T32);
+    drop(h->btY); drop(h->btS); drop(h->btE); drop(h->btP);
+    drop(h->btY32);
 }
 
 static int batch_make_group(ibpm_batch* b, const std::vector<ibpm_handle*>& mem) {
@@ -2139,8 +2146,8 @@ static int batch_make_groups(ibpm_batch* b) {
 
 static void batch_free_groups(ibpm_batch* b) {
     for (auto& gr : b->groups) {
-        for (auto* h : gr.mem) forget_arena_fields(h);
-        for (void* a : gr.arenas) cudaFree(a);
+        for (auto* h : gr.mem) forget_arena_fields(h, gr);
+        for (const auto& a : gr.arenas) cudaFree(a.first);
         if (gr.den) cudaFree(gr.den);
         if (gr.cA) cudaFree(gr.cA);
         for (auto* r : gr.rhs) if (r) cudaFree(r);
