@@ -994,6 +994,7 @@ template <int N, class T, int PL>
 cudaError_t launch_y_n(const Geom& g, const DstPlan& py, const DstPlan& px, void* data, SlabMap map, int nslabs,
                        const SpecParams& sp, cudaStream_t st) {
     constexpr int TW = y_tile_w<N, T, PL>();
+    if (g.n2 != N - 1) return cudaErrorInvalidValue;   // the tile's column stride is fixed by N
     const size_t smem = y_smem_bytes<N, T, PL>(g.n2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     dim3 grid((g.n1 + TW - 1) / TW, nslabs);
@@ -1014,6 +1015,7 @@ template <int N, class T, int PL>
 cudaError_t launch_ybc_n(const Geom& g, const DstPlan& py, const DstPlan& px, void* out, SlabMap map, int nslabs,
                          const SpecParams& sp, const BtSynth& bs, cudaStream_t st) {
     constexpr int TW = y_tile_w<N, T, PL>();
+    if (g.n2 != N - 1) return cudaErrorInvalidValue;   // the tile's column stride is fixed by N
     const size_t smem = y_smem_bytes<N, T, PL, true>(g.n2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     dim3 grid((g.n1 + TW - 1) / TW, nslabs);
