@@ -627,19 +627,33 @@ template <int N, class T, int PL>
 __host__ __device__ constexpr int y_tile_w() { return 2 * y_groups<N, T, PL>(); }
 __host__ __device__ constexpr int round4(int n) { return ((n + 3) / 4) * 4; }
 // The column tile is column-major, element (row j, column c) at
-// c·CS + j + j/E (E = elements per 128-byte line: one pad every E rows).
-// The transform reads consecutive rows, and its post-processing writes rows 8
-// apart (each thread owns a run of the scan), both free of bank conflicts
-// with that padding; CS ≡ E/TW (mod E) makes the row-major fill and store
-// (TW columns of E/TW rows per access) conflict-free too.
+// c·CS + j + ⌊j/PI⌋: one pad element every PI rows.  E is the number of
+// elements in one 128-byte line, the period of the shared-memory banks.
+// Each thread of the post-processing scan owns a run of C consecutive
+// outputs, so one warp access writes rows 2C apart.  PI = E·(odd part of C)
+// puts those 32 rows into distinct banks (for C = 1, 2, 4 a pad every line;
+// for C = 3, one every three lines), and consecutive rows (the transform's
+// reads, the divide) meet at most one pad per access.  CS ≡ E/TW (mod E)
+// makes the row-major fill and store (TW columns of E/TW rows per access)
+// conflict-free too.
 template <class T>
 __host__ __device__ constexpr int y_line_elems() { return 128 / (int)sizeof(T); }
+template <int N, int PL>
+__host__ __device__ constexpr int y_scan_run() { return (N / 2 + ct_tp(N, PL) - 1) / ct_tp(N, PL); }
+template <int N, class T, int PL>
+__host__ __device__ constexpr int y_pad_every() {
+    int c = y_scan_run<N, PL>();
+    while (c % 2 == 0) c /= 2;
+    return y_line_elems<T>() * c;
+}
+template <int N, class T, int PL>
+__host__ __device__ constexpr int y_off(int j) { return j + j / y_pad_every<N, T, PL>(); }
 template <int N, class T, int PL>
 __host__ __device__ constexpr int y_col_stride(int n2) {
     constexpr int E = y_line_elems<T>();
     constexpr int TW = 2 * y_groups<N, T, PL>();
     constexpr int R = (E / TW) > 0 ? E / TW : 1;
-    const int base = n2 + (n2 - 1) / E + 1;       // one past the last padded row
+    const int base = y_off<N, T, PL>(n2 - 1) + 2;   // one spare element past the last row
     return base + ((R - base % E) % E + E) % E;
 }
 template <int N, class T, int PL>
@@ -678,7 +692,6 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
     constexpr int TP = ct_tp(N, PL);
     constexpr int G = y_groups<N, T, PL>();
     constexpr int TW = y_tile_w<N, T, PL>();
-    constexpr int E = y_line_elems<T>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P = g.P, n1 = g.n1, n2 = g.n2;
     const Tabs<T> tb = tabs_of<T>(p, PL);
@@ -688,7 +701,7 @@ __global__ void __launch_bounds__(y_threads<N, T, PL>(),
     T* tile = cyv + round4(n2);
     const int tile_d = y_tile_elems<N, T, PL>(n2);
     constexpr int CS = y_col_stride<N, T, PL>(N - 1);   // n2 = N − 1 in the y-pass
-    auto off = [](int j) -> int { return j + j / E; };   // row j within a column
+    auto off = [](int j) -> int { return y_off<N, T, PL>(j); };   // row j within a column
     auto at = [&](int j, int c) -> int { return c * CS + off(j); };
     const int gid = threadIdx.x / TP, tid = threadIdx.x % TP;
     V* buf = reinterpret_cast<V*>(tile + tile_d) + gid * ct_buf(N);
