@@ -631,9 +631,10 @@ __host__ __device__ constexpr int round4(int n) { return ((n + 3) / 4) * 4; }
 // elements in one 128-byte line, the period of the shared-memory banks.
 // Each thread of the post-processing scan owns a run of C consecutive
 // outputs, so one warp access writes rows 2C apart.  PI = E·(odd part of C)
-// puts those 32 rows into distinct banks (for C = 1, 2, 4 a pad every line;
-// for C = 3, one every three lines), and consecutive rows (the transform's
-// reads, the divide) meet at most one pad per access.  CS ≡ E/TW (mod E)
+// puts those 32 rows into distinct banks, except where they wrap past two
+// pads (for C = 1, 2, 4 a pad every line; for C = 3, one every three lines),
+// and consecutive rows (the transform's reads, the divide) meet at most one
+// pad per access.  CS ≡ E/TW (mod E)
 // makes the row-major fill and store (TW columns of E/TW rows per access)
 // conflict-free too.
 template <class T>
